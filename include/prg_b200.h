@@ -1,0 +1,148 @@
+/*
+ * prg_b200.h — C ABI of the B200 PageRank library (libprg_b200.so).
+ *
+ * This is the drop-in boundary for rust-igraph's PageRank hot path.  A Rust
+ * wrapper crate (build.rs compiles the CUDA sources with nvcc for sm_100a and
+ * links this library) binds these symbols behind the crate's own signatures:
+ *
+ *   pagerank(&Graph) -> IgraphResult<Vec<f64>>
+ *       src/algorithms/properties/pagerank.rs:52          -> prg_pagerank
+ *   pagerank_weighted(&Graph, &[f64]) -> IgraphResult<Vec<f64>>
+ *       src/algorithms/properties/pagerank_weighted.rs:52 -> prg_pagerank_weighted
+ *   personalized_pagerank(&Graph, &[f64], f64) -> IgraphResult<Vec<f64>>
+ *       src/algorithms/properties/personalized_pagerank.rs:65  -> prg_personalized_pagerank
+ *   personalized_pagerank_default(&Graph, &[f64])
+ *       src/algorithms/properties/personalized_pagerank.rs:206 -> prg_personalized_pagerank (d = 0.85)
+ *   personalized_pagerank_vs(&Graph, &[u32], f64)
+ *       src/algorithms/properties/personalized_pagerank.rs:241 -> prg_personalized_pagerank_vs
+ *
+ * The graph crosses the boundary as rust-igraph stores it: n, the edge list
+ * (from[e], to[e]) in edge-id order (src/core/graph.rs:126-152, Graph::edge
+ * at :1152) and the directedness flag (:582).  Outputs are caller-allocated
+ * double[n] host arrays.  Every entry point is synchronous; calls on
+ * different graph handles may run from different threads (each handle owns
+ * a CUDA stream); one handle must not be used by two threads at once (the
+ * reference Graph is !Sync, src/core/cache.rs:88-91).
+ *
+ * Status codes map one-to-one onto rust-igraph's IgraphError variants
+ * (src/core/error.rs:14-66); prg_last_error() returns the message text
+ * (the reference's own wording for validation errors).
+ */
+#ifndef PRG_B200_H
+#define PRG_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct prg_graph prg_graph;
+
+enum prg_status {
+    PRG_OK = 0,
+    PRG_ERR_INVALID_ARGUMENT = 1,     /* IgraphError::InvalidArgument(String) */
+    PRG_ERR_VERTEX_OUT_OF_RANGE = 2,  /* IgraphError::VertexOutOfRange */
+    PRG_ERR_INTERNAL = 3,             /* IgraphError::Internal(&'static str) */
+    PRG_ERR_CUDA = 4,                 /* IgraphError::Internal("cuda: ...") */
+    PRG_ERR_OUT_OF_MEMORY = 5,        /* IgraphError::Internal("cuda: out of memory") */
+    PRG_ERR_DID_NOT_CONVERGE = 6,     /* IgraphError::DidNotConverge (never raised by the drop-ins) */
+    PRG_ERR_TIMEOUT = 7               /* a bounded device wait expired (batched solver) */
+};
+
+enum prg_precision {
+    PRG_PRECISION_FP64 = 0,           /* FP64 power iteration (the drop-in path) */
+    PRG_PRECISION_FP32_REFINED = 1    /* FP32 SpMV, FP64 residual refinement */
+};
+
+enum prg_stop {
+    PRG_STOP_SUCCESSIVE = 0,          /* reference rule: stop when successive L1 change < eps */
+    PRG_STOP_ERROR_BOUND = 1          /* stop when the certified L1 error vs the fixed point <= eps */
+};
+
+typedef struct prg_options {
+    double damping;        /* default 0.85 (pagerank.rs:23) */
+    double eps;            /* default 1e-10 (pagerank.rs:24) */
+    uint32_t max_iter;     /* default 1000 (pagerank.rs:25); refined: cap on all SpMV passes */
+    int32_t precision;     /* enum prg_precision */
+    int32_t stop;          /* enum prg_stop (refined precision always uses ERROR_BOUND) */
+    int32_t normalise;     /* refined: divide the result by its FP64 sum (default 1) */
+    const double *start;   /* optional start vector (warm start), length n, host memory; NULL = reference start */
+} prg_options;
+
+typedef struct prg_stats {
+    uint32_t iterations;       /* SpMV passes of any precision */
+    uint32_t fp64_passes;
+    uint32_t fp32_passes;
+    uint32_t residual_passes;  /* FP64 residual passes of the refined solver */
+    double last_diff;          /* last successive L1 change (FP64 path) */
+    double residual_l1;        /* ||G(x) - x||_1 of the returned vector's predecessor */
+    double error_bound;        /* certified bound on ||x - x*||_1 */
+    double solve_ms;           /* device time of the solve (CUDA events) */
+    double build_ms;           /* device time of the graph build */
+    uint64_t arcs;
+    uint32_t n_dangling;
+    uint32_t pad;
+} prg_stats;
+
+/* Fills the reference defaults: d = 0.85, eps = 1e-10, max_iter = 1000,
+ * FP64, successive-change stop, normalise = 1, no start vector. */
+void prg_default_options(prg_options *opt);
+
+/* ---- drop-ins: one call = upload, build, iterate, download ------------ */
+
+/* rust-igraph pagerank() (pagerank.rs:52-143). */
+int32_t prg_pagerank(uint32_t n, uint64_t m, const uint32_t *from, const uint32_t *to, int32_t directed,
+                     double *out);
+
+/* rust-igraph pagerank_weighted() (pagerank_weighted.rs:52-161).
+ * weights_len is the caller's slice length (checked against m like :62-68). */
+int32_t prg_pagerank_weighted(uint32_t n, uint64_t m, const uint32_t *from, const uint32_t *to,
+                              int32_t directed, const double *weights, uint64_t weights_len, double *out);
+
+/* rust-igraph personalized_pagerank() (personalized_pagerank.rs:65-182). */
+int32_t prg_personalized_pagerank(uint32_t n, uint64_t m, const uint32_t *from, const uint32_t *to,
+                                  int32_t directed, const double *reset, uint64_t reset_len, double damping,
+                                  double *out);
+
+/* rust-igraph personalized_pagerank_vs() (personalized_pagerank.rs:241-268). */
+int32_t prg_personalized_pagerank_vs(uint32_t n, uint64_t m, const uint32_t *from, const uint32_t *to,
+                                     int32_t directed, const uint32_t *reset_vids, uint64_t nvids,
+                                     double damping, double *out);
+
+/* ---- resident graphs: build once in HBM, solve many times ------------- */
+
+/* Builds the device CSR from host arrays (weights may be NULL). */
+int32_t prg_graph_create(uint32_t n, uint64_t m, const uint32_t *from, const uint32_t *to,
+                         const double *weights, int32_t directed, prg_graph **out);
+/* Same from device arrays (already in this GPU's memory). */
+int32_t prg_graph_create_device(uint32_t n, uint64_t m, const uint32_t *d_from, const uint32_t *d_to,
+                                const double *d_weights, int32_t directed, prg_graph **out);
+void prg_graph_destroy(prg_graph *g);
+/* n, in-CSR arc count, dangling vertices, row-blocks, hub rows, build time (ms). */
+int32_t prg_graph_info(const prg_graph *g, uint32_t *n, uint64_t *arcs, uint32_t *n_dangling, uint32_t *n_rowblocks,
+                       uint32_t *n_hubs, double *build_ms);
+/* The CUDA stream (cudaStream_t) every call on this handle runs on. */
+void *prg_graph_stream(prg_graph *g);
+
+/* Solve on a resident graph.  reset: host teleport vector (length n, raw,
+ * normalised inside like personalized_pagerank.rs:110-111) or NULL for the
+ * uniform teleport of pagerank().  out: host double[n]. */
+int32_t prg_solve(prg_graph *g, const prg_options *opt, const double *reset, double *out, prg_stats *stats);
+/* Same with device pointers: d_reset (already normalised, or NULL) and d_out. */
+int32_t prg_solve_device(prg_graph *g, const prg_options *opt, const double *d_reset, double *d_out,
+                         prg_stats *stats);
+
+/* Message of the last error on this thread ("" if none). */
+const char *prg_last_error(void);
+
+/* ---- device R-MAT generator (benchmark inputs) ------------------------ */
+/* Counter-based R-MAT (same edge stream as the CPU generator in the tests):
+ * writes m edges into device arrays d_from/d_to. */
+int32_t prg_rmat_device(uint32_t scale, uint64_t m, double a, double b, double c, uint64_t seed,
+                        uint32_t *d_from, uint32_t *d_to, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PRG_B200_H */

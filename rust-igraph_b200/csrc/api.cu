@@ -1,0 +1,530 @@
+// api.cu — the extern "C" boundary (include/prg_b200.h).
+//
+// Validation order and messages follow rust-igraph so a binding can hand
+// the status/message pair straight to IgraphError:
+//   pagerank            pagerank.rs:52-101
+//   pagerank_weighted   pagerank_weighted.rs:52-79
+//   personalized        personalized_pagerank.rs:65-107
+//   _vs                 personalized_pagerank.rs:241-268
+// There is no CPU fallback: every solve runs the CUDA kernels, and a missing
+// or unusable GPU is reported as PRG_ERR_CUDA.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/prg_b200.h"
+#include "graph.cuh"
+#include "solver.cuh"
+
+struct prg_graph {
+    prg::DeviceGraph g;
+    prg::Workspace ws;
+    cudaStream_t stream = nullptr;
+    double *d_reset = nullptr;  // normalised reset staging (n doubles)
+    double *d_out = nullptr;    // output staging (n doubles)
+    double *d_start = nullptr;  // warm-start staging
+};
+
+namespace {
+
+thread_local std::string g_err;
+
+int32_t fail(int32_t code, const std::string &msg) {
+    g_err = msg;
+    return code;
+}
+
+int32_t from_cuda(const prg::CudaError &e) {
+    if (e.err == cudaErrorMemoryAllocation) return fail(PRG_ERR_OUT_OF_MEMORY, "cuda: out of memory");
+    return fail(PRG_ERR_CUDA, std::string("cuda: ") + cudaGetErrorString(e.err) + " (" + e.what + ")");
+}
+
+// Display of an f64 the way Rust's `{}` formats it: shortest round-trip
+// digits, never exponent notation, "NaN"/"inf"/"-inf".
+std::string rust_f64(double v) {
+    if (std::isnan(v)) return "NaN";
+    if (std::isinf(v)) return v > 0 ? "inf" : "-inf";
+    char buf[64];
+    int prec = 1;
+    for (; prec <= 17; prec++) {
+        std::snprintf(buf, sizeof buf, "%.*e", prec - 1, v);
+        if (std::strtod(buf, nullptr) == v) break;
+    }
+    // buf = d.ddddde[+-]XX ; expand to plain decimal
+    std::string s(buf);
+    bool neg = false;
+    if (s[0] == '-') {
+        neg = true;
+        s = s.substr(1);
+    }
+    size_t epos = s.find('e');
+    int ex = std::atoi(s.c_str() + epos + 1);
+    std::string digits;
+    for (size_t i = 0; i < epos; i++)
+        if (s[i] != '.') digits += s[i];
+    while (digits.size() > 1 && digits.back() == '0') digits.pop_back();
+    std::string out;
+    int point = ex + 1;  // digits before the decimal point
+    if (point <= 0) {
+        out = "0." + std::string(-point, '0') + digits;
+    } else if ((size_t)point >= digits.size()) {
+        out = digits + std::string(point - digits.size(), '0');
+    } else {
+        out = digits.substr(0, point) + "." + digits.substr(point);
+    }
+    if (v == 0.0) out = "0";
+    return (neg ? "-" : "") + out;
+}
+
+bool ensure_pool_config() {
+    static bool done = false;
+    if (done) return true;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return false;
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+        uint64_t thr = UINT64_MAX;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+    }
+    done = true;
+    return true;
+}
+
+// Checks that every endpoint is < n (Graph::add_edges rejects others with
+// IgraphError::VertexOutOfRange, graph.rs:756-785).
+__global__ void max_endpoint_kernel(const uint32_t *a, const uint32_t *b, uint64_t m, uint32_t *out) {
+    uint32_t mx = 0;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += (uint64_t)gridDim.x * blockDim.x)
+        mx = max(mx, max(a[i], b[i]));
+    for (int o = 16; o > 0; o >>= 1) mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(out, mx);
+}
+
+// Creates a handle from device edge arrays (copies nothing on the host).
+int32_t create_from_device(uint32_t n, uint64_t m, const uint32_t *d_from, const uint32_t *d_to, const double *d_w,
+                           int32_t directed, cudaStream_t s, prg_graph **out) {
+    if (m > 0xFFFFFFFFull) return fail(PRG_ERR_INTERNAL, "ecount overflows u32");
+    const uint64_t arcs = directed ? m : 2 * m;
+    if (arcs + prg::kColPad >= 0xFFFFFFFFull)
+        return fail(PRG_ERR_INTERNAL, "arc count exceeds the u32 CSR index range");
+    prg_graph *h = new prg_graph();
+    h->stream = s;
+    h->g.n = n;
+    h->g.m = m;
+    h->g.directed = directed != 0;
+    PRG_CUDA(cudaGetDevice(&h->g.device));
+    if (m > 0) {
+        uint32_t *d_mx = nullptr, mx = 0;
+        PRG_CUDA(cudaMallocAsync((void **)&d_mx, 4, s));
+        PRG_CUDA(cudaMemsetAsync(d_mx, 0, 4, s));
+        max_endpoint_kernel<<<148 * 8, 256, 0, s>>>(d_from, d_to, m, d_mx);
+        PRG_CUDA(cudaGetLastError());
+        PRG_CUDA(cudaMemcpyAsync(&mx, d_mx, 4, cudaMemcpyDeviceToHost, s));
+        PRG_CUDA(cudaFreeAsync(d_mx, s));
+        PRG_CUDA(cudaStreamSynchronize(s));
+        if (mx >= n) {
+            delete h;
+            return fail(PRG_ERR_VERTEX_OUT_OF_RANGE, "vertex id " + std::to_string(mx) +
+                                                         " out of range (vcount = " + std::to_string(n) + ")");
+        }
+    }
+    prg::build_graph(h->g, d_from, d_to, d_w, s);
+    *out = h;
+    return PRG_OK;
+}
+
+int32_t create_from_host(uint32_t n, uint64_t m, const uint32_t *from, const uint32_t *to, const double *w,
+                         int32_t directed, prg_graph **out) {
+    if (!ensure_pool_config()) return fail(PRG_ERR_CUDA, "cuda: no usable device");
+    cudaStream_t s;
+    PRG_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    if (m > 0xFFFFFFFFull) {
+        cudaStreamDestroy(s);
+        return fail(PRG_ERR_INTERNAL, "ecount overflows u32");
+    }
+    uint32_t *d_f = nullptr, *d_t = nullptr;
+    double *d_w = nullptr;
+    const uint64_t mm = m ? m : 1;
+    PRG_CUDA(cudaMallocAsync((void **)&d_f, mm * 4, s));
+    PRG_CUDA(cudaMallocAsync((void **)&d_t, mm * 4, s));
+    if (m) {
+        PRG_CUDA(cudaMemcpyAsync(d_f, from, m * 4, cudaMemcpyHostToDevice, s));
+        PRG_CUDA(cudaMemcpyAsync(d_t, to, m * 4, cudaMemcpyHostToDevice, s));
+    }
+    if (w) {
+        PRG_CUDA(cudaMallocAsync((void **)&d_w, mm * 8, s));
+        if (m) PRG_CUDA(cudaMemcpyAsync(d_w, w, m * 8, cudaMemcpyHostToDevice, s));
+    }
+    int32_t rc = create_from_device(n, m, d_f, d_t, w ? d_w : nullptr, directed, s, out);
+    cudaFreeAsync(d_f, s);
+    cudaFreeAsync(d_t, s);
+    if (d_w) cudaFreeAsync(d_w, s);
+    if (rc != PRG_OK) {
+        cudaStreamSynchronize(s);
+        cudaStreamDestroy(s);
+    }
+    return rc;
+}
+
+void destroy(prg_graph *h) {
+    if (!h) return;
+    cudaStream_t s = h->stream;
+    prg::workspace_free(h->ws, s);
+    auto f = [&](void *p) {
+        if (p) cudaFreeAsync(p, s);
+    };
+    f(h->g.row_ptr);
+    f(h->g.col);
+    f(h->g.w64);
+    f(h->g.w32);
+    f(h->g.deg);
+    f(h->g.dval);
+    f(h->g.inv32);
+    f(h->g.rb);
+    f(h->g.hubs);
+    f(h->d_reset);
+    f(h->d_out);
+    f(h->d_start);
+    cudaStreamSynchronize(s);
+    cudaStreamDestroy(s);
+    delete h;
+}
+
+prg::SolveOpts to_solve_opts(const prg_options *o) {
+    prg::SolveOpts so;
+    if (o) {
+        so.damping = o->damping;
+        so.eps = o->eps;
+        so.max_iter = o->max_iter;
+        so.precision = o->precision;
+        so.stop = o->stop;
+        so.normalise = o->normalise;
+    }
+    return so;
+}
+
+void fill_stats(prg_stats *st, const prg::SolveStats &s, const prg_graph *h) {
+    if (!st) return;
+    std::memset(st, 0, sizeof(*st));
+    st->iterations = s.iterations;
+    st->fp64_passes = s.fp64_passes;
+    st->fp32_passes = s.fp32_passes;
+    st->residual_passes = s.residual_passes;
+    st->last_diff = s.last_diff;
+    st->residual_l1 = s.residual_l1;
+    st->error_bound = s.error_bound;
+    st->solve_ms = s.solve_ms;
+    st->build_ms = h->g.build_ms;
+    st->arcs = h->g.arcs;
+    st->n_dangling = h->g.n_dangling;
+}
+
+// Host-side solve: stages the (already normalised) reset and start vectors,
+// runs, copies the result into `out`.
+int32_t solve_host(prg_graph *h, const prg::SolveOpts &so_in, const double *norm_reset, const double *start,
+                   double *out, prg_stats *st) {
+    cudaStream_t s = h->stream;
+    const uint64_t n = h->g.n;
+    prg::SolveOpts so = so_in;
+    if (!h->d_out) PRG_CUDA(cudaMallocAsync((void **)&h->d_out, n * 8, s));
+    const double *d_t = nullptr;
+    if (norm_reset) {
+        if (!h->d_reset) PRG_CUDA(cudaMallocAsync((void **)&h->d_reset, n * 8, s));
+        PRG_CUDA(cudaMemcpyAsync(h->d_reset, norm_reset, n * 8, cudaMemcpyHostToDevice, s));
+        d_t = h->d_reset;
+    }
+    if (start) {
+        if (!h->d_start) PRG_CUDA(cudaMallocAsync((void **)&h->d_start, n * 8, s));
+        PRG_CUDA(cudaMemcpyAsync(h->d_start, start, n * 8, cudaMemcpyHostToDevice, s));
+        so.d_start = h->d_start;
+    }
+    prg::SolveStats ss;
+    prg::solve(h->g, h->ws, so, d_t, h->d_out, ss, s);
+    PRG_CUDA(cudaMemcpyAsync(out, h->d_out, n * 8, cudaMemcpyDeviceToHost, s));
+    PRG_CUDA(cudaStreamSynchronize(s));
+    fill_stats(st, ss, h);
+    return PRG_OK;
+}
+
+// One-shot drop-in: build, solve with the reference's constants, download.
+int32_t dropin(uint32_t n, uint64_t m, const uint32_t *from, const uint32_t *to, int32_t directed, const double *w,
+               const double *norm_reset, double damping, double *out) {
+    prg_graph *h = nullptr;
+    int32_t rc = create_from_host(n, m, from, to, w, directed, &h);
+    if (rc != PRG_OK) return rc;
+    prg::SolveOpts so;
+    so.damping = damping;
+    try {
+        rc = solve_host(h, so, norm_reset, nullptr, out, nullptr);
+    } catch (...) {
+        destroy(h);
+        throw;
+    }
+    destroy(h);
+    return rc;
+}
+
+}  // namespace
+
+#define PRG_GUARD_BEGIN try {
+#define PRG_GUARD_END                                                   \
+    }                                                                   \
+    catch (const prg::CudaError &e) {                                   \
+        return from_cuda(e);                                            \
+    }                                                                   \
+    catch (const std::bad_alloc &) {                                    \
+        return fail(PRG_ERR_OUT_OF_MEMORY, "host: out of memory");      \
+    }                                                                   \
+    catch (...) {                                                       \
+        return fail(PRG_ERR_INTERNAL, "unexpected exception");          \
+    }
+
+extern "C" {
+
+void prg_default_options(prg_options *o) {
+    if (!o) return;
+    o->damping = 0.85;
+    o->eps = 1e-10;
+    o->max_iter = 1000;
+    o->precision = PRG_PRECISION_FP64;
+    o->stop = PRG_STOP_SUCCESSIVE;
+    o->normalise = 1;
+    o->start = nullptr;
+}
+
+const char *prg_last_error(void) { return g_err.c_str(); }
+
+int32_t prg_pagerank(uint32_t n, uint64_t m, const uint32_t *from, const uint32_t *to, int32_t directed,
+                     double *out) {
+    g_err.clear();
+    PRG_GUARD_BEGIN
+    if (n == 0) return PRG_OK;  // pagerank.rs:55-57
+    if (n == 1) {               // pagerank.rs:58-60
+        out[0] = 1.0;
+        return PRG_OK;
+    }
+    return dropin(n, m, from, to, directed, nullptr, nullptr, 0.85, out);
+    PRG_GUARD_END
+}
+
+int32_t prg_pagerank_weighted(uint32_t n, uint64_t m, const uint32_t *from, const uint32_t *to, int32_t directed,
+                              const double *weights, uint64_t weights_len, double *out) {
+    g_err.clear();
+    PRG_GUARD_BEGIN
+    if (n == 0) return PRG_OK;  // pagerank_weighted.rs:55-57
+    if (n == 1) {
+        out[0] = 1.0;
+        return PRG_OK;
+    }
+    if (weights_len != m)  // :62-68
+        return fail(PRG_ERR_INVALID_ARGUMENT, "weights vector size (" + std::to_string(weights_len) +
+                                                  ") differs from edge count (" + std::to_string(m) + ")");
+    for (uint64_t e = 0; e < m; e++) {  // :69-76
+        const double w = weights[e];
+        if (std::isnan(w) || w < 0.0 || !std::isfinite(w))
+            return fail(PRG_ERR_INVALID_ARGUMENT, "weight at edge " + std::to_string(e) +
+                                                      " must be non-negative and finite (got " + rust_f64(w) + ")");
+    }
+    return dropin(n, m, from, to, directed, weights, nullptr, 0.85, out);
+    PRG_GUARD_END
+}
+
+// personalized_pagerank.rs:65-111: validation, n==1, reset normalisation.
+static int32_t ppr_validate(uint32_t n, const double *reset, uint64_t reset_len, double damping,
+                            std::vector<double> &norm, bool *trivial) {
+    *trivial = false;
+    if (n == 0) {
+        if (reset_len == 0) {
+            *trivial = true;
+            return PRG_OK;
+        }
+        return fail(PRG_ERR_INVALID_ARGUMENT,
+                    "personalized_pagerank: reset vector non-empty but graph has no vertices");
+    }
+    if (reset_len != n)
+        return fail(PRG_ERR_INVALID_ARGUMENT, "personalized_pagerank: reset length (" + std::to_string(reset_len) +
+                                                  ") does not match vcount (" + std::to_string(n) + ")");
+    if (damping <= 0.0 || damping >= 1.0)
+        return fail(PRG_ERR_INVALID_ARGUMENT,
+                    "personalized_pagerank: damping (" + rust_f64(damping) + ") must be in (0, 1)");
+    double sum = 0.0;
+    for (uint32_t i = 0; i < n; i++) sum += reset[i];
+    if (sum <= 0.0)
+        return fail(PRG_ERR_INVALID_ARGUMENT, "personalized_pagerank: reset vector must sum to a positive value");
+    for (uint32_t i = 0; i < n; i++)
+        if (reset[i] < 0.0)
+            return fail(PRG_ERR_INVALID_ARGUMENT, "personalized_pagerank: negative reset value (" +
+                                                      rust_f64(reset[i]) + ") at index " + std::to_string(i));
+    if (n == 1) {
+        *trivial = true;
+        return PRG_OK;
+    }
+    const double inv = 1.0 / sum;
+    norm.resize(n);
+    for (uint32_t i = 0; i < n; i++) norm[i] = reset[i] * inv;
+    return PRG_OK;
+}
+
+int32_t prg_personalized_pagerank(uint32_t n, uint64_t m, const uint32_t *from, const uint32_t *to,
+                                  int32_t directed, const double *reset, uint64_t reset_len, double damping,
+                                  double *out) {
+    g_err.clear();
+    PRG_GUARD_BEGIN
+    std::vector<double> norm;
+    bool trivial = false;
+    int32_t rc = ppr_validate(n, reset, reset_len, damping, norm, &trivial);
+    if (rc != PRG_OK) return rc;
+    if (trivial) {
+        if (n == 1) out[0] = 1.0;
+        return PRG_OK;
+    }
+    return dropin(n, m, from, to, directed, nullptr, norm.data(), damping, out);
+    PRG_GUARD_END
+}
+
+int32_t prg_personalized_pagerank_vs(uint32_t n, uint64_t m, const uint32_t *from, const uint32_t *to,
+                                     int32_t directed, const uint32_t *reset_vids, uint64_t nvids, double damping,
+                                     double *out) {
+    g_err.clear();
+    PRG_GUARD_BEGIN
+    if (nvids == 0) return fail(PRG_ERR_INVALID_ARGUMENT, "reset_vids must not be empty");
+    std::vector<double> reset(n, 0.0);
+    const double weight = 1.0 / (double)nvids;
+    for (uint64_t i = 0; i < nvids; i++) {
+        const uint32_t v = reset_vids[i];
+        if (v >= n)
+            return fail(PRG_ERR_INVALID_ARGUMENT, "reset vertex " + std::to_string(v) + " out of range (vcount = " +
+                                                      std::to_string(n) + ")");
+        reset[v] += weight;
+    }
+    return prg_personalized_pagerank(n, m, from, to, directed, reset.data(), n, damping, out);
+    PRG_GUARD_END
+}
+
+int32_t prg_graph_create(uint32_t n, uint64_t m, const uint32_t *from, const uint32_t *to, const double *weights,
+                         int32_t directed, prg_graph **out) {
+    g_err.clear();
+    PRG_GUARD_BEGIN
+    if (!out) return fail(PRG_ERR_INVALID_ARGUMENT, "null output handle");
+    *out = nullptr;
+    if (weights) {
+        for (uint64_t e = 0; e < m; e++) {
+            const double w = weights[e];
+            if (std::isnan(w) || w < 0.0 || !std::isfinite(w))
+                return fail(PRG_ERR_INVALID_ARGUMENT, "weight at edge " + std::to_string(e) +
+                                                          " must be non-negative and finite (got " + rust_f64(w) +
+                                                          ")");
+        }
+    }
+    return create_from_host(n, m, from, to, weights, directed, out);
+    PRG_GUARD_END
+}
+
+int32_t prg_graph_create_device(uint32_t n, uint64_t m, const uint32_t *d_from, const uint32_t *d_to,
+                                const double *d_weights, int32_t directed, prg_graph **out) {
+    g_err.clear();
+    PRG_GUARD_BEGIN
+    if (!out) return fail(PRG_ERR_INVALID_ARGUMENT, "null output handle");
+    *out = nullptr;
+    if (!ensure_pool_config()) return fail(PRG_ERR_CUDA, "cuda: no usable device");
+    cudaStream_t s;
+    PRG_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    int32_t rc = create_from_device(n, m, d_from, d_to, d_weights, directed, s, out);
+    if (rc != PRG_OK) cudaStreamDestroy(s);
+    return rc;
+    PRG_GUARD_END
+}
+
+void prg_graph_destroy(prg_graph *g) {
+    try {
+        destroy(g);
+    } catch (...) {
+    }
+}
+
+int32_t prg_graph_info(const prg_graph *h, uint32_t *n, uint64_t *arcs, uint32_t *n_dangling, uint32_t *nrb,
+                       uint32_t *nhub, double *build_ms) {
+    if (!h) return fail(PRG_ERR_INVALID_ARGUMENT, "null graph handle");
+    if (n) *n = h->g.n;
+    if (arcs) *arcs = h->g.arcs;
+    if (n_dangling) *n_dangling = h->g.n_dangling;
+    if (nrb) *nrb = h->g.nrb;
+    if (nhub) *nhub = h->g.nhub;
+    if (build_ms) *build_ms = h->g.build_ms;
+    return PRG_OK;
+}
+
+void *prg_graph_stream(prg_graph *h) { return h ? (void *)h->stream : nullptr; }
+
+int32_t prg_solve(prg_graph *h, const prg_options *opt, const double *reset, double *out, prg_stats *st) {
+    g_err.clear();
+    PRG_GUARD_BEGIN
+    if (!h) return fail(PRG_ERR_INVALID_ARGUMENT, "null graph handle");
+    prg_options o;
+    prg_default_options(&o);
+    if (opt) o = *opt;
+    const uint32_t n = h->g.n;
+    if (n == 0) return PRG_OK;
+    if (reset) {
+        std::vector<double> norm;
+        bool trivial = false;
+        int32_t rc = ppr_validate(n, reset, n, o.damping, norm, &trivial);
+        if (rc != PRG_OK) return rc;
+        if (trivial) {
+            out[0] = 1.0;
+            return PRG_OK;
+        }
+        return solve_host(h, to_solve_opts(&o), norm.data(), o.start, out, st);
+    }
+    if (o.damping <= 0.0 || o.damping >= 1.0)
+        return fail(PRG_ERR_INVALID_ARGUMENT, "damping (" + rust_f64(o.damping) + ") must be in (0, 1)");
+    if (n == 1) {
+        out[0] = 1.0;
+        return PRG_OK;
+    }
+    return solve_host(h, to_solve_opts(&o), nullptr, o.start, out, st);
+    PRG_GUARD_END
+}
+
+int32_t prg_solve_device(prg_graph *h, const prg_options *opt, const double *d_reset, double *d_out,
+                         prg_stats *st) {
+    g_err.clear();
+    PRG_GUARD_BEGIN
+    if (!h) return fail(PRG_ERR_INVALID_ARGUMENT, "null graph handle");
+    prg_options o;
+    prg_default_options(&o);
+    if (opt) o = *opt;
+    if (!(o.damping > 0.0 && o.damping < 1.0))
+        return fail(PRG_ERR_INVALID_ARGUMENT, "damping (" + rust_f64(o.damping) + ") must be in (0, 1)");
+    if (h->g.n < 2) return fail(PRG_ERR_INVALID_ARGUMENT, "device solve needs vcount >= 2");
+    prg::SolveOpts so = to_solve_opts(&o);
+    so.d_start = o.start;  // device pointer on this entry point
+    cudaStream_t s = h->stream;
+    const double *d_t = nullptr;
+    if (d_reset) {
+        if (!h->d_reset) PRG_CUDA(cudaMallocAsync((void **)&h->d_reset, (uint64_t)h->g.n * 8, s));
+        PRG_CUDA(cudaMemcpyAsync(h->d_reset, d_reset, (uint64_t)h->g.n * 8, cudaMemcpyDeviceToDevice, s));
+        d_t = h->d_reset;
+    }
+    prg::SolveStats ss;
+    prg::solve(h->g, h->ws, so, d_t, d_out, ss, s);
+    fill_stats(st, ss, h);
+    return PRG_OK;
+    PRG_GUARD_END
+}
+
+int32_t prg_rmat_device(uint32_t scale, uint64_t m, double a, double b, double c, uint64_t seed, uint32_t *d_from,
+                        uint32_t *d_to, void *stream) {
+    g_err.clear();
+    PRG_GUARD_BEGIN
+    if (scale == 0 || scale > 32) return fail(PRG_ERR_INVALID_ARGUMENT, "scale must be in 1..=32");
+    prg::rmat_generate(scale, m, a, b, c, seed, d_from, d_to, (cudaStream_t)stream);
+    return PRG_OK;
+    PRG_GUARD_END
+}
+
+}  // extern "C"

@@ -1,0 +1,595 @@
+// csr_build.cu — device construction of the in-arc CSR (the transpose the
+// power iteration pulls over), out-degree / out-strength and the row-block
+// work list of the SpMV.
+//
+// Semantics follow rust-igraph exactly:
+//   * arcs: directed edge u->v gives in_adj[v] += u; an undirected edge
+//     {u,v} gives in_adj[u] += v then in_adj[v] += u, a self-loop gives
+//     in_adj[v] += v twice (pagerank.rs:76-101, pagerank_weighted.rs:103-124,
+//     personalized_pagerank.rs:125-143);
+//   * rows keep edge-id order: the arcs are produced in edge order and
+//     sorted by destination with a STABLE radix sort, so row v lists its
+//     in-neighbours in the same order as the reference's Vec<Vec<u32>>;
+//   * out-degree = neighbors_iter(v).len(): out-edges for directed graphs,
+//     all incident edge ends (self-loop twice) for undirected ones
+//     (graph.rs:877-900, pagerank.rs:69-72);
+//   * out-strength accumulates w per arc end (self-loop adds 2w,
+//     pagerank_weighted.rs:81-101); a vertex is dangling iff its divisor is 0.
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <algorithm>
+#include <cstdio>
+
+#include "graph.cuh"
+#include "prims.cuh"
+
+namespace prg {
+
+static inline unsigned grid_for(uint64_t n, unsigned per_block, unsigned cap = 148u * 64u) {
+    uint64_t g = (n + per_block - 1) / per_block;
+    if (g < 1) g = 1;
+    if (g > cap) g = cap;
+    return (unsigned)g;
+}
+
+template <class T>
+static T *dalloc(uint64_t count, cudaStream_t s) {
+    void *p = nullptr;
+    PRG_CUDA(cudaMallocAsync(&p, std::max<uint64_t>(count, 1) * sizeof(T), s));
+    return (T *)p;
+}
+template <class T>
+static void dfree(T *&p, cudaStream_t s) {
+    if (p) cudaFreeAsync(p, s);
+    p = nullptr;
+}
+
+// ------------------------------------------------------------------ scan
+
+constexpr int kScanItems = 16;
+constexpr int kScanTile = kThreads * kScanItems;
+
+__global__ void __launch_bounds__(kThreads) scan_tile_sums(const uint32_t *in, uint64_t n, uint32_t *bsum) {
+    __shared__ uint32_t sh[32];
+    uint64_t base = (uint64_t)blockIdx.x * kScanTile;
+    uint32_t acc = 0;
+#pragma unroll
+    for (int i = 0; i < kScanItems; i++) {
+        uint64_t idx = base + (uint64_t)i * kThreads + threadIdx.x;
+        if (idx < n) acc += in[idx];
+    }
+    uint32_t t = block_sum<uint32_t>(acc, sh);
+    if (threadIdx.x == 0) bsum[blockIdx.x] = t;
+}
+
+// Single-block exclusive scan of a (moderate) array in place; writes total.
+__global__ void __launch_bounds__(1024) scan_single_block(uint32_t *a, uint64_t n, uint32_t *total) {
+    __shared__ uint32_t sh[33];
+    uint64_t per = (n + blockDim.x - 1) / blockDim.x;
+    uint64_t lo = per * threadIdx.x, hi = lo + per < n ? lo + per : n;
+    uint32_t s = 0;
+    for (uint64_t i = lo; i < hi; i++) s += a[i];
+    uint32_t tot;
+    uint32_t pre = block_excl_scan(s, sh, &tot);
+    for (uint64_t i = lo; i < hi; i++) {
+        uint32_t v = a[i];
+        a[i] = pre;
+        pre += v;
+    }
+    if (threadIdx.x == 0 && total) *total = tot;
+}
+
+__global__ void __launch_bounds__(kThreads) scan_tiles_apply(const uint32_t *in, uint32_t *out, uint64_t n,
+                                                             const uint32_t *boff) {
+    __shared__ uint32_t sh[33];
+    __shared__ uint32_t tile[kScanTile];
+    uint64_t base = (uint64_t)blockIdx.x * kScanTile;
+    // coalesced load into shared, then each thread scans a contiguous run
+#pragma unroll
+    for (int i = 0; i < kScanItems; i++) {
+        uint64_t idx = base + (uint64_t)i * kThreads + threadIdx.x;
+        tile[i * kThreads + threadIdx.x] = idx < n ? in[idx] : 0u;
+    }
+    __syncthreads();
+    uint32_t run[kScanItems];
+    uint32_t s = 0;
+#pragma unroll
+    for (int i = 0; i < kScanItems; i++) {
+        run[i] = tile[threadIdx.x * kScanItems + i];
+        s += run[i];
+    }
+    uint32_t tot;
+    uint32_t pre = block_excl_scan(s, sh, &tot) + boff[blockIdx.x];
+#pragma unroll
+    for (int i = 0; i < kScanItems; i++) {
+        tile[threadIdx.x * kScanItems + i] = pre;
+        pre += run[i];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < kScanItems; i++) {
+        uint64_t idx = base + (uint64_t)i * kThreads + threadIdx.x;
+        if (idx < n) out[idx] = tile[i * kThreads + threadIdx.x];
+    }
+}
+
+void exclusive_scan_u32(const uint32_t *in, uint32_t *out, uint64_t n, cudaStream_t s) {
+    uint64_t nb = (n + kScanTile - 1) / kScanTile;
+    if (nb == 0) nb = 1;
+    uint32_t *bsum = dalloc<uint32_t>(nb + 1, s);
+    scan_tile_sums<<<(unsigned)nb, kThreads, 0, s>>>(in, n, bsum);
+    scan_single_block<<<1, 1024, 0, s>>>(bsum, nb, out + n);
+    scan_tiles_apply<<<(unsigned)nb, kThreads, 0, s>>>(in, out, n, bsum);
+    PRG_CUDA(cudaGetLastError());
+    dfree(bsum, s);
+}
+
+// ------------------------------------------------------------------ radix sort
+
+constexpr int kRsItems = 8;
+constexpr int kRsTile = kThreads * kRsItems;  // 2048 keys
+constexpr int kRsWarps = kThreads / 32;
+
+__global__ void __launch_bounds__(kThreads) rs_upsweep(const uint32_t *keys, uint64_t N, uint64_t chunk, int shift,
+                                                       uint32_t *counts, uint32_t G) {
+    __shared__ uint32_t h[kRsWarps][256];
+    for (int i = threadIdx.x; i < kRsWarps * 256; i += kThreads) (&h[0][0])[i] = 0;
+    __syncthreads();
+    uint64_t begin = (uint64_t)blockIdx.x * chunk;
+    uint64_t end = begin + chunk < N ? begin + chunk : N;
+    int w = threadIdx.x >> 5;
+    for (uint64_t i = begin + threadIdx.x; i < end; i += kThreads) {
+        uint32_t d = (keys[i] >> shift) & 255u;
+        atomicAdd(&h[w][d], 1u);
+    }
+    __syncthreads();
+    uint32_t t = threadIdx.x;
+    uint32_t s = 0;
+#pragma unroll
+    for (int k = 0; k < kRsWarps; k++) s += h[k][t];
+    counts[(uint64_t)t * G + blockIdx.x] = s;
+}
+
+// Stable scatter: each chunk is processed tile by tile; within a tile keys
+// are ranked per warp with __match_any_sync in position order, then ordered
+// by digit in shared memory and written out in digit runs (coalesced).
+__global__ void __launch_bounds__(kThreads) rs_downsweep(const uint32_t *kin, const uint32_t *vin, uint32_t *kout,
+                                                         uint32_t *vout, uint64_t N, uint64_t chunk, int shift,
+                                                         const uint32_t *offsets, uint32_t G) {
+    __shared__ uint32_t s_wh[kRsWarps][256];
+    __shared__ uint32_t s_keys[kRsTile];
+    __shared__ uint32_t s_vals[kRsTile];
+    __shared__ uint32_t s_cnt[256];
+    __shared__ uint32_t s_dstart[256];
+    __shared__ uint32_t s_off[256];
+    __shared__ uint32_t s_scan[33];
+
+    const int tid = threadIdx.x, w = tid >> 5, lane = tid & 31;
+    uint64_t begin = (uint64_t)blockIdx.x * chunk;
+    uint64_t end = begin + chunk < N ? begin + chunk : N;
+    s_off[tid] = offsets[(uint64_t)tid * G + blockIdx.x];
+    const uint32_t ltmask = lanemask_lt();
+
+    for (uint64_t tb = begin; tb < end; tb += kRsTile) {
+        for (int i = tid; i < kRsWarps * 256; i += kThreads) (&s_wh[0][0])[i] = 0;
+        __syncthreads();
+        uint32_t key[kRsItems], val[kRsItems], dig[kRsItems], rank[kRsItems];
+#pragma unroll
+        for (int i = 0; i < kRsItems; i++) {
+            uint64_t pos = tb + (uint64_t)w * (32 * kRsItems) + (uint64_t)i * 32 + lane;
+            bool valid = pos < end;
+            key[i] = valid ? kin[pos] : 0u;
+            val[i] = valid ? vin[pos] : 0u;
+            dig[i] = valid ? ((key[i] >> shift) & 255u) : 256u;
+        }
+#pragma unroll
+        for (int i = 0; i < kRsItems; i++) {
+            uint32_t d = dig[i];
+            uint32_t peers = __match_any_sync(0xffffffffu, d);
+            uint32_t before = d < 256u ? s_wh[w][d] : 0u;
+            __syncwarp();
+            if (d < 256u && (peers & ltmask) == 0u) s_wh[w][d] = before + __popc(peers);
+            __syncwarp();
+            rank[i] = before + __popc(peers & ltmask);
+        }
+        __syncthreads();
+        {  // per digit: exclusive prefix across warps, tile count
+            uint32_t run = 0;
+#pragma unroll
+            for (int k = 0; k < kRsWarps; k++) {
+                uint32_t c = s_wh[k][tid];
+                s_wh[k][tid] = run;
+                run += c;
+            }
+            s_cnt[tid] = run;
+        }
+        __syncthreads();
+        uint32_t tot;
+        uint32_t ds = block_excl_scan(s_cnt[tid], s_scan, &tot);
+        s_dstart[tid] = ds;
+        __syncthreads();
+#pragma unroll
+        for (int i = 0; i < kRsItems; i++) {
+            uint32_t d = dig[i];
+            if (d < 256u) {
+                uint32_t lp = s_dstart[d] + s_wh[w][d] + rank[i];
+                s_keys[lp] = key[i];
+                s_vals[lp] = val[i];
+            }
+        }
+        __syncthreads();
+        uint32_t nvalid = tot;
+        for (uint32_t j = tid; j < nvalid; j += kThreads) {
+            uint32_t k = s_keys[j];
+            uint32_t d = (k >> shift) & 255u;
+            uint64_t gpos = (uint64_t)s_off[d] + (j - s_dstart[d]);
+            kout[gpos] = k;
+            vout[gpos] = s_vals[j];
+        }
+        __syncthreads();
+        s_off[tid] += s_cnt[tid];
+        __syncthreads();
+    }
+}
+
+void radix_sort_pairs(uint32_t **keys, uint32_t **vals, uint32_t **keys_alt, uint32_t **vals_alt, uint64_t N,
+                      int key_bits, cudaStream_t s) {
+    if (N <= 1 || key_bits <= 0) return;
+    uint64_t tiles = (N + kRsTile - 1) / kRsTile;
+    uint64_t G = std::min<uint64_t>(tiles, 148u * 8u);
+    uint64_t chunk_tiles = (tiles + G - 1) / G;
+    uint64_t chunk = chunk_tiles * kRsTile;
+    G = (N + chunk - 1) / chunk;
+    uint32_t *counts = dalloc<uint32_t>(256 * G, s);
+    for (int shift = 0; shift < key_bits; shift += 8) {
+        rs_upsweep<<<(unsigned)G, kThreads, 0, s>>>(*keys, N, chunk, shift, counts, (uint32_t)G);
+        scan_single_block<<<1, 1024, 0, s>>>(counts, 256 * G, nullptr);
+        rs_downsweep<<<(unsigned)G, kThreads, 0, s>>>(*keys, *vals, *keys_alt, *vals_alt, N, chunk, shift, counts,
+                                                     (uint32_t)G);
+        PRG_CUDA(cudaGetLastError());
+        std::swap(*keys, *keys_alt);
+        std::swap(*vals, *vals_alt);
+    }
+    dfree(counts, s);
+}
+
+// ------------------------------------------------------------------ CSR
+
+// Arc a of the in-CSR before sorting: key = destination row, value = source
+// (unweighted) or arc id (weighted, to fetch the edge weight after the sort).
+__global__ void make_arcs(const uint32_t *from, const uint32_t *to, uint64_t m, bool directed, bool carry_id,
+                          uint32_t *key, uint32_t *val) {
+    for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e < m; e += (uint64_t)gridDim.x * blockDim.x) {
+        uint32_t u = from[e], v = to[e];
+        if (directed) {
+            key[e] = v;
+            val[e] = carry_id ? (uint32_t)e : u;
+        } else {
+            // arc 2e: in_adj[u] += v ; arc 2e+1: in_adj[v] += u (self-loop: both v)
+            key[2 * e] = u;
+            val[2 * e] = carry_id ? (uint32_t)(2 * e) : v;
+            key[2 * e + 1] = v;
+            val[2 * e + 1] = carry_id ? (uint32_t)(2 * e + 1) : u;
+        }
+    }
+}
+
+__global__ void histogram_u32(const uint32_t *key, uint64_t N, uint32_t *hist) {
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < N; i += (uint64_t)gridDim.x * blockDim.x)
+        atomicAdd(&hist[key[i]], 1u);
+}
+
+__global__ void out_degree_kernel(const uint32_t *from, const uint32_t *to, uint64_t m, bool directed,
+                                  uint32_t *deg) {
+    for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e < m; e += (uint64_t)gridDim.x * blockDim.x) {
+        atomicAdd(&deg[from[e]], 1u);
+        if (!directed) atomicAdd(&deg[to[e]], 1u);
+    }
+}
+
+// After sorting arc ids: fetch source and weight of every arc.
+__global__ void gather_arcs(const uint32_t *ids, const uint32_t *from, const uint32_t *to, const double *w,
+                            uint64_t arcs, bool directed, uint32_t *col, double *w64, float *w32) {
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < arcs;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        uint32_t a = ids[i];
+        uint64_t e = directed ? a : (a >> 1);
+        uint32_t src = directed ? from[e] : ((a & 1u) ? from[e] : to[e]);
+        col[i] = src;
+        double we = w[e];
+        w64[i] = we;
+        w32[i] = (float)we;
+    }
+}
+
+// Segmented row sums of per-arc weights (one warp per row, fixed tree).
+__global__ void row_weight_sums(const uint32_t *ptr, const double *wv, const uint32_t *perm, uint32_t nrows,
+                                double *outsum) {
+    uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    uint32_t lane = threadIdx.x & 31;
+    uint32_t nw = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t r = warp; r < nrows; r += nw) {
+        double acc = 0.0;
+        for (uint32_t p = ptr[r] + lane; p < ptr[r + 1]; p += 32) acc += perm ? wv[perm[p]] : wv[p];
+        acc = warp_sum(acc);
+        if (lane == 0) outsum[r] = acc;
+    }
+}
+
+__global__ void finish_degrees(uint32_t n, const uint32_t *deg, double *strength_io, bool weighted, double *dval,
+                               float *inv32, uint32_t *n_dangling) {
+    uint32_t cnt = 0;
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+        double d = weighted ? strength_io[v] : (double)deg[v];
+        dval[v] = d;
+        inv32[v] = d > 0.0 ? (float)(1.0 / d) : 0.0f;
+        cnt += d == 0.0 ? 1u : 0u;
+    }
+    cnt = warp_sum(cnt);
+    if ((threadIdx.x & 31) == 0 && cnt) atomicAdd(n_dangling, cnt);
+}
+
+__global__ void max_degree_kernel(const uint32_t *row_ptr, uint32_t n, uint32_t *out) {
+    uint32_t mx = 0;
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x)
+        mx = max(mx, row_ptr[v + 1] - row_ptr[v]);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(out, mx);
+}
+
+// ------------------------------------------------------------------ row-blocks
+//
+// A row is "short" (deg <= cap), "long" (cap < deg <= split: one block) or a
+// hub (deg > split: ceil(deg/split) chunk blocks whose partial sums are
+// combined by the last chunk to finish).  A run of short rows forms a stream
+// row-block; a new one starts at row r when r % rowcap == 0, when the
+// previous row was not short, or when row r's first arc crosses a multiple of
+// cap.  Every stream block therefore holds <= rowcap rows and < 2*cap arcs.
+
+__global__ void rb_count(const uint32_t *rp, uint32_t n, uint32_t cap, uint32_t rowcap, uint32_t split,
+                         uint32_t *cnt, uint32_t *hubflag) {
+    for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
+        uint32_t deg = rp[r + 1] - rp[r];
+        uint32_t c, h = 0;
+        if (deg > split) {
+            c = (deg + split - 1) / split;
+            h = 1;
+        } else if (deg > cap) {
+            c = 1;
+        } else {
+            bool start = (r == 0) || (r % rowcap == 0);
+            if (!start) {
+                uint32_t pdeg = rp[r] - rp[r - 1];
+                start = (pdeg > cap) || (rp[r] / cap != rp[r - 1] / cap);
+            }
+            c = start ? 1u : 0u;
+        }
+        cnt[r] = c;
+        hubflag[r] = h;
+    }
+}
+
+__global__ void rb_fill(const uint32_t *rp, uint32_t n, uint32_t cap, uint32_t split, const uint32_t *off,
+                        const uint32_t *hoff, uint4 *rb, Hub *hubs) {
+    for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
+        uint32_t k = off[r], c = off[r + 1] - k;
+        if (c == 0) continue;
+        uint32_t deg = rp[r + 1] - rp[r];
+        if (deg > split) {
+            uint32_t h = hoff[r];
+            hubs[h] = Hub{r, c, k, 0};
+            for (uint32_t j = 0; j < c; j++) rb[k + j] = make_uint4(r, r + 1, RB_CHUNK | (j << 2), h);
+        } else if (deg > cap) {
+            rb[k] = make_uint4(r, r + 1, RB_LONG, 0);
+        } else {
+            rb[k] = make_uint4(r, 0, RB_STREAM, 0);
+        }
+    }
+}
+
+__global__ void rb_fix(uint4 *rb, uint32_t nrb, uint32_t n) {
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < nrb; k += gridDim.x * blockDim.x) {
+        uint4 d = rb[k];
+        if ((d.z & 3u) == RB_STREAM) {
+            d.y = (k + 1 < nrb) ? rb[k + 1].x : n;
+            rb[k] = d;
+        }
+    }
+}
+
+void build_row_blocks(DeviceGraph &g, uint32_t cap, uint32_t rowcap, uint32_t split, cudaStream_t s) {
+    // the iteration kernel's shared buffers hold 2*kCap products and kRowCap+1 row offsets
+    cap = std::max<uint32_t>(32u, std::min<uint32_t>(cap, kCap));
+    rowcap = std::max<uint32_t>(1u, std::min<uint32_t>(rowcap, kRowCap));
+    split = std::max<uint32_t>(split, cap);
+    uint32_t n = g.n;
+    if (g.rb) cudaFreeAsync(g.rb, s);
+    if (g.hubs) cudaFreeAsync(g.hubs, s);
+    g.rb = nullptr;
+    g.hubs = nullptr;
+    uint32_t *cnt = dalloc<uint32_t>(n + 1, s), *off = dalloc<uint32_t>(n + 1, s);
+    uint32_t *hf = dalloc<uint32_t>(n + 1, s), *hoff = dalloc<uint32_t>(n + 1, s);
+    unsigned gb = grid_for(n, kThreads);
+    rb_count<<<gb, kThreads, 0, s>>>(g.row_ptr, n, cap, rowcap, split, cnt, hf);
+    exclusive_scan_u32(cnt, off, n, s);
+    exclusive_scan_u32(hf, hoff, n, s);
+    uint32_t hv[2];
+    PRG_CUDA(cudaMemcpyAsync(&hv[0], off + n, 4, cudaMemcpyDeviceToHost, s));
+    PRG_CUDA(cudaMemcpyAsync(&hv[1], hoff + n, 4, cudaMemcpyDeviceToHost, s));
+    PRG_CUDA(cudaStreamSynchronize(s));
+    g.nrb = hv[0];
+    g.nhub = hv[1];
+    g.ngroups = (g.nrb + kGroup - 1) / kGroup;
+    g.rb = dalloc<uint4>(g.nrb, s);
+    g.hubs = dalloc<Hub>(g.nhub, s);
+    rb_fill<<<gb, kThreads, 0, s>>>(g.row_ptr, n, cap, split, off, hoff, g.rb, g.hubs);
+    rb_fix<<<grid_for(g.nrb, kThreads), kThreads, 0, s>>>(g.rb, g.nrb, n);
+    PRG_CUDA(cudaGetLastError());
+    dfree(cnt, s);
+    dfree(off, s);
+    dfree(hf, s);
+    dfree(hoff, s);
+    g.cap = cap;
+    g.rowcap = rowcap;
+    g.split = split;
+}
+
+static int bits_for(uint32_t maxkey) {
+    int b = 0;
+    while (b < 32 && (maxkey >> b) != 0) b++;
+    return b;
+}
+
+void build_graph(DeviceGraph &g, const uint32_t *d_from, const uint32_t *d_to, const double *d_w, cudaStream_t s) {
+    cudaEvent_t e0, e1;
+    PRG_CUDA(cudaEventCreate(&e0));
+    PRG_CUDA(cudaEventCreate(&e1));
+    PRG_CUDA(cudaEventRecord(e0, s));
+    const uint32_t n = g.n;
+    const uint64_t m = g.m;
+    const bool directed = g.directed, weighted = d_w != nullptr;
+    g.weighted = weighted;
+    const uint64_t arcs = directed ? m : 2 * m;
+    g.arcs = arcs;
+    unsigned ge = grid_for(m, kThreads), ga = grid_for(arcs, kThreads), gn = grid_for(n, kThreads);
+
+    // out-degree (unweighted divisor; also kept for weighted graphs)
+    PRG_CUDA(cudaMallocAsync((void **)&g.deg, std::max<uint64_t>(n, 1) * 4, s));
+    PRG_CUDA(cudaMemsetAsync(g.deg, 0, std::max<uint64_t>(n, 1) * 4, s));
+    if (m) out_degree_kernel<<<ge, kThreads, 0, s>>>(d_from, d_to, m, directed, g.deg);
+
+    // arcs in edge order, then stable sort by destination
+    uint32_t *k0 = dalloc<uint32_t>(arcs, s), *v0 = dalloc<uint32_t>(arcs, s);
+    uint32_t *k1 = dalloc<uint32_t>(arcs, s), *v1 = dalloc<uint32_t>(arcs, s);
+    if (m) make_arcs<<<ge, kThreads, 0, s>>>(d_from, d_to, m, directed, weighted, k0, v0);
+
+    // row_ptr from the in-degree histogram
+    uint32_t *indeg = dalloc<uint32_t>(n + 1, s);
+    PRG_CUDA(cudaMemsetAsync(indeg, 0, (uint64_t)(n + 1) * 4, s));
+    if (arcs) histogram_u32<<<ga, kThreads, 0, s>>>(k0, arcs, indeg);
+    PRG_CUDA(cudaMallocAsync((void **)&g.row_ptr, (uint64_t)(n + 1) * 4, s));
+    exclusive_scan_u32(indeg, g.row_ptr, n, s);
+    dfree(indeg, s);
+
+    radix_sort_pairs(&k0, &v0, &k1, &v1, arcs, bits_for(n ? n - 1 : 0), s);
+
+    const uint64_t padded = arcs + kColPad;
+    PRG_CUDA(cudaMallocAsync((void **)&g.col, padded * 4, s));
+    PRG_CUDA(cudaMemsetAsync(g.col, 0, padded * 4, s));
+    double *strength = nullptr;
+    if (!weighted) {
+        if (arcs) PRG_CUDA(cudaMemcpyAsync(g.col, v0, arcs * 4, cudaMemcpyDeviceToDevice, s));
+    } else {
+        PRG_CUDA(cudaMallocAsync((void **)&g.w64, padded * 8, s));
+        PRG_CUDA(cudaMallocAsync((void **)&g.w32, padded * 4, s));
+        PRG_CUDA(cudaMemsetAsync(g.w64, 0, padded * 8, s));
+        PRG_CUDA(cudaMemsetAsync(g.w32, 0, padded * 4, s));
+        if (arcs) gather_arcs<<<ga, kThreads, 0, s>>>(v0, d_from, d_to, d_w, arcs, directed, g.col, g.w64, g.w32);
+        strength = dalloc<double>(n, s);
+        if (!directed) {
+            // undirected: arcs out of u are exactly the arcs into u (same weights)
+            row_weight_sums<<<grid_for((uint64_t)n * 32, kThreads), kThreads, 0, s>>>(g.row_ptr, g.w64, nullptr, n,
+                                                                                   strength);
+        } else {
+            // directed: group edge ids by source with a second stable sort
+            uint32_t *sk = dalloc<uint32_t>(m, s), *sv = dalloc<uint32_t>(m, s);
+            uint32_t *sk1 = dalloc<uint32_t>(m, s), *sv1 = dalloc<uint32_t>(m, s);
+            uint32_t *optr = dalloc<uint32_t>(n + 1, s), *oh = dalloc<uint32_t>(n + 1, s);
+            if (m) {
+                PRG_CUDA(cudaMemcpyAsync(sk, d_from, m * 4, cudaMemcpyDeviceToDevice, s));
+                make_arcs<<<ge, kThreads, 0, s>>>(d_from, d_to, m, true, true, sk1, sv);  // sv = edge ids
+            }
+            PRG_CUDA(cudaMemsetAsync(oh, 0, (uint64_t)(n + 1) * 4, s));
+            if (m) histogram_u32<<<ge, kThreads, 0, s>>>(sk, m, oh);
+            exclusive_scan_u32(oh, optr, n, s);
+            radix_sort_pairs(&sk, &sv, &sk1, &sv1, m, bits_for(n ? n - 1 : 0), s);
+            row_weight_sums<<<grid_for((uint64_t)n * 32, kThreads), kThreads, 0, s>>>(optr, d_w, sv, n, strength);
+            dfree(sk, s);
+            dfree(sv, s);
+            dfree(sk1, s);
+            dfree(sv1, s);
+            dfree(optr, s);
+            dfree(oh, s);
+        }
+    }
+    dfree(k0, s);
+    dfree(v0, s);
+    dfree(k1, s);
+    dfree(v1, s);
+
+    PRG_CUDA(cudaMallocAsync((void **)&g.dval, std::max<uint64_t>(n, 1) * 8, s));
+    PRG_CUDA(cudaMallocAsync((void **)&g.inv32, std::max<uint64_t>(n, 1) * 4, s));
+    uint32_t *d_nd = dalloc<uint32_t>(2, s);
+    PRG_CUDA(cudaMemsetAsync(d_nd, 0, 8, s));
+    finish_degrees<<<gn, kThreads, 0, s>>>(n, g.deg, strength, weighted, g.dval, g.inv32, d_nd);
+    max_degree_kernel<<<gn, kThreads, 0, s>>>(g.row_ptr, n, d_nd + 1);
+    PRG_CUDA(cudaGetLastError());
+    uint32_t hnd[2];
+    PRG_CUDA(cudaMemcpyAsync(hnd, d_nd, 8, cudaMemcpyDeviceToHost, s));
+    dfree(strength, s);
+    dfree(d_nd, s);
+    PRG_CUDA(cudaStreamSynchronize(s));
+    g.n_dangling = hnd[0];
+    g.max_in_degree = hnd[1];
+
+    build_row_blocks(g, g.cap, g.rowcap, g.split, s);
+    PRG_CUDA(cudaEventRecord(e1, s));
+    PRG_CUDA(cudaEventSynchronize(e1));
+    PRG_CUDA(cudaEventElapsedTime(&g.build_ms, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+}
+
+void free_graph(DeviceGraph &g) {
+    cudaFree(g.row_ptr);
+    cudaFree(g.col);
+    cudaFree(g.w64);
+    cudaFree(g.w32);
+    cudaFree(g.deg);
+    cudaFree(g.dval);
+    cudaFree(g.inv32);
+    cudaFree(g.rb);
+    cudaFree(g.hubs);
+    g = DeviceGraph{};
+}
+
+// ------------------------------------------------------------------ R-MAT
+
+// Counter-based R-MAT: edge e draws `scale` uniforms from its own SplitMix64
+// stream seeded with seed ^ (e * 0xD1B54A32D192ED03).  Bit-identical to the
+// CPU generator used by the tests (same integer mixing, same double compare).
+__global__ void rmat_kernel(uint32_t scale, uint64_t m, double t1, double t2, double t3, uint64_t seed,
+                            uint32_t *from, uint32_t *to) {
+    for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e < m; e += (uint64_t)gridDim.x * blockDim.x) {
+        uint64_t st = seed ^ (e * 0xD1B54A32D192ED03ULL);
+        uint32_t u = 0, v = 0;
+        for (uint32_t l = 0; l < scale; l++) {
+            st += 0x9E3779B97F4A7C15ULL;
+            uint64_t z = st;
+            z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+            z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+            z ^= z >> 31;
+            double x = (double)(z >> 11) * (1.0 / 9007199254740992.0);
+            uint32_t rb, cb;
+            if (x < t1) { rb = 0; cb = 0; }
+            else if (x < t2) { rb = 0; cb = 1; }
+            else if (x < t3) { rb = 1; cb = 0; }
+            else { rb = 1; cb = 1; }
+            u = (u << 1) | rb;
+            v = (v << 1) | cb;
+        }
+        from[e] = u;
+        to[e] = v;
+    }
+}
+
+void rmat_generate(uint32_t scale, uint64_t m, double a, double b, double c, uint64_t seed, uint32_t *d_from,
+                   uint32_t *d_to, cudaStream_t s) {
+    double t1 = a, t2 = a + b, t3 = a + b + c;
+    rmat_kernel<<<grid_for(m, kThreads, 148u * 32u), kThreads, 0, s>>>(scale, m, t1, t2, t3, seed, d_from, d_to);
+    PRG_CUDA(cudaGetLastError());
+}
+
+}  // namespace prg

@@ -1,0 +1,64 @@
+// graph.cuh — the device-resident graph behind a prg_graph handle and the
+// build entry points (csr_build.cu).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "prg_internal.cuh"
+
+namespace prg {
+
+struct DeviceGraph {
+    uint32_t n = 0;
+    uint64_t m = 0;      // edges as the caller passed them
+    uint64_t arcs = 0;   // in-CSR entries (2m for undirected graphs)
+    bool directed = true;
+    bool weighted = false;
+    int device = 0;
+
+    uint32_t *row_ptr = nullptr;  // n+1
+    uint32_t *col = nullptr;      // arcs + kColPad
+    double *w64 = nullptr;        // arcs + kColPad (weighted)
+    float *w32 = nullptr;         // arcs + kColPad (weighted)
+    uint32_t *deg = nullptr;      // n
+    double *dval = nullptr;       // n: out-degree / out-strength as double
+    float *inv32 = nullptr;       // n: 1/dval in FP32, 0 when dangling
+
+    uint4 *rb = nullptr;          // row-blocks {row_begin, row_end, kind|chunk<<2, hub}
+    uint32_t nrb = 0;
+    uint32_t ngroups = 0;
+    Hub *hubs = nullptr;
+    uint32_t nhub = 0;
+    uint32_t n_dangling = 0;
+    uint32_t max_in_degree = 0;
+
+    // row-block tuning used to build `rb` (autotuned or defaults)
+    uint32_t cap = kCap;
+    uint32_t rowcap = kRowCap;
+    uint32_t split = kSplit;
+
+    float build_ms = 0.f;
+};
+
+// Builds the in-CSR, degrees and row-blocks from device edge arrays.
+// d_w may be null (unweighted).  All work is on `s`; temporaries use the
+// stream-ordered allocator.
+void build_graph(DeviceGraph &g, const uint32_t *d_from, const uint32_t *d_to, const double *d_w,
+                 cudaStream_t s);
+// Rebuilds only the row-blocks with new tuning (autotuner).
+void build_row_blocks(DeviceGraph &g, uint32_t cap, uint32_t rowcap, uint32_t split, cudaStream_t s);
+void free_graph(DeviceGraph &g);
+
+// Stable LSD radix sort of (key, value) u32 pairs on the low `key_bits` bits.
+// On return *keys / *vals point at the sorted data (buffers may be swapped
+// with *keys_alt / *vals_alt).
+void radix_sort_pairs(uint32_t **keys, uint32_t **vals, uint32_t **keys_alt, uint32_t **vals_alt, uint64_t N,
+                      int key_bits, cudaStream_t s);
+// out[0..n] = exclusive prefix sums of in[0..n), out[n] = total (u32).
+void exclusive_scan_u32(const uint32_t *in, uint32_t *out, uint64_t n, cudaStream_t s);
+
+// Device R-MAT generator (same stream layout as the oracle's or_rmat).
+void rmat_generate(uint32_t scale, uint64_t m, double a, double b, double c, uint64_t seed, uint32_t *d_from,
+                   uint32_t *d_to, cudaStream_t s);
+
+}  // namespace prg

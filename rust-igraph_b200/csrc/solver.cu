@@ -1,0 +1,297 @@
+// solver.cu — drives the fused iteration kernels: FP64 power iteration (the
+// drop-in) and FP32 iteration with FP64 residual refinement.  Iterations run
+// inside captured CUDA graphs of `unroll` iteration pairs; the kernels stop
+// themselves (Ctl::done) so the host only polls a pinned copy of Ctl once per
+// graph launch.
+//
+// Refinement (FP32 SpMV, FP64 residual):
+//   G(x) = d*P^T(x/s) + d*(sum_dangling x)*t + (1-d)*t  is an L1 contraction
+//   with factor d, so ||x - x*||_1 <= ||G(x) - x||_1 / (1-d).
+//   repeat: g = G(x) and r = g - x in FP64 (MODE_RESID64);
+//           if ||r||_1 <= eps*(1-d)/d: return g (error <= d*||r||/(1-d) <= eps)
+//           solve e = d*M e + r approximately in FP32 (MODE_CORR32, seeded
+//           with e0 = r) until its successive change <= max(rho*||r||, floor);
+//           x <- x + e in FP64.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+#include "solver.cuh"
+
+namespace prg {
+
+template <class T>
+static void walloc(T *&p, uint64_t count, cudaStream_t s) {
+    PRG_CUDA(cudaMallocAsync((void **)&p, std::max<uint64_t>(count, 1) * sizeof(T), s));
+}
+template <class T>
+static void wfree(T *&p, cudaStream_t s) {
+    if (p) cudaFreeAsync(p, s);
+    p = nullptr;
+}
+
+constexpr uint32_t kPrepParts = 148u * 4u;
+
+void workspace_free(Workspace &ws, cudaStream_t s) {
+    for (auto &kv : ws.graphs) cudaGraphExecDestroy(kv.second);
+    ws.graphs.clear();
+    for (int i = 0; i < 2; i++) {
+        wfree(ws.x64[i], s);
+        wfree(ws.xt64[i], s);
+        wfree(ws.e32[i], s);
+        wfree(ws.et32[i], s);
+    }
+    wfree(ws.b32, s);
+    wfree(ws.t64, s);
+    wfree(ws.t32, s);
+    wfree(ws.ctl, s);
+    wfree(ws.rb_part, s);
+    wfree(ws.grp_part, s);
+    wfree(ws.hub_rec, s);
+    wfree(ws.chunk_part, s);
+    wfree(ws.grp_ticket, s);
+    wfree(ws.hub_ticket, s);
+    if (ws.h_ctl) cudaFreeHost(ws.h_ctl);
+    ws.h_ctl = nullptr;
+    if (ws.ev0) cudaEventDestroy(ws.ev0);
+    if (ws.ev1) cudaEventDestroy(ws.ev1);
+    ws.ev0 = ws.ev1 = nullptr;
+    ws.ready = false;
+}
+
+void workspace_ensure(Workspace &ws, const DeviceGraph &g, cudaStream_t s) {
+    if (ws.ready && ws.n == g.n && ws.nrb == g.nrb && ws.nhub == g.nhub) return;
+    if (ws.ready) workspace_free(ws, s);
+    ws.n = g.n;
+    ws.nrb = g.nrb;
+    ws.ngroups = g.ngroups;
+    ws.nhub = g.nhub;
+    const uint64_t n = g.n;
+    for (int i = 0; i < 2; i++) {
+        walloc(ws.x64[i], n, s);
+        walloc(ws.xt64[i], n, s);
+        walloc(ws.e32[i], n, s);
+        walloc(ws.et32[i], n, s);
+    }
+    walloc(ws.b32, n, s);
+    walloc(ws.t64, n, s);
+    walloc(ws.t32, n, s);
+    walloc(ws.ctl, 1, s);
+    walloc(ws.rb_part, std::max<uint64_t>(g.nrb, kPrepParts), s);
+    walloc(ws.grp_part, g.ngroups, s);
+    walloc(ws.hub_rec, g.nhub, s);
+    walloc(ws.chunk_part, g.nrb, s);
+    walloc(ws.grp_ticket, g.ngroups, s);
+    walloc(ws.hub_ticket, g.nhub, s);
+    PRG_CUDA(cudaMemsetAsync(ws.grp_ticket, 0, std::max<uint64_t>(g.ngroups, 1) * 4, s));
+    PRG_CUDA(cudaMemsetAsync(ws.hub_ticket, 0, std::max<uint64_t>(g.nhub, 1) * 4, s));
+    PRG_CUDA(cudaMemsetAsync(ws.hub_rec, 0, std::max<uint64_t>(g.nhub, 1) * sizeof(double4), s));
+    PRG_CUDA(cudaMallocHost((void **)&ws.h_ctl, sizeof(Ctl)));
+    PRG_CUDA(cudaEventCreate(&ws.ev0));
+    PRG_CUDA(cudaEventCreate(&ws.ev1));
+    ws.ready = true;
+}
+
+static IterArgs base_args(const DeviceGraph &g, Workspace &ws, double damping) {
+    IterArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.row_ptr = g.row_ptr;
+    a.col = g.col;
+    a.w64 = g.w64;
+    a.w32 = g.w32;
+    a.dval = g.dval;
+    a.inv32 = g.inv32;
+    a.rb = g.rb;
+    a.hubs = g.hubs;
+    a.nrb = g.nrb;
+    a.ngroups = g.ngroups;
+    a.nhub = g.nhub;
+    a.n = g.n;
+    a.split = g.split;
+    a.damping = damping;
+    a.inv_n = 1.0 / (double)g.n;
+    a.ctl = ws.ctl;
+    a.rb_part = ws.rb_part;
+    a.grp_part = ws.grp_part;
+    a.chunk_part = ws.chunk_part;
+    a.hub_rec = ws.hub_rec;
+    a.grp_ticket = ws.grp_ticket;
+    a.hub_ticket = ws.hub_ticket;
+    return a;
+}
+
+static uint64_t graph_key(int mode, bool has_t, double damping) {
+    uint64_t bits;
+    std::memcpy(&bits, &damping, 8);
+    return (bits * 0x9E3779B97F4A7C15ULL) ^ ((uint64_t)mode << 1) ^ (uint64_t)has_t;
+}
+
+// Captured graph of `unroll` (parity 0, parity 1) launch pairs.
+static cudaGraphExec_t loop_graph(const DeviceGraph &g, Workspace &ws, int mode, bool has_t, double damping,
+                                  const IterArgs &a0, const IterArgs &a1, cudaStream_t s) {
+    const uint64_t key = graph_key(mode, has_t, damping);
+    auto it = ws.graphs.find(key);
+    if (it != ws.graphs.end()) return it->second;
+    cudaGraph_t graph;
+    PRG_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    for (int u = 0; u < ws.unroll; u++) {
+        launch_iteration(mode, g.weighted, a0, s);
+        launch_iteration(mode, g.weighted, a1, s);
+    }
+    PRG_CUDA(cudaStreamEndCapture(s, &graph));
+    cudaGraphExec_t exec;
+    PRG_CUDA(cudaGraphInstantiate(&exec, graph, 0));
+    cudaGraphDestroy(graph);
+    ws.graphs[key] = exec;
+    return exec;
+}
+
+// Launches the loop graph until the kernels raise Ctl::done.
+static void run_loop(Workspace &ws, cudaGraphExec_t exec, uint32_t max_iter, cudaStream_t s) {
+    const uint64_t max_launches = (uint64_t)max_iter / (2u * ws.unroll) + 2u;
+    for (uint64_t k = 0; k < max_launches; k++) {
+        PRG_CUDA(cudaGraphLaunch(exec, s));
+        PRG_CUDA(cudaMemcpyAsync(ws.h_ctl, ws.ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, s));
+        PRG_CUDA(cudaStreamSynchronize(s));
+        if (ws.h_ctl->done) return;
+    }
+}
+
+static void read_ctl(Workspace &ws, cudaStream_t s) {
+    PRG_CUDA(cudaMemcpyAsync(ws.h_ctl, ws.ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, s));
+    PRG_CUDA(cudaStreamSynchronize(s));
+}
+
+__global__ void to_f32_kernel(const double *a, float *b, uint32_t n) {
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) b[v] = (float)a[v];
+}
+
+static void solve_fp64(const DeviceGraph &g, Workspace &ws, const SolveOpts &o, const double *d_t, double *d_out,
+                       SolveStats &st, cudaStream_t s) {
+    const bool ppr = d_t != nullptr;
+    if (o.d_start) PRG_CUDA(cudaMemcpyAsync(ws.x64[0], o.d_start, (uint64_t)g.n * 8, cudaMemcpyDeviceToDevice, s));
+    else launch_fill_start(ws.x64[0], d_t, g.n, s);
+    Ctl c;
+    std::memset(&c, 0, sizeof(c));
+    c.thr = o.stop == 1 ? o.eps * (1.0 - o.damping) / o.damping : o.eps;
+    c.max_iter = o.max_iter;
+    PRG_CUDA(cudaMemcpyAsync(ws.ctl, &c, sizeof(Ctl), cudaMemcpyHostToDevice, s));
+    launch_prepare64(g, ws.x64[0], nullptr, ws.xt64[0], ws.ctl, 0, ws.rb_part, s);
+    IterArgs a0 = base_args(g, ws, o.damping), a1 = a0;
+    a0.t64 = a1.t64 = d_t;
+    a0.parity = 0;
+    a0.x64_in = ws.x64[0];
+    a0.xt64_in = ws.xt64[0];
+    a0.x64_out = ws.x64[1];
+    a0.xt64_out = ws.xt64[1];
+    a1.parity = 1;
+    a1.x64_in = ws.x64[1];
+    a1.xt64_in = ws.xt64[1];
+    a1.x64_out = ws.x64[0];
+    a1.xt64_out = ws.xt64[0];
+    const int mode = ppr ? MODE_PPR64 : MODE_PLAIN64;
+    if (o.max_iter > 0) {
+        cudaGraphExec_t ex = loop_graph(g, ws, mode, ppr, o.damping, a0, a1, s);
+        run_loop(ws, ex, o.max_iter, s);
+    } else {
+        read_ctl(ws, s);
+    }
+    const Ctl &h = *ws.h_ctl;
+    const double *res = (h.iters == 0) ? ws.x64[0] : (h.parity_last == 0 ? ws.x64[1] : ws.x64[0]);
+    PRG_CUDA(cudaMemcpyAsync(d_out, res, (uint64_t)g.n * 8, cudaMemcpyDeviceToDevice, s));
+    st.iterations = st.fp64_passes = h.iters;
+    st.last_diff = h.diff;
+    st.residual_l1 = h.diff;
+    st.error_bound = h.diff * o.damping / (1.0 - o.damping);
+}
+
+static void solve_refined(const DeviceGraph &g, Workspace &ws, const SolveOpts &o, const double *d_t,
+                          double *d_out, SolveStats &st, cudaStream_t s) {
+    const bool ppr = d_t != nullptr;
+    const double thr_final = o.eps * (1.0 - o.damping) / o.damping;
+    if (o.d_start) PRG_CUDA(cudaMemcpyAsync(ws.x64[0], o.d_start, (uint64_t)g.n * 8, cudaMemcpyDeviceToDevice, s));
+    else launch_fill_start(ws.x64[0], d_t, g.n, s);
+    if (ppr) to_f32_kernel<<<148 * 4, kThreads, 0, s>>>(d_t, ws.t32, g.n);
+    Ctl c;
+    std::memset(&c, 0, sizeof(c));
+    c.rho = 4e-6;
+    c.floor_abs = 0.05 * thr_final;
+    const uint32_t inner_cap = std::max<uint32_t>(16u, std::min<uint32_t>(o.max_iter, 400u));
+    c.max_iter = inner_cap;
+    PRG_CUDA(cudaMemcpyAsync(ws.ctl, &c, sizeof(Ctl), cudaMemcpyHostToDevice, s));
+    launch_prepare64(g, ws.x64[0], nullptr, ws.xt64[0], ws.ctl, 1, ws.rb_part, s);
+
+    IterArgs r = base_args(g, ws, o.damping);
+    r.t64 = d_t;
+    r.parity = 1;
+    r.x64_in = ws.x64[0];
+    r.xt64_in = ws.xt64[0];
+    r.x64_out = ws.x64[1];
+    r.b32_out = ws.b32;
+    r.x32_out = ws.e32[0];
+    r.xt32_out = ws.et32[0];
+
+    IterArgs a0 = base_args(g, ws, o.damping), a1 = a0;
+    a0.t32 = a1.t32 = ppr ? ws.t32 : nullptr;
+    a0.b32 = a1.b32 = ws.b32;
+    a0.parity = 0;
+    a0.x32_in = ws.e32[0];
+    a0.xt32_in = ws.et32[0];
+    a0.x32_out = ws.e32[1];
+    a0.xt32_out = ws.et32[1];
+    a1.parity = 1;
+    a1.x32_in = ws.e32[1];
+    a1.xt32_in = ws.et32[1];
+    a1.x32_out = ws.e32[0];
+    a1.xt32_out = ws.et32[0];
+    cudaGraphExec_t ex = loop_graph(g, ws, MODE_CORR32, ppr, o.damping, a0, a1, s);
+
+    const uint32_t pass_cap = std::max<uint32_t>(o.max_iter, 64u);
+    uint32_t fp32 = 0, fp64 = 0;
+    for (int outer = 0; outer < 64; outer++) {
+        launch_iteration(MODE_RESID64, g.weighted, r, s);
+        fp64++;
+        read_ctl(ws, s);
+        const double rn = ws.h_ctl->rnorm;
+        st.residual_l1 = rn;
+        if (!(rn > thr_final) || fp32 + fp64 >= pass_cap) break;
+        run_loop(ws, ex, inner_cap, s);
+        fp32 += ws.h_ctl->iters;
+        const float *e_fin = ws.h_ctl->parity_last == 0 ? ws.e32[1] : ws.e32[0];
+        launch_prepare64(g, ws.x64[0], e_fin, ws.xt64[0], ws.ctl, 1, ws.rb_part, s);
+    }
+    if (o.normalise) {
+        // result = g / sum(g) (FP64), sum taken by the last residual pass
+        PRG_CUDA(cudaMemcpyAsync(d_out, ws.x64[1], (uint64_t)g.n * 8, cudaMemcpyDeviceToDevice, s));
+        launch_normalise(d_out, g.n, ws.ctl, s);
+    } else {
+        PRG_CUDA(cudaMemcpyAsync(d_out, ws.x64[1], (uint64_t)g.n * 8, cudaMemcpyDeviceToDevice, s));
+    }
+    st.fp32_passes = fp32;
+    st.fp64_passes = fp64;
+    st.residual_passes = fp64;
+    st.iterations = fp32 + fp64;
+    st.last_diff = ws.h_ctl->diff;
+    st.error_bound = st.residual_l1 * o.damping / (1.0 - o.damping);
+}
+
+void solve(const DeviceGraph &g, Workspace &ws, const SolveOpts &o, const double *d_t, double *d_out,
+           SolveStats &st, cudaStream_t s) {
+    workspace_ensure(ws, g, s);
+    PRG_CUDA(cudaMemsetAsync(ws.grp_ticket, 0, std::max<uint64_t>(g.ngroups, 1) * 4, s));
+    PRG_CUDA(cudaMemsetAsync(ws.hub_ticket, 0, std::max<uint64_t>(g.nhub, 1) * 4, s));
+    PRG_CUDA(cudaEventRecord(ws.ev0, s));
+    st = SolveStats{};
+    if (o.precision == 1) solve_refined(g, ws, o, d_t, d_out, st, s);
+    else solve_fp64(g, ws, o, d_t, d_out, st, s);
+    PRG_CUDA(cudaEventRecord(ws.ev1, s));
+    PRG_CUDA(cudaEventSynchronize(ws.ev1));
+    float ms = 0.f;
+    PRG_CUDA(cudaEventElapsedTime(&ms, ws.ev0, ws.ev1));
+    st.solve_ms = ms;
+    PRG_CUDA(cudaGetLastError());
+}
+
+}  // namespace prg

@@ -1,0 +1,60 @@
+// solver.cuh — host orchestration of a PageRank solve on a resident graph.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <map>
+
+#include "graph.cuh"
+#include "spmv.cuh"
+
+namespace prg {
+
+struct SolveOpts {
+    double damping = 0.85;
+    double eps = 1e-10;
+    uint32_t max_iter = 1000;
+    int precision = 0;      // 0 FP64, 1 FP32-refined
+    int stop = 0;           // 0 successive (reference), 1 error bound
+    int normalise = 1;
+    const double *d_start = nullptr;  // device start vector (warm start) or null
+};
+
+struct SolveStats {
+    uint32_t iterations = 0, fp64_passes = 0, fp32_passes = 0, residual_passes = 0;
+    double last_diff = 0, residual_l1 = 0, error_bound = 0, solve_ms = 0;
+};
+
+// Reusable per-handle solve buffers and captured CUDA graphs.
+struct Workspace {
+    bool ready = false;
+    uint32_t n = 0, nrb = 0, ngroups = 0, nhub = 0;
+    double *x64[2] = {nullptr, nullptr};
+    double *xt64[2] = {nullptr, nullptr};
+    float *e32[2] = {nullptr, nullptr};
+    float *et32[2] = {nullptr, nullptr};
+    float *b32 = nullptr;
+    double *t64 = nullptr;
+    float *t32 = nullptr;
+    Ctl *ctl = nullptr;
+    Ctl *h_ctl = nullptr;  // pinned mirror
+    double4 *rb_part = nullptr;
+    double4 *grp_part = nullptr;
+    double4 *hub_rec = nullptr;
+    double *chunk_part = nullptr;
+    uint32_t *grp_ticket = nullptr;
+    uint32_t *hub_ticket = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    std::map<uint64_t, cudaGraphExec_t> graphs;
+    int unroll = 8;  // iteration pairs per graph launch
+};
+
+void workspace_ensure(Workspace &ws, const DeviceGraph &g, cudaStream_t s);
+void workspace_free(Workspace &ws, cudaStream_t s);
+
+// Solves on graph g.  d_t: normalised teleport/reset vector on the device
+// (null = uniform 1/n).  d_out: device double[n].
+void solve(const DeviceGraph &g, Workspace &ws, const SolveOpts &o, const double *d_t, double *d_out,
+           SolveStats &st, cudaStream_t s);
+
+}  // namespace prg

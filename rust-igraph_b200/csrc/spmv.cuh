@@ -1,0 +1,76 @@
+// spmv.cuh — launch interface of the fused PageRank iteration kernels.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "graph.cuh"
+
+namespace prg {
+
+// Iteration flavours.  All share one kernel body (spmv.cu); they differ in
+// the gather precision and the per-vertex epilogue.
+enum IterMode : int {
+    // FP64, uniform teleport, the reference's update
+    //   x'[v] = (1-d)/n + d*dsum/n + d*sum_{u->v} w*x[u]/s[u]   (pagerank.rs:116-129)
+    MODE_PLAIN64 = 0,
+    // FP64, reset-vector teleport and dangling redistribution
+    //   x'[v] = (1-d)*r[v] + d*(sum + dsum*r[v])               (personalized_pagerank.rs:169-170)
+    MODE_PPR64 = 1,
+    // FP64 residual pass of the refined solver: g = G(x), r = g - x (stored
+    // FP32), and the FP32 correction iteration is seeded with e0 = r
+    MODE_RESID64 = 2,
+    // FP32 correction iteration  e' = d*P^T(e/s) + d*dsum_e*t + r
+    MODE_CORR32 = 3,
+};
+
+struct IterArgs {
+    // graph
+    const uint32_t *row_ptr;
+    const uint32_t *col;
+    const double *w64;
+    const float *w32;
+    const double *dval;
+    const float *inv32;
+    const uint4 *rb;
+    const Hub *hubs;
+    uint32_t nrb, ngroups, nhub, n;
+    uint32_t split;
+    // vectors (FP64 modes use the *64 pointers, CORR32 the *32 ones)
+    const double *xt64_in;
+    const double *x64_in;
+    double *x64_out;
+    double *xt64_out;
+    const float *xt32_in;
+    const float *x32_in;
+    float *x32_out;
+    float *xt32_out;
+    const double *t64;  // teleport distribution (null = uniform 1/n)
+    const float *t32;
+    const float *b32;   // CORR32: additive residual r
+    float *b32_out;     // RESID64: residual r written here
+    // scalars
+    double damping;
+    double inv_n;
+    // reduction scratch
+    Ctl *ctl;
+    double4 *rb_part;
+    double4 *grp_part;
+    double *chunk_part;
+    double4 *hub_rec;
+    uint32_t *grp_ticket;
+    uint32_t *hub_ticket;
+    int parity;
+};
+
+void launch_iteration(int mode, bool weighted, const IterArgs &a, cudaStream_t s);
+
+// x <- x + e (e may be null), xt <- x / dval, dangling sum and total sum of
+// x into ctl->dsum[parity] / ctl->gsum via a deterministic two-level tree.
+void launch_prepare64(const DeviceGraph &g, double *x, const float *e, double *xt, Ctl *ctl, int parity,
+                      double4 *rb_part, cudaStream_t s);
+// x <- x / sum (final FP64 normalisation of the refined result).
+void launch_normalise(double *x, uint32_t n, const Ctl *ctl, cudaStream_t s);
+// x <- t (FP64 copy) or uniform 1/n when t is null.
+void launch_fill_start(double *x, const double *t, uint32_t n, cudaStream_t s);
+
+}  // namespace prg

@@ -1,0 +1,402 @@
+"""Python host side of the B200 PageRank library.
+
+Mirrors the slice of rust-igraph's public API that the PageRank hot path
+uses, with the same names, argument meaning and error behaviour:
+
+* ``Graph`` — ``with_vertices``, ``new``, ``add_edge``, ``add_edges``,
+  ``vcount``, ``ecount``, ``is_directed``, ``edge`` (src/core/graph.rs:126-152,
+  :518, :170, :740-785, :547, :564, :582, :1152).  Undirected edges are stored
+  as (min, max) like ``Graph::add_edges``.
+* ``pagerank``, ``pagerank_weighted``, ``personalized_pagerank``,
+  ``personalized_pagerank_default``, ``personalized_pagerank_vs``
+  (src/algorithms/properties/pagerank.rs:52, pagerank_weighted.rs:52,
+  personalized_pagerank.rs:65, :206, :241) returning a float64 numpy array
+  or raising the ``IgraphError`` subclass the reference would return.
+* ``DeviceGraph`` — a graph kept resident in HBM for repeated solves with
+  the extended options (FP32 + FP64-refined precision, error-bound stop,
+  warm start) and the batched personalized solver.
+
+Every call goes through ``libprg_b200.so`` (include/prg_b200.h).  There is no
+CPU implementation here: if the library or a GPU is missing the call raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass
+from typing import Iterable, Optional, Sequence
+
+import numpy as np
+
+_PKG_DIR = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(os.path.dirname(_PKG_DIR), "libprg_b200.so")
+
+# ------------------------------------------------------------------ errors
+
+
+class IgraphError(Exception):
+    """Base of the error variants (rust-igraph src/core/error.rs:14-66)."""
+
+
+class InvalidArgument(IgraphError):
+    pass
+
+
+class VertexOutOfRange(IgraphError):
+    pass
+
+
+class Internal(IgraphError):
+    pass
+
+
+class DidNotConverge(IgraphError):
+    pass
+
+
+class DeviceTimeout(Internal):
+    pass
+
+
+PRG_OK = 0
+_ERRORS = {1: InvalidArgument, 2: VertexOutOfRange, 3: Internal, 4: Internal, 5: Internal, 6: DidNotConverge,
+           7: DeviceTimeout}
+
+# ------------------------------------------------------------------ library
+
+
+class prg_options(C.Structure):
+    _fields_ = [("damping", C.c_double), ("eps", C.c_double), ("max_iter", C.c_uint32),
+                ("precision", C.c_int32), ("stop", C.c_int32), ("normalise", C.c_int32),
+                ("start", C.c_void_p)]
+
+
+class prg_stats(C.Structure):
+    _fields_ = [("iterations", C.c_uint32), ("fp64_passes", C.c_uint32), ("fp32_passes", C.c_uint32),
+                ("residual_passes", C.c_uint32), ("last_diff", C.c_double), ("residual_l1", C.c_double),
+                ("error_bound", C.c_double), ("solve_ms", C.c_double), ("build_ms", C.c_double),
+                ("arcs", C.c_uint64), ("n_dangling", C.c_uint32), ("pad", C.c_uint32)]
+
+
+_lib = None
+
+
+def library_path() -> str:
+    return _LIB_PATH
+
+
+def lib():
+    """Loads libprg_b200.so (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(_LIB_PATH):
+        raise ImportError(f"{_LIB_PATH} is missing: build it with `python rust-igraph_b200/build.py`")
+    L = C.CDLL(_LIB_PATH)
+    u32p, f64p, vp = C.c_void_p, C.c_void_p, C.c_void_p
+    L.prg_default_options.restype = None
+    L.prg_default_options.argtypes = [C.POINTER(prg_options)]
+    L.prg_last_error.restype = C.c_char_p
+    L.prg_last_error.argtypes = []
+    L.prg_pagerank.restype = C.c_int32
+    L.prg_pagerank.argtypes = [C.c_uint32, C.c_uint64, u32p, u32p, C.c_int32, f64p]
+    L.prg_pagerank_weighted.restype = C.c_int32
+    L.prg_pagerank_weighted.argtypes = [C.c_uint32, C.c_uint64, u32p, u32p, C.c_int32, f64p, C.c_uint64, f64p]
+    L.prg_personalized_pagerank.restype = C.c_int32
+    L.prg_personalized_pagerank.argtypes = [C.c_uint32, C.c_uint64, u32p, u32p, C.c_int32, f64p, C.c_uint64,
+                                            C.c_double, f64p]
+    L.prg_personalized_pagerank_vs.restype = C.c_int32
+    L.prg_personalized_pagerank_vs.argtypes = [C.c_uint32, C.c_uint64, u32p, u32p, C.c_int32, u32p, C.c_uint64,
+                                               C.c_double, f64p]
+    L.prg_graph_create.restype = C.c_int32
+    L.prg_graph_create.argtypes = [C.c_uint32, C.c_uint64, u32p, u32p, f64p, C.c_int32, C.POINTER(C.c_void_p)]
+    L.prg_graph_create_device.restype = C.c_int32
+    L.prg_graph_create_device.argtypes = [C.c_uint32, C.c_uint64, vp, vp, vp, C.c_int32, C.POINTER(C.c_void_p)]
+    L.prg_graph_destroy.restype = None
+    L.prg_graph_destroy.argtypes = [vp]
+    L.prg_graph_info.restype = C.c_int32
+    L.prg_graph_info.argtypes = [vp, C.POINTER(C.c_uint32), C.POINTER(C.c_uint64), C.POINTER(C.c_uint32),
+                                 C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.POINTER(C.c_double)]
+    L.prg_graph_stream.restype = C.c_void_p
+    L.prg_graph_stream.argtypes = [vp]
+    L.prg_solve.restype = C.c_int32
+    L.prg_solve.argtypes = [vp, C.POINTER(prg_options), f64p, f64p, C.POINTER(prg_stats)]
+    L.prg_solve_device.restype = C.c_int32
+    L.prg_solve_device.argtypes = [vp, C.POINTER(prg_options), vp, vp, C.POINTER(prg_stats)]
+    L.prg_rmat_device.restype = C.c_int32
+    L.prg_rmat_device.argtypes = [C.c_uint32, C.c_uint64, C.c_double, C.c_double, C.c_double, C.c_uint64,
+                                  vp, vp, vp]
+    _lib = L
+    return L
+
+
+def _check(rc: int) -> None:
+    if rc != PRG_OK:
+        msg = lib().prg_last_error().decode("utf-8", "replace")
+        raise _ERRORS.get(rc, Internal)(msg)
+
+
+def _ptr(a: Optional[np.ndarray]):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+# ------------------------------------------------------------------ Graph mirror
+
+
+class Graph:
+    """The edge-list view of rust-igraph's Graph that crosses the boundary."""
+
+    def __init__(self, n: int = 0, directed: bool = False):
+        self._n = int(n)
+        self._directed = bool(directed)
+        self._from: list[int] = []
+        self._to: list[int] = []
+        self._arr = None
+
+    # constructors (graph.rs:170, :518)
+    @classmethod
+    def new(cls, n: int, directed: bool) -> "Graph":
+        return cls(n, directed)
+
+    @classmethod
+    def with_vertices(cls, n: int) -> "Graph":
+        return cls(n, False)
+
+    @classmethod
+    def from_edge_arrays(cls, n: int, frm, to, directed: bool) -> "Graph":
+        """Bulk constructor equivalent to ``new(n, directed)`` + ``add_edges``."""
+        g = cls(n, directed)
+        f = np.ascontiguousarray(frm, dtype=np.uint32)
+        t = np.ascontiguousarray(to, dtype=np.uint32)
+        if f.shape != t.shape:
+            raise InvalidArgument("from/to length mismatch")
+        if len(f) and max(int(f.max()), int(t.max())) >= n:
+            raise VertexOutOfRange(f"vertex out of range (vcount = {n})")
+        if not directed:
+            lo, hi = np.minimum(f, t), np.maximum(f, t)
+            f, t = lo, hi
+        g._arr = (f, t)
+        return g
+
+    def _materialise(self):
+        if self._arr is None:
+            self._arr = (np.asarray(self._from, dtype=np.uint32), np.asarray(self._to, dtype=np.uint32))
+        return self._arr
+
+    def add_edge(self, u: int, v: int) -> None:
+        self.add_edges([(u, v)])
+
+    def add_edges(self, edges: Iterable[Sequence[int]]) -> None:
+        if self._arr is not None:
+            f, t = self._arr
+            self._from, self._to = f.tolist(), t.tolist()
+            self._arr = None
+        new = []
+        for u, v in edges:
+            if not (0 <= u < self._n):
+                raise VertexOutOfRange(f"vertex {u} out of range (vcount = {self._n})")
+            if not (0 <= v < self._n):
+                raise VertexOutOfRange(f"vertex {v} out of range (vcount = {self._n})")
+            new.append((v, u) if (not self._directed and u > v) else (u, v))
+        for u, v in new:
+            self._from.append(u)
+            self._to.append(v)
+
+    def vcount(self) -> int:
+        return self._n
+
+    def ecount(self) -> int:
+        return len(self._materialise()[0]) if self._arr is not None else len(self._from)
+
+    def is_directed(self) -> bool:
+        return self._directed
+
+    def edge(self, e: int):
+        f, t = self._materialise()
+        return int(f[e]), int(t[e])
+
+    def edge_arrays(self):
+        return self._materialise()
+
+
+# ------------------------------------------------------------------ drop-ins
+
+
+def pagerank(graph: Graph) -> np.ndarray:
+    """rust-igraph ``pagerank(&Graph)`` (pagerank.rs:52-143) on the GPU."""
+    n = graph.vcount()
+    f, t = graph.edge_arrays()
+    out = np.empty(max(n, 1), np.float64)
+    _check(lib().prg_pagerank(n, len(f), _ptr(f), _ptr(t), int(graph.is_directed()), _ptr(out)))
+    return out[:n]
+
+
+def pagerank_weighted(graph: Graph, weights) -> np.ndarray:
+    """rust-igraph ``pagerank_weighted(&Graph, &[f64])`` (pagerank_weighted.rs:52-161)."""
+    n = graph.vcount()
+    f, t = graph.edge_arrays()
+    w = np.ascontiguousarray(weights, dtype=np.float64)
+    out = np.empty(max(n, 1), np.float64)
+    wp = _ptr(w) if len(w) else None
+    _check(lib().prg_pagerank_weighted(n, len(f), _ptr(f), _ptr(t), int(graph.is_directed()), wp, len(w),
+                                       _ptr(out)))
+    return out[:n]
+
+
+def personalized_pagerank(graph: Graph, reset, damping: float) -> np.ndarray:
+    """rust-igraph ``personalized_pagerank`` (personalized_pagerank.rs:65-182)."""
+    n = graph.vcount()
+    f, t = graph.edge_arrays()
+    r = np.ascontiguousarray(reset, dtype=np.float64)
+    out = np.empty(max(n, 1), np.float64)
+    rp = _ptr(r) if len(r) else None
+    _check(lib().prg_personalized_pagerank(n, len(f), _ptr(f), _ptr(t), int(graph.is_directed()), rp, len(r),
+                                           float(damping), _ptr(out)))
+    return out[:n]
+
+
+def personalized_pagerank_default(graph: Graph, reset) -> np.ndarray:
+    """rust-igraph ``personalized_pagerank_default`` (personalized_pagerank.rs:206-208)."""
+    return personalized_pagerank(graph, reset, 0.85)
+
+
+def personalized_pagerank_vs(graph: Graph, reset_vids, damping: float) -> np.ndarray:
+    """rust-igraph ``personalized_pagerank_vs`` (personalized_pagerank.rs:241-268)."""
+    n = graph.vcount()
+    f, t = graph.edge_arrays()
+    v = np.ascontiguousarray(reset_vids, dtype=np.uint32)
+    out = np.empty(max(n, 1), np.float64)
+    vp = _ptr(v) if len(v) else None
+    _check(lib().prg_personalized_pagerank_vs(n, len(f), _ptr(f), _ptr(t), int(graph.is_directed()), vp, len(v),
+                                              float(damping), _ptr(out)))
+    return out[:n]
+
+
+# ------------------------------------------------------------------ resident graphs
+
+PRECISION_FP64 = 0
+PRECISION_FP32_REFINED = 1
+STOP_SUCCESSIVE = 0
+STOP_ERROR_BOUND = 1
+
+
+@dataclass
+class Options:
+    damping: float = 0.85
+    eps: float = 1e-10
+    max_iter: int = 1000
+    precision: int = PRECISION_FP64
+    stop: int = STOP_SUCCESSIVE
+    normalise: bool = True
+
+    def to_c(self, start_ptr=None) -> prg_options:
+        o = prg_options()
+        o.damping, o.eps, o.max_iter = self.damping, self.eps, self.max_iter
+        o.precision, o.stop, o.normalise = self.precision, self.stop, int(self.normalise)
+        o.start = start_ptr
+        return o
+
+
+@dataclass
+class Stats:
+    iterations: int
+    fp64_passes: int
+    fp32_passes: int
+    residual_passes: int
+    last_diff: float
+    residual_l1: float
+    error_bound: float
+    solve_ms: float
+    build_ms: float
+    arcs: int
+    n_dangling: int
+
+    @classmethod
+    def from_c(cls, s: prg_stats) -> "Stats":
+        return cls(s.iterations, s.fp64_passes, s.fp32_passes, s.residual_passes, s.last_diff, s.residual_l1,
+                   s.error_bound, s.solve_ms, s.build_ms, s.arcs, s.n_dangling)
+
+
+class DeviceGraph:
+    """A graph resident in HBM (prg_graph handle)."""
+
+    def __init__(self, handle):
+        self._h = handle
+        n, arcs, nd, nrb, nhub, bms = C.c_uint32(), C.c_uint64(), C.c_uint32(), C.c_uint32(), C.c_uint32(), \
+            C.c_double()
+        _check(lib().prg_graph_info(self._h, C.byref(n), C.byref(arcs), C.byref(nd), C.byref(nrb), C.byref(nhub),
+                                    C.byref(bms)))
+        self.n, self.arcs, self.n_dangling = n.value, arcs.value, nd.value
+        self.n_rowblocks, self.n_hubs, self.build_ms = nrb.value, nhub.value, bms.value
+
+    @classmethod
+    def from_host(cls, n: int, frm, to, directed: bool, weights=None) -> "DeviceGraph":
+        f = np.ascontiguousarray(frm, dtype=np.uint32)
+        t = np.ascontiguousarray(to, dtype=np.uint32)
+        w = None if weights is None else np.ascontiguousarray(weights, dtype=np.float64)
+        h = C.c_void_p()
+        _check(lib().prg_graph_create(n, len(f), _ptr(f), _ptr(t), _ptr(w), int(directed), C.byref(h)))
+        return cls(h)
+
+    @classmethod
+    def from_graph(cls, g: Graph, weights=None) -> "DeviceGraph":
+        f, t = g.edge_arrays()
+        return cls.from_host(g.vcount(), f, t, g.is_directed(), weights)
+
+    @classmethod
+    def from_device(cls, n: int, m: int, d_from: int, d_to: int, directed: bool, d_weights: int = 0):
+        h = C.c_void_p()
+        _check(lib().prg_graph_create_device(n, m, C.c_void_p(d_from), C.c_void_p(d_to),
+                                             C.c_void_p(d_weights) if d_weights else None, int(directed),
+                                             C.byref(h)))
+        return cls(h)
+
+    @property
+    def handle(self):
+        return self._h
+
+    def stream(self) -> int:
+        return lib().prg_graph_stream(self._h) or 0
+
+    def solve(self, options: Optional[Options] = None, reset=None, start=None):
+        """Host solve: returns (x float64[n], Stats)."""
+        o = options or Options()
+        st = prg_stats()
+        out = np.empty(max(self.n, 1), np.float64)
+        r = None if reset is None else np.ascontiguousarray(reset, dtype=np.float64)
+        s0 = None if start is None else np.ascontiguousarray(start, dtype=np.float64)
+        co = o.to_c(_ptr(s0))
+        _check(lib().prg_solve(self._h, C.byref(co), _ptr(r), _ptr(out), C.byref(st)))
+        return out[: self.n], Stats.from_c(st)
+
+    def solve_device(self, d_out: int, options: Optional[Options] = None, d_reset: int = 0, d_start: int = 0):
+        """Device solve into a device pointer (e.g. a torch tensor's data_ptr())."""
+        o = options or Options()
+        st = prg_stats()
+        co = o.to_c(C.c_void_p(d_start) if d_start else None)
+        _check(lib().prg_solve_device(self._h, C.byref(co), C.c_void_p(d_reset) if d_reset else None,
+                                      C.c_void_p(d_out), C.byref(st)))
+        return Stats.from_c(st)
+
+    def close(self):
+        if self._h:
+            lib().prg_graph_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+
+def rmat_device(scale: int, m: int, d_from: int, d_to: int, a=0.57, b=0.19, c=0.19, seed=1, stream: int = 0):
+    """Counter-based R-MAT edge list written straight into device arrays."""
+    _check(lib().prg_rmat_device(scale, m, a, b, c, seed, C.c_void_p(d_from), C.c_void_p(d_to),
+                                 C.c_void_p(stream) if stream else None))
