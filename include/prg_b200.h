@@ -82,7 +82,9 @@ typedef struct prg_stats {
     double build_ms;           /* device time of the graph build */
     uint64_t arcs;
     uint32_t n_dangling;
-    uint32_t pad;
+    uint32_t kernel_launches;  /* CUDA kernels this solve launched (graph nodes included) */
+    double fp32_ms;            /* device time of the FP32 iteration graphs (CUDA events) */
+    double fp64_ms;            /* device time of the FP64 iteration graphs / residual passes */
 } prg_stats;
 
 /* Fills the reference defaults: d = 0.85, eps = 1e-10, max_iter = 1000,
@@ -132,6 +134,16 @@ int32_t prg_solve(prg_graph *g, const prg_options *opt, const double *reset, dou
 /* Same with device pointers: d_reset (already normalised, or NULL) and d_out. */
 int32_t prg_solve_device(prg_graph *g, const prg_options *opt, const double *d_reset, double *d_out,
                          prg_stats *stats);
+
+/* 1 if the graph uses degree-sorted internal vertex ids (results are always
+ * returned in the caller's ids), else 0. */
+int32_t prg_graph_relabelled(const prg_graph *g);
+
+/* Process-wide tuning applied to graphs created afterwards (the autotuner's
+ * knobs): "capw", "shortmax", "split" (row-block shape), "blocks_per_sm"
+ * (persistent grid, 0 = occupancy maximum), "relabel" (0 off, 1 on, 2 auto on
+ * skewed degree distributions), "unroll" (iteration pairs per CUDA graph). */
+int32_t prg_set_tuning(const char *key, int64_t value);
 
 /* Message of the last error on this thread ("" if none). */
 const char *prg_last_error(void);

@@ -111,11 +111,21 @@ int32_t create_from_device(uint32_t n, uint64_t m, const uint32_t *d_from, const
     const uint64_t arcs = directed ? m : 2 * m;
     if (arcs + prg::kColPad >= 0xFFFFFFFFull)
         return fail(PRG_ERR_INTERNAL, "arc count exceeds the u32 CSR index range");
+    if (n >= prg::kChunkFlag) return fail(PRG_ERR_INTERNAL, "vertex count exceeds 2^31 - 1");
     prg_graph *h = new prg_graph();
     h->stream = s;
     h->g.n = n;
     h->g.m = m;
     h->g.directed = directed != 0;
+    {
+        const prg::Tuning &t = prg::tuning();
+        h->g.capw = t.capw;
+        h->g.shortmax = t.shortmax;
+        h->g.split = t.split;
+        h->g.blocks_per_sm = t.blocks_per_sm;
+        h->g.relabel = t.relabel;
+        h->ws.unroll = t.unroll;
+    }
     PRG_CUDA(cudaGetDevice(&h->g.device));
     if (m > 0) {
         uint32_t *d_mx = nullptr, mx = 0;
@@ -186,6 +196,8 @@ void destroy(prg_graph *h) {
     f(h->g.inv32);
     f(h->g.rb);
     f(h->g.hubs);
+    f(h->g.perm);
+    f(h->g.iperm);
     f(h->d_reset);
     f(h->d_out);
     f(h->d_start);
@@ -221,6 +233,9 @@ void fill_stats(prg_stats *st, const prg::SolveStats &s, const prg_graph *h) {
     st->build_ms = h->g.build_ms;
     st->arcs = h->g.arcs;
     st->n_dangling = h->g.n_dangling;
+    st->kernel_launches = s.kernel_launches;
+    st->fp32_ms = s.fp32_ms;
+    st->fp64_ms = s.fp64_ms;
 }
 
 // Host-side solve: stages the (already normalised) reset and start vectors,
@@ -446,6 +461,8 @@ void prg_graph_destroy(prg_graph *g) {
     }
 }
 
+int32_t prg_graph_relabelled(const prg_graph *h) { return h && h->g.perm ? 1 : 0; }
+
 int32_t prg_graph_info(const prg_graph *h, uint32_t *n, uint64_t *arcs, uint32_t *n_dangling, uint32_t *nrb,
                        uint32_t *nhub, double *build_ms) {
     if (!h) return fail(PRG_ERR_INVALID_ARGUMENT, "null graph handle");
@@ -515,6 +532,28 @@ int32_t prg_solve_device(prg_graph *h, const prg_options *opt, const double *d_r
     fill_stats(st, ss, h);
     return PRG_OK;
     PRG_GUARD_END
+}
+
+int32_t prg_set_tuning(const char *key, int64_t value) {
+    g_err.clear();
+    if (!key) return fail(PRG_ERR_INVALID_ARGUMENT, "null tuning key");
+    prg::Tuning &t = prg::tuning();
+    const std::string k(key);
+    if (value < 0) return fail(PRG_ERR_INVALID_ARGUMENT, "tuning value must be >= 0");
+    if (k == "capw") t.capw = (uint32_t)value;
+    else if (k == "shortmax") t.shortmax = (uint32_t)value;
+    else if (k == "split") t.split = (uint32_t)value;
+    else if (k == "blocks_per_sm") t.blocks_per_sm = (uint32_t)value;
+    else if (k == "relabel") {
+        if (value > 2) return fail(PRG_ERR_INVALID_ARGUMENT, "relabel must be 0, 1 or 2");
+        t.relabel = (int)value;
+    } else if (k == "unroll") {
+        if (value < 1 || value > 64) return fail(PRG_ERR_INVALID_ARGUMENT, "unroll must be in 1..=64");
+        t.unroll = (int)value;
+    } else {
+        return fail(PRG_ERR_INVALID_ARGUMENT, "unknown tuning key: " + k);
+    }
+    return PRG_OK;
 }
 
 int32_t prg_rmat_device(uint32_t scale, uint64_t m, double a, double b, double c, uint64_t seed, uint32_t *d_from,

@@ -256,6 +256,58 @@ void radix_sort_pairs(uint32_t **keys, uint32_t **vals, uint32_t **keys_alt, uin
 
 // ------------------------------------------------------------------ CSR
 
+Tuning &tuning() {
+    static Tuning t;
+    return t;
+}
+
+__global__ void gather_f64_kernel(double *dst, const double *src, const uint32_t *idx, uint32_t n) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) dst[i] = src[idx[i]];
+}
+
+void gather_f64(double *dst, const double *src, const uint32_t *idx, uint32_t n, cudaStream_t s) {
+    gather_f64_kernel<<<grid_for(n, kThreads), kThreads, 0, s>>>(dst, src, idx, n);
+    PRG_CUDA(cudaGetLastError());
+}
+
+// ---- degree-sorted relabelling.  On skewed (power-law) graphs the vertices
+// that are gathered most often are those with the largest out-degree; giving
+// them the smallest internal ids packs the hot part of the rank vector into a
+// few cache lines (L1/L2 hits instead of one sector per arc).  The order is
+// out-degree descending, ties by caller id (stable sort).
+
+__global__ void max_u32_kernel(const uint32_t *a, uint32_t n, uint32_t *out) {
+    uint32_t mx = 0;
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) mx = max(mx, a[v]);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(out, mx);
+}
+
+__global__ void relabel_keys(const uint32_t *deg, uint32_t n, uint32_t maxdeg, uint32_t *key, uint32_t *val) {
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+        key[v] = maxdeg - deg[v];
+        val[v] = v;
+    }
+}
+
+__global__ void relabel_finish(const uint32_t *perm, const uint32_t *deg_old, uint32_t n, uint32_t *iperm,
+                               uint32_t *deg_new) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t o = perm[i];
+        iperm[o] = i;
+        deg_new[i] = deg_old[o];
+    }
+}
+
+__global__ void relabel_edges(const uint32_t *from, const uint32_t *to, uint64_t m, const uint32_t *iperm,
+                              uint32_t *rf, uint32_t *rt) {
+    for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e < m; e += (uint64_t)gridDim.x * blockDim.x) {
+        rf[e] = iperm[from[e]];
+        rt[e] = iperm[to[e]];
+    }
+}
+
 // Arc a of the in-CSR before sorting: key = destination row, value = source
 // (unweighted) or arc id (weighted, to fetch the edge weight after the sort).
 __global__ void make_arcs(const uint32_t *from, const uint32_t *to, uint64_t m, bool directed, bool carry_id,
@@ -341,28 +393,31 @@ __global__ void max_degree_kernel(const uint32_t *row_ptr, uint32_t n, uint32_t 
 
 // ------------------------------------------------------------------ row-blocks
 //
-// A row is "short" (deg <= cap), "long" (cap < deg <= split: one block) or a
-// hub (deg > split: ceil(deg/split) chunk blocks whose partial sums are
-// combined by the last chunk to finish).  A run of short rows forms a stream
-// row-block; a new one starts at row r when r % rowcap == 0, when the
-// previous row was not short, or when row r's first arc crosses a multiple of
-// cap.  Every stream block therefore holds <= rowcap rows and < 2*cap arcs.
+// Row-blocks are the work units of one warp of the iteration kernel.  A row
+// is "short" (deg <= shortmax), "long" (shortmax < deg <= split: one warp
+// streams it) or a hub (deg > split: ceil(deg/split) chunk row-blocks whose
+// partial sums are combined by the last chunk to finish).  A run of short
+// rows forms a stream row-block; a new one starts at row r when r is a
+// multiple of 32, when the previous row was not short, or when row r's first
+// arc crosses a multiple of capw.  A stream block therefore holds <= 32 rows
+// (32-row aligned, so its epilogue stores are coalesced) and
+// < capw + shortmax <= kWarpBuf arcs.
 
-__global__ void rb_count(const uint32_t *rp, uint32_t n, uint32_t cap, uint32_t rowcap, uint32_t split,
+__global__ void rb_count(const uint32_t *rp, uint32_t n, uint32_t capw, uint32_t shortmax, uint32_t split,
                          uint32_t *cnt, uint32_t *hubflag) {
     for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
-        uint32_t deg = rp[r + 1] - rp[r];
+        const uint32_t deg = rp[r + 1] - rp[r];
         uint32_t c, h = 0;
         if (deg > split) {
             c = (deg + split - 1) / split;
             h = 1;
-        } else if (deg > cap) {
+        } else if (deg > shortmax) {
             c = 1;
         } else {
-            bool start = (r == 0) || (r % rowcap == 0);
+            bool start = (r % kRowCap == 0);
             if (!start) {
-                uint32_t pdeg = rp[r] - rp[r - 1];
-                start = (pdeg > cap) || (rp[r] / cap != rp[r - 1] / cap);
+                const uint32_t pdeg = rp[r] - rp[r - 1];
+                start = (pdeg > shortmax) || (rp[r] / capw != rp[r - 1] / capw);
             }
             c = start ? 1u : 0u;
         }
@@ -371,48 +426,52 @@ __global__ void rb_count(const uint32_t *rp, uint32_t n, uint32_t cap, uint32_t 
     }
 }
 
-__global__ void rb_fill(const uint32_t *rp, uint32_t n, uint32_t cap, uint32_t split, const uint32_t *off,
+__global__ void rb_fill(const uint32_t *rp, uint32_t n, uint32_t shortmax, uint32_t split, const uint32_t *off,
                         const uint32_t *hoff, uint4 *rb, Hub *hubs) {
     for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
-        uint32_t k = off[r], c = off[r + 1] - k;
+        const uint32_t k = off[r], c = off[r + 1] - k;
         if (c == 0) continue;
-        uint32_t deg = rp[r + 1] - rp[r];
+        const uint32_t p0 = rp[r], p1 = rp[r + 1], deg = p1 - p0;
         if (deg > split) {
-            uint32_t h = hoff[r];
+            const uint32_t h = hoff[r];
             hubs[h] = Hub{r, c, k, 0};
-            for (uint32_t j = 0; j < c; j++) rb[k + j] = make_uint4(r, r + 1, RB_CHUNK | (j << 2), h);
-        } else if (deg > cap) {
-            rb[k] = make_uint4(r, r + 1, RB_LONG, 0);
+            for (uint32_t j = 0; j < c; j++) {
+                const uint32_t lo = p0 + j * split, hi = min(p1, lo + split);
+                rb[k + j] = make_uint4(r, kChunkFlag | h, lo, hi);
+            }
+        } else if (deg > shortmax) {
+            rb[k] = make_uint4(r, r + 1, p0, p1);
         } else {
-            rb[k] = make_uint4(r, 0, RB_STREAM, 0);
+            rb[k] = make_uint4(r, 0, p0, 0);  // end filled by rb_fix
         }
     }
 }
 
-__global__ void rb_fix(uint4 *rb, uint32_t nrb, uint32_t n) {
+__global__ void rb_fix(const uint32_t *rp, uint4 *rb, uint32_t nrb, uint32_t n) {
     for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < nrb; k += gridDim.x * blockDim.x) {
         uint4 d = rb[k];
-        if ((d.z & 3u) == RB_STREAM) {
+        if (d.y == 0u) {  // stream row-block: runs to the next row-block's first row
             d.y = (k + 1 < nrb) ? rb[k + 1].x : n;
+            d.w = rp[d.y];
             rb[k] = d;
         }
     }
 }
 
-void build_row_blocks(DeviceGraph &g, uint32_t cap, uint32_t rowcap, uint32_t split, cudaStream_t s) {
-    // the iteration kernel's shared buffers hold 2*kCap products and kRowCap+1 row offsets
-    cap = std::max<uint32_t>(32u, std::min<uint32_t>(cap, kCap));
-    rowcap = std::max<uint32_t>(1u, std::min<uint32_t>(rowcap, kRowCap));
-    split = std::max<uint32_t>(split, cap);
-    uint32_t n = g.n;
+void build_row_blocks(DeviceGraph &g, uint32_t capw, uint32_t shortmax, uint32_t split, cudaStream_t s) {
+    // a stream row-block holds < capw + shortmax arcs, which must fit the warp buffer
+    shortmax = std::max<uint32_t>(1u, std::min<uint32_t>(shortmax, kWarpBuf / 2));
+    capw = std::max<uint32_t>(32u, std::min<uint32_t>(capw, kWarpBuf - shortmax));
+    split = std::max<uint32_t>(split, std::max<uint32_t>(shortmax, 256u));
+    const uint32_t n = g.n;
     if (g.rb) cudaFreeAsync(g.rb, s);
     if (g.hubs) cudaFreeAsync(g.hubs, s);
     g.rb = nullptr;
     g.hubs = nullptr;
     uint32_t *cnt = dalloc<uint32_t>(n + 1, s), *off = dalloc<uint32_t>(n + 1, s);
     uint32_t *hf = dalloc<uint32_t>(n + 1, s), *hoff = dalloc<uint32_t>(n + 1, s);
-    unsigned gb = grid_for(n, kThreads);
-    rb_count<<<gb, kThreads, 0, s>>>(g.row_ptr, n, cap, rowcap, split, cnt, hf);
+    const unsigned gb = grid_for(n, kThreads);
+    rb_count<<<gb, kThreads, 0, s>>>(g.row_ptr, n, capw, shortmax, split, cnt, hf);
     exclusive_scan_u32(cnt, off, n, s);
     exclusive_scan_u32(hf, hoff, n, s);
     uint32_t hv[2];
@@ -421,18 +480,17 @@ void build_row_blocks(DeviceGraph &g, uint32_t cap, uint32_t rowcap, uint32_t sp
     PRG_CUDA(cudaStreamSynchronize(s));
     g.nrb = hv[0];
     g.nhub = hv[1];
-    g.ngroups = (g.nrb + kGroup - 1) / kGroup;
     g.rb = dalloc<uint4>(g.nrb, s);
     g.hubs = dalloc<Hub>(g.nhub, s);
-    rb_fill<<<gb, kThreads, 0, s>>>(g.row_ptr, n, cap, split, off, hoff, g.rb, g.hubs);
-    rb_fix<<<grid_for(g.nrb, kThreads), kThreads, 0, s>>>(g.rb, g.nrb, n);
+    rb_fill<<<gb, kThreads, 0, s>>>(g.row_ptr, n, shortmax, split, off, hoff, g.rb, g.hubs);
+    rb_fix<<<grid_for(g.nrb, kThreads), kThreads, 0, s>>>(g.row_ptr, g.rb, g.nrb, n);
     PRG_CUDA(cudaGetLastError());
     dfree(cnt, s);
     dfree(off, s);
     dfree(hf, s);
     dfree(hoff, s);
-    g.cap = cap;
-    g.rowcap = rowcap;
+    g.capw = capw;
+    g.shortmax = shortmax;
     g.split = split;
 }
 
@@ -460,10 +518,47 @@ void build_graph(DeviceGraph &g, const uint32_t *d_from, const uint32_t *d_to, c
     PRG_CUDA(cudaMemsetAsync(g.deg, 0, std::max<uint64_t>(n, 1) * 4, s));
     if (m) out_degree_kernel<<<ge, kThreads, 0, s>>>(d_from, d_to, m, directed, g.deg);
 
+    // optional degree-sorted relabelling (internal ids); the edge list the CSR
+    // is built from becomes (ef, et)
+    const uint32_t *ef = d_from, *et = d_to;
+    uint32_t *rf = nullptr, *rt = nullptr;
+    if (n >= 2 && g.relabel != 0) {
+        uint32_t *d_mx = dalloc<uint32_t>(1, s), maxdeg = 0;
+        PRG_CUDA(cudaMemsetAsync(d_mx, 0, 4, s));
+        max_u32_kernel<<<gn, kThreads, 0, s>>>(g.deg, n, d_mx);
+        PRG_CUDA(cudaMemcpyAsync(&maxdeg, d_mx, 4, cudaMemcpyDeviceToHost, s));
+        PRG_CUDA(cudaStreamSynchronize(s));
+        dfree(d_mx, s);
+        const double mean = (double)arcs / (double)n;
+        const bool skewed = n >= 4096 && (double)maxdeg >= 32.0 * (mean > 1.0 ? mean : 1.0);
+        if (g.relabel == 1 || skewed) {
+            uint32_t *pk = dalloc<uint32_t>(n, s), *pv = dalloc<uint32_t>(n, s);
+            uint32_t *pk1 = dalloc<uint32_t>(n, s), *pv1 = dalloc<uint32_t>(n, s);
+            relabel_keys<<<gn, kThreads, 0, s>>>(g.deg, n, maxdeg, pk, pv);
+            radix_sort_pairs(&pk, &pv, &pk1, &pv1, n, bits_for(maxdeg), s);
+            PRG_CUDA(cudaMallocAsync((void **)&g.perm, (uint64_t)n * 4, s));
+            PRG_CUDA(cudaMallocAsync((void **)&g.iperm, (uint64_t)n * 4, s));
+            PRG_CUDA(cudaMemcpyAsync(g.perm, pv, (uint64_t)n * 4, cudaMemcpyDeviceToDevice, s));
+            uint32_t *deg_new = dalloc<uint32_t>(n, s);
+            relabel_finish<<<gn, kThreads, 0, s>>>(g.perm, g.deg, n, g.iperm, deg_new);
+            cudaFreeAsync(g.deg, s);
+            g.deg = deg_new;
+            rf = dalloc<uint32_t>(m, s);
+            rt = dalloc<uint32_t>(m, s);
+            if (m) relabel_edges<<<ge, kThreads, 0, s>>>(d_from, d_to, m, g.iperm, rf, rt);
+            ef = rf;
+            et = rt;
+            dfree(pk, s);
+            dfree(pv, s);
+            dfree(pk1, s);
+            dfree(pv1, s);
+        }
+    }
+
     // arcs in edge order, then stable sort by destination
     uint32_t *k0 = dalloc<uint32_t>(arcs, s), *v0 = dalloc<uint32_t>(arcs, s);
     uint32_t *k1 = dalloc<uint32_t>(arcs, s), *v1 = dalloc<uint32_t>(arcs, s);
-    if (m) make_arcs<<<ge, kThreads, 0, s>>>(d_from, d_to, m, directed, weighted, k0, v0);
+    if (m) make_arcs<<<ge, kThreads, 0, s>>>(ef, et, m, directed, weighted, k0, v0);
 
     // row_ptr from the in-degree histogram
     uint32_t *indeg = dalloc<uint32_t>(n + 1, s);
@@ -486,7 +581,7 @@ void build_graph(DeviceGraph &g, const uint32_t *d_from, const uint32_t *d_to, c
         PRG_CUDA(cudaMallocAsync((void **)&g.w32, padded * 4, s));
         PRG_CUDA(cudaMemsetAsync(g.w64, 0, padded * 8, s));
         PRG_CUDA(cudaMemsetAsync(g.w32, 0, padded * 4, s));
-        if (arcs) gather_arcs<<<ga, kThreads, 0, s>>>(v0, d_from, d_to, d_w, arcs, directed, g.col, g.w64, g.w32);
+        if (arcs) gather_arcs<<<ga, kThreads, 0, s>>>(v0, ef, et, d_w, arcs, directed, g.col, g.w64, g.w32);
         strength = dalloc<double>(n, s);
         if (!directed) {
             // undirected: arcs out of u are exactly the arcs into u (same weights)
@@ -498,8 +593,8 @@ void build_graph(DeviceGraph &g, const uint32_t *d_from, const uint32_t *d_to, c
             uint32_t *sk1 = dalloc<uint32_t>(m, s), *sv1 = dalloc<uint32_t>(m, s);
             uint32_t *optr = dalloc<uint32_t>(n + 1, s), *oh = dalloc<uint32_t>(n + 1, s);
             if (m) {
-                PRG_CUDA(cudaMemcpyAsync(sk, d_from, m * 4, cudaMemcpyDeviceToDevice, s));
-                make_arcs<<<ge, kThreads, 0, s>>>(d_from, d_to, m, true, true, sk1, sv);  // sv = edge ids
+                PRG_CUDA(cudaMemcpyAsync(sk, ef, m * 4, cudaMemcpyDeviceToDevice, s));
+                make_arcs<<<ge, kThreads, 0, s>>>(ef, et, m, true, true, sk1, sv);  // sv = edge ids
             }
             PRG_CUDA(cudaMemsetAsync(oh, 0, (uint64_t)(n + 1) * 4, s));
             if (m) histogram_u32<<<ge, kThreads, 0, s>>>(sk, m, oh);
@@ -518,6 +613,8 @@ void build_graph(DeviceGraph &g, const uint32_t *d_from, const uint32_t *d_to, c
     dfree(v0, s);
     dfree(k1, s);
     dfree(v1, s);
+    dfree(rf, s);
+    dfree(rt, s);
 
     PRG_CUDA(cudaMallocAsync((void **)&g.dval, std::max<uint64_t>(n, 1) * 8, s));
     PRG_CUDA(cudaMallocAsync((void **)&g.inv32, std::max<uint64_t>(n, 1) * 4, s));
@@ -534,7 +631,7 @@ void build_graph(DeviceGraph &g, const uint32_t *d_from, const uint32_t *d_to, c
     g.n_dangling = hnd[0];
     g.max_in_degree = hnd[1];
 
-    build_row_blocks(g, g.cap, g.rowcap, g.split, s);
+    build_row_blocks(g, g.capw, g.shortmax, g.split, s);
     PRG_CUDA(cudaEventRecord(e1, s));
     PRG_CUDA(cudaEventSynchronize(e1));
     PRG_CUDA(cudaEventElapsedTime(&g.build_ms, e0, e1));
@@ -552,6 +649,8 @@ void free_graph(DeviceGraph &g) {
     cudaFree(g.inv32);
     cudaFree(g.rb);
     cudaFree(g.hubs);
+    cudaFree(g.perm);
+    cudaFree(g.iperm);
     g = DeviceGraph{};
 }
 

@@ -24,18 +24,21 @@ struct DeviceGraph {
     double *dval = nullptr;       // n: out-degree / out-strength as double
     float *inv32 = nullptr;       // n: 1/dval in FP32, 0 when dangling
 
-    uint4 *rb = nullptr;          // row-blocks {row_begin, row_end, kind|chunk<<2, hub}
+    uint32_t *perm = nullptr;     // internal id -> caller id (null when not relabelled)
+    uint32_t *iperm = nullptr;    // caller id -> internal id
+    uint4 *rb = nullptr;          // row-blocks {row_begin, row_end | kChunkFlag|hub, arc_begin, arc_end}
     uint32_t nrb = 0;
-    uint32_t ngroups = 0;
     Hub *hubs = nullptr;
     uint32_t nhub = 0;
     uint32_t n_dangling = 0;
     uint32_t max_in_degree = 0;
 
     // row-block tuning used to build `rb` (autotuned or defaults)
-    uint32_t cap = kCap;
-    uint32_t rowcap = kRowCap;
+    uint32_t capw = kCapW;
+    uint32_t shortmax = kShortMax;
     uint32_t split = kSplit;
+    uint32_t blocks_per_sm = 0;  // persistent grid = SMs x this (0 = occupancy maximum)
+    int relabel = 2;             // 0 keep caller ids, 1 degree-sorted ids, 2 decide from the degree skew
 
     float build_ms = 0.f;
 };
@@ -46,8 +49,19 @@ struct DeviceGraph {
 void build_graph(DeviceGraph &g, const uint32_t *d_from, const uint32_t *d_to, const double *d_w,
                  cudaStream_t s);
 // Rebuilds only the row-blocks with new tuning (autotuner).
-void build_row_blocks(DeviceGraph &g, uint32_t cap, uint32_t rowcap, uint32_t split, cudaStream_t s);
+void build_row_blocks(DeviceGraph &g, uint32_t capw, uint32_t shortmax, uint32_t split, cudaStream_t s);
 void free_graph(DeviceGraph &g);
+
+// Process-wide defaults applied to graphs built afterwards (prg_set_tuning).
+struct Tuning {
+    uint32_t capw = kCapW, shortmax = kShortMax, split = kSplit, blocks_per_sm = 0;
+    int relabel = 2;
+    int unroll = 8;
+};
+Tuning &tuning();
+
+// dst[i] = src[idx[i]] for i < n (FP64 vectors).
+void gather_f64(double *dst, const double *src, const uint32_t *idx, uint32_t n, cudaStream_t s);
 
 // Stable LSD radix sort of (key, value) u32 pairs on the low `key_bits` bits.
 // On return *keys / *vals point at the sorted data (buffers may be swapped

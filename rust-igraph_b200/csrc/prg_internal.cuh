@@ -7,7 +7,8 @@
 //   deg      u32[n]        out-degree as rust-igraph counts it (graph.rs:877-900)
 //   dval     f64[n]        out-degree or out-strength as a double (divisor)
 //   inv32    f32[n]        1/dval in FP32 (0 for dangling vertices)
-//   rb       uint4[nrb]    row-blocks: the SpMV work units (see spmv.cu)
+//   rb       uint4[nrb]    row-blocks, the SpMV work units of one warp:
+//                          {row_begin, row_end | 0x80000000|hub, arc_begin, arc_end}
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -17,13 +18,15 @@
 namespace prg {
 
 constexpr int kThreads = 256;         // threads per block for all hot kernels
-constexpr uint32_t kCap = 1024;       // stream row-block arc budget (<= 2*kCap arcs)
-constexpr uint32_t kRowCap = 256;     // max rows per stream row-block
-constexpr uint32_t kSplit = 16384;    // rows longer than this are split into chunks
-constexpr uint32_t kGroup = 256;      // row-blocks per reduction group
+constexpr int kWarps = kThreads / 32;
+constexpr uint32_t kWarpBuf = 512;    // products staged per warp (shared memory)
+constexpr uint32_t kRowCap = 32;      // rows per stream row-block (one lane per row)
+constexpr uint32_t kCapW = 448;       // default stream window: a new row-block starts when a row's
+                                      // first arc crosses a multiple of kCapW
+constexpr uint32_t kShortMax = 64;    // default: rows with more arcs are handled by a whole warp
+constexpr uint32_t kSplit = 8192;     // default: rows with more arcs are split into chunks
 constexpr uint32_t kColPad = 16;      // extra u32 slots after col[] for aligned vector loads
-
-enum RbKind : uint32_t { RB_STREAM = 0, RB_LONG = 1, RB_CHUNK = 2 };
+constexpr uint32_t kChunkFlag = 0x80000000u;
 
 // Per-solve device control block.  Scalars that an iteration reads and the
 // next one writes are double-buffered by launch parity.

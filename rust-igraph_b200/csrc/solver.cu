@@ -46,18 +46,18 @@ void workspace_free(Workspace &ws, cudaStream_t s) {
     wfree(ws.b32, s);
     wfree(ws.t64, s);
     wfree(ws.t32, s);
+    wfree(ws.out_tmp, s);
     wfree(ws.ctl, s);
-    wfree(ws.rb_part, s);
-    wfree(ws.grp_part, s);
+    wfree(ws.blk_part, s);
     wfree(ws.hub_rec, s);
     wfree(ws.chunk_part, s);
-    wfree(ws.grp_ticket, s);
     wfree(ws.hub_ticket, s);
     if (ws.h_ctl) cudaFreeHost(ws.h_ctl);
     ws.h_ctl = nullptr;
-    if (ws.ev0) cudaEventDestroy(ws.ev0);
-    if (ws.ev1) cudaEventDestroy(ws.ev1);
-    ws.ev0 = ws.ev1 = nullptr;
+    for (cudaEvent_t *e : {&ws.ev0, &ws.ev1, &ws.eva, &ws.evb}) {
+        if (*e) cudaEventDestroy(*e);
+        *e = nullptr;
+    }
     ws.ready = false;
 }
 
@@ -66,8 +66,12 @@ void workspace_ensure(Workspace &ws, const DeviceGraph &g, cudaStream_t s) {
     if (ws.ready) workspace_free(ws, s);
     ws.n = g.n;
     ws.nrb = g.nrb;
-    ws.ngroups = g.ngroups;
     ws.nhub = g.nhub;
+    unsigned gmax = kPrepParts;
+    for (int m = 0; m < 4; m++) {
+        ws.grid[m] = iteration_grid(m, g.weighted, g.blocks_per_sm);
+        gmax = std::max(gmax, ws.grid[m]);
+    }
     const uint64_t n = g.n;
     for (int i = 0; i < 2; i++) {
         walloc(ws.x64[i], n, s);
@@ -78,19 +82,19 @@ void workspace_ensure(Workspace &ws, const DeviceGraph &g, cudaStream_t s) {
     walloc(ws.b32, n, s);
     walloc(ws.t64, n, s);
     walloc(ws.t32, n, s);
+    if (g.perm) walloc(ws.out_tmp, n, s);
     walloc(ws.ctl, 1, s);
-    walloc(ws.rb_part, std::max<uint64_t>(g.nrb, kPrepParts), s);
-    walloc(ws.grp_part, g.ngroups, s);
+    walloc(ws.blk_part, gmax, s);
     walloc(ws.hub_rec, g.nhub, s);
     walloc(ws.chunk_part, g.nrb, s);
-    walloc(ws.grp_ticket, g.ngroups, s);
     walloc(ws.hub_ticket, g.nhub, s);
-    PRG_CUDA(cudaMemsetAsync(ws.grp_ticket, 0, std::max<uint64_t>(g.ngroups, 1) * 4, s));
     PRG_CUDA(cudaMemsetAsync(ws.hub_ticket, 0, std::max<uint64_t>(g.nhub, 1) * 4, s));
     PRG_CUDA(cudaMemsetAsync(ws.hub_rec, 0, std::max<uint64_t>(g.nhub, 1) * sizeof(double4), s));
     PRG_CUDA(cudaMallocHost((void **)&ws.h_ctl, sizeof(Ctl)));
     PRG_CUDA(cudaEventCreate(&ws.ev0));
     PRG_CUDA(cudaEventCreate(&ws.ev1));
+    PRG_CUDA(cudaEventCreate(&ws.eva));
+    PRG_CUDA(cudaEventCreate(&ws.evb));
     ws.ready = true;
 }
 
@@ -106,18 +110,14 @@ static IterArgs base_args(const DeviceGraph &g, Workspace &ws, double damping) {
     a.rb = g.rb;
     a.hubs = g.hubs;
     a.nrb = g.nrb;
-    a.ngroups = g.ngroups;
     a.nhub = g.nhub;
     a.n = g.n;
-    a.split = g.split;
     a.damping = damping;
     a.inv_n = 1.0 / (double)g.n;
     a.ctl = ws.ctl;
-    a.rb_part = ws.rb_part;
-    a.grp_part = ws.grp_part;
+    a.blk_part = ws.blk_part;
     a.chunk_part = ws.chunk_part;
     a.hub_rec = ws.hub_rec;
-    a.grp_ticket = ws.grp_ticket;
     a.hub_ticket = ws.hub_ticket;
     return a;
 }
@@ -137,8 +137,8 @@ static cudaGraphExec_t loop_graph(const DeviceGraph &g, Workspace &ws, int mode,
     cudaGraph_t graph;
     PRG_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
     for (int u = 0; u < ws.unroll; u++) {
-        launch_iteration(mode, g.weighted, a0, s);
-        launch_iteration(mode, g.weighted, a1, s);
+        launch_iteration(mode, g.weighted, a0, ws.grid[mode], s);
+        launch_iteration(mode, g.weighted, a1, ws.grid[mode], s);
     }
     PRG_CUDA(cudaStreamEndCapture(s, &graph));
     cudaGraphExec_t exec;
@@ -148,13 +148,22 @@ static cudaGraphExec_t loop_graph(const DeviceGraph &g, Workspace &ws, int mode,
     return exec;
 }
 
-// Launches the loop graph until the kernels raise Ctl::done.
-static void run_loop(Workspace &ws, cudaGraphExec_t exec, uint32_t max_iter, cudaStream_t s) {
+// Launches the loop graph until the kernels raise Ctl::done.  Adds the
+// device time of the graph launches (CUDA events on `s`) to *ms and the
+// kernels they contain to *launches.
+static void run_loop(Workspace &ws, cudaGraphExec_t exec, uint32_t max_iter, cudaStream_t s, double *ms,
+                     uint32_t *launches) {
     const uint64_t max_launches = (uint64_t)max_iter / (2u * ws.unroll) + 2u;
     for (uint64_t k = 0; k < max_launches; k++) {
+        PRG_CUDA(cudaEventRecord(ws.eva, s));
         PRG_CUDA(cudaGraphLaunch(exec, s));
+        PRG_CUDA(cudaEventRecord(ws.evb, s));
         PRG_CUDA(cudaMemcpyAsync(ws.h_ctl, ws.ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, s));
         PRG_CUDA(cudaStreamSynchronize(s));
+        float t = 0.f;
+        PRG_CUDA(cudaEventElapsedTime(&t, ws.eva, ws.evb));
+        *ms += t;
+        *launches += 2u * ws.unroll;
         if (ws.h_ctl->done) return;
     }
 }
@@ -178,7 +187,8 @@ static void solve_fp64(const DeviceGraph &g, Workspace &ws, const SolveOpts &o, 
     c.thr = o.stop == 1 ? o.eps * (1.0 - o.damping) / o.damping : o.eps;
     c.max_iter = o.max_iter;
     PRG_CUDA(cudaMemcpyAsync(ws.ctl, &c, sizeof(Ctl), cudaMemcpyHostToDevice, s));
-    launch_prepare64(g, ws.x64[0], nullptr, ws.xt64[0], ws.ctl, 0, ws.rb_part, s);
+    launch_prepare64(g, ws.x64[0], nullptr, ws.xt64[0], ws.ctl, 0, ws.blk_part, s);
+    st.kernel_launches += (o.d_start ? 0u : 1u) + 2u;
     IterArgs a0 = base_args(g, ws, o.damping), a1 = a0;
     a0.t64 = a1.t64 = d_t;
     a0.parity = 0;
@@ -194,7 +204,7 @@ static void solve_fp64(const DeviceGraph &g, Workspace &ws, const SolveOpts &o, 
     const int mode = ppr ? MODE_PPR64 : MODE_PLAIN64;
     if (o.max_iter > 0) {
         cudaGraphExec_t ex = loop_graph(g, ws, mode, ppr, o.damping, a0, a1, s);
-        run_loop(ws, ex, o.max_iter, s);
+        run_loop(ws, ex, o.max_iter, s, &st.fp64_ms, &st.kernel_launches);
     } else {
         read_ctl(ws, s);
     }
@@ -221,7 +231,8 @@ static void solve_refined(const DeviceGraph &g, Workspace &ws, const SolveOpts &
     const uint32_t inner_cap = std::max<uint32_t>(16u, std::min<uint32_t>(o.max_iter, 400u));
     c.max_iter = inner_cap;
     PRG_CUDA(cudaMemcpyAsync(ws.ctl, &c, sizeof(Ctl), cudaMemcpyHostToDevice, s));
-    launch_prepare64(g, ws.x64[0], nullptr, ws.xt64[0], ws.ctl, 1, ws.rb_part, s);
+    launch_prepare64(g, ws.x64[0], nullptr, ws.xt64[0], ws.ctl, 1, ws.blk_part, s);
+    st.kernel_launches += (o.d_start ? 0u : 1u) + (ppr ? 1u : 0u) + 2u;
 
     IterArgs r = base_args(g, ws, o.damping);
     r.t64 = d_t;
@@ -251,21 +262,31 @@ static void solve_refined(const DeviceGraph &g, Workspace &ws, const SolveOpts &
     const uint32_t pass_cap = std::max<uint32_t>(o.max_iter, 64u);
     uint32_t fp32 = 0, fp64 = 0;
     for (int outer = 0; outer < 64; outer++) {
-        launch_iteration(MODE_RESID64, g.weighted, r, s);
+        PRG_CUDA(cudaEventRecord(ws.eva, s));
+        launch_iteration(MODE_RESID64, g.weighted, r, ws.grid[MODE_RESID64], s);
+        PRG_CUDA(cudaEventRecord(ws.evb, s));
         fp64++;
+        st.kernel_launches += 1u;
         read_ctl(ws, s);
+        {
+            float t = 0.f;
+            PRG_CUDA(cudaEventElapsedTime(&t, ws.eva, ws.evb));
+            st.fp64_ms += t;
+        }
         const double rn = ws.h_ctl->rnorm;
         st.residual_l1 = rn;
         if (!(rn > thr_final) || fp32 + fp64 >= pass_cap) break;
-        run_loop(ws, ex, inner_cap, s);
+        run_loop(ws, ex, inner_cap, s, &st.fp32_ms, &st.kernel_launches);
         fp32 += ws.h_ctl->iters;
         const float *e_fin = ws.h_ctl->parity_last == 0 ? ws.e32[1] : ws.e32[0];
-        launch_prepare64(g, ws.x64[0], e_fin, ws.xt64[0], ws.ctl, 1, ws.rb_part, s);
+        launch_prepare64(g, ws.x64[0], e_fin, ws.xt64[0], ws.ctl, 1, ws.blk_part, s);
+        st.kernel_launches += 2u;
     }
     if (o.normalise) {
         // result = g / sum(g) (FP64), sum taken by the last residual pass
         PRG_CUDA(cudaMemcpyAsync(d_out, ws.x64[1], (uint64_t)g.n * 8, cudaMemcpyDeviceToDevice, s));
         launch_normalise(d_out, g.n, ws.ctl, s);
+        st.kernel_launches += 1u;
     } else {
         PRG_CUDA(cudaMemcpyAsync(d_out, ws.x64[1], (uint64_t)g.n * 8, cudaMemcpyDeviceToDevice, s));
     }
@@ -277,15 +298,40 @@ static void solve_refined(const DeviceGraph &g, Workspace &ws, const SolveOpts &
     st.error_bound = st.residual_l1 * o.damping / (1.0 - o.damping);
 }
 
-void solve(const DeviceGraph &g, Workspace &ws, const SolveOpts &o, const double *d_t, double *d_out,
+void solve(const DeviceGraph &g, Workspace &ws, const SolveOpts &o_in, const double *d_t, double *d_out,
            SolveStats &st, cudaStream_t s) {
+    st = SolveStats{};
     workspace_ensure(ws, g, s);
-    PRG_CUDA(cudaMemsetAsync(ws.grp_ticket, 0, std::max<uint64_t>(g.ngroups, 1) * 4, s));
     PRG_CUDA(cudaMemsetAsync(ws.hub_ticket, 0, std::max<uint64_t>(g.nhub, 1) * 4, s));
     PRG_CUDA(cudaEventRecord(ws.ev0, s));
-    st = SolveStats{};
-    if (o.precision == 1) solve_refined(g, ws, o, d_t, d_out, st, s);
-    else solve_fp64(g, ws, o, d_t, d_out, st, s);
+    // Vectors cross into internal ids here: the teleport vector always lives
+    // in ws.t64 (so captured graphs stay valid), a start vector goes straight
+    // into x64[0], and the result is gathered back to caller ids at the end.
+    SolveOpts o = o_in;
+    const double *t = nullptr;
+    if (d_t) {
+        if (g.perm) {
+            gather_f64(ws.t64, d_t, g.perm, g.n, s);
+            st.kernel_launches += 1u;
+        } else if (d_t != ws.t64) {
+            PRG_CUDA(cudaMemcpyAsync(ws.t64, d_t, (uint64_t)g.n * 8, cudaMemcpyDeviceToDevice, s));
+        }
+        t = ws.t64;
+    }
+    if (o.d_start) {
+        if (g.perm) {
+            gather_f64(ws.x64[1], o.d_start, g.perm, g.n, s);
+            st.kernel_launches += 1u;
+            o.d_start = ws.x64[1];
+        }
+    }
+    double *out = g.perm ? ws.out_tmp : d_out;
+    if (o.precision == 1) solve_refined(g, ws, o, t, out, st, s);
+    else solve_fp64(g, ws, o, t, out, st, s);
+    if (g.perm) {
+        gather_f64(d_out, ws.out_tmp, g.iperm, g.n, s);
+        st.kernel_launches += 1u;
+    }
     PRG_CUDA(cudaEventRecord(ws.ev1, s));
     PRG_CUDA(cudaEventSynchronize(ws.ev1));
     float ms = 0.f;

@@ -23,12 +23,15 @@ struct SolveOpts {
 struct SolveStats {
     uint32_t iterations = 0, fp64_passes = 0, fp32_passes = 0, residual_passes = 0;
     double last_diff = 0, residual_l1 = 0, error_bound = 0, solve_ms = 0;
+    uint32_t kernel_launches = 0;
+    double fp32_ms = 0, fp64_ms = 0;
 };
 
 // Reusable per-handle solve buffers and captured CUDA graphs.
 struct Workspace {
     bool ready = false;
-    uint32_t n = 0, nrb = 0, ngroups = 0, nhub = 0;
+    uint32_t n = 0, nrb = 0, nhub = 0;
+    unsigned grid[4] = {0, 0, 0, 0};  // persistent grid per iteration mode
     double *x64[2] = {nullptr, nullptr};
     double *xt64[2] = {nullptr, nullptr};
     float *e32[2] = {nullptr, nullptr};
@@ -36,15 +39,14 @@ struct Workspace {
     float *b32 = nullptr;
     double *t64 = nullptr;
     float *t32 = nullptr;
+    double *out_tmp = nullptr;  // result in internal ids before un-permuting
     Ctl *ctl = nullptr;
     Ctl *h_ctl = nullptr;  // pinned mirror
-    double4 *rb_part = nullptr;
-    double4 *grp_part = nullptr;
+    double4 *blk_part = nullptr;   // per-block records (iteration and prepare kernels)
     double4 *hub_rec = nullptr;
     double *chunk_part = nullptr;
-    uint32_t *grp_ticket = nullptr;
     uint32_t *hub_ticket = nullptr;
-    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr, eva = nullptr, evb = nullptr;
     std::map<uint64_t, cudaGraphExec_t> graphs;
     int unroll = 8;  // iteration pairs per graph launch
 };

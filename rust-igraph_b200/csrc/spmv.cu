@@ -1,24 +1,27 @@
-// spmv.cu — the fused PageRank iteration: one kernel per power step.
+// spmv.cu — the fused PageRank iteration: one kernel launch per power step.
 //
-// Work unit: a row-block (csr_build.cu) of the pull CSR.  One CUDA block of
-// 256 threads handles one row-block:
-//   stream  — a run of short rows: the block streams the rows' contiguous arc
-//             range with 16-byte evict-first index loads, gathers the scaled
-//             rank vector xt = x / outdeg through the read-only path
-//             (evict-last in L2), stages the products in shared memory and
-//             reduces each row with a power-of-two thread group;
-//   long    — one row with cap < deg <= split: whole block, strided, tree sum;
-//   chunk   — a slice of a hub row (deg > split); slices write partial sums
-//             and the last slice to finish (atomic ticket) combines them in
-//             slice order and finishes the row.
-// The epilogue of every row is fused: teleport + dangling share + damping,
-// the row's L1 change |x'[v]-x[v]|, the next dangling mass and the next
-// scaled vector xt'[v] = x'[v] / outdeg[v].  Per-row-block partial sums are
-// reduced in two fixed-order levels (groups of 256 row-blocks, then groups);
-// the last group's block writes the iteration's scalars into Ctl and raises
-// `done` when the stop rule holds, so later launches in the same CUDA graph
-// return immediately.  No floating-point atomics: results are
-// bit-reproducible run to run.
+// Persistent grid (SMs x resident blocks) of 256-thread blocks; every warp
+// walks the row-block list (csr_build.cu) with a static round-robin stride,
+// prefetching its next descriptor.  Per row-block:
+//   stream — <= 32 consecutive short rows with < kWarpBuf arcs: the warp
+//            streams the contiguous arc range with 16-byte evict-first index
+//            loads, gathers the scaled rank vector xt = x / outdeg through the
+//            read-only path (evict-last in L2), stages the products in its
+//            shared-memory buffer, then lane i sums row r0+i and runs its
+//            epilogue (32 consecutive rows -> coalesced stores);
+//   long   — one row: warp-strided accumulation, shuffle reduction;
+//   chunk  — a slice of a hub row: the slice sum goes to chunk_part, and the
+//            last slice to finish (atomic ticket) adds the slices in order
+//            and runs the row's epilogue.
+// The epilogue is fused: teleport + dangling share + damping, the row's L1
+// change |x'[v]-x[v]|, the next dangling mass and the next scaled vector
+// xt'[v] = x'[v] / outdeg[v].  Lanes accumulate (diff, dangling, sum) in
+// FP64 registers; blocks reduce them with a fixed tree, and the last block to
+// finish (atomic ticket) adds the block records and hub records in index
+// order, writes the iteration's scalars into Ctl and raises `done` when the
+// stop rule holds, so later launches in the same CUDA graph return at once.
+// The schedule is static and no floating-point atomics are used, so results
+// are bit-reproducible run to run on a given GPU model.
 //
 // Semantics mirror rust-igraph's loop body (pagerank.rs:107-140,
 // pagerank_weighted.rs:129-159, personalized_pagerank.rs:149-182).
@@ -43,7 +46,7 @@ __device__ __forceinline__ void block_sum3(double &a, double &b, double &c, doub
     a = warp_sum(a);
     b = warp_sum(b);
     c = warp_sum(c);
-    int w = threadIdx.x >> 5, l = threadIdx.x & 31, nw = blockDim.x >> 5;
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31, nw = blockDim.x >> 5;
     __syncthreads();
     if (l == 0) {
         sh[w] = a;
@@ -61,21 +64,6 @@ __device__ __forceinline__ void block_sum3(double &a, double &b, double &c, doub
     }
 }
 
-template <class A>
-__device__ __forceinline__ A block_sum_t(A v, A *sh) {
-    v = warp_sum(v);
-    int w = threadIdx.x >> 5, l = threadIdx.x & 31, nw = blockDim.x >> 5;
-    __syncthreads();
-    if (l == 0) sh[w] = v;
-    __syncthreads();
-    A r = A(0);
-    if (w == 0) {
-        r = l < nw ? sh[l] : A(0);
-        r = warp_sum(r);
-    }
-    return r;
-}
-
 __device__ __forceinline__ double4 ldcg4(const double4 *p) {
     const double2 a = __ldcg(reinterpret_cast<const double2 *>(p));
     const double2 b = __ldcg(reinterpret_cast<const double2 *>(p) + 1);
@@ -87,48 +75,68 @@ struct Uni {
     double d, dsum, tele, dshare;
 };
 
+// Epilogue operands of one row, loaded before the row's gathers so their
+// latency overlaps them.
+struct Pre {
+    double old, dv, t;
+    float iv, b;
+};
+
+template <int MODE>
+__device__ __forceinline__ Pre epi_load(const IterArgs &a, uint32_t v) {
+    Pre p;
+    if constexpr (MODE == MODE_CORR32) {
+        p.old = a.x32_in[v];
+        p.b = a.b32[v];
+        p.iv = a.inv32[v];
+        p.t = a.t32 ? (double)a.t32[v] : a.inv_n;
+        p.dv = 0.0;
+    } else {
+        p.old = a.x64_in[v];
+        p.dv = a.dval[v];
+        p.t = a.t64 ? a.t64[v] : 0.0;
+        p.iv = (MODE == MODE_RESID64) ? a.inv32[v] : 0.0f;
+        p.b = 0.0f;
+    }
+    return p;
+}
+
 template <int MODE>
 __device__ __forceinline__ void epilogue(const IterArgs &a, const Uni &u, uint32_t v, typename ModeT<MODE>::A y,
-                                         double &pd, double &pds, double &ps) {
+                                         const Pre &p, double &pd, double &pds, double &ps) {
     if constexpr (MODE == MODE_CORR32) {
         const float df = (float)u.d;
-        const float t = a.t32 ? a.t32[v] : (float)a.inv_n;
-        const float out = df * y + ((float)(u.d * u.dsum)) * t + a.b32[v];
-        const float old = a.x32_in[v];
+        const float out = df * y + ((float)(u.d * u.dsum)) * (float)p.t + p.b;
         a.x32_out[v] = out;
-        pd += fabs((double)out - (double)old);
-        const float iv = a.inv32[v];
-        a.xt32_out[v] = out * iv;
-        if (iv == 0.0f) pds += (double)out;
+        pd += fabs((double)out - p.old);
+        a.xt32_out[v] = out * p.iv;
+        if (p.iv == 0.0f) pds += (double)out;
     } else {
         double out;
         if (a.t64) {
             // personalized_pagerank.rs:169-170
-            const double t = a.t64[v];
-            out = __dadd_rn(__dmul_rn(1.0 - u.d, t), __dmul_rn(u.d, __dadd_rn(y, __dmul_rn(u.dsum, t))));
+            out = __dadd_rn(__dmul_rn(1.0 - u.d, p.t), __dmul_rn(u.d, __dadd_rn(y, __dmul_rn(u.dsum, p.t))));
         } else {
             // pagerank.rs:129: teleport + dangling_share + d * incoming
             out = __dadd_rn(__dadd_rn(u.tele, u.dshare), __dmul_rn(u.d, y));
         }
-        const double old = a.x64_in[v];
-        const double dv = a.dval[v];
         a.x64_out[v] = out;
         if constexpr (MODE == MODE_RESID64) {
-            const double r = out - old;
+            const double r = out - p.old;
             pd += fabs(r);
             ps += out;
             const float r32 = (float)r;
             a.b32_out[v] = r32;
             a.x32_out[v] = r32;  // the correction iteration starts from e0 = r
-            a.xt32_out[v] = r32 * a.inv32[v];
-            if (dv == 0.0) pds += (double)r32;
+            a.xt32_out[v] = r32 * p.iv;
+            if (p.dv == 0.0) pds += (double)r32;
         } else {
-            pd += fabs(out - old);
-            if (dv == 0.0) {
+            pd += fabs(out - p.old);
+            if (p.dv == 0.0) {
                 pds += out;
                 a.xt64_out[v] = 0.0;
             } else {
-                a.xt64_out[v] = out / dv;  // the reference's pr[u] / out_deg(u)
+                a.xt64_out[v] = out / p.dv;  // the reference's pr[u] / out_deg(u)
             }
         }
     }
@@ -140,67 +148,101 @@ __device__ __forceinline__ const typename ModeT<MODE>::A *gather_src(const IterA
     else return a.xt64_in;
 }
 
-// Accumulates (or stores) w * xt[col] for arcs [p_lo, p_hi) using aligned
-// 16-byte index loads.  STORE: s_prod[p - p_lo] = product; else acc += product.
-template <int MODE, bool W, bool STORE>
-__device__ __forceinline__ void arc_products(const IterArgs &a, uint32_t p_lo, uint32_t p_hi,
-                                             typename ModeT<MODE>::A *s_prod, typename ModeT<MODE>::A &acc) {
+// Products w * xt[col] of the 4 arcs at aligned position `base`; lanes outside
+// [lo, hi) get 0 and issue no gather.
+template <int MODE, bool W>
+__device__ __forceinline__ void quad(const IterArgs &a, uint32_t base, uint32_t lo, uint32_t hi, uint64_t pol_s,
+                                     uint64_t pol_g, typename ModeT<MODE>::A (&out)[4]) {
     using A = typename ModeT<MODE>::A;
     const A *xt = gather_src<MODE>(a);
-    const uint32_t a0 = p_lo & ~3u;
-    const uint32_t nvec = (p_hi - a0 + 3u) >> 2;
-    const uint64_t pol_s = policy_evict_first(), pol_g = policy_evict_last();
-    for (uint32_t vi = threadIdx.x; vi < nvec; vi += blockDim.x) {
-        const uint32_t base = a0 + 4u * vi;
-        const uint4 c = ld_stream_u4(reinterpret_cast<const uint4 *>(a.col + base), pol_s);
-        const uint32_t cc[4] = {c.x, c.y, c.z, c.w};
-        A wv[4] = {A(1), A(1), A(1), A(1)};
-        if constexpr (W) {
-            if constexpr (MODE == MODE_CORR32) {
-                const float4 q = ld_stream_f4(reinterpret_cast<const float4 *>(a.w32 + base), pol_s);
-                wv[0] = q.x; wv[1] = q.y; wv[2] = q.z; wv[3] = q.w;
-            } else {
-                const double2 q0 = ld_stream_d2(reinterpret_cast<const double2 *>(a.w64 + base), pol_s);
-                const double2 q1 = ld_stream_d2(reinterpret_cast<const double2 *>(a.w64 + base + 2), pol_s);
-                wv[0] = q0.x; wv[1] = q0.y; wv[2] = q1.x; wv[3] = q1.y;
-            }
-        }
-        A g[4];
-#pragma unroll
-        for (int k = 0; k < 4; k++) {
-            const uint32_t p = base + k;
-            g[k] = (p >= p_lo && p < p_hi) ? ld_gather(xt + cc[k], pol_g) : A(0);
-        }
-#pragma unroll
-        for (int k = 0; k < 4; k++) {
-            const uint32_t p = base + k;
-            if (p >= p_lo && p < p_hi) {
-                const A prod = W ? wv[k] * g[k] : g[k];
-                if constexpr (STORE) s_prod[p - p_lo] = prod;
-                else acc += prod;
-            }
+    const uint4 c = ld_stream_u4(reinterpret_cast<const uint4 *>(a.col + base), pol_s);
+    const uint32_t cc[4] = {c.x, c.y, c.z, c.w};
+    A wv[4] = {A(1), A(1), A(1), A(1)};
+    if constexpr (W) {
+        if constexpr (MODE == MODE_CORR32) {
+            const float4 q = ld_stream_f4(reinterpret_cast<const float4 *>(a.w32 + base), pol_s);
+            wv[0] = q.x; wv[1] = q.y; wv[2] = q.z; wv[3] = q.w;
+        } else {
+            const double2 q0 = ld_stream_d2(reinterpret_cast<const double2 *>(a.w64 + base), pol_s);
+            const double2 q1 = ld_stream_d2(reinterpret_cast<const double2 *>(a.w64 + base + 2), pol_s);
+            wv[0] = q0.x; wv[1] = q0.y; wv[2] = q1.x; wv[3] = q1.y;
         }
     }
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        const uint32_t p = base + k;
+        const A g = (p >= lo && p < hi) ? ld_gather(xt + cc[k], pol_g) : A(0);
+        out[k] = W ? wv[k] * g : g;
+    }
+}
+
+// Warp: stage products of arcs [lo, hi) (hi - lo <= kWarpBuf) into buf[p - lo].
+template <int MODE, bool W>
+__device__ __forceinline__ void stage(const IterArgs &a, uint32_t lo, uint32_t hi, typename ModeT<MODE>::A *buf,
+                                      uint32_t lane, uint64_t pol_s, uint64_t pol_g) {
+    using A = typename ModeT<MODE>::A;
+    const uint32_t a0 = lo & ~3u;
+    const uint32_t nvec = (hi - a0 + 3u) >> 2;
+    uint32_t vi = lane;
+    for (; vi + 32 < nvec; vi += 64) {
+        A g0[4], g1[4];
+        quad<MODE, W>(a, a0 + 4u * vi, lo, hi, pol_s, pol_g, g0);
+        quad<MODE, W>(a, a0 + 4u * (vi + 32), lo, hi, pol_s, pol_g, g1);
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            uint32_t p = a0 + 4u * vi + k;
+            if (p >= lo && p < hi) buf[p - lo] = g0[k];
+            p = a0 + 4u * (vi + 32) + k;
+            if (p >= lo && p < hi) buf[p - lo] = g1[k];
+        }
+    }
+    if (vi < nvec) {
+        A g0[4];
+        quad<MODE, W>(a, a0 + 4u * vi, lo, hi, pol_s, pol_g, g0);
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            const uint32_t p = a0 + 4u * vi + k;
+            if (p >= lo && p < hi) buf[p - lo] = g0[k];
+        }
+    }
+}
+
+// Warp: sum of products of arcs [lo, hi) (any length), result in every lane.
+template <int MODE, bool W>
+__device__ __forceinline__ typename ModeT<MODE>::A warp_row_sum(const IterArgs &a, uint32_t lo, uint32_t hi,
+                                                                 uint32_t lane, uint64_t pol_s, uint64_t pol_g) {
+    using A = typename ModeT<MODE>::A;
+    const uint32_t a0 = lo & ~3u;
+    const uint32_t nvec = (hi - a0 + 3u) >> 2;
+    A acc0 = A(0), acc1 = A(0);
+    uint32_t vi = lane;
+    for (; vi + 32 < nvec; vi += 64) {
+        A g0[4], g1[4];
+        quad<MODE, W>(a, a0 + 4u * vi, lo, hi, pol_s, pol_g, g0);
+        quad<MODE, W>(a, a0 + 4u * (vi + 32), lo, hi, pol_s, pol_g, g1);
+        acc0 += (g0[0] + g0[1]) + (g0[2] + g0[3]);
+        acc1 += (g1[0] + g1[1]) + (g1[2] + g1[3]);
+    }
+    if (vi < nvec) {
+        A g0[4];
+        quad<MODE, W>(a, a0 + 4u * vi, lo, hi, pol_s, pol_g, g0);
+        acc0 += (g0[0] + g0[1]) + (g0[2] + g0[3]);
+    }
+    return warp_sum(acc0 + acc1);
 }
 
 template <int MODE, bool W>
 __global__ void __launch_bounds__(kThreads) iter_kernel(const IterArgs a) {
     using A = typename ModeT<MODE>::A;
-    __shared__ A s_prod[2 * kCap];
-    __shared__ uint32_t s_rp[kRowCap + 1];
+    __shared__ A s_buf[kWarps][kWarpBuf];
     __shared__ double s_red[96];
-    __shared__ A s_redA[32];
     __shared__ int s_flag;
 
     Ctl *ctl = a.ctl;
     if constexpr (MODE != MODE_RESID64) {
         if (*(volatile int32_t *)&ctl->done) return;
     }
-    const uint32_t rb = blockIdx.x;
-    const uint4 d = a.rb[rb];
-    const uint32_t kind = d.z & 3u;
-    const uint32_t tid = threadIdx.x;
-
+    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     Uni u;
     u.d = a.damping;
     u.dsum = *(volatile double *)&ctl->dsum[a.parity];
@@ -209,135 +251,149 @@ __global__ void __launch_bounds__(kThreads) iter_kernel(const IterArgs a) {
         u.tele = __ddiv_rn(1.0 - u.d, nf);
         u.dshare = __ddiv_rn(__dmul_rn(u.d, u.dsum), nf);
     }
+    const uint64_t pol_s = policy_evict_first(), pol_g = policy_evict_last();
+    A *buf = s_buf[warp];
     double pd = 0.0, pds = 0.0, ps = 0.0;
 
-    if (kind == RB_STREAM) {
-        const uint32_t r0 = d.x, r1 = d.y, nrows = r1 - r0;
-        const uint32_t p0 = __ldg(&a.row_ptr[r0]);
-        for (uint32_t i = tid; i <= nrows; i += blockDim.x) s_rp[i] = __ldg(&a.row_ptr[r0 + i]) - p0;
-        __syncthreads();
-        const uint32_t cnt = s_rp[nrows];
-        A dummy = A(0);
-        arc_products<MODE, W, true>(a, p0, p0 + cnt, s_prod, dummy);
-        __syncthreads();
-        uint32_t tpr = 32;
-        while (tpr > 1 && tpr * nrows > blockDim.x) tpr >>= 1;
-        const uint32_t ngrp = blockDim.x / tpr, grp = tid / tpr, gl = tid % tpr;
-        const uint32_t rounds = (nrows + ngrp - 1) / ngrp;
-        for (uint32_t rd = 0; rd < rounds; rd++) {
-            const uint32_t row = rd * ngrp + grp;
-            const bool valid = row < nrows;
-            A acc = A(0);
-            if (valid)
-                for (uint32_t j = s_rp[row] + gl; j < s_rp[row + 1]; j += tpr) acc += s_prod[j];
-            for (uint32_t o = tpr >> 1; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-            if (valid && gl == 0) epilogue<MODE>(a, u, r0 + row, acc, pd, pds, ps);
-        }
-    } else {
-        const uint32_t r = d.x;
-        const uint32_t p0 = __ldg(&a.row_ptr[r]), p1 = __ldg(&a.row_ptr[r + 1]);
-        uint32_t lo = p0, hi = p1;
-        if (kind == RB_CHUNK) {
-            const uint32_t c = d.z >> 2;
-            lo = p0 + c * a.split;
-            hi = min(p1, lo + a.split);
-        }
-        A acc = A(0);
-        arc_products<MODE, W, false>(a, lo, hi, nullptr, acc);
-        const A tot = block_sum_t<A>(acc, s_redA);
-        if (tid == 0) {
-            if (kind == RB_LONG) {
-                epilogue<MODE>(a, u, r, tot, pd, pds, ps);
-            } else {
-                const Hub h = a.hubs[d.w];
-                a.chunk_part[rb] = (double)tot;
+    const uint32_t stride = gridDim.x * kWarps;
+    uint32_t rb = blockIdx.x * kWarps + warp;
+    uint4 d = rb < a.nrb ? __ldg(&a.rb[rb]) : make_uint4(0, 0, 0, 0);
+    while (rb < a.nrb) {
+        const uint32_t nxt = rb + stride;
+        const uint4 dn = nxt < a.nrb ? __ldg(&a.rb[nxt]) : make_uint4(0, 0, 0, 0);
+        if (d.y & kChunkFlag) {
+            // slice of a hub row
+            const A s = warp_row_sum<MODE, W>(a, d.z, d.w, lane, pol_s, pol_g);
+            if (lane == 0) {
+                const uint32_t h = d.y & ~kChunkFlag;
+                const Hub hb = a.hubs[h];
+                a.chunk_part[rb] = (double)s;
                 __threadfence();
-                const uint32_t t = atomicAdd(&a.hub_ticket[d.w], 1u);
-                if (t == h.nchunks - 1) {
+                const uint32_t t = atomicAdd(&a.hub_ticket[h], 1u);
+                if (t == hb.nchunks - 1) {
                     __threadfence();
                     double y = 0.0;
-                    for (uint32_t j = 0; j < h.nchunks; j++) y += __ldcg(&a.chunk_part[h.first_rb + j]);
+                    for (uint32_t j = 0; j < hb.nchunks; j++) y += __ldcg(&a.chunk_part[hb.first_rb + j]);
                     double hd = 0.0, hds = 0.0, hs = 0.0;
-                    epilogue<MODE>(a, u, r, (A)y, hd, hds, hs);
-                    a.hub_rec[d.w] = make_double4(hd, hds, hs, 0.0);
-                    a.hub_ticket[d.w] = 0u;
+                    const Pre pr = epi_load<MODE>(a, hb.row);
+                    epilogue<MODE>(a, u, hb.row, (A)y, pr, hd, hds, hs);
+                    a.hub_rec[h] = make_double4(hd, hds, hs, 0.0);
+                    a.hub_ticket[h] = 0u;
                 }
             }
+        } else if (d.y - d.x == 1u) {
+            // a single row: whole warp
+            Pre pr;
+            if (lane == 0) pr = epi_load<MODE>(a, d.x);
+            const A s = warp_row_sum<MODE, W>(a, d.z, d.w, lane, pol_s, pol_g);
+            if (lane == 0) epilogue<MODE>(a, u, d.x, s, pr, pd, pds, ps);
+        } else {
+            // up to 32 short rows, one lane each
+            const uint32_t r0 = d.x, p0 = d.z;
+            const bool has_row = lane < d.y - r0;
+            const uint32_t v = r0 + lane;
+            uint32_t rs = 0, re = 0;
+            Pre pr;
+            if (has_row) {
+                rs = __ldg(&a.row_ptr[v]) - p0;
+                re = __ldg(&a.row_ptr[v + 1]) - p0;
+                pr = epi_load<MODE>(a, v);
+            }
+            stage<MODE, W>(a, p0, d.w, buf, lane, pol_s, pol_g);
+            __syncwarp();
+            if (has_row) {
+                A acc0 = A(0), acc1 = A(0);
+                uint32_t j = rs;
+                for (; j + 1 < re; j += 2) {
+                    acc0 += buf[j];
+                    acc1 += buf[j + 1];
+                }
+                if (j < re) acc0 += buf[j];
+                epilogue<MODE>(a, u, v, acc0 + acc1, pr, pd, pds, ps);
+            }
+            __syncwarp();
         }
+        rb = nxt;
+        d = dn;
     }
 
-    // ---- deterministic two-level reduction of (diff, dangling, sum)
+    // ---- deterministic reduction of (diff, dangling, sum): block tree, then
+    // the last block adds block and hub records in index order
     block_sum3(pd, pds, ps, s_red);
-    const uint32_t g = rb / kGroup;
-    if (tid == 0) {
-        a.rb_part[rb] = make_double4(pd, pds, ps, 0.0);
+    if (threadIdx.x == 0) {
+        a.blk_part[blockIdx.x] = make_double4(pd, pds, ps, 0.0);
         __threadfence();
-        const uint32_t gsize = min(kGroup, a.nrb - g * kGroup);
-        const uint32_t t = atomicAdd(&a.grp_ticket[g], 1u);
-        s_flag = (t == gsize - 1);
+        const uint32_t t = atomicAdd(&ctl->groups_done, 1u);
+        s_flag = (t == gridDim.x - 1);
     }
     __syncthreads();
     if (!s_flag) return;
     __threadfence();
-    {
-        const uint32_t gsize = min(kGroup, a.nrb - g * kGroup);
-        double x = 0.0, y = 0.0, z = 0.0;
-        if (tid < gsize) {
-            const double4 q = ldcg4(&a.rb_part[g * kGroup + tid]);
-            x = q.x; y = q.y; z = q.z;
-        }
-        block_sum3(x, y, z, s_red);
-        if (tid == 0) {
-            a.grp_part[g] = make_double4(x, y, z, 0.0);
-            a.grp_ticket[g] = 0u;
-            __threadfence();
-            const uint32_t t = atomicAdd(&ctl->groups_done, 1u);
-            s_flag = (t == a.ngroups - 1);
-        }
+    double x = 0.0, y = 0.0, z = 0.0;
+    for (uint32_t i = threadIdx.x; i < gridDim.x; i += blockDim.x) {
+        const double4 q = ldcg4(&a.blk_part[i]);
+        x += q.x;
+        y += q.y;
+        z += q.z;
     }
-    __syncthreads();
-    if (!s_flag) return;
-    __threadfence();
-    {
-        double x = 0.0, y = 0.0, z = 0.0;
-        for (uint32_t i = tid; i < a.ngroups; i += blockDim.x) {
-            const double4 q = ldcg4(&a.grp_part[i]);
-            x += q.x; y += q.y; z += q.z;
+    block_sum3(x, y, z, s_red);
+    double hx = 0.0, hy = 0.0, hz = 0.0;
+    for (uint32_t i = threadIdx.x; i < a.nhub; i += blockDim.x) {
+        const double4 q = ldcg4(&a.hub_rec[i]);
+        hx += q.x;
+        hy += q.y;
+        hz += q.z;
+    }
+    block_sum3(hx, hy, hz, s_red);
+    if (threadIdx.x == 0) {
+        const double diff = x + hx, dsn = y + hy, sum = z + hz;
+        ctl->groups_done = 0u;
+        ctl->dsum[a.parity ^ 1] = dsn;
+        if constexpr (MODE == MODE_RESID64) {
+            ctl->rnorm = diff;
+            ctl->gsum = sum;
+            ctl->resid_passes += 1u;
+            const double t = ctl->rho * diff;
+            ctl->thr = t > ctl->floor_abs ? t : ctl->floor_abs;
+            ctl->iters = 0u;
+            ctl->done = 0;
+            ctl->parity_last = a.parity;
+        } else {
+            ctl->diff = diff;
+            ctl->iters += 1u;
+            ctl->total_iters += 1u;
+            ctl->parity_last = a.parity;
+            if (diff < ctl->thr || ctl->iters >= ctl->max_iter) ctl->done = 1;
         }
-        block_sum3(x, y, z, s_red);
-        double hx = 0.0, hy = 0.0, hz = 0.0;
-        for (uint32_t i = tid; i < a.nhub; i += blockDim.x) {
-            const double4 q = ldcg4(&a.hub_rec[i]);
-            hx += q.x; hy += q.y; hz += q.z;
-        }
-        block_sum3(hx, hy, hz, s_red);
-        if (tid == 0) {
-            const double diff = x + hx, dsn = y + hy, sum = z + hz;
-            ctl->groups_done = 0u;
-            ctl->dsum[a.parity ^ 1] = dsn;
-            if constexpr (MODE == MODE_RESID64) {
-                ctl->rnorm = diff;
-                ctl->gsum = sum;
-                ctl->resid_passes += 1u;
-                const double t = ctl->rho * diff;
-                ctl->thr = t > ctl->floor_abs ? t : ctl->floor_abs;
-                ctl->iters = 0u;
-                ctl->done = 0;
-                ctl->parity_last = a.parity;
-            } else {
-                ctl->diff = diff;
-                ctl->iters += 1u;
-                ctl->total_iters += 1u;
-                ctl->parity_last = a.parity;
-                if (diff < ctl->thr || ctl->iters >= ctl->max_iter) ctl->done = 1;
-            }
-            __threadfence();
-        }
+        __threadfence();
     }
 }
 
-void launch_iteration(int mode, bool weighted, const IterArgs &a, cudaStream_t s) {
-    const dim3 grid(a.nrb), block(kThreads);
+template <int MODE, bool W>
+static unsigned grid_of(uint32_t blocks_per_sm) {
+    static int sms = 0, occ = 0;
+    if (sms == 0) {
+        int dev = 0;
+        PRG_CUDA(cudaGetDevice(&dev));
+        PRG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    }
+    if (occ == 0) PRG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, iter_kernel<MODE, W>, kThreads, 0));
+    int per = occ > 0 ? occ : 1;
+    if (blocks_per_sm > 0 && (int)blocks_per_sm < per) per = (int)blocks_per_sm;
+    return (unsigned)(sms * per);
+}
+
+unsigned iteration_grid(int mode, bool weighted, uint32_t bps) {
+    switch (mode) {
+        case MODE_PLAIN64: return weighted ? grid_of<MODE_PLAIN64, true>(bps) : grid_of<MODE_PLAIN64, false>(bps);
+        case MODE_PPR64: return weighted ? grid_of<MODE_PPR64, true>(bps) : grid_of<MODE_PPR64, false>(bps);
+        case MODE_RESID64: return weighted ? grid_of<MODE_RESID64, true>(bps) : grid_of<MODE_RESID64, false>(bps);
+        default: return weighted ? grid_of<MODE_CORR32, true>(bps) : grid_of<MODE_CORR32, false>(bps);
+    }
+}
+
+void launch_iteration(int mode, bool weighted, const IterArgs &a, unsigned grid, cudaStream_t s) {
+    const dim3 block(kThreads);
 #define PRG_LAUNCH(M)                                                           \
     if (weighted) iter_kernel<M, true><<<grid, block, 0, s>>>(a);               \
     else iter_kernel<M, false><<<grid, block, 0, s>>>(a);

@@ -33,8 +33,7 @@ struct IterArgs {
     const float *inv32;
     const uint4 *rb;
     const Hub *hubs;
-    uint32_t nrb, ngroups, nhub, n;
-    uint32_t split;
+    uint32_t nrb, nhub, n, pad0;
     // vectors (FP64 modes use the *64 pointers, CORR32 the *32 ones)
     const double *xt64_in;
     const double *x64_in;
@@ -53,21 +52,22 @@ struct IterArgs {
     double inv_n;
     // reduction scratch
     Ctl *ctl;
-    double4 *rb_part;
-    double4 *grp_part;
-    double *chunk_part;
-    double4 *hub_rec;
-    uint32_t *grp_ticket;
+    double4 *blk_part;   // one record per block of the persistent grid
+    double *chunk_part;  // one partial sum per chunk row-block
+    double4 *hub_rec;    // (diff, dangling, sum) contribution of each hub row
     uint32_t *hub_ticket;
     int parity;
 };
 
-void launch_iteration(int mode, bool weighted, const IterArgs &a, cudaStream_t s);
+// Persistent grid of the iteration kernel for this device (SMs x resident
+// blocks per SM, or SMs x blocks_per_sm when nonzero).
+unsigned iteration_grid(int mode, bool weighted, uint32_t blocks_per_sm);
+void launch_iteration(int mode, bool weighted, const IterArgs &a, unsigned grid, cudaStream_t s);
 
 // x <- x + e (e may be null), xt <- x / dval, dangling sum and total sum of
 // x into ctl->dsum[parity] / ctl->gsum via a deterministic two-level tree.
 void launch_prepare64(const DeviceGraph &g, double *x, const float *e, double *xt, Ctl *ctl, int parity,
-                      double4 *rb_part, cudaStream_t s);
+                      double4 *part, cudaStream_t s);
 // x <- x / sum (final FP64 normalisation of the refined result).
 void launch_normalise(double *x, uint32_t n, const Ctl *ctl, cudaStream_t s);
 // x <- t (FP64 copy) or uniform 1/n when t is null.

@@ -75,7 +75,8 @@ class prg_stats(C.Structure):
     _fields_ = [("iterations", C.c_uint32), ("fp64_passes", C.c_uint32), ("fp32_passes", C.c_uint32),
                 ("residual_passes", C.c_uint32), ("last_diff", C.c_double), ("residual_l1", C.c_double),
                 ("error_bound", C.c_double), ("solve_ms", C.c_double), ("build_ms", C.c_double),
-                ("arcs", C.c_uint64), ("n_dangling", C.c_uint32), ("pad", C.c_uint32)]
+                ("arcs", C.c_uint64), ("n_dangling", C.c_uint32), ("kernel_launches", C.c_uint32),
+                ("fp32_ms", C.c_double), ("fp64_ms", C.c_double)]
 
 
 _lib = None
@@ -123,6 +124,10 @@ def lib():
     L.prg_solve.argtypes = [vp, C.POINTER(prg_options), f64p, f64p, C.POINTER(prg_stats)]
     L.prg_solve_device.restype = C.c_int32
     L.prg_solve_device.argtypes = [vp, C.POINTER(prg_options), vp, vp, C.POINTER(prg_stats)]
+    L.prg_set_tuning.restype = C.c_int32
+    L.prg_set_tuning.argtypes = [C.c_char_p, C.c_int64]
+    L.prg_graph_relabelled.restype = C.c_int32
+    L.prg_graph_relabelled.argtypes = [vp]
     L.prg_rmat_device.restype = C.c_int32
     L.prg_rmat_device.argtypes = [C.c_uint32, C.c_uint64, C.c_double, C.c_double, C.c_double, C.c_uint64,
                                   vp, vp, vp]
@@ -310,11 +315,15 @@ class Stats:
     build_ms: float
     arcs: int
     n_dangling: int
+    kernel_launches: int
+    fp32_ms: float
+    fp64_ms: float
 
     @classmethod
     def from_c(cls, s: prg_stats) -> "Stats":
         return cls(s.iterations, s.fp64_passes, s.fp32_passes, s.residual_passes, s.last_diff, s.residual_l1,
-                   s.error_bound, s.solve_ms, s.build_ms, s.arcs, s.n_dangling)
+                   s.error_bound, s.solve_ms, s.build_ms, s.arcs, s.n_dangling, s.kernel_launches, s.fp32_ms,
+                   s.fp64_ms)
 
 
 class DeviceGraph:
@@ -355,14 +364,21 @@ class DeviceGraph:
     def handle(self):
         return self._h
 
+    @property
+    def relabelled(self) -> bool:
+        return bool(lib().prg_graph_relabelled(self._h))
+
     def stream(self) -> int:
         return lib().prg_graph_stream(self._h) or 0
 
-    def solve(self, options: Optional[Options] = None, reset=None, start=None):
-        """Host solve: returns (x float64[n], Stats)."""
+    def solve(self, options: Optional[Options] = None, reset=None, start=None, out=None):
+        """Host solve: returns (x float64[n], Stats).  `out` may be a caller
+        float64 buffer (e.g. pinned memory) of length >= n."""
         o = options or Options()
         st = prg_stats()
-        out = np.empty(max(self.n, 1), np.float64)
+        if out is None:
+            out = np.empty(max(self.n, 1), np.float64)
+        assert out.dtype == np.float64 and out.flags["C_CONTIGUOUS"] and len(out) >= self.n
         r = None if reset is None else np.ascontiguousarray(reset, dtype=np.float64)
         s0 = None if start is None else np.ascontiguousarray(start, dtype=np.float64)
         co = o.to_c(_ptr(s0))
@@ -394,6 +410,19 @@ class DeviceGraph:
 
     def __exit__(self, *a):
         self.close()
+
+
+def set_tuning(key: str, value: int) -> None:
+    """Process-wide tuning for graphs created afterwards (see prg_set_tuning)."""
+    _check(lib().prg_set_tuning(key.encode(), int(value)))
+
+
+TUNING_DEFAULTS = {"capw": 448, "shortmax": 64, "split": 8192, "blocks_per_sm": 0, "relabel": 2, "unroll": 8}
+
+
+def reset_tuning() -> None:
+    for k, v in TUNING_DEFAULTS.items():
+        set_tuning(k, v)
 
 
 def rmat_device(scale: int, m: int, d_from: int, d_to: int, a=0.57, b=0.19, c=0.19, seed=1, stream: int = 0):

@@ -229,3 +229,39 @@ def test_large_rmat_properties(cuda_ok):
     # both certified within 1e-10 of the fixed point => within 2e-10 of each other
     assert np.abs(x64 - x32).sum() <= 2 * L1_TOL
     assert s32.error_bound <= L1_TOL and s64.error_bound <= L1_TOL
+
+
+@pytest.mark.parametrize("relabel", [0, 1])
+def test_relabel_modes_match_oracle(cuda_ok, relabel):
+    # degree-sorted internal ids must not change any result (caller ids out)
+    ig.set_tuning("relabel", relabel)
+    try:
+        n = 20_000
+        f, t = O.barabasi_game_bag(n, 5, False, True, 21)
+        g = G(n, f, t, True)
+        assert maxabs(ig.pagerank(g), O.pagerank(n, f, t, True)) <= PARITY
+        w = O.uniform_weights(len(f), 8)
+        assert maxabs(ig.pagerank_weighted(g, w), O.pagerank_weighted(n, f, t, True, w)) <= PARITY
+        r = np.zeros(n)
+        r[[5, 17, 19000]] = [1.0, 0.5, 2.0]
+        assert maxabs(ig.personalized_pagerank(g, r, 0.8), O.personalized_pagerank(n, f, t, True, r, 0.8)) <= PARITY
+        with ig.DeviceGraph.from_host(n, f, t, True) as dg:
+            assert dg.relabelled == bool(relabel)
+            tight, _, _ = O.pagerank_tight(n, f, t, True, tol=1e-15)
+            x, _ = dg.solve(ig.Options(precision=ig.PRECISION_FP32_REFINED))
+            assert np.abs(x - tight).sum() <= L1_TOL
+            # a warm start in caller ids is honoured
+            xs, st = dg.solve(ig.Options(stop=ig.STOP_ERROR_BOUND), start=tight)
+            assert st.iterations <= 3 and np.abs(xs - tight).sum() <= L1_TOL
+    finally:
+        ig.reset_tuning()
+
+
+def test_rmat_auto_relabel(cuda_ok):
+    scale = 15
+    n = 1 << scale
+    f, t = O.rmat(scale, 16 * n, seed=4)
+    with ig.DeviceGraph.from_host(n, f, t, True) as dg:
+        assert dg.relabelled
+        x, _ = dg.solve(ig.Options())
+    assert maxabs(x, O.pagerank(n, f, t, True)) <= PARITY
