@@ -395,6 +395,8 @@ def main():
                    "l2": "inputs larger than L2 (CSR 1.07 GB) and a 256 MiB write between steps",
                    "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU"},
         "time_to_tol_ms": ms_max / args.steps,
+        "solve_ms_each": [round(s.solve_ms, 2) for s in stats],
+        "kernel_ms_each": [round(s.fp32_ms + s.fp64_ms, 2) for s in stats],
         "passes_per_solve": passes / args.steps,
         "fp32_passes_per_solve": fp32_passes / args.steps,
         "residual_passes_per_solve": s0.residual_passes,

@@ -139,11 +139,51 @@ int32_t prg_solve_device(prg_graph *g, const prg_options *opt, const double *d_r
  * returned in the caller's ids), else 0. */
 int32_t prg_graph_relabelled(const prg_graph *g);
 
+/* Read-only views of the device CSR in internal ids (row_ptr[n+1], col[arcs],
+ * perm = internal -> caller id or NULL, inv32 = 1/out-degree in FP32), for
+ * callers that run their own kernels over the resident graph. */
+int32_t prg_graph_device_csr(const prg_graph *g, const uint32_t **row_ptr, const uint32_t **col,
+                             const uint32_t **perm, const float **inv32);
+
 /* Process-wide tuning applied to graphs created afterwards (the autotuner's
  * knobs): "capw", "shortmax", "split" (row-block shape), "blocks_per_sm"
  * (persistent grid, 0 = occupancy maximum), "relabel" (0 off, 1 on, 2 auto on
- * skewed degree distributions), "unroll" (iteration pairs per CUDA graph). */
+ * skewed degree distributions), "refine_switch_e12" (refined precision: FP64
+ * power steps until the successive change is below value * 1e-12, then FP32
+ * corrections; default 500000), "batch_vec" (batched columns per lane: 1, 2
+ * or 4), "hot_cache" (1: relabelled graphs gather
+ * their hot vertices from shared memory), "unroll" (iteration pairs per CUDA
+ * graph). */
 int32_t prg_set_tuning(const char *key, int64_t value);
+
+/* ---- batched personalized PageRank ---------------------------------- */
+
+typedef struct prg_batch_stats {
+    uint64_t column_iterations; /* sum over columns of the iterations each ran */
+    uint32_t max_iters;         /* iterations of the slowest column */
+    uint32_t tiles;             /* column tiles (one persistent launch each) */
+    uint32_t tile_width;        /* columns per tile (32 * vec) */
+    uint32_t kernel_launches;
+    double ms;                  /* device time (CUDA events) */
+} prg_batch_stats;
+
+/* K personalized PageRank vectors at once (FP32 SpMM with FP32 accumulation).
+ * Column k is rust-igraph personalized_pagerank_vs(graph, seeds_k, damping)
+ * (personalized_pagerank.rs:241-268 building the reset, :65-182 iterating)
+ * with seeds_k = seeds[seed_offsets[k] .. seed_offsets[k+1]) in caller ids,
+ * stopped per column when its successive L1 change is < tol (the column then
+ * freezes while the others continue) or after max_iter iterations.
+ * tile_vec: columns per tile = 32 * tile_vec (1, 2 or 4; 0 = autotuned or 1).
+ * out: host float[n * K], out[v * K + k].  column_iters: optional host
+ * uint32[K].  Validation follows _vs: empty seed list or vertex >= n ->
+ * PRG_ERR_INVALID_ARGUMENT; a device barrier that times out -> PRG_ERR_TIMEOUT. */
+int32_t prg_ppr_batch(prg_graph *g, uint32_t K, const uint64_t *seed_offsets, const uint32_t *seeds, double damping,
+                      double tol, uint32_t max_iter, uint32_t tile_vec, float *out, uint32_t *column_iters,
+                      prg_batch_stats *stats);
+/* Same with a device output buffer d_out (float[n * K]). */
+int32_t prg_ppr_batch_device(prg_graph *g, uint32_t K, const uint64_t *seed_offsets, const uint32_t *seeds,
+                             double damping, double tol, uint32_t max_iter, uint32_t tile_vec, float *d_out,
+                             uint32_t *column_iters, prg_batch_stats *stats);
 
 /* Message of the last error on this thread ("" if none). */
 const char *prg_last_error(void);

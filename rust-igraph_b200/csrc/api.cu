@@ -18,6 +18,7 @@
 
 #include "../../include/prg_b200.h"
 #include "graph.cuh"
+#include "ppr_batch.cuh"
 #include "solver.cuh"
 
 struct prg_graph {
@@ -124,6 +125,7 @@ int32_t create_from_device(uint32_t n, uint64_t m, const uint32_t *d_from, const
         h->g.split = t.split;
         h->g.blocks_per_sm = t.blocks_per_sm;
         h->g.relabel = t.relabel;
+        h->g.hot_cache = t.hot_cache;
         h->ws.unroll = t.unroll;
     }
     PRG_CUDA(cudaGetDevice(&h->g.device));
@@ -208,6 +210,7 @@ void destroy(prg_graph *h) {
 
 prg::SolveOpts to_solve_opts(const prg_options *o) {
     prg::SolveOpts so;
+    so.refine_switch = prg::tuning().refine_switch;
     if (o) {
         so.damping = o->damping;
         so.eps = o->eps;
@@ -463,6 +466,16 @@ void prg_graph_destroy(prg_graph *g) {
 
 int32_t prg_graph_relabelled(const prg_graph *h) { return h && h->g.perm ? 1 : 0; }
 
+int32_t prg_graph_device_csr(const prg_graph *h, const uint32_t **row_ptr, const uint32_t **col,
+                             const uint32_t **perm, const float **inv32) {
+    if (!h) return fail(PRG_ERR_INVALID_ARGUMENT, "null graph handle");
+    if (row_ptr) *row_ptr = h->g.row_ptr;
+    if (col) *col = h->g.col;
+    if (perm) *perm = h->g.perm;
+    if (inv32) *inv32 = h->g.inv32;
+    return PRG_OK;
+}
+
 int32_t prg_graph_info(const prg_graph *h, uint32_t *n, uint64_t *arcs, uint32_t *n_dangling, uint32_t *nrb,
                        uint32_t *nhub, double *build_ms) {
     if (!h) return fail(PRG_ERR_INVALID_ARGUMENT, "null graph handle");
@@ -534,6 +547,68 @@ int32_t prg_solve_device(prg_graph *h, const prg_options *opt, const double *d_r
     PRG_GUARD_END
 }
 
+static int32_t batch_common(prg_graph *h, uint32_t K, const uint64_t *off, const uint32_t *seeds, double damping,
+                            double tol, uint32_t max_iter, uint32_t vec, float *d_out, uint32_t *column_iters,
+                            prg_batch_stats *st) {
+    if (!h) return fail(PRG_ERR_INVALID_ARGUMENT, "null graph handle");
+    if (K == 0) return fail(PRG_ERR_INVALID_ARGUMENT, "batch needs at least one column");
+    if (!(damping > 0.0 && damping < 1.0))
+        return fail(PRG_ERR_INVALID_ARGUMENT,
+                    "personalized_pagerank: damping (" + rust_f64(damping) + ") must be in (0, 1)");
+    const uint32_t n = h->g.n;
+    if (n < 2) return fail(PRG_ERR_INVALID_ARGUMENT, "batched solve needs vcount >= 2");
+    if (off[0] != 0) return fail(PRG_ERR_INVALID_ARGUMENT, "seed_offsets[0] must be 0");
+    for (uint32_t k = 0; k < K; k++) {
+        if (off[k + 1] <= off[k]) return fail(PRG_ERR_INVALID_ARGUMENT, "reset_vids must not be empty");
+        for (uint64_t i = off[k]; i < off[k + 1]; i++)
+            if (seeds[i] >= n)
+                return fail(PRG_ERR_INVALID_ARGUMENT, "reset vertex " + std::to_string(seeds[i]) +
+                                                          " out of range (vcount = " + std::to_string(n) + ")");
+    }
+    if (vec == 0) vec = prg::tuning().batch_vec;
+    prg::BatchStats bs;
+    const int rc = prg::ppr_batch(h->g, K, off, seeds, damping, tol, max_iter, vec, d_out, bs, h->stream);
+    if (column_iters)
+        for (uint32_t k = 0; k < K; k++) column_iters[k] = bs.column_iters[k];
+    if (st) {
+        st->column_iterations = bs.column_iterations;
+        st->max_iters = bs.max_iters;
+        st->tiles = bs.tiles;
+        st->tile_width = 32 * bs.vec;
+        st->kernel_launches = bs.kernel_launches;
+        st->ms = bs.ms;
+    }
+    if (rc == PRG_ERR_TIMEOUT) return fail(PRG_ERR_TIMEOUT, "batched solve: a grid barrier timed out");
+    if (rc != 0) return fail(PRG_ERR_INTERNAL, "batched solve: device status " + std::to_string(rc));
+    return PRG_OK;
+}
+
+int32_t prg_ppr_batch_device(prg_graph *h, uint32_t K, const uint64_t *off, const uint32_t *seeds, double damping,
+                             double tol, uint32_t max_iter, uint32_t vec, float *d_out, uint32_t *column_iters,
+                             prg_batch_stats *st) {
+    g_err.clear();
+    PRG_GUARD_BEGIN
+    return batch_common(h, K, off, seeds, damping, tol, max_iter, vec, d_out, column_iters, st);
+    PRG_GUARD_END
+}
+
+int32_t prg_ppr_batch(prg_graph *h, uint32_t K, const uint64_t *off, const uint32_t *seeds, double damping,
+                      double tol, uint32_t max_iter, uint32_t vec, float *out, uint32_t *column_iters,
+                      prg_batch_stats *st) {
+    g_err.clear();
+    PRG_GUARD_BEGIN
+    if (!h) return fail(PRG_ERR_INVALID_ARGUMENT, "null graph handle");
+    float *d_out = nullptr;
+    const size_t bytes = (size_t)h->g.n * K * 4;
+    PRG_CUDA(cudaMallocAsync((void **)&d_out, std::max<size_t>(bytes, 16), h->stream));
+    int32_t rc = batch_common(h, K, off, seeds, damping, tol, max_iter, vec, d_out, column_iters, st);
+    if (rc == PRG_OK) PRG_CUDA(cudaMemcpyAsync(out, d_out, bytes, cudaMemcpyDeviceToHost, h->stream));
+    cudaFreeAsync(d_out, h->stream);
+    PRG_CUDA(cudaStreamSynchronize(h->stream));
+    return rc;
+    PRG_GUARD_END
+}
+
 int32_t prg_set_tuning(const char *key, int64_t value) {
     g_err.clear();
     if (!key) return fail(PRG_ERR_INVALID_ARGUMENT, "null tuning key");
@@ -547,6 +622,13 @@ int32_t prg_set_tuning(const char *key, int64_t value) {
     else if (k == "relabel") {
         if (value > 2) return fail(PRG_ERR_INVALID_ARGUMENT, "relabel must be 0, 1 or 2");
         t.relabel = (int)value;
+    } else if (k == "batch_vec") {
+        if (value != 1 && value != 2 && value != 4) return fail(PRG_ERR_INVALID_ARGUMENT, "batch_vec must be 1, 2 or 4");
+        t.batch_vec = (uint32_t)value;
+    } else if (k == "refine_switch_e12") {
+        t.refine_switch = (double)value * 1e-12;
+    } else if (k == "hot_cache") {
+        t.hot_cache = value != 0;
     } else if (k == "unroll") {
         if (value < 1 || value > 64) return fail(PRG_ERR_INVALID_ARGUMENT, "unroll must be in 1..=64");
         t.unroll = (int)value;

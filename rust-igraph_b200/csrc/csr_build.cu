@@ -401,7 +401,8 @@ __global__ void max_degree_kernel(const uint32_t *row_ptr, uint32_t n, uint32_t 
 // multiple of 32, when the previous row was not short, or when row r's first
 // arc crosses a multiple of capw.  A stream block therefore holds <= 32 rows
 // (32-row aligned, so its epilogue stores are coalesced) and
-// < capw + shortmax <= kWarpBuf arcs.
+// < capw + shortmax <= kWarpBuf arcs; the kernel sums each of its rows with a
+// power-of-two group of lanes sized to the row count.
 
 __global__ void rb_count(const uint32_t *rp, uint32_t n, uint32_t capw, uint32_t shortmax, uint32_t split,
                          uint32_t *cnt, uint32_t *hubflag) {

@@ -39,6 +39,7 @@ struct DeviceGraph {
     uint32_t split = kSplit;
     uint32_t blocks_per_sm = 0;  // persistent grid = SMs x this (0 = occupancy maximum)
     int relabel = 2;             // 0 keep caller ids, 1 degree-sorted ids, 2 decide from the degree skew
+    bool hot_cache = false;      // relabelled graphs: cache the hot prefix of the rank vector in shared memory
 
     float build_ms = 0.f;
 };
@@ -57,6 +58,9 @@ struct Tuning {
     uint32_t capw = kCapW, shortmax = kShortMax, split = kSplit, blocks_per_sm = 0;
     int relabel = 2;
     int unroll = 8;
+    bool hot_cache = false;
+    double refine_switch = 5e-7;
+    uint32_t batch_vec = 1;
 };
 Tuning &tuning();
 

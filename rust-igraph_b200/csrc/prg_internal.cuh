@@ -21,9 +21,9 @@ constexpr int kThreads = 256;         // threads per block for all hot kernels
 constexpr int kWarps = kThreads / 32;
 constexpr uint32_t kWarpBuf = 512;    // products staged per warp (shared memory)
 constexpr uint32_t kRowCap = 32;      // rows per stream row-block (one lane per row)
-constexpr uint32_t kCapW = 448;       // default stream window: a new row-block starts when a row's
+constexpr uint32_t kCapW = 256;       // default stream window: a new row-block starts when a row's
                                       // first arc crosses a multiple of kCapW
-constexpr uint32_t kShortMax = 64;    // default: rows with more arcs are handled by a whole warp
+constexpr uint32_t kShortMax = 256;   // default: rows with more arcs are handled by a whole warp
 constexpr uint32_t kSplit = 8192;     // default: rows with more arcs are split into chunks
 constexpr uint32_t kColPad = 16;      // extra u32 slots after col[] for aligned vector loads
 constexpr uint32_t kChunkFlag = 0x80000000u;

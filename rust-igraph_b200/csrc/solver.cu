@@ -16,6 +16,8 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 
 #include "solver.cuh"
@@ -68,9 +70,10 @@ void workspace_ensure(Workspace &ws, const DeviceGraph &g, cudaStream_t s) {
     ws.nrb = g.nrb;
     ws.nhub = g.nhub;
     unsigned gmax = kPrepParts;
+    const bool hot = g.perm != nullptr && g.hot_cache;
     for (int m = 0; m < 4; m++) {
-        ws.grid[m] = iteration_grid(m, g.weighted, g.blocks_per_sm);
-        gmax = std::max(gmax, ws.grid[m]);
+        ws.cfg[m] = iteration_config(m, g.weighted, hot, g.blocks_per_sm, g.n);
+        gmax = std::max(gmax, ws.cfg[m].grid);
     }
     const uint64_t n = g.n;
     for (int i = 0; i < 2; i++) {
@@ -137,8 +140,8 @@ static cudaGraphExec_t loop_graph(const DeviceGraph &g, Workspace &ws, int mode,
     cudaGraph_t graph;
     PRG_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
     for (int u = 0; u < ws.unroll; u++) {
-        launch_iteration(mode, g.weighted, a0, ws.grid[mode], s);
-        launch_iteration(mode, g.weighted, a1, ws.grid[mode], s);
+        launch_iteration(mode, g.weighted, a0, ws.cfg[mode], s);
+        launch_iteration(mode, g.weighted, a1, ws.cfg[mode], s);
     }
     PRG_CUDA(cudaStreamEndCapture(s, &graph));
     cudaGraphExec_t exec;
@@ -177,15 +180,18 @@ __global__ void to_f32_kernel(const double *a, float *b, uint32_t n) {
     for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) b[v] = (float)a[v];
 }
 
-static void solve_fp64(const DeviceGraph &g, Workspace &ws, const SolveOpts &o, const double *d_t, double *d_out,
-                       SolveStats &st, cudaStream_t s) {
+// FP64 power iteration (PLAIN64 / PPR64) from the start vector until the
+// successive L1 change is < thr or max_iter iterations ran.  Returns the
+// buffer holding the newest iterate.
+static const double *fp64_loop(const DeviceGraph &g, Workspace &ws, const SolveOpts &o, const double *d_t, double thr,
+                               uint32_t max_iter, SolveStats &st, cudaStream_t s) {
     const bool ppr = d_t != nullptr;
     if (o.d_start) PRG_CUDA(cudaMemcpyAsync(ws.x64[0], o.d_start, (uint64_t)g.n * 8, cudaMemcpyDeviceToDevice, s));
     else launch_fill_start(ws.x64[0], d_t, g.n, s);
     Ctl c;
     std::memset(&c, 0, sizeof(c));
-    c.thr = o.stop == 1 ? o.eps * (1.0 - o.damping) / o.damping : o.eps;
-    c.max_iter = o.max_iter;
+    c.thr = thr;
+    c.max_iter = max_iter;
     PRG_CUDA(cudaMemcpyAsync(ws.ctl, &c, sizeof(Ctl), cudaMemcpyHostToDevice, s));
     launch_prepare64(g, ws.x64[0], nullptr, ws.xt64[0], ws.ctl, 0, ws.blk_part, s);
     st.kernel_launches += (o.d_start ? 0u : 1u) + 2u;
@@ -202,28 +208,52 @@ static void solve_fp64(const DeviceGraph &g, Workspace &ws, const SolveOpts &o, 
     a1.x64_out = ws.x64[0];
     a1.xt64_out = ws.xt64[0];
     const int mode = ppr ? MODE_PPR64 : MODE_PLAIN64;
-    if (o.max_iter > 0) {
+    if (max_iter > 0) {
         cudaGraphExec_t ex = loop_graph(g, ws, mode, ppr, o.damping, a0, a1, s);
-        run_loop(ws, ex, o.max_iter, s, &st.fp64_ms, &st.kernel_launches);
+        run_loop(ws, ex, max_iter, s, &st.fp64_ms, &st.kernel_launches);
     } else {
         read_ctl(ws, s);
     }
     const Ctl &h = *ws.h_ctl;
-    const double *res = (h.iters == 0) ? ws.x64[0] : (h.parity_last == 0 ? ws.x64[1] : ws.x64[0]);
-    PRG_CUDA(cudaMemcpyAsync(d_out, res, (uint64_t)g.n * 8, cudaMemcpyDeviceToDevice, s));
-    st.iterations = st.fp64_passes = h.iters;
+    st.fp64_passes += h.iters;
+    st.iterations += h.iters;
     st.last_diff = h.diff;
-    st.residual_l1 = h.diff;
-    st.error_bound = h.diff * o.damping / (1.0 - o.damping);
+    return (h.iters == 0) ? ws.x64[0] : (h.parity_last == 0 ? ws.x64[1] : ws.x64[0]);
 }
 
+static void solve_fp64(const DeviceGraph &g, Workspace &ws, const SolveOpts &o, const double *d_t, double *d_out,
+                       SolveStats &st, cudaStream_t s) {
+    const double thr = o.stop == 1 ? o.eps * (1.0 - o.damping) / o.damping : o.eps;
+    const double *res = fp64_loop(g, ws, o, d_t, thr, o.max_iter, st, s);
+    PRG_CUDA(cudaMemcpyAsync(d_out, res, (uint64_t)g.n * 8, cudaMemcpyDeviceToDevice, s));
+    st.residual_l1 = st.last_diff;
+    st.error_bound = st.last_diff * o.damping / (1.0 - o.damping);
+}
+
+// Refined solve.  FP32 corrections carry a rounding error of ~1e-7 of the
+// correction's size, spread over every eigen-direction of the operator, and
+// slow directions decay only at the rate d.  Corrections therefore start
+// once the FP64 power iteration has brought the successive change below
+// `refine_switch` (so that noise sits far under the tolerance); above it the
+// iteration stays in FP64.
 static void solve_refined(const DeviceGraph &g, Workspace &ws, const SolveOpts &o, const double *d_t,
                           double *d_out, SolveStats &st, cudaStream_t s) {
     const bool ppr = d_t != nullptr;
     const double thr_final = o.eps * (1.0 - o.damping) / o.damping;
-    if (o.d_start) PRG_CUDA(cudaMemcpyAsync(ws.x64[0], o.d_start, (uint64_t)g.n * 8, cudaMemcpyDeviceToDevice, s));
-    else launch_fill_start(ws.x64[0], d_t, g.n, s);
-    if (ppr) to_f32_kernel<<<148 * 4, kThreads, 0, s>>>(d_t, ws.t32, g.n);
+    const double sw = std::max(o.refine_switch, thr_final);
+    const double *xa = fp64_loop(g, ws, o, d_t, sw, o.max_iter, st, s);
+    if (!(st.last_diff >= thr_final) && st.fp64_passes > 0) {
+        // the FP64 phase already met the error bound
+        PRG_CUDA(cudaMemcpyAsync(d_out, xa, (uint64_t)g.n * 8, cudaMemcpyDeviceToDevice, s));
+        st.residual_l1 = st.last_diff;
+        st.error_bound = st.last_diff * o.damping / (1.0 - o.damping);
+        return;
+    }
+    if (xa != ws.x64[0]) PRG_CUDA(cudaMemcpyAsync(ws.x64[0], xa, (uint64_t)g.n * 8, cudaMemcpyDeviceToDevice, s));
+    if (ppr) {
+        to_f32_kernel<<<148 * 4, kThreads, 0, s>>>(d_t, ws.t32, g.n);
+        st.kernel_launches += 1u;
+    }
     Ctl c;
     std::memset(&c, 0, sizeof(c));
     c.rho = 4e-6;
@@ -232,7 +262,7 @@ static void solve_refined(const DeviceGraph &g, Workspace &ws, const SolveOpts &
     c.max_iter = inner_cap;
     PRG_CUDA(cudaMemcpyAsync(ws.ctl, &c, sizeof(Ctl), cudaMemcpyHostToDevice, s));
     launch_prepare64(g, ws.x64[0], nullptr, ws.xt64[0], ws.ctl, 1, ws.blk_part, s);
-    st.kernel_launches += (o.d_start ? 0u : 1u) + (ppr ? 1u : 0u) + 2u;
+    st.kernel_launches += 2u;
 
     IterArgs r = base_args(g, ws, o.damping);
     r.t64 = d_t;
@@ -260,10 +290,10 @@ static void solve_refined(const DeviceGraph &g, Workspace &ws, const SolveOpts &
     cudaGraphExec_t ex = loop_graph(g, ws, MODE_CORR32, ppr, o.damping, a0, a1, s);
 
     const uint32_t pass_cap = std::max<uint32_t>(o.max_iter, 64u);
-    uint32_t fp32 = 0, fp64 = 0;
+    uint32_t fp32 = 0, fp64 = st.fp64_passes;
     for (int outer = 0; outer < 64; outer++) {
         PRG_CUDA(cudaEventRecord(ws.eva, s));
-        launch_iteration(MODE_RESID64, g.weighted, r, ws.grid[MODE_RESID64], s);
+        launch_iteration(MODE_RESID64, g.weighted, r, ws.cfg[MODE_RESID64], s);
         PRG_CUDA(cudaEventRecord(ws.evb, s));
         fp64++;
         st.kernel_launches += 1u;
@@ -275,6 +305,8 @@ static void solve_refined(const DeviceGraph &g, Workspace &ws, const SolveOpts &
         }
         const double rn = ws.h_ctl->rnorm;
         st.residual_l1 = rn;
+        if (std::getenv("PRG_TRACE"))
+            std::fprintf(stderr, "[prg] residual pass %u: ||r||_1 = %.3e (after %u fp32 passes)\n", fp64, rn, fp32);
         if (!(rn > thr_final) || fp32 + fp64 >= pass_cap) break;
         run_loop(ws, ex, inner_cap, s, &st.fp32_ms, &st.kernel_launches);
         fp32 += ws.h_ctl->iters;
@@ -291,8 +323,8 @@ static void solve_refined(const DeviceGraph &g, Workspace &ws, const SolveOpts &
         PRG_CUDA(cudaMemcpyAsync(d_out, ws.x64[1], (uint64_t)g.n * 8, cudaMemcpyDeviceToDevice, s));
     }
     st.fp32_passes = fp32;
+    st.residual_passes = fp64 - st.fp64_passes;
     st.fp64_passes = fp64;
-    st.residual_passes = fp64;
     st.iterations = fp32 + fp64;
     st.last_diff = ws.h_ctl->diff;
     st.error_bound = st.residual_l1 * o.damping / (1.0 - o.damping);

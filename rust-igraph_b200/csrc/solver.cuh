@@ -18,6 +18,7 @@ struct SolveOpts {
     int stop = 0;           // 0 successive (reference), 1 error bound
     int normalise = 1;
     const double *d_start = nullptr;  // device start vector (warm start) or null
+    double refine_switch = 5e-7;      // refined: FP64 steps until the successive change is below this
 };
 
 struct SolveStats {
@@ -31,7 +32,7 @@ struct SolveStats {
 struct Workspace {
     bool ready = false;
     uint32_t n = 0, nrb = 0, nhub = 0;
-    unsigned grid[4] = {0, 0, 0, 0};  // persistent grid per iteration mode
+    LaunchCfg cfg[4];  // persistent launch shape per iteration mode
     double *x64[2] = {nullptr, nullptr};
     double *xt64[2] = {nullptr, nullptr};
     float *e32[2] = {nullptr, nullptr};

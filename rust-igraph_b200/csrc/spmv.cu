@@ -28,6 +28,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <algorithm>
+
 #include "prims.cuh"
 #include "spmv.cuh"
 
@@ -149,10 +151,15 @@ __device__ __forceinline__ const typename ModeT<MODE>::A *gather_src(const IterA
 }
 
 // Products w * xt[col] of the 4 arcs at aligned position `base`; lanes outside
-// [lo, hi) get 0 and issue no gather.
+// [lo, hi) get 0 and issue no gather.  Sources below `hot` are read from the
+// block's shared-memory copy of the rank vector's hot prefix (degree-sorted
+// ids put the most-gathered vertices there): a warp's random shared-memory
+// reads cost a few bank wavefronts where the same global gathers cost about
+// one L1 wavefront per lane.
 template <int MODE, bool W>
 __device__ __forceinline__ void quad(const IterArgs &a, uint32_t base, uint32_t lo, uint32_t hi, uint64_t pol_s,
-                                     uint64_t pol_g, typename ModeT<MODE>::A (&out)[4]) {
+                                     uint64_t pol_g, const typename ModeT<MODE>::A *s_hot, uint32_t hot,
+                                     typename ModeT<MODE>::A (&out)[4]) {
     using A = typename ModeT<MODE>::A;
     const A *xt = gather_src<MODE>(a);
     const uint4 c = ld_stream_u4(reinterpret_cast<const uint4 *>(a.col + base), pol_s);
@@ -171,7 +178,8 @@ __device__ __forceinline__ void quad(const IterArgs &a, uint32_t base, uint32_t 
 #pragma unroll
     for (int k = 0; k < 4; k++) {
         const uint32_t p = base + k;
-        const A g = (p >= lo && p < hi) ? ld_gather(xt + cc[k], pol_g) : A(0);
+        A g = A(0);
+        if (p >= lo && p < hi) g = cc[k] < hot ? s_hot[cc[k]] : ld_gather(xt + cc[k], pol_g);
         out[k] = W ? wv[k] * g : g;
     }
 }
@@ -179,15 +187,16 @@ __device__ __forceinline__ void quad(const IterArgs &a, uint32_t base, uint32_t 
 // Warp: stage products of arcs [lo, hi) (hi - lo <= kWarpBuf) into buf[p - lo].
 template <int MODE, bool W>
 __device__ __forceinline__ void stage(const IterArgs &a, uint32_t lo, uint32_t hi, typename ModeT<MODE>::A *buf,
-                                      uint32_t lane, uint64_t pol_s, uint64_t pol_g) {
+                                      uint32_t lane, uint64_t pol_s, uint64_t pol_g,
+                                      const typename ModeT<MODE>::A *s_hot, uint32_t hot) {
     using A = typename ModeT<MODE>::A;
     const uint32_t a0 = lo & ~3u;
     const uint32_t nvec = (hi - a0 + 3u) >> 2;
     uint32_t vi = lane;
     for (; vi + 32 < nvec; vi += 64) {
         A g0[4], g1[4];
-        quad<MODE, W>(a, a0 + 4u * vi, lo, hi, pol_s, pol_g, g0);
-        quad<MODE, W>(a, a0 + 4u * (vi + 32), lo, hi, pol_s, pol_g, g1);
+        quad<MODE, W>(a, a0 + 4u * vi, lo, hi, pol_s, pol_g, s_hot, hot, g0);
+        quad<MODE, W>(a, a0 + 4u * (vi + 32), lo, hi, pol_s, pol_g, s_hot, hot, g1);
 #pragma unroll
         for (int k = 0; k < 4; k++) {
             uint32_t p = a0 + 4u * vi + k;
@@ -198,7 +207,7 @@ __device__ __forceinline__ void stage(const IterArgs &a, uint32_t lo, uint32_t h
     }
     if (vi < nvec) {
         A g0[4];
-        quad<MODE, W>(a, a0 + 4u * vi, lo, hi, pol_s, pol_g, g0);
+        quad<MODE, W>(a, a0 + 4u * vi, lo, hi, pol_s, pol_g, s_hot, hot, g0);
 #pragma unroll
         for (int k = 0; k < 4; k++) {
             const uint32_t p = a0 + 4u * vi + k;
@@ -207,40 +216,66 @@ __device__ __forceinline__ void stage(const IterArgs &a, uint32_t lo, uint32_t h
     }
 }
 
+__device__ __forceinline__ void comp_add(float &acc, float &c, float x) {
+    const float y = __fsub_rn(x, c);
+    const float t = __fadd_rn(acc, y);
+    c = __fsub_rn(__fsub_rn(t, acc), y);
+    acc = t;
+}
+__device__ __forceinline__ void comp_add(double &acc, double &, double x) { acc += x; }
+
 // Warp: sum of products of arcs [lo, hi) (any length), result in every lane.
+// FP32 lanes accumulate with Kahan compensation so long (hub) rows keep
+// ~1-ulp sums; FP64 lanes add plainly.
 template <int MODE, bool W>
 __device__ __forceinline__ typename ModeT<MODE>::A warp_row_sum(const IterArgs &a, uint32_t lo, uint32_t hi,
-                                                                 uint32_t lane, uint64_t pol_s, uint64_t pol_g) {
+                                                                 uint32_t lane, uint64_t pol_s, uint64_t pol_g,
+                                                                 const typename ModeT<MODE>::A *s_hot,
+                                                                 uint32_t hot) {
     using A = typename ModeT<MODE>::A;
     const uint32_t a0 = lo & ~3u;
     const uint32_t nvec = (hi - a0 + 3u) >> 2;
-    A acc0 = A(0), acc1 = A(0);
+    A acc0 = A(0), acc1 = A(0), c0 = A(0), c1 = A(0);
     uint32_t vi = lane;
     for (; vi + 32 < nvec; vi += 64) {
         A g0[4], g1[4];
-        quad<MODE, W>(a, a0 + 4u * vi, lo, hi, pol_s, pol_g, g0);
-        quad<MODE, W>(a, a0 + 4u * (vi + 32), lo, hi, pol_s, pol_g, g1);
-        acc0 += (g0[0] + g0[1]) + (g0[2] + g0[3]);
-        acc1 += (g1[0] + g1[1]) + (g1[2] + g1[3]);
+        quad<MODE, W>(a, a0 + 4u * vi, lo, hi, pol_s, pol_g, s_hot, hot, g0);
+        quad<MODE, W>(a, a0 + 4u * (vi + 32), lo, hi, pol_s, pol_g, s_hot, hot, g1);
+        comp_add(acc0, c0, (g0[0] + g0[1]) + (g0[2] + g0[3]));
+        comp_add(acc1, c1, (g1[0] + g1[1]) + (g1[2] + g1[3]));
     }
     if (vi < nvec) {
         A g0[4];
-        quad<MODE, W>(a, a0 + 4u * vi, lo, hi, pol_s, pol_g, g0);
-        acc0 += (g0[0] + g0[1]) + (g0[2] + g0[3]);
+        quad<MODE, W>(a, a0 + 4u * vi, lo, hi, pol_s, pol_g, s_hot, hot, g0);
+        comp_add(acc0, c0, (g0[0] + g0[1]) + (g0[2] + g0[3]));
     }
-    return warp_sum(acc0 + acc1);
+    return warp_sum((acc0 - c0) + (acc1 - c1));
 }
 
-template <int MODE, bool W>
-__global__ void __launch_bounds__(kThreads) iter_kernel(const IterArgs a) {
+// Dynamic shared memory layout: [NT/32 warp buffers of kWarpBuf][hot prefix].
+template <int MODE, bool W, int NT>
+__global__ void __launch_bounds__(NT) iter_kernel(const IterArgs a) {
     using A = typename ModeT<MODE>::A;
-    __shared__ A s_buf[kWarps][kWarpBuf];
+    constexpr int kW = NT / 32;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    A *s_buf = reinterpret_cast<A *>(smem_raw);
+    A *s_hot = s_buf + kW * kWarpBuf;
     __shared__ double s_red[96];
     __shared__ int s_flag;
 
     Ctl *ctl = a.ctl;
     if constexpr (MODE != MODE_RESID64) {
         if (*(volatile int32_t *)&ctl->done) return;
+    }
+    const uint32_t hot = a.hot;
+    if (hot) {
+        // hot prefix of the gathered vector -> shared memory (16-byte loads;
+        // hot is a multiple of 4 and the vector is 256-byte aligned)
+        const A *xt = gather_src<MODE>(a);
+        constexpr int kPer = 16 / sizeof(A);
+        for (uint32_t i = threadIdx.x * kPer; i < hot; i += NT * kPer)
+            *reinterpret_cast<uint4 *>(s_hot + i) = __ldcg(reinterpret_cast<const uint4 *>(xt + i));
+        __syncthreads();
     }
     const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     Uni u;
@@ -252,18 +287,18 @@ __global__ void __launch_bounds__(kThreads) iter_kernel(const IterArgs a) {
         u.dshare = __ddiv_rn(__dmul_rn(u.d, u.dsum), nf);
     }
     const uint64_t pol_s = policy_evict_first(), pol_g = policy_evict_last();
-    A *buf = s_buf[warp];
+    A *buf = s_buf + warp * kWarpBuf;
     double pd = 0.0, pds = 0.0, ps = 0.0;
 
-    const uint32_t stride = gridDim.x * kWarps;
-    uint32_t rb = blockIdx.x * kWarps + warp;
+    const uint32_t stride = gridDim.x * kW;
+    uint32_t rb = blockIdx.x * kW + warp;
     uint4 d = rb < a.nrb ? __ldg(&a.rb[rb]) : make_uint4(0, 0, 0, 0);
     while (rb < a.nrb) {
         const uint32_t nxt = rb + stride;
         const uint4 dn = nxt < a.nrb ? __ldg(&a.rb[nxt]) : make_uint4(0, 0, 0, 0);
         if (d.y & kChunkFlag) {
             // slice of a hub row
-            const A s = warp_row_sum<MODE, W>(a, d.z, d.w, lane, pol_s, pol_g);
+            const A s = warp_row_sum<MODE, W>(a, d.z, d.w, lane, pol_s, pol_g, s_hot, hot);
             if (lane == 0) {
                 const uint32_t h = d.y & ~kChunkFlag;
                 const Hub hb = a.hubs[h];
@@ -285,32 +320,39 @@ __global__ void __launch_bounds__(kThreads) iter_kernel(const IterArgs a) {
             // a single row: whole warp
             Pre pr;
             if (lane == 0) pr = epi_load<MODE>(a, d.x);
-            const A s = warp_row_sum<MODE, W>(a, d.z, d.w, lane, pol_s, pol_g);
+            const A s = warp_row_sum<MODE, W>(a, d.z, d.w, lane, pol_s, pol_g, s_hot, hot);
             if (lane == 0) epilogue<MODE>(a, u, d.x, s, pr, pd, pds, ps);
         } else {
-            // up to 32 short rows, one lane each
-            const uint32_t r0 = d.x, p0 = d.z;
-            const bool has_row = lane < d.y - r0;
-            const uint32_t v = r0 + lane;
+            // 2..32 rows with < kWarpBuf arcs in total: products are staged in
+            // the warp's buffer, then each row is summed by a group of tpr
+            // lanes (the largest power of two with tpr * rows <= 32)
+            const uint32_t r0 = d.x, p0 = d.z, nrows = d.y - r0;
+            uint32_t tpr = 32;
+            while (tpr > 1 && tpr * nrows > 32) tpr >>= 1;
+            const uint32_t grp = lane / tpr, gl = lane % tpr;
+            const bool has_row = grp < nrows;
+            const uint32_t v = r0 + grp;
             uint32_t rs = 0, re = 0;
             Pre pr;
             if (has_row) {
                 rs = __ldg(&a.row_ptr[v]) - p0;
                 re = __ldg(&a.row_ptr[v + 1]) - p0;
-                pr = epi_load<MODE>(a, v);
+                if (gl == 0) pr = epi_load<MODE>(a, v);
             }
-            stage<MODE, W>(a, p0, d.w, buf, lane, pol_s, pol_g);
+            stage<MODE, W>(a, p0, d.w, buf, lane, pol_s, pol_g, s_hot, hot);
             __syncwarp();
+            A acc0 = A(0), acc1 = A(0);
             if (has_row) {
-                A acc0 = A(0), acc1 = A(0);
-                uint32_t j = rs;
-                for (; j + 1 < re; j += 2) {
+                uint32_t j = rs + gl;
+                for (; j + tpr < re; j += 2 * tpr) {
                     acc0 += buf[j];
-                    acc1 += buf[j + 1];
+                    acc1 += buf[j + tpr];
                 }
                 if (j < re) acc0 += buf[j];
-                epilogue<MODE>(a, u, v, acc0 + acc1, pr, pd, pds, ps);
             }
+            A acc = acc0 + acc1;
+            for (uint32_t o = tpr >> 1; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+            if (has_row && gl == 0) epilogue<MODE>(a, u, v, acc, pr, pd, pds, ps);
             __syncwarp();
         }
         rb = nxt;
@@ -369,34 +411,67 @@ __global__ void __launch_bounds__(kThreads) iter_kernel(const IterArgs a) {
     }
 }
 
-template <int MODE, bool W>
-static unsigned grid_of(uint32_t blocks_per_sm) {
-    static int sms = 0, occ = 0;
+template <int MODE, bool W, int NT>
+static void kernel_config(bool big, uint32_t blocks_per_sm, uint32_t n, LaunchCfg &c) {
+    using A = typename ModeT<MODE>::A;
+    static int sms = 0, smem_optin = 0;
     if (sms == 0) {
         int dev = 0;
         PRG_CUDA(cudaGetDevice(&dev));
         PRG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        PRG_CUDA(cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
     }
-    if (occ == 0) PRG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, iter_kernel<MODE, W>, kThreads, 0));
+    const size_t bufs = (size_t)(NT / 32) * kWarpBuf * sizeof(A);
+    size_t hot = 0;
+    if (big) {
+        // leave room for the kernel's static shared memory (reduction scratch)
+        const size_t avail = (size_t)smem_optin - bufs - 2048;
+        hot = std::min<size_t>(avail / sizeof(A), n) & ~(size_t)3;
+    }
+    c.smem = bufs + hot * sizeof(A);
+    c.hot = (uint32_t)hot;
+    c.threads = NT;
+    PRG_CUDA(cudaFuncSetAttribute(iter_kernel<MODE, W, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c.smem));
+    int occ = 0;
+    PRG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, iter_kernel<MODE, W, NT>, NT, c.smem));
     int per = occ > 0 ? occ : 1;
     if (blocks_per_sm > 0 && (int)blocks_per_sm < per) per = (int)blocks_per_sm;
-    return (unsigned)(sms * per);
+    c.grid = (unsigned)(sms * per);
 }
 
-unsigned iteration_grid(int mode, bool weighted, uint32_t bps) {
-    switch (mode) {
-        case MODE_PLAIN64: return weighted ? grid_of<MODE_PLAIN64, true>(bps) : grid_of<MODE_PLAIN64, false>(bps);
-        case MODE_PPR64: return weighted ? grid_of<MODE_PPR64, true>(bps) : grid_of<MODE_PPR64, false>(bps);
-        case MODE_RESID64: return weighted ? grid_of<MODE_RESID64, true>(bps) : grid_of<MODE_RESID64, false>(bps);
-        default: return weighted ? grid_of<MODE_CORR32, true>(bps) : grid_of<MODE_CORR32, false>(bps);
+LaunchCfg iteration_config(int mode, bool weighted, bool hot_cache, uint32_t blocks_per_sm, uint32_t n) {
+    LaunchCfg c;
+#define PRG_CFG(M)                                                                              \
+    if (hot_cache) {                                                                            \
+        if (weighted) kernel_config<M, true, kThreadsBig>(true, blocks_per_sm, n, c);           \
+        else kernel_config<M, false, kThreadsBig>(true, blocks_per_sm, n, c);                   \
+    } else {                                                                                    \
+        if (weighted) kernel_config<M, true, kThreads>(false, blocks_per_sm, n, c);             \
+        else kernel_config<M, false, kThreads>(false, blocks_per_sm, n, c);                     \
     }
+    switch (mode) {
+        case MODE_PLAIN64: PRG_CFG(MODE_PLAIN64); break;
+        case MODE_PPR64: PRG_CFG(MODE_PPR64); break;
+        case MODE_RESID64: PRG_CFG(MODE_RESID64); break;
+        default: PRG_CFG(MODE_CORR32); break;
+    }
+#undef PRG_CFG
+    return c;
 }
 
-void launch_iteration(int mode, bool weighted, const IterArgs &a, unsigned grid, cudaStream_t s) {
-    const dim3 block(kThreads);
-#define PRG_LAUNCH(M)                                                           \
-    if (weighted) iter_kernel<M, true><<<grid, block, 0, s>>>(a);               \
-    else iter_kernel<M, false><<<grid, block, 0, s>>>(a);
+void launch_iteration(int mode, bool weighted, const IterArgs &a_in, const LaunchCfg &c, cudaStream_t s) {
+    IterArgs a = a_in;
+    a.hot = c.hot;
+    const dim3 grid(c.grid), block(c.threads);
+    const bool big = c.threads == kThreadsBig;
+#define PRG_LAUNCH(M)                                                                          \
+    if (big) {                                                                                 \
+        if (weighted) iter_kernel<M, true, kThreadsBig><<<grid, block, c.smem, s>>>(a);        \
+        else iter_kernel<M, false, kThreadsBig><<<grid, block, c.smem, s>>>(a);                \
+    } else {                                                                                   \
+        if (weighted) iter_kernel<M, true, kThreads><<<grid, block, c.smem, s>>>(a);           \
+        else iter_kernel<M, false, kThreads><<<grid, block, c.smem, s>>>(a);                   \
+    }
     switch (mode) {
         case MODE_PLAIN64: PRG_LAUNCH(MODE_PLAIN64); break;
         case MODE_PPR64: PRG_LAUNCH(MODE_PPR64); break;

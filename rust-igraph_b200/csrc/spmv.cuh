@@ -33,7 +33,8 @@ struct IterArgs {
     const float *inv32;
     const uint4 *rb;
     const Hub *hubs;
-    uint32_t nrb, nhub, n, pad0;
+    uint32_t nrb, nhub, n;
+    uint32_t hot;  // sources below this id are gathered from the shared-memory hot prefix (set at launch)
     // vectors (FP64 modes use the *64 pointers, CORR32 the *32 ones)
     const double *xt64_in;
     const double *x64_in;
@@ -59,10 +60,20 @@ struct IterArgs {
     int parity;
 };
 
-// Persistent grid of the iteration kernel for this device (SMs x resident
-// blocks per SM, or SMs x blocks_per_sm when nonzero).
-unsigned iteration_grid(int mode, bool weighted, uint32_t blocks_per_sm);
-void launch_iteration(int mode, bool weighted, const IterArgs &a, unsigned grid, cudaStream_t s);
+constexpr int kThreadsBig = 1024;  // one block per SM with the shared-memory hot prefix
+
+struct LaunchCfg {
+    unsigned grid = 0;
+    int threads = kThreads;
+    size_t smem = 0;   // dynamic shared memory (warp buffers + hot prefix)
+    uint32_t hot = 0;  // hot-prefix length (vertices)
+};
+
+// Persistent launch shape of the iteration kernel on this device: either
+// 256-thread blocks at full occupancy, or (hot_cache) one 1024-thread block
+// per SM whose remaining shared memory caches the rank vector's hot prefix.
+LaunchCfg iteration_config(int mode, bool weighted, bool hot_cache, uint32_t blocks_per_sm, uint32_t n);
+void launch_iteration(int mode, bool weighted, const IterArgs &a, const LaunchCfg &c, cudaStream_t s);
 
 // x <- x + e (e may be null), xt <- x / dval, dangling sum and total sum of
 // x into ctl->dsum[parity] / ctl->gsum via a deterministic two-level tree.

@@ -79,6 +79,11 @@ class prg_stats(C.Structure):
                 ("fp32_ms", C.c_double), ("fp64_ms", C.c_double)]
 
 
+class prg_batch_stats(C.Structure):
+    _fields_ = [("column_iterations", C.c_uint64), ("max_iters", C.c_uint32), ("tiles", C.c_uint32),
+                ("tile_width", C.c_uint32), ("kernel_launches", C.c_uint32), ("ms", C.c_double)]
+
+
 _lib = None
 
 
@@ -128,6 +133,11 @@ def lib():
     L.prg_set_tuning.argtypes = [C.c_char_p, C.c_int64]
     L.prg_graph_relabelled.restype = C.c_int32
     L.prg_graph_relabelled.argtypes = [vp]
+    for name in ("prg_ppr_batch", "prg_ppr_batch_device"):
+        f = getattr(L, name)
+        f.restype = C.c_int32
+        f.argtypes = [vp, C.c_uint32, vp, vp, C.c_double, C.c_double, C.c_uint32, C.c_uint32, vp, vp,
+                      C.POINTER(prg_batch_stats)]
     L.prg_rmat_device.restype = C.c_int32
     L.prg_rmat_device.argtypes = [C.c_uint32, C.c_uint64, C.c_double, C.c_double, C.c_double, C.c_uint64,
                                   vp, vp, vp]
@@ -394,6 +404,30 @@ class DeviceGraph:
                                       C.c_void_p(d_out), C.byref(st)))
         return Stats.from_c(st)
 
+    def ppr_batch(self, seed_lists, damping: float = 0.85, tol: float = 1e-8, max_iter: int = 1000,
+                  vec: int = 0, d_out: int = 0):
+        """Batched personalized PageRank (one column per seed list, like
+        personalized_pagerank_vs).  Returns (X float32[n, K] or None when
+        d_out is given, column_iters uint32[K], stats dict)."""
+        K = len(seed_lists)
+        off = np.zeros(K + 1, np.uint64)
+        off[1:] = np.cumsum([len(x) for x in seed_lists])
+        seeds = np.ascontiguousarray(np.concatenate([np.asarray(x, np.uint32) for x in seed_lists])
+                                     if K else np.zeros(1, np.uint32), dtype=np.uint32)
+        iters = np.zeros(max(K, 1), np.uint32)
+        st = prg_batch_stats()
+        if d_out:
+            _check(lib().prg_ppr_batch_device(self._h, K, _ptr(off), _ptr(seeds), damping, tol, max_iter, vec,
+                                              C.c_void_p(d_out), _ptr(iters), C.byref(st)))
+            X = None
+        else:
+            X = np.empty((self.n, K), np.float32)
+            _check(lib().prg_ppr_batch(self._h, K, _ptr(off), _ptr(seeds), damping, tol, max_iter, vec, _ptr(X),
+                                       _ptr(iters), C.byref(st)))
+        stats = {"column_iterations": st.column_iterations, "max_iters": st.max_iters, "tiles": st.tiles,
+                 "tile_width": st.tile_width, "kernel_launches": st.kernel_launches, "ms": st.ms}
+        return X, iters[:K], stats
+
     def close(self):
         if self._h:
             lib().prg_graph_destroy(self._h)
@@ -417,7 +451,8 @@ def set_tuning(key: str, value: int) -> None:
     _check(lib().prg_set_tuning(key.encode(), int(value)))
 
 
-TUNING_DEFAULTS = {"capw": 448, "shortmax": 64, "split": 8192, "blocks_per_sm": 0, "relabel": 2, "unroll": 8}
+TUNING_DEFAULTS = {"capw": 256, "shortmax": 256, "split": 8192, "blocks_per_sm": 0, "relabel": 2, "unroll": 8,
+                   "hot_cache": 0, "refine_switch_e12": 500000, "batch_vec": 1}
 
 
 def reset_tuning() -> None:
