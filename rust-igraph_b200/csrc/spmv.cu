@@ -79,38 +79,42 @@ struct Uni {
 
 // Epilogue operands of one row, loaded before the row's gathers so their
 // latency overlaps them.
+template <int MODE>
 struct Pre {
     double old, dv, t;
-    float iv, b;
+    float iv;
+};
+template <>
+struct Pre<MODE_CORR32> {
+    float old, t, iv, b;
 };
 
 template <int MODE>
-__device__ __forceinline__ Pre epi_load(const IterArgs &a, uint32_t v) {
-    Pre p;
+__device__ __forceinline__ Pre<MODE> epi_load(const IterArgs &a, uint32_t v) {
+    Pre<MODE> p;
     if constexpr (MODE == MODE_CORR32) {
         p.old = a.x32_in[v];
         p.b = a.b32[v];
         p.iv = a.inv32[v];
-        p.t = a.t32 ? (double)a.t32[v] : a.inv_n;
-        p.dv = 0.0;
+        p.t = a.t32 ? a.t32[v] : (float)a.inv_n;
     } else {
         p.old = a.x64_in[v];
         p.dv = a.dval[v];
         p.t = a.t64 ? a.t64[v] : 0.0;
-        p.iv = (MODE == MODE_RESID64) ? a.inv32[v] : 0.0f;
-        p.b = 0.0f;
+        if constexpr (MODE == MODE_RESID64) p.iv = a.inv32[v];
+        else p.iv = 0.0f;
     }
     return p;
 }
 
 template <int MODE>
 __device__ __forceinline__ void epilogue(const IterArgs &a, const Uni &u, uint32_t v, typename ModeT<MODE>::A y,
-                                         const Pre &p, double &pd, double &pds, double &ps) {
+                                         const Pre<MODE> &p, double &pd, double &pds, double &ps) {
     if constexpr (MODE == MODE_CORR32) {
         const float df = (float)u.d;
-        const float out = df * y + ((float)(u.d * u.dsum)) * (float)p.t + p.b;
+        const float out = df * y + ((float)(u.d * u.dsum)) * p.t + p.b;
         a.x32_out[v] = out;
-        pd += fabs((double)out - p.old);
+        pd += fabs((double)out - (double)p.old);
         a.xt32_out[v] = out * p.iv;
         if (p.iv == 0.0f) pds += (double)out;
     } else {
@@ -156,12 +160,14 @@ __device__ __forceinline__ const typename ModeT<MODE>::A *gather_src(const IterA
 // ids put the most-gathered vertices there): a warp's random shared-memory
 // reads cost a few bank wavefronts where the same global gathers cost about
 // one L1 wavefront per lane.
-template <int MODE, bool W>
+template <int MODE, bool W, bool HOT>
 __device__ __forceinline__ void quad(const IterArgs &a, uint32_t base, uint32_t lo, uint32_t hi, uint64_t pol_s,
                                      uint64_t pol_g, const typename ModeT<MODE>::A *s_hot, uint32_t hot,
                                      typename ModeT<MODE>::A (&out)[4]) {
     using A = typename ModeT<MODE>::A;
     const A *xt = gather_src<MODE>(a);
+    pol_s = policy_evict_first();
+    pol_g = policy_evict_last();
     const uint4 c = ld_stream_u4(reinterpret_cast<const uint4 *>(a.col + base), pol_s);
     const uint32_t cc[4] = {c.x, c.y, c.z, c.w};
     A wv[4] = {A(1), A(1), A(1), A(1)};
@@ -179,13 +185,16 @@ __device__ __forceinline__ void quad(const IterArgs &a, uint32_t base, uint32_t 
     for (int k = 0; k < 4; k++) {
         const uint32_t p = base + k;
         A g = A(0);
-        if (p >= lo && p < hi) g = cc[k] < hot ? s_hot[cc[k]] : ld_gather(xt + cc[k], pol_g);
+        if (p >= lo && p < hi) {
+            if constexpr (HOT) g = cc[k] < hot ? s_hot[cc[k]] : ld_gather(xt + cc[k], pol_g);
+            else g = ld_gather(xt + cc[k], pol_g);
+        }
         out[k] = W ? wv[k] * g : g;
     }
 }
 
 // Warp: stage products of arcs [lo, hi) (hi - lo <= kWarpBuf) into buf[p - lo].
-template <int MODE, bool W>
+template <int MODE, bool W, bool HOT>
 __device__ __forceinline__ void stage(const IterArgs &a, uint32_t lo, uint32_t hi, typename ModeT<MODE>::A *buf,
                                       uint32_t lane, uint64_t pol_s, uint64_t pol_g,
                                       const typename ModeT<MODE>::A *s_hot, uint32_t hot) {
@@ -195,8 +204,8 @@ __device__ __forceinline__ void stage(const IterArgs &a, uint32_t lo, uint32_t h
     uint32_t vi = lane;
     for (; vi + 32 < nvec; vi += 64) {
         A g0[4], g1[4];
-        quad<MODE, W>(a, a0 + 4u * vi, lo, hi, pol_s, pol_g, s_hot, hot, g0);
-        quad<MODE, W>(a, a0 + 4u * (vi + 32), lo, hi, pol_s, pol_g, s_hot, hot, g1);
+        quad<MODE, W, HOT>(a, a0 + 4u * vi, lo, hi, pol_s, pol_g, s_hot, hot, g0);
+        quad<MODE, W, HOT>(a, a0 + 4u * (vi + 32), lo, hi, pol_s, pol_g, s_hot, hot, g1);
 #pragma unroll
         for (int k = 0; k < 4; k++) {
             uint32_t p = a0 + 4u * vi + k;
@@ -207,7 +216,7 @@ __device__ __forceinline__ void stage(const IterArgs &a, uint32_t lo, uint32_t h
     }
     if (vi < nvec) {
         A g0[4];
-        quad<MODE, W>(a, a0 + 4u * vi, lo, hi, pol_s, pol_g, s_hot, hot, g0);
+        quad<MODE, W, HOT>(a, a0 + 4u * vi, lo, hi, pol_s, pol_g, s_hot, hot, g0);
 #pragma unroll
         for (int k = 0; k < 4; k++) {
             const uint32_t p = a0 + 4u * vi + k;
@@ -227,7 +236,7 @@ __device__ __forceinline__ void comp_add(double &acc, double &, double x) { acc 
 // Warp: sum of products of arcs [lo, hi) (any length), result in every lane.
 // FP32 lanes accumulate with Kahan compensation so long (hub) rows keep
 // ~1-ulp sums; FP64 lanes add plainly.
-template <int MODE, bool W>
+template <int MODE, bool W, bool HOT>
 __device__ __forceinline__ typename ModeT<MODE>::A warp_row_sum(const IterArgs &a, uint32_t lo, uint32_t hi,
                                                                  uint32_t lane, uint64_t pol_s, uint64_t pol_g,
                                                                  const typename ModeT<MODE>::A *s_hot,
@@ -239,14 +248,14 @@ __device__ __forceinline__ typename ModeT<MODE>::A warp_row_sum(const IterArgs &
     uint32_t vi = lane;
     for (; vi + 32 < nvec; vi += 64) {
         A g0[4], g1[4];
-        quad<MODE, W>(a, a0 + 4u * vi, lo, hi, pol_s, pol_g, s_hot, hot, g0);
-        quad<MODE, W>(a, a0 + 4u * (vi + 32), lo, hi, pol_s, pol_g, s_hot, hot, g1);
+        quad<MODE, W, HOT>(a, a0 + 4u * vi, lo, hi, pol_s, pol_g, s_hot, hot, g0);
+        quad<MODE, W, HOT>(a, a0 + 4u * (vi + 32), lo, hi, pol_s, pol_g, s_hot, hot, g1);
         comp_add(acc0, c0, (g0[0] + g0[1]) + (g0[2] + g0[3]));
         comp_add(acc1, c1, (g1[0] + g1[1]) + (g1[2] + g1[3]));
     }
     if (vi < nvec) {
         A g0[4];
-        quad<MODE, W>(a, a0 + 4u * vi, lo, hi, pol_s, pol_g, s_hot, hot, g0);
+        quad<MODE, W, HOT>(a, a0 + 4u * vi, lo, hi, pol_s, pol_g, s_hot, hot, g0);
         comp_add(acc0, c0, (g0[0] + g0[1]) + (g0[2] + g0[3]));
     }
     return warp_sum((acc0 - c0) + (acc1 - c1));
@@ -254,9 +263,10 @@ __device__ __forceinline__ typename ModeT<MODE>::A warp_row_sum(const IterArgs &
 
 // Dynamic shared memory layout: [NT/32 warp buffers of kWarpBuf][hot prefix].
 template <int MODE, bool W, int NT>
-__global__ void __launch_bounds__(NT) iter_kernel(const IterArgs a) {
+__global__ void __launch_bounds__(NT, NT == kThreads ? (MODE == MODE_CORR32 ? 5 : 4) : 1) iter_kernel(const IterArgs a) {
     using A = typename ModeT<MODE>::A;
     constexpr int kW = NT / 32;
+    constexpr bool HOT = NT == kThreadsBig;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     A *s_buf = reinterpret_cast<A *>(smem_raw);
     A *s_hot = s_buf + kW * kWarpBuf;
@@ -267,8 +277,8 @@ __global__ void __launch_bounds__(NT) iter_kernel(const IterArgs a) {
     if constexpr (MODE != MODE_RESID64) {
         if (*(volatile int32_t *)&ctl->done) return;
     }
-    const uint32_t hot = a.hot;
-    if (hot) {
+    const uint32_t hot = HOT ? a.hot : 0u;
+    if (HOT && hot) {
         // hot prefix of the gathered vector -> shared memory (16-byte loads;
         // hot is a multiple of 4 and the vector is 256-byte aligned)
         const A *xt = gather_src<MODE>(a);
@@ -286,7 +296,7 @@ __global__ void __launch_bounds__(NT) iter_kernel(const IterArgs a) {
         u.tele = __ddiv_rn(1.0 - u.d, nf);
         u.dshare = __ddiv_rn(__dmul_rn(u.d, u.dsum), nf);
     }
-    const uint64_t pol_s = policy_evict_first(), pol_g = policy_evict_last();
+    const uint64_t pol_s = 0, pol_g = 0;  // created next to each load (saves registers)
     A *buf = s_buf + warp * kWarpBuf;
     double pd = 0.0, pds = 0.0, ps = 0.0;
 
@@ -298,7 +308,7 @@ __global__ void __launch_bounds__(NT) iter_kernel(const IterArgs a) {
         const uint4 dn = nxt < a.nrb ? __ldg(&a.rb[nxt]) : make_uint4(0, 0, 0, 0);
         if (d.y & kChunkFlag) {
             // slice of a hub row
-            const A s = warp_row_sum<MODE, W>(a, d.z, d.w, lane, pol_s, pol_g, s_hot, hot);
+            const A s = warp_row_sum<MODE, W, HOT>(a, d.z, d.w, lane, pol_s, pol_g, s_hot, hot);
             if (lane == 0) {
                 const uint32_t h = d.y & ~kChunkFlag;
                 const Hub hb = a.hubs[h];
@@ -310,7 +320,7 @@ __global__ void __launch_bounds__(NT) iter_kernel(const IterArgs a) {
                     double y = 0.0;
                     for (uint32_t j = 0; j < hb.nchunks; j++) y += __ldcg(&a.chunk_part[hb.first_rb + j]);
                     double hd = 0.0, hds = 0.0, hs = 0.0;
-                    const Pre pr = epi_load<MODE>(a, hb.row);
+                    const Pre<MODE> pr = epi_load<MODE>(a, hb.row);
                     epilogue<MODE>(a, u, hb.row, (A)y, pr, hd, hds, hs);
                     a.hub_rec[h] = make_double4(hd, hds, hs, 0.0);
                     a.hub_ticket[h] = 0u;
@@ -318,9 +328,9 @@ __global__ void __launch_bounds__(NT) iter_kernel(const IterArgs a) {
             }
         } else if (d.y - d.x == 1u) {
             // a single row: whole warp
-            Pre pr;
+            Pre<MODE> pr;
             if (lane == 0) pr = epi_load<MODE>(a, d.x);
-            const A s = warp_row_sum<MODE, W>(a, d.z, d.w, lane, pol_s, pol_g, s_hot, hot);
+            const A s = warp_row_sum<MODE, W, HOT>(a, d.z, d.w, lane, pol_s, pol_g, s_hot, hot);
             if (lane == 0) epilogue<MODE>(a, u, d.x, s, pr, pd, pds, ps);
         } else {
             // 2..32 rows with < kWarpBuf arcs in total: products are staged in
@@ -333,13 +343,13 @@ __global__ void __launch_bounds__(NT) iter_kernel(const IterArgs a) {
             const bool has_row = grp < nrows;
             const uint32_t v = r0 + grp;
             uint32_t rs = 0, re = 0;
-            Pre pr;
+            Pre<MODE> pr;
             if (has_row) {
                 rs = __ldg(&a.row_ptr[v]) - p0;
                 re = __ldg(&a.row_ptr[v + 1]) - p0;
                 if (gl == 0) pr = epi_load<MODE>(a, v);
             }
-            stage<MODE, W>(a, p0, d.w, buf, lane, pol_s, pol_g, s_hot, hot);
+            stage<MODE, W, HOT>(a, p0, d.w, buf, lane, pol_s, pol_g, s_hot, hot);
             __syncwarp();
             A acc0 = A(0), acc1 = A(0);
             if (has_row) {
