@@ -185,6 +185,21 @@ int32_t prg_ppr_batch_device(prg_graph *g, uint32_t K, const uint64_t *seed_offs
                              double damping, double tol, uint32_t max_iter, uint32_t tile_vec, float *d_out,
                              uint32_t *column_iters, prg_batch_stats *stats);
 
+/* Allocation-free FP64 solve (no counterpart in the reference; an addition
+ * for callers that must not allocate device memory at solve time, such as a
+ * real-time loop that reserves memory up front or code running under another
+ * framework's memory budget).  Same iteration and stop rule as prg_solve at
+ * PRG_PRECISION_FP64 on a graph created earlier; d_reset: optional
+ * normalised teleport vector, d_out: double[n], both device memory in caller
+ * ids.  All solve scratch lives in one static device array (about 26.6 MiB
+ * per GPU, held until exit); limits: n <= 524,288, <= 262,144 row-blocks,
+ * <= 8,192 hub rows, FP64 only (else PRG_ERR_INVALID_ARGUMENT).  The first
+ * call on a device looks up the array's address (cudaGetSymbolAddress):
+ * make it before any stream capture.  Calls share the array, so calls that
+ * overlap on the GPU race; run them one at a time. */
+int32_t prg_solve_noalloc(prg_graph *g, const prg_options *opt, const double *d_reset, double *d_out,
+                          prg_stats *stats);
+
 /* Message of the last error on this thread ("" if none). */
 const char *prg_last_error(void);
 

@@ -18,17 +18,9 @@
 
 #include "../../include/prg_b200.h"
 #include "graph.cuh"
+#include "handle.cuh"
 #include "ppr_batch.cuh"
 #include "solver.cuh"
-
-struct prg_graph {
-    prg::DeviceGraph g;
-    prg::Workspace ws;
-    cudaStream_t stream = nullptr;
-    double *d_reset = nullptr;  // normalised reset staging (n doubles)
-    double *d_out = nullptr;    // output staging (n doubles)
-    double *d_start = nullptr;  // warm-start staging
-};
 
 namespace {
 
@@ -38,6 +30,15 @@ int32_t fail(int32_t code, const std::string &msg) {
     g_err = msg;
     return code;
 }
+
+}  // namespace
+
+namespace prg {
+// Lets entry points defined in other files report through prg_last_error().
+void set_last_error(const std::string &msg) { g_err = msg; }
+}  // namespace prg
+
+namespace {
 
 int32_t from_cuda(const prg::CudaError &e) {
     if (e.err == cudaErrorMemoryAllocation) return fail(PRG_ERR_OUT_OF_MEMORY, "cuda: out of memory");

@@ -138,6 +138,8 @@ def lib():
         f.restype = C.c_int32
         f.argtypes = [vp, C.c_uint32, vp, vp, C.c_double, C.c_double, C.c_uint32, C.c_uint32, vp, vp,
                       C.POINTER(prg_batch_stats)]
+    L.prg_solve_noalloc.restype = C.c_int32
+    L.prg_solve_noalloc.argtypes = [vp, C.POINTER(prg_options), vp, vp, C.POINTER(prg_stats)]
     L.prg_rmat_device.restype = C.c_int32
     L.prg_rmat_device.argtypes = [C.c_uint32, C.c_uint64, C.c_double, C.c_double, C.c_double, C.c_uint64,
                                   vp, vp, vp]
@@ -402,6 +404,16 @@ class DeviceGraph:
         co = o.to_c(C.c_void_p(d_start) if d_start else None)
         _check(lib().prg_solve_device(self._h, C.byref(co), C.c_void_p(d_reset) if d_reset else None,
                                       C.c_void_p(d_out), C.byref(st)))
+        return Stats.from_c(st)
+
+    def solve_noalloc(self, d_out: int, options: Optional[Options] = None, d_reset: int = 0):
+        """FP64 solve into a device buffer with no device allocation inside
+        the call (prg_solve_noalloc); d_reset: normalised teleport vector."""
+        o = options or Options()
+        st = prg_stats()
+        co = o.to_c(None)
+        _check(lib().prg_solve_noalloc(self._h, C.byref(co), C.c_void_p(d_reset) if d_reset else None,
+                                       C.c_void_p(d_out), C.byref(st)))
         return Stats.from_c(st)
 
     def ppr_batch(self, seed_lists, damping: float = 0.85, tol: float = 1e-8, max_iter: int = 1000,
