@@ -48,6 +48,7 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-plain", action="store_true")
     p.add_argument("--cpu-iters", type=int, default=2)
+    p.add_argument("--no-autotune", action="store_true")
     return p.parse_args()
 
 
@@ -254,6 +255,7 @@ def main():
     torch.cuda.synchronize()
     dg = ig.DeviceGraph.from_device(n, m, df.data_ptr(), dt.data_ptr(), True)
     arcs = dg.arcs
+    tune = None if args.no_autotune else dg.autotune(batch=False)
     stream = torch.cuda.ExternalStream(dg.stream(), device=dev)
     out = torch.empty(n, dtype=torch.float64, device=dev)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)  # > L2 (126 MB)
@@ -402,6 +404,7 @@ def main():
         "residual_passes_per_solve": s0.residual_passes,
         "error_bound": s0.error_bound,
         "build_ms": dg.build_ms,
+        "autotune": tune,
         "roofline": roofline,
         "cpu_baseline": cpu,
         "e2e": e2e,

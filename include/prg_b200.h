@@ -145,6 +145,25 @@ int32_t prg_graph_relabelled(const prg_graph *g);
 int32_t prg_graph_device_csr(const prg_graph *g, const uint32_t **row_ptr, const uint32_t **col,
                              const uint32_t **perm, const float **inv32);
 
+/* ---- autotuner --------------------------------------------------------- */
+
+typedef struct prg_tune_result {
+    uint32_t capw, shortmax, split;  /* row-block shape chosen */
+    uint32_t blocks_per_sm;          /* persistent grid (0 = occupancy maximum) */
+    uint32_t batch_tile_width;       /* batched solver columns per tile */
+    uint32_t candidates;             /* configurations timed */
+    int32_t from_cache;              /* 1 if read from cache_path instead of timed */
+    uint32_t pad;
+    double default_ms, best_ms;      /* FP64 + FP32 iteration time before / after */
+} prg_tune_result;
+
+/* Times candidate row-block shapes (stream window, short-row limit, hub
+ * split), persistent-grid occupancies and (tune_batch != 0) batched tile
+ * widths on this graph with CUDA events and keeps the fastest.  cache_path
+ * (optional): a text file of earlier results keyed by (n, arcs, directed,
+ * weighted); a hit is applied without timing, a new result is appended. */
+int32_t prg_autotune(prg_graph *g, int32_t tune_batch, const char *cache_path, prg_tune_result *out);
+
 /* Process-wide tuning applied to graphs created afterwards (the autotuner's
  * knobs): "capw", "shortmax", "split" (row-block shape), "blocks_per_sm"
  * (persistent grid, 0 = occupancy maximum), "relabel" (0 off, 1 on, 2 auto on

@@ -17,6 +17,7 @@
 #include <vector>
 
 #include "../../include/prg_b200.h"
+#include "autotune.cuh"
 #include "graph.cuh"
 #include "handle.cuh"
 #include "ppr_batch.cuh"
@@ -566,7 +567,7 @@ static int32_t batch_common(prg_graph *h, uint32_t K, const uint64_t *off, const
                 return fail(PRG_ERR_INVALID_ARGUMENT, "reset vertex " + std::to_string(seeds[i]) +
                                                           " out of range (vcount = " + std::to_string(n) + ")");
     }
-    if (vec == 0) vec = prg::tuning().batch_vec;
+    if (vec == 0) vec = h->g.batch_vec ? h->g.batch_vec : prg::tuning().batch_vec;
     prg::BatchStats bs;
     const int rc = prg::ppr_batch(h->g, K, off, seeds, damping, tol, max_iter, vec, d_out, bs, h->stream);
     if (column_iters)
@@ -607,6 +608,28 @@ int32_t prg_ppr_batch(prg_graph *h, uint32_t K, const uint64_t *off, const uint3
     cudaFreeAsync(d_out, h->stream);
     PRG_CUDA(cudaStreamSynchronize(h->stream));
     return rc;
+    PRG_GUARD_END
+}
+
+int32_t prg_autotune(prg_graph *h, int32_t tune_batch, const char *cache_path, prg_tune_result *out) {
+    g_err.clear();
+    PRG_GUARD_BEGIN
+    if (!h) return fail(PRG_ERR_INVALID_ARGUMENT, "null graph handle");
+    if (h->g.n < 2) return fail(PRG_ERR_INVALID_ARGUMENT, "autotune needs vcount >= 2");
+    prg::TuneResult r;
+    prg::autotune(h->g, h->ws, h->stream, tune_batch != 0, cache_path, r);
+    if (out) {
+        out->capw = r.capw;
+        out->shortmax = r.shortmax;
+        out->split = r.split;
+        out->blocks_per_sm = r.blocks_per_sm;
+        out->batch_tile_width = 32 * r.batch_vec;
+        out->candidates = r.tried;
+        out->from_cache = r.from_cache ? 1 : 0;
+        out->default_ms = r.default_ms;
+        out->best_ms = r.best_ms;
+    }
+    return PRG_OK;
     PRG_GUARD_END
 }
 

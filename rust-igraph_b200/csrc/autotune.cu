@@ -1,0 +1,153 @@
+// autotune.cu — picks the row-block shape, the persistent-grid occupancy and
+// the batched tile width for one resident graph by timing real launches.
+//
+// Row-block shape (csr_build.cu): `capw` (stream window), `shortmax` (rows
+// up to this many arcs are summed by lane groups inside a stream block;
+// longer rows get a whole warp) and `split` (rows longer than this are cut
+// into chunks).  Each candidate is built, then the FP64 iteration and the
+// FP32 correction iteration are each timed over a few back-to-back launches
+// with CUDA events; the candidate with the smallest sum wins.  The persistent
+// grid is then tried at the occupancy maximum and at reduced blocks per SM.
+// The batched solver's tile width (32, 64 or 128 columns per tile) is timed
+// on a few iterations of 128 random single-seed columns.  A result can be
+// cached in a text file keyed by (n, arcs, directed, weighted).
+#include <cuda_runtime.h>
+
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <random>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include "autotune.cuh"
+#include "ppr_batch.cuh"
+#include "spmv.cuh"
+
+namespace prg {
+
+static std::string cache_key(const DeviceGraph &g) {
+    std::ostringstream k;
+    k << g.n << ' ' << g.arcs << ' ' << (g.directed ? 1 : 0) << ' ' << (g.weighted ? 1 : 0);
+    return k.str();
+}
+
+static bool cache_lookup(const char *path, const DeviceGraph &g, TuneResult &r) {
+    if (!path || !*path) return false;
+    std::ifstream in(path);
+    if (!in) return false;
+    const std::string key = cache_key(g);
+    std::string line;
+    while (std::getline(in, line)) {
+        std::istringstream ls(line);
+        uint32_t n, dir, w;
+        uint64_t arcs;
+        if (!(ls >> n >> arcs >> dir >> w)) continue;
+        std::ostringstream k;
+        k << n << ' ' << arcs << ' ' << dir << ' ' << w;
+        if (k.str() != key) continue;
+        if (ls >> r.capw >> r.shortmax >> r.split >> r.blocks_per_sm >> r.batch_vec >> r.best_ms) {
+            r.from_cache = true;
+            return true;
+        }
+    }
+    return false;
+}
+
+static void cache_store(const char *path, const DeviceGraph &g, const TuneResult &r) {
+    if (!path || !*path) return;
+    std::ofstream out(path, std::ios::app);
+    if (!out) return;
+    out << cache_key(g) << ' ' << r.capw << ' ' << r.shortmax << ' ' << r.split << ' ' << r.blocks_per_sm << ' '
+        << r.batch_vec << ' ' << r.best_ms << '\n';
+}
+
+static double probe(DeviceGraph &g, Workspace &ws, cudaStream_t s, uint32_t iters) {
+    return time_iterations(g, ws, MODE_PLAIN64, iters, s) + time_iterations(g, ws, MODE_CORR32, iters, s);
+}
+
+int autotune(DeviceGraph &g, Workspace &ws, cudaStream_t s, bool tune_batch, const char *cache_path,
+             TuneResult &r) {
+    r = TuneResult{};
+    if (cache_lookup(cache_path, g, r)) {
+        g.blocks_per_sm = r.blocks_per_sm;
+        build_row_blocks(g, r.capw, r.shortmax, r.split, s);
+        ws.ready = ws.ready && false;  // grid shapes depend on blocks_per_sm
+        workspace_free(ws, s);
+        g.batch_vec = r.batch_vec;
+        return 0;
+    }
+    const uint32_t iters = 4;
+    const uint32_t cap0 = g.capw, short0 = g.shortmax, split0 = g.split, bps0 = g.blocks_per_sm;
+    r.default_ms = probe(g, ws, s, iters);
+    r.capw = cap0;
+    r.shortmax = short0;
+    r.split = split0;
+    r.blocks_per_sm = bps0;
+    r.best_ms = r.default_ms;
+    r.tried = 1;
+    const uint32_t shapes[][2] = {{128, 32}, {128, 128}, {192, 64}, {256, 64}, {256, 128},
+                                  {256, 256}, {384, 64}, {384, 128}, {448, 64}};
+    const uint32_t splits[] = {2048, 8192, 32768};
+    for (const auto &sh : shapes) {
+        for (uint32_t sp : splits) {
+            if (sh[0] == cap0 && sh[1] == short0 && sp == split0) continue;
+            build_row_blocks(g, sh[0], sh[1], sp, s);
+            const double t = probe(g, ws, s, iters);
+            r.tried++;
+            if (t < r.best_ms) {
+                r.best_ms = t;
+                r.capw = g.capw;
+                r.shortmax = g.shortmax;
+                r.split = g.split;
+            }
+        }
+    }
+    build_row_blocks(g, r.capw, r.shortmax, r.split, s);
+    for (uint32_t bps : {3u, 4u}) {
+        g.blocks_per_sm = bps;
+        workspace_free(ws, s);
+        const double t = probe(g, ws, s, iters);
+        r.tried++;
+        if (t < r.best_ms) {
+            r.best_ms = t;
+            r.blocks_per_sm = bps;
+        }
+    }
+    g.blocks_per_sm = r.blocks_per_sm;
+    workspace_free(ws, s);
+
+    r.batch_vec = g.batch_vec ? g.batch_vec : 1;
+    if (tune_batch && g.n >= 2) {
+        std::mt19937_64 rng(12345);
+        const uint32_t K = 128;
+        std::vector<uint64_t> off(K + 1);
+        std::vector<uint32_t> seeds(K);
+        for (uint32_t k = 0; k < K; k++) {
+            off[k] = k;
+            seeds[k] = (uint32_t)(rng() % g.n);
+        }
+        off[K] = K;
+        float *d_out = nullptr;
+        PRG_CUDA(cudaMallocAsync((void **)&d_out, (size_t)g.n * K * 4, s));
+        double best = 1e300;
+        for (uint32_t vec : {1u, 2u, 4u}) {
+            BatchStats bs;
+            ppr_batch(g, K, off.data(), seeds.data(), 0.85, 0.0, 3, vec, d_out, bs, s);
+            const double per = bs.ms / (double)std::max<uint64_t>(bs.column_iterations, 1);
+            r.tried++;
+            if (per < best) {
+                best = per;
+                r.batch_vec = vec;
+            }
+        }
+        cudaFreeAsync(d_out, s);
+        PRG_CUDA(cudaStreamSynchronize(s));
+        g.batch_vec = r.batch_vec;
+    }
+    cache_store(cache_path, g, r);
+    return 0;
+}
+
+}  // namespace prg

@@ -40,6 +40,7 @@ struct DeviceGraph {
     uint32_t blocks_per_sm = 0;  // persistent grid = SMs x this (0 = occupancy maximum)
     int relabel = 2;             // 0 keep caller ids, 1 degree-sorted ids, 2 decide from the degree skew
     bool hot_cache = false;      // relabelled graphs: cache the hot prefix of the rank vector in shared memory
+    uint32_t batch_vec = 0;      // batched tile width / 32 chosen by the autotuner (0 = process default)
 
     float build_ms = 0.f;
 };

@@ -64,6 +64,12 @@ void workspace_free(Workspace &ws, cudaStream_t s) {
 }
 
 void workspace_ensure(Workspace &ws, const DeviceGraph &g, cudaStream_t s) {
+    if (ws.ready && ws.graphs_rb != (const void *)g.rb) {
+        // row-blocks were rebuilt (autotuner): captured graphs hold the old list
+        for (auto &kv : ws.graphs) cudaGraphExecDestroy(kv.second);
+        ws.graphs.clear();
+        ws.graphs_rb = g.rb;
+    }
     if (ws.ready && ws.n == g.n && ws.nrb == g.nrb && ws.nhub == g.nhub) return;
     if (ws.ready) workspace_free(ws, s);
     ws.n = g.n;
@@ -98,6 +104,7 @@ void workspace_ensure(Workspace &ws, const DeviceGraph &g, cudaStream_t s) {
     PRG_CUDA(cudaEventCreate(&ws.ev1));
     PRG_CUDA(cudaEventCreate(&ws.eva));
     PRG_CUDA(cudaEventCreate(&ws.evb));
+    ws.graphs_rb = g.rb;
     ws.ready = true;
 }
 
@@ -328,6 +335,49 @@ static void solve_refined(const DeviceGraph &g, Workspace &ws, const SolveOpts &
     st.iterations = fp32 + fp64;
     st.last_diff = ws.h_ctl->diff;
     st.error_bound = st.residual_l1 * o.damping / (1.0 - o.damping);
+}
+
+double time_iterations(const DeviceGraph &g, Workspace &ws, int mode, uint32_t iters, cudaStream_t s) {
+    workspace_ensure(ws, g, s);
+    PRG_CUDA(cudaMemsetAsync(ws.hub_ticket, 0, std::max<uint64_t>(g.nhub, 1) * 4, s));
+    const uint64_t n = g.n;
+    launch_fill_start(ws.x64[0], nullptr, g.n, s);
+    for (int i = 0; i < 2; i++) {
+        PRG_CUDA(cudaMemsetAsync(ws.e32[i], 0, n * 4, s));
+        PRG_CUDA(cudaMemsetAsync(ws.et32[i], 0, n * 4, s));
+    }
+    PRG_CUDA(cudaMemsetAsync(ws.b32, 0, n * 4, s));
+    Ctl c;
+    std::memset(&c, 0, sizeof(c));
+    c.thr = -1.0;  // never converges: every launch does the full work
+    c.max_iter = 0xFFFFFFFFu;
+    PRG_CUDA(cudaMemcpyAsync(ws.ctl, &c, sizeof(Ctl), cudaMemcpyHostToDevice, s));
+    launch_prepare64(g, ws.x64[0], nullptr, ws.xt64[0], ws.ctl, 0, ws.blk_part, s);
+    IterArgs a[2];
+    a[0] = base_args(g, ws, 0.85);
+    a[1] = a[0];
+    for (int p = 0; p < 2; p++) {
+        a[p].parity = p;
+        a[p].x64_in = ws.x64[p];
+        a[p].xt64_in = ws.xt64[p];
+        a[p].x64_out = ws.x64[p ^ 1];
+        a[p].xt64_out = ws.xt64[p ^ 1];
+        a[p].x32_in = ws.e32[p];
+        a[p].xt32_in = ws.et32[p];
+        a[p].x32_out = ws.e32[p ^ 1];
+        a[p].xt32_out = ws.et32[p ^ 1];
+        a[p].b32 = ws.b32;
+        a[p].b32_out = ws.b32;
+    }
+    const int m = mode == MODE_RESID64 ? MODE_PLAIN64 : mode;
+    for (int k = 0; k < 2; k++) launch_iteration(m, g.weighted, a[k & 1], ws.cfg[m], s);
+    PRG_CUDA(cudaEventRecord(ws.eva, s));
+    for (uint32_t k = 0; k < iters; k++) launch_iteration(m, g.weighted, a[k & 1], ws.cfg[m], s);
+    PRG_CUDA(cudaEventRecord(ws.evb, s));
+    PRG_CUDA(cudaEventSynchronize(ws.evb));
+    float ms = 0.f;
+    PRG_CUDA(cudaEventElapsedTime(&ms, ws.eva, ws.evb));
+    return (double)ms / (double)std::max<uint32_t>(iters, 1u);
 }
 
 void solve(const DeviceGraph &g, Workspace &ws, const SolveOpts &o_in, const double *d_t, double *d_out,

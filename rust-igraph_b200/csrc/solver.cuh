@@ -49,10 +49,15 @@ struct Workspace {
     uint32_t *hub_ticket = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr, eva = nullptr, evb = nullptr;
     std::map<uint64_t, cudaGraphExec_t> graphs;
+    const void *graphs_rb = nullptr;  // row-block list the cached graphs were captured with
     int unroll = 8;  // iteration pairs per graph launch
 };
 
 void workspace_ensure(Workspace &ws, const DeviceGraph &g, cudaStream_t s);
+
+// Device time of one iteration of `mode` (ms), averaged over `iters`
+// back-to-back launches that never converge (autotuner probe).
+double time_iterations(const DeviceGraph &g, Workspace &ws, int mode, uint32_t iters, cudaStream_t s);
 void workspace_free(Workspace &ws, cudaStream_t s);
 
 // Solves on graph g.  d_t: normalised teleport/reset vector on the device

@@ -84,6 +84,12 @@ class prg_batch_stats(C.Structure):
                 ("tile_width", C.c_uint32), ("kernel_launches", C.c_uint32), ("ms", C.c_double)]
 
 
+class prg_tune_result(C.Structure):
+    _fields_ = [("capw", C.c_uint32), ("shortmax", C.c_uint32), ("split", C.c_uint32),
+                ("blocks_per_sm", C.c_uint32), ("batch_tile_width", C.c_uint32), ("candidates", C.c_uint32),
+                ("from_cache", C.c_int32), ("pad", C.c_uint32), ("default_ms", C.c_double), ("best_ms", C.c_double)]
+
+
 _lib = None
 
 
@@ -138,6 +144,8 @@ def lib():
         f.restype = C.c_int32
         f.argtypes = [vp, C.c_uint32, vp, vp, C.c_double, C.c_double, C.c_uint32, C.c_uint32, vp, vp,
                       C.POINTER(prg_batch_stats)]
+    L.prg_autotune.restype = C.c_int32
+    L.prg_autotune.argtypes = [vp, C.c_int32, C.c_char_p, C.POINTER(prg_tune_result)]
     L.prg_solve_noalloc.restype = C.c_int32
     L.prg_solve_noalloc.argtypes = [vp, C.POINTER(prg_options), vp, vp, C.POINTER(prg_stats)]
     L.prg_rmat_device.restype = C.c_int32
@@ -405,6 +413,13 @@ class DeviceGraph:
         _check(lib().prg_solve_device(self._h, C.byref(co), C.c_void_p(d_reset) if d_reset else None,
                                       C.c_void_p(d_out), C.byref(st)))
         return Stats.from_c(st)
+
+    def autotune(self, batch: bool = True, cache_path: Optional[str] = None) -> dict:
+        """Times row-block shapes, grid occupancy and batched tile widths on
+        this graph and keeps the fastest (prg_autotune)."""
+        r = prg_tune_result()
+        _check(lib().prg_autotune(self._h, int(batch), cache_path.encode() if cache_path else None, C.byref(r)))
+        return {k: getattr(r, k) for k, _ in prg_tune_result._fields_ if k != "pad"}
 
     def solve_noalloc(self, d_out: int, options: Optional[Options] = None, d_reset: int = 0):
         """FP64 solve into a device buffer with no device allocation inside
