@@ -145,6 +145,32 @@ int32_t prg_graph_relabelled(const prg_graph *g);
 int32_t prg_graph_device_csr(const prg_graph *g, const uint32_t **row_ptr, const uint32_t **col,
                              const uint32_t **perm, const float **inv32);
 
+/* ---- learned warm start --------------------------------------------------- */
+/* A two-layer message-passing network (hidden 32, 8-channel messages scaled
+ * by 1/out-degree, BF16 weights, FP32 accumulation on the tensor cores) that
+ * predicts the PageRank vector from degree features.  Its normalised output
+ * is only a start vector for prg_solve / prg_solve_device (prg_options.start):
+ * the fixed point, stop rule and checks are those of the plain method.  No
+ * counterpart in the reference (an addition of this library). */
+typedef struct prg_gnn prg_gnn;
+
+uint32_t prg_gnn_param_count(void);
+/* New network with seeded random weights. */
+int32_t prg_gnn_create(uint64_t seed, prg_gnn **out);
+void prg_gnn_destroy(prg_gnn *net);
+/* FP32 master parameters to / from host float[prg_gnn_param_count()]. */
+int32_t prg_gnn_get_params(const prg_gnn *net, float *host);
+int32_t prg_gnn_set_params(prg_gnn *net, const float *host);
+/* Predicted start vector (caller ids, sums to 1) into device double[n];
+ * *ms = device time of the inference. */
+int32_t prg_gnn_predict(prg_gnn *net, prg_graph *g, double *d_start, double *ms);
+/* Loss sum_v w_v (y_v - log(n x*_v))^2 / n (w_v = n x*_v) against a target
+ * PageRank vector (device, caller ids) and its gradient (host float[count],
+ * optional), without updating the weights. */
+int32_t prg_gnn_loss_grad(prg_gnn *net, prg_graph *g, const double *d_target, double *loss, float *host_grad);
+/* One Adam step (lr) on that loss. */
+int32_t prg_gnn_train_step(prg_gnn *net, prg_graph *g, const double *d_target, float lr, double *loss);
+
 /* ---- autotuner --------------------------------------------------------- */
 
 typedef struct prg_tune_result {
@@ -227,6 +253,14 @@ const char *prg_last_error(void);
  * writes m edges into device arrays d_from/d_to. */
 int32_t prg_rmat_device(uint32_t scale, uint64_t m, double a, double b, double c, uint64_t seed,
                         uint32_t *d_from, uint32_t *d_to, void *stream);
+
+/* Seeded device generators for warm-start training graphs: kind 0 R-MAT
+ * (p0, p1, p2 = a, b, c; vertex ids < next power of two >= n), 1 Chung-Lu
+ * power law (p0 = exponent alpha of the weight (i + p1)^-alpha), 2 block
+ * model with a fixed edge count (p0 = number of equal blocks, p1 = probability
+ * that an edge stays inside its block).  Writes m edges. */
+int32_t prg_generate_device(int32_t kind, uint32_t n, uint64_t m, double p0, double p1, double p2, uint64_t seed,
+                            uint32_t *d_from, uint32_t *d_to, void *stream);
 
 #ifdef __cplusplus
 }

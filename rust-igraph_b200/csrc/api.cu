@@ -18,6 +18,7 @@
 
 #include "../../include/prg_b200.h"
 #include "autotune.cuh"
+#include "gnn.cuh"
 #include "graph.cuh"
 #include "handle.cuh"
 #include "ppr_batch.cuh"
@@ -633,6 +634,142 @@ int32_t prg_autotune(prg_graph *h, int32_t tune_batch, const char *cache_path, p
     PRG_GUARD_END
 }
 
+// ---- learned warm start ----------------------------------------------------
+
+struct prg_gnn {
+    prg::gnn::Net net;
+    double *tmp = nullptr;  // n doubles (target / prediction in internal ids)
+    uint32_t tmp_n = 0;
+};
+
+static double *gnn_tmp(prg_gnn *net, uint32_t n, cudaStream_t s) {
+    if (net->tmp_n < n) {
+        if (net->tmp) cudaFreeAsync(net->tmp, s);
+        PRG_CUDA(cudaMallocAsync((void **)&net->tmp, (size_t)n * 8, s));
+        net->tmp_n = n;
+    }
+    return net->tmp;
+}
+
+uint32_t prg_gnn_param_count(void) { return (uint32_t)prg::gnn::param_count(); }
+
+int32_t prg_gnn_create(uint64_t seed, prg_gnn **out) {
+    g_err.clear();
+    PRG_GUARD_BEGIN
+    if (!out) return fail(PRG_ERR_INVALID_ARGUMENT, "null output handle");
+    if (!ensure_pool_config()) return fail(PRG_ERR_CUDA, "cuda: no usable device");
+    prg_gnn *net = new prg_gnn();
+    net->net.init(seed, 0);
+    PRG_CUDA(cudaStreamSynchronize(0));
+    *out = net;
+    return PRG_OK;
+    PRG_GUARD_END
+}
+
+void prg_gnn_destroy(prg_gnn *net) {
+    if (!net) return;
+    try {
+        net->net.free(0);
+        if (net->tmp) cudaFreeAsync(net->tmp, 0);
+        cudaStreamSynchronize(0);
+    } catch (...) {
+    }
+    delete net;
+}
+
+int32_t prg_gnn_get_params(const prg_gnn *net, float *host) {
+    g_err.clear();
+    PRG_GUARD_BEGIN
+    if (!net || !host) return fail(PRG_ERR_INVALID_ARGUMENT, "null argument");
+    net->net.get_params(host, 0);
+    return PRG_OK;
+    PRG_GUARD_END
+}
+
+int32_t prg_gnn_set_params(prg_gnn *net, const float *host) {
+    g_err.clear();
+    PRG_GUARD_BEGIN
+    if (!net || !host) return fail(PRG_ERR_INVALID_ARGUMENT, "null argument");
+    for (int i = 0; i < prg::gnn::param_count(); i++)
+        if (!std::isfinite(host[i])) return fail(PRG_ERR_INVALID_ARGUMENT, "parameters must be finite");
+    net->net.set_params(host, 0);
+    return PRG_OK;
+    PRG_GUARD_END
+}
+
+int32_t prg_gnn_predict(prg_gnn *net, prg_graph *h, double *d_start, double *ms) {
+    g_err.clear();
+    PRG_GUARD_BEGIN
+    if (!net || !h || !d_start) return fail(PRG_ERR_INVALID_ARGUMENT, "null argument");
+    if (h->g.n < 2) return fail(PRG_ERR_INVALID_ARGUMENT, "prediction needs vcount >= 2");
+    cudaStream_t s = h->stream;
+    PRG_CUDA(cudaStreamSynchronize(0));
+    cudaEvent_t e0, e1;
+    PRG_CUDA(cudaEventCreate(&e0));
+    PRG_CUDA(cudaEventCreate(&e1));
+    PRG_CUDA(cudaEventRecord(e0, s));
+    if (h->g.iperm) {
+        double *x = gnn_tmp(net, h->g.n, s);
+        net->net.predict(h->g, x, s);
+        prg::gather_f64(d_start, x, h->g.iperm, h->g.n, s);
+    } else {
+        net->net.predict(h->g, d_start, s);
+    }
+    PRG_CUDA(cudaEventRecord(e1, s));
+    PRG_CUDA(cudaEventSynchronize(e1));
+    float t = 0.f;
+    PRG_CUDA(cudaEventElapsedTime(&t, e0, e1));
+    if (ms) *ms = t;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return PRG_OK;
+    PRG_GUARD_END
+}
+
+static int32_t gnn_loss(prg_gnn *net, prg_graph *h, const double *d_target, double *loss) {
+    cudaStream_t s = h->stream;
+    PRG_CUDA(cudaStreamSynchronize(0));
+    const double *t = d_target;
+    if (h->g.perm) {
+        double *tt = gnn_tmp(net, h->g.n, s);
+        prg::gather_f64(tt, d_target, h->g.perm, h->g.n, s);
+        t = tt;
+    }
+    const double l = net->net.loss_grad(h->g, t, s);
+    if (loss) *loss = l;
+    return PRG_OK;
+}
+
+int32_t prg_gnn_loss_grad(prg_gnn *net, prg_graph *h, const double *d_target, double *loss, float *host_grad) {
+    g_err.clear();
+    PRG_GUARD_BEGIN
+    if (!net || !h || !d_target) return fail(PRG_ERR_INVALID_ARGUMENT, "null argument");
+    if (h->g.n < 2) return fail(PRG_ERR_INVALID_ARGUMENT, "training needs vcount >= 2");
+    int32_t rc = gnn_loss(net, h, d_target, loss);
+    if (rc == PRG_OK && host_grad) {
+        PRG_CUDA(cudaMemcpyAsync(host_grad, net->net.G, (size_t)prg::gnn::param_count() * 4, cudaMemcpyDeviceToHost,
+                                 h->stream));
+        PRG_CUDA(cudaStreamSynchronize(h->stream));
+    }
+    return rc;
+    PRG_GUARD_END
+}
+
+int32_t prg_gnn_train_step(prg_gnn *net, prg_graph *h, const double *d_target, float lr, double *loss) {
+    g_err.clear();
+    PRG_GUARD_BEGIN
+    if (!net || !h || !d_target) return fail(PRG_ERR_INVALID_ARGUMENT, "null argument");
+    if (h->g.n < 2) return fail(PRG_ERR_INVALID_ARGUMENT, "training needs vcount >= 2");
+    if (!(lr > 0.0f)) return fail(PRG_ERR_INVALID_ARGUMENT, "learning rate must be > 0");
+    int32_t rc = gnn_loss(net, h, d_target, loss);
+    if (rc == PRG_OK) {
+        net->net.adam(lr, h->stream);
+        PRG_CUDA(cudaStreamSynchronize(h->stream));
+    }
+    return rc;
+    PRG_GUARD_END
+}
+
 int32_t prg_set_tuning(const char *key, int64_t value) {
     g_err.clear();
     if (!key) return fail(PRG_ERR_INVALID_ARGUMENT, "null tuning key");
@@ -660,6 +797,19 @@ int32_t prg_set_tuning(const char *key, int64_t value) {
         return fail(PRG_ERR_INVALID_ARGUMENT, "unknown tuning key: " + k);
     }
     return PRG_OK;
+}
+
+int32_t prg_generate_device(int32_t kind, uint32_t n, uint64_t m, double p0, double p1, double p2, uint64_t seed,
+                            uint32_t *d_from, uint32_t *d_to, void *stream) {
+    g_err.clear();
+    PRG_GUARD_BEGIN
+    if (kind < 0 || kind > 2) return fail(PRG_ERR_INVALID_ARGUMENT, "generator kind must be 0, 1 or 2");
+    if (n < 2) return fail(PRG_ERR_INVALID_ARGUMENT, "generator needs n >= 2");
+    if (kind == 2 && (p0 < 1.0 || (uint32_t)p0 > n)) return fail(PRG_ERR_INVALID_ARGUMENT, "bad block count");
+    if (kind == 0 && (n & (n - 1)) != 0) return fail(PRG_ERR_INVALID_ARGUMENT, "R-MAT needs n = 2^scale");
+    prg::generate_device(kind, n, m, p0, p1, p2, seed, d_from, d_to, (cudaStream_t)stream);
+    return PRG_OK;
+    PRG_GUARD_END
 }
 
 int32_t prg_rmat_device(uint32_t scale, uint64_t m, double a, double b, double c, uint64_t seed, uint32_t *d_from,

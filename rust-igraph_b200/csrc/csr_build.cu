@@ -693,3 +693,77 @@ void rmat_generate(uint32_t scale, uint64_t m, double a, double b, double c, uin
 }
 
 }  // namespace prg
+
+namespace prg {
+
+// ---- further seeded generators (training graphs for the warm start) ------
+// Counter-based like the R-MAT generator: edge e draws from its own
+// SplitMix64 stream seeded with seed ^ (e * 0xD1B54A32D192ED03).
+
+__device__ __forceinline__ double sm_unit(uint64_t &st) {
+    st += 0x9E3779B97F4A7C15ULL;
+    uint64_t z = st;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+    z ^= z >> 31;
+    return (double)(z >> 11) * (1.0 / 9007199254740992.0);
+}
+
+// Chung-Lu power law: both endpoints drawn with probability proportional to
+// (i + i0)^(-alpha) by inverting the continuous cumulative weight; alpha =
+// 1/(gamma - 1) (gamma = 3 gives the degree law of preferential attachment).
+__global__ void chung_lu_kernel(uint32_t n, uint64_t m, double alpha, double i0, uint64_t seed, uint32_t *from,
+                                uint32_t *to) {
+    const double b = 1.0 - alpha;
+    const double lo = pow(i0, b), hi = pow((double)n + i0, b);
+    for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e < m; e += (uint64_t)gridDim.x * blockDim.x) {
+        uint64_t st = seed ^ (e * 0xD1B54A32D192ED03ULL);
+        uint32_t ends[2];
+        for (int k = 0; k < 2; k++) {
+            const double u = sm_unit(st);
+            double x = pow(lo + u * (hi - lo), 1.0 / b) - i0;
+            uint32_t v = x < 0.0 ? 0u : (uint32_t)x;
+            ends[k] = v >= n ? n - 1 : v;
+        }
+        from[e] = ends[0];
+        to[e] = ends[1];
+    }
+}
+
+// Block model with a fixed edge count: block of the edge uniform among
+// `blocks` equal blocks; with probability p_in both ends in that block,
+// otherwise the target in another uniformly chosen block.
+__global__ void sbm_edges_kernel(uint32_t n, uint64_t m, uint32_t blocks, double p_in, uint64_t seed, uint32_t *from,
+                                 uint32_t *to) {
+    const uint32_t bs = n / blocks;
+    for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e < m; e += (uint64_t)gridDim.x * blockDim.x) {
+        uint64_t st = seed ^ (e * 0xD1B54A32D192ED03ULL);
+        const uint32_t b0 = min((uint32_t)(sm_unit(st) * blocks), blocks - 1);
+        uint32_t b1 = b0;
+        if (sm_unit(st) >= p_in && blocks > 1) {
+            b1 = min((uint32_t)(sm_unit(st) * (blocks - 1)), blocks - 2);
+            if (b1 >= b0) b1++;
+        }
+        const uint32_t u = b0 * bs + min((uint32_t)(sm_unit(st) * bs), bs - 1);
+        const uint32_t v = b1 * bs + min((uint32_t)(sm_unit(st) * bs), bs - 1);
+        from[e] = u;
+        to[e] = v;
+    }
+}
+
+void generate_device(int kind, uint32_t n, uint64_t m, double p0, double p1, double p2, uint64_t seed,
+                     uint32_t *d_from, uint32_t *d_to, cudaStream_t s) {
+    const unsigned grid = grid_for(m, kThreads, 148u * 32u);
+    if (kind == 0) {
+        uint32_t scale = 0;
+        while ((1ull << scale) < n) scale++;
+        rmat_generate(scale, m, p0, p1, p2, seed, d_from, d_to, s);
+    } else if (kind == 1) {
+        chung_lu_kernel<<<grid, kThreads, 0, s>>>(n, m, p0, p1 > 0 ? p1 : 1.0, seed, d_from, d_to);
+    } else {
+        sbm_edges_kernel<<<grid, kThreads, 0, s>>>(n, m, (uint32_t)p0, p1, seed, d_from, d_to);
+    }
+    PRG_CUDA(cudaGetLastError());
+}
+
+}  // namespace prg

@@ -76,6 +76,12 @@ void radix_sort_pairs(uint32_t **keys, uint32_t **vals, uint32_t **keys_alt, uin
 // out[0..n] = exclusive prefix sums of in[0..n), out[n] = total (u32).
 void exclusive_scan_u32(const uint32_t *in, uint32_t *out, uint64_t n, cudaStream_t s);
 
+// Seeded device generators: kind 0 R-MAT (p0..p2 = a, b, c; n rounded up to
+// a power of two), 1 Chung-Lu power law (p0 = alpha, p1 = offset), 2 block
+// model (p0 = blocks, p1 = intra-block probability).
+void generate_device(int kind, uint32_t n, uint64_t m, double p0, double p1, double p2, uint64_t seed,
+                     uint32_t *d_from, uint32_t *d_to, cudaStream_t s);
+
 // Device R-MAT generator (same stream layout as the oracle's or_rmat).
 void rmat_generate(uint32_t scale, uint64_t m, double a, double b, double c, uint64_t seed, uint32_t *d_from,
                    uint32_t *d_to, cudaStream_t s);

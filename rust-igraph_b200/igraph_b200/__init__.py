@@ -146,6 +146,25 @@ def lib():
                       C.POINTER(prg_batch_stats)]
     L.prg_autotune.restype = C.c_int32
     L.prg_autotune.argtypes = [vp, C.c_int32, C.c_char_p, C.POINTER(prg_tune_result)]
+    L.prg_generate_device.restype = C.c_int32
+    L.prg_generate_device.argtypes = [C.c_int32, C.c_uint32, C.c_uint64, C.c_double, C.c_double, C.c_double,
+                                      C.c_uint64, vp, vp, vp]
+    L.prg_gnn_param_count.restype = C.c_uint32
+    L.prg_gnn_param_count.argtypes = []
+    L.prg_gnn_create.restype = C.c_int32
+    L.prg_gnn_create.argtypes = [C.c_uint64, C.POINTER(C.c_void_p)]
+    L.prg_gnn_destroy.restype = None
+    L.prg_gnn_destroy.argtypes = [vp]
+    L.prg_gnn_get_params.restype = C.c_int32
+    L.prg_gnn_get_params.argtypes = [vp, vp]
+    L.prg_gnn_set_params.restype = C.c_int32
+    L.prg_gnn_set_params.argtypes = [vp, vp]
+    L.prg_gnn_predict.restype = C.c_int32
+    L.prg_gnn_predict.argtypes = [vp, vp, vp, C.POINTER(C.c_double)]
+    L.prg_gnn_loss_grad.restype = C.c_int32
+    L.prg_gnn_loss_grad.argtypes = [vp, vp, vp, C.POINTER(C.c_double), vp]
+    L.prg_gnn_train_step.restype = C.c_int32
+    L.prg_gnn_train_step.argtypes = [vp, vp, vp, C.c_float, C.POINTER(C.c_double)]
     L.prg_solve_noalloc.restype = C.c_int32
     L.prg_solve_noalloc.argtypes = [vp, C.POINTER(prg_options), vp, vp, C.POINTER(prg_stats)]
     L.prg_rmat_device.restype = C.c_int32
@@ -471,6 +490,16 @@ class DeviceGraph:
 
     def __exit__(self, *a):
         self.close()
+
+
+GEN_RMAT, GEN_POWERLAW, GEN_BLOCKS = 0, 1, 2
+
+
+def generate_device(kind: int, n: int, m: int, d_from: int, d_to: int, p0=0.0, p1=0.0, p2=0.0, seed=1,
+                    stream: int = 0) -> None:
+    """Seeded device edge generators (prg_generate_device)."""
+    _check(lib().prg_generate_device(kind, n, m, p0, p1, p2, seed, C.c_void_p(d_from), C.c_void_p(d_to),
+                                     C.c_void_p(stream) if stream else None))
 
 
 def set_tuning(key: str, value: int) -> None:

@@ -1,0 +1,82 @@
+"""Warm-start network: CUDA forward/backward against the float64 CPU
+restatement, training on the GPU, and what the trained start saves."""
+import numpy as np
+import pytest
+
+import igraph_b200 as ig
+import oracle as O
+from igraph_b200 import warmstart as W
+import gnn_oracle as GO
+
+pytestmark = pytest.mark.gpu
+
+
+def _small_graph():
+    n = 3000
+    f, t = O.barabasi_game_bag(n, 4, False, True, 17)
+    x = O.pagerank(n, f, t, True)
+    return n, f, t, x
+
+
+def test_gradient_matches_cpu_oracle(cuda_ok):
+    import torch
+
+    n, f, t, x = _small_graph()
+    net = W.WarmStartNet(seed=3)
+    # perturb away from the symmetric start so every block of the gradient is live
+    p = net.params()
+    p += np.random.default_rng(1).normal(0, 0.05, p.shape).astype(np.float32)
+    net.set_params(p)
+    with ig.DeviceGraph.from_host(n, f, t, True) as dg:
+        xt = torch.tensor(x, dtype=torch.float64, device="cuda")
+        loss, g = net.loss_grad(dg, xt.data_ptr())
+        start = torch.empty(n, dtype=torch.float64, device="cuda")
+        net.predict(dg, start.data_ptr())
+    l_ref, g_ref, pred_ref = GO.loss_and_grad(net.params(), n, f, t, True, x)
+    assert abs(loss - l_ref) <= 1e-3 * abs(l_ref) + 1e-6
+    # relative error of the whole gradient and of each parameter block
+    assert np.linalg.norm(g - g_ref) <= 2e-2 * np.linalg.norm(g_ref)
+    for a, b in [(GO.oW1, GO.oB1), (GO.oWm1, GO.oW2), (GO.oW2, GO.oB2), (GO.oWm2, GO.oW3), (GO.oW3, GO.oB3)]:
+        assert np.linalg.norm(g[a:b] - g_ref[a:b]) <= 5e-2 * np.linalg.norm(g_ref[a:b]) + 1e-7, (a, b)
+    # prediction = softmax of the same outputs
+    assert np.abs(start.cpu().numpy() - pred_ref).sum() <= 1e-2
+    net.close()
+
+
+def test_training_lowers_loss_and_start_error(cuda_ok):
+    import torch
+
+    specs = W.training_specs(6, seed=9, n_min=20_000, n_max=60_000)
+    net = W.WarmStartNet(seed=2)
+    hist = W.train(net, specs, epochs=12, lr=1e-2, log=lambda *_: None)
+    assert hist[-1] < 0.5 * hist[0]
+    # held-out graph: the predicted start is closer to the answer than uniform
+    spec = W.heldout_rmat(16)
+    dg = W.build(spec)
+    x, _ = W.label(dg)
+    start = torch.empty(dg.n, dtype=torch.float64, device="cuda")
+    net.predict(dg, start.data_ptr())
+    uni = torch.full_like(start, 1.0 / dg.n)
+    assert abs(float(start.sum()) - 1.0) < 1e-12
+    assert float((start - x).abs().sum()) < float((uni - x).abs().sum())
+    dg.close()
+    net.close()
+
+
+def test_warm_start_solution_unchanged(cuda_ok):
+    # whatever the start, the solver returns the same fixed point within the bound
+    import torch
+
+    n = 1 << 14
+    f, t = O.rmat(14, 16 * n, seed=21)
+    tight, _, _ = O.pagerank_tight(n, f, t, True, tol=1e-15)
+    net = W.WarmStartNet(seed=4)
+    with ig.DeviceGraph.from_host(n, f, t, True) as dg:
+        start = torch.empty(n, dtype=torch.float64, device="cuda")
+        net.predict(dg, start.data_ptr())
+        out = torch.empty(n, dtype=torch.float64, device="cuda")
+        for prec in (ig.PRECISION_FP64, ig.PRECISION_FP32_REFINED):
+            dg.solve_device(out.data_ptr(), ig.Options(precision=prec, stop=ig.STOP_ERROR_BOUND),
+                            d_start=start.data_ptr())
+            assert np.abs(out.cpu().numpy() - tight).sum() <= 1e-10
+    net.close()
