@@ -471,6 +471,178 @@ __global__ void to_bf16_kernel(const float *P, Ws *w) {
     if (i < 8 * kZ) w->W3[i] = __float2bfloat16_rn(P[oW3 + i]);
 }
 
+
+// ---- fused inference path ---------------------------------------------------
+// The same layer chain as the forward pass above, with the hidden layers kept
+// in registers: the FP32 accumulator fragments of one mma.m16n8k16 are the
+// BF16 A-operand fragments of the next layer once packed (C tile 2k / 2k+1
+// of n-columns 16k..16k+15 -> A registers {0,1} / {2,3} of k-tile k), so H0
+// and H1 never reach memory (they are recomputed where needed).  The
+// rounding points and the mma sequence are those of rowwise_kernel, so the
+// prediction is that of the training forward pass.
+
+__device__ __forceinline__ float feat(uint32_t r, int c, uint32_t n, float ln, const uint32_t *row_ptr,
+                                      const uint32_t *deg) {
+    if (r >= n || c > 5) return 0.0f;
+    const float li = log1pf((float)(row_ptr[r + 1] - row_ptr[r]));
+    const float lo = log1pf((float)deg[r]);
+    switch (c) {
+        case 0: return li * 0.125f;
+        case 1: return lo * 0.125f;
+        case 2: return deg[r] == 0 ? 1.0f : 0.0f;
+        case 3: return 1.0f;
+        case 4: return (li - lo) * 0.125f;
+        default: return ln;
+    }
+}
+
+__device__ __forceinline__ void mma_bf16(float (&c)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};"
+        : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+// acc[j] += A(k-tiles) x W^T for n-tiles j < NT; W row-major [N x K] in smem
+template <int NT, int KT>
+__device__ __forceinline__ void layer(float (&acc)[NT][4], const uint32_t (&a)[KT][4], const __nv_bfloat16 *sW,
+                                      int K, int g, int t) {
+#pragma unroll
+    for (int j = 0; j < NT; j++) acc[j][0] = acc[j][1] = acc[j][2] = acc[j][3] = 0.0f;
+#pragma unroll
+    for (int kt = 0; kt < KT; kt++) {
+#pragma unroll
+        for (int j = 0; j < NT; j++) {
+            const int col = j * 8 + g;
+            const uint32_t b0 = *reinterpret_cast<const uint32_t *>(sW + col * K + kt * 16 + 2 * t);
+            const uint32_t b1 = *reinterpret_cast<const uint32_t *>(sW + col * K + kt * 16 + 2 * t + 8);
+            mma_bf16(acc[j], a[kt], b0, b1);
+        }
+    }
+}
+
+// relu(acc + bias) -> BF16 A fragments of the next layer (32 columns = 2 k-tiles)
+__device__ __forceinline__ void to_afrag(const float (&acc)[4][4], const float *bias, int t, uint32_t (&a)[2][4]) {
+#pragma unroll
+    for (int kt = 0; kt < 2; kt++) {
+        float v[2][4];
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+            const int j = 2 * kt + h, c0 = j * 8 + 2 * t;
+            v[h][0] = fmaxf(acc[j][0] + bias[c0], 0.0f);
+            v[h][1] = fmaxf(acc[j][1] + bias[c0 + 1], 0.0f);
+            v[h][2] = fmaxf(acc[j][2] + bias[c0], 0.0f);
+            v[h][3] = fmaxf(acc[j][3] + bias[c0 + 1], 0.0f);
+        }
+        a[kt][0] = pack_bf16(v[0][0], v[0][1]);
+        a[kt][1] = pack_bf16(v[0][2], v[0][3]);
+        a[kt][2] = pack_bf16(v[1][0], v[1][1]);
+        a[kt][3] = pack_bf16(v[1][2], v[1][3]);
+    }
+}
+
+__device__ __forceinline__ uint32_t ld_pair(const __nv_bfloat16 *A, uint32_t r, uint32_t n, int k) {
+    return r < n ? *reinterpret_cast<const uint32_t *>(A + (size_t)r * 16 + k) : 0u;
+}
+
+// STAGE 0: write M0 = s * (H0 Wm1^T); 1: write M1; 2: write y
+template <int STAGE>
+__global__ void __launch_bounds__(128) fused_kernel(uint32_t n, const uint32_t *row_ptr, const uint32_t *deg,
+                                                    const __nv_bfloat16 *A1, const __nv_bfloat16 *A2, const Ws *Wg,
+                                                    const float *P, const float *scale, float *out) {
+    __shared__ __align__(16) __nv_bfloat16 sW1[kH * kF], sWm[kC * kH], sW2[kH * kZ], sW3[8 * kZ];
+    __shared__ float sb1[kH], sb2[kH];
+    for (int i = threadIdx.x; i < kH * kF; i += blockDim.x) sW1[i] = Wg->W1[i];
+    for (int i = threadIdx.x; i < kC * kH; i += blockDim.x) sWm[i] = STAGE == 0 ? Wg->Wm1[i] : Wg->Wm2[i];
+    for (int i = threadIdx.x; i < kH * kZ; i += blockDim.x) sW2[i] = Wg->W2[i];
+    for (int i = threadIdx.x; i < 8 * kZ; i += blockDim.x) sW3[i] = Wg->W3[i];
+    for (int i = threadIdx.x; i < kH; i += blockDim.x) {
+        sb1[i] = P[oB1 + i];
+        sb2[i] = P[oB2 + i];
+    }
+    __syncthreads();
+    const float ln = logf((float)n) * 0.0625f;
+    const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+    const uint32_t ntiles = (n + 15) / 16;
+    const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nwarps = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t tile = warp; tile < ntiles; tile += nwarps) {
+        const uint32_t r0 = tile * 16 + g, r1 = r0 + 8;
+        uint32_t ax[1][4];
+        ax[0][0] = pack_bf16(feat(r0, 2 * t, n, ln, row_ptr, deg), feat(r0, 2 * t + 1, n, ln, row_ptr, deg));
+        ax[0][1] = pack_bf16(feat(r1, 2 * t, n, ln, row_ptr, deg), feat(r1, 2 * t + 1, n, ln, row_ptr, deg));
+        ax[0][2] = pack_bf16(feat(r0, 2 * t + 8, n, ln, row_ptr, deg), feat(r0, 2 * t + 9, n, ln, row_ptr, deg));
+        ax[0][3] = pack_bf16(feat(r1, 2 * t + 8, n, ln, row_ptr, deg), feat(r1, 2 * t + 9, n, ln, row_ptr, deg));
+        float acc[4][4];
+        layer<4, 1>(acc, ax, sW1, kF, g, t);
+        uint32_t ah[3][4];
+        {
+            uint32_t h0[2][4];
+            to_afrag(acc, sb1, t, h0);
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                ah[0][q] = h0[0][q];
+                ah[1][q] = h0[1][q];
+            }
+        }
+        if constexpr (STAGE >= 1) {
+            // k-tile 2 of [H0 | A1]
+            ah[2][0] = ld_pair(A1, r0, n, 2 * t);
+            ah[2][1] = ld_pair(A1, r1, n, 2 * t);
+            ah[2][2] = ld_pair(A1, r0, n, 2 * t + 8);
+            ah[2][3] = ld_pair(A1, r1, n, 2 * t + 8);
+            layer<4, 3>(acc, ah, sW2, kZ, g, t);
+            uint32_t h1[2][4];
+            to_afrag(acc, sb2, t, h1);
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                ah[0][q] = h1[0][q];
+                ah[1][q] = h1[1][q];
+            }
+        }
+        if constexpr (STAGE <= 1) {
+            float m[1][4];
+            uint32_t a2[2][4];
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                a2[0][q] = ah[0][q];
+                a2[1][q] = ah[1][q];
+            }
+            layer<1, 2>(m, a2, sWm, kH, g, t);
+            const int c0 = 2 * t;
+            if (r0 < n) {
+                const float sc = scale[r0];
+                out[(size_t)r0 * kC + c0] = m[0][0] * sc;
+                out[(size_t)r0 * kC + c0 + 1] = m[0][1] * sc;
+            }
+            if (r1 < n) {
+                const float sc = scale[r1];
+                out[(size_t)r1 * kC + c0] = m[0][2] * sc;
+                out[(size_t)r1 * kC + c0 + 1] = m[0][3] * sc;
+            }
+        } else {
+            ah[2][0] = ld_pair(A2, r0, n, 2 * t);
+            ah[2][1] = ld_pair(A2, r1, n, 2 * t);
+            ah[2][2] = ld_pair(A2, r0, n, 2 * t + 8);
+            ah[2][3] = ld_pair(A2, r1, n, 2 * t + 8);
+            float yv[1][4];
+            layer<1, 3>(yv, ah, sW3, kZ, g, t);
+            if (t == 0) {
+                if (r0 < n) out[r0] = yv[0][0] + P[oB3];
+                if (r1 < n) out[r1] = yv[0][2] + P[oB3];
+            }
+        }
+    }
+}
+
+template <int STAGE>
+static void fused(uint32_t n, const DeviceGraph &g, const __nv_bfloat16 *A1, const __nv_bfloat16 *A2, const Ws *W,
+                  const float *P, const float *scale, float *out, cudaStream_t s) {
+    const uint32_t tiles = (n + 15) / 16;
+    const unsigned grid = (unsigned)std::max<uint32_t>(1, std::min<uint32_t>((tiles + 3) / 4, 148u * 16u));
+    fused_kernel<STAGE><<<grid, 128, 0, s>>>(n, g.row_ptr, g.deg, A1, A2, W, P, scale, out);
+    PRG_CUDA(cudaGetLastError());
+}
+
 // ---- host side -------------------------------------------------------------
 
 int param_count() { return kParams; }
@@ -623,8 +795,24 @@ void Net::forward(const DeviceGraph &g, cudaStream_t s) {
 }
 
 void Net::predict(const DeviceGraph &g, double *x_internal, cudaStream_t s) {
-    forward(g, s);
+    // fused inference: M0, A1, M1, A2, y without materialising H0 / H1
+    ensure(g.n, s);
     Views V = views(buf, g.n);
+    const Ws *W = (const Ws *)w;
+    const uint32_t n = g.n;
+    scale_kernel<<<grid_n(n), 256, 0, s>>>(g.deg, n, V.s);
+    fused<0>(n, g, nullptr, nullptr, W, P, V.s, V.M0, s);
+    for (int layer = 0; layer < 2; layer++) {
+        const float *M = layer ? V.M1 : V.M0;
+        __nv_bfloat16 *A = layer ? V.A2 : V.A1;
+        float *S = layer ? V.S2 : V.S1;
+        PRG_CUDA(cudaMemsetAsync(V.nheavy, 0, 4, s));
+        aggregate_kernel<<<148 * 16, 256, 0, s>>>(n, g.row_ptr, g.col, M, A, S, V.heavy, V.nheavy);
+        aggregate_heavy_kernel<<<148 * 4, 256, 0, s>>>(g.row_ptr, g.col, M, A, S, V.heavy, V.nheavy);
+        PRG_CUDA(cudaGetLastError());
+        if (layer == 0) fused<1>(n, g, V.A1, nullptr, W, P, V.s, V.M1, s);
+    }
+    fused<2>(n, g, V.A1, V.A2, W, P, V.s, V.y, s);
     const unsigned gb = 296;
     max_kernel<<<gb, 256, 0, s>>>(V.y, g.n, V.fpart);
     expsum_kernel<<<gb, 256, 0, s>>>(V.y, g.n, V.fpart, gb, x_internal, V.dpart);

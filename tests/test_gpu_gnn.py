@@ -80,3 +80,19 @@ def test_warm_start_solution_unchanged(cuda_ok):
                             d_start=start.data_ptr())
             assert np.abs(out.cpu().numpy() - tight).sum() <= 1e-10
     net.close()
+
+
+def test_committed_weights_load_and_predict(cuda_ok):
+    # the shipped weights (trained on the GPU by these kernels) give a start
+    # closer to the answer than the uniform start on a held-out R-MAT
+    import torch
+
+    net = W.WarmStartNet.load()
+    dg = W.build(W.heldout_rmat(17, seed=4242))
+    x, _ = W.label(dg)
+    start = torch.empty(dg.n, dtype=torch.float64, device="cuda")
+    net.predict(dg, start.data_ptr())
+    uni = torch.full_like(start, 1.0 / dg.n)
+    assert float((start - x).abs().sum()) < 0.25 * float((uni - x).abs().sum())
+    dg.close()
+    net.close()
