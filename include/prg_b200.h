@@ -52,7 +52,14 @@ enum prg_status {
 
 enum prg_precision {
     PRG_PRECISION_FP64 = 0,           /* FP64 power iteration (the drop-in path) */
-    PRG_PRECISION_FP32_REFINED = 1    /* FP32 SpMV, FP64 residual refinement */
+    PRG_PRECISION_FP32_REFINED = 1,   /* FP32 SpMV inner solves, FP64 residual refinement, certified stop */
+    PRG_PRECISION_FP64_KRYLOV = 2,    /* FP64 BiCGStab on the linear system, certified stop */
+    PRG_PRECISION_LINSYS = 3          /* pagerank_linsys() rule: ||b - Ax||_2 < 1e-13 ||b||_2, returns x */
+};
+
+enum prg_inner {
+    PRG_INNER_KRYLOV = 0,             /* refined: BiCGStab on A e = r in FP32 (default) */
+    PRG_INNER_RICHARDSON = 1          /* refined: power-style correction e <- d M e + r in FP32 */
 };
 
 enum prg_stop {
@@ -68,6 +75,7 @@ typedef struct prg_options {
     int32_t stop;          /* enum prg_stop (refined precision always uses ERROR_BOUND) */
     int32_t normalise;     /* refined: divide the result by its FP64 sum (default 1) */
     const double *start;   /* optional start vector (warm start), length n, host memory; NULL = reference start */
+    int32_t inner;         /* enum prg_inner (refined precision only) */
 } prg_options;
 
 typedef struct prg_stats {
@@ -96,6 +104,12 @@ void prg_default_options(prg_options *opt);
 /* rust-igraph pagerank() (pagerank.rs:52-143). */
 int32_t prg_pagerank(uint32_t n, uint64_t m, const uint32_t *from, const uint32_t *to, int32_t directed,
                      double *out);
+
+/* rust-igraph pagerank_linsys() (pagerank_linsys.rs:99-160): the same fixed
+ * point as a linear system (I - 0.85 M^T) x = 0.15/n * 1, solved to
+ * ||b - A x||_2 < 1e-13 ||b||_2 from the uniform start; unweighted. */
+int32_t prg_pagerank_linsys(uint32_t n, uint64_t m, const uint32_t *from, const uint32_t *to, int32_t directed,
+                            double *out);
 
 /* rust-igraph pagerank_weighted() (pagerank_weighted.rs:52-161).
  * weights_len is the caller's slice length (checked against m like :62-68). */

@@ -219,6 +219,7 @@ prg::SolveOpts to_solve_opts(const prg_options *o) {
         so.eps = o->eps;
         so.max_iter = o->max_iter;
         so.precision = o->precision;
+        so.inner = o->inner;
         so.stop = o->stop;
         so.normalise = o->normalise;
     }
@@ -271,14 +272,26 @@ int32_t solve_host(prg_graph *h, const prg::SolveOpts &so_in, const double *norm
     return PRG_OK;
 }
 
+int32_t check_options(const prg_options &o) {
+    if (o.precision < PRG_PRECISION_FP64 || o.precision > PRG_PRECISION_LINSYS)
+        return fail(PRG_ERR_INVALID_ARGUMENT, "unknown precision " + std::to_string(o.precision));
+    if (o.inner != PRG_INNER_KRYLOV && o.inner != PRG_INNER_RICHARDSON)
+        return fail(PRG_ERR_INVALID_ARGUMENT, "unknown inner solver " + std::to_string(o.inner));
+    if (o.stop != PRG_STOP_SUCCESSIVE && o.stop != PRG_STOP_ERROR_BOUND)
+        return fail(PRG_ERR_INVALID_ARGUMENT, "unknown stop rule " + std::to_string(o.stop));
+    if (!(o.eps > 0.0)) return fail(PRG_ERR_INVALID_ARGUMENT, "eps must be positive (got " + rust_f64(o.eps) + ")");
+    return PRG_OK;
+}
+
 // One-shot drop-in: build, solve with the reference's constants, download.
 int32_t dropin(uint32_t n, uint64_t m, const uint32_t *from, const uint32_t *to, int32_t directed, const double *w,
-               const double *norm_reset, double damping, double *out) {
+               const double *norm_reset, double damping, double *out, int precision = PRG_PRECISION_FP64) {
     prg_graph *h = nullptr;
     int32_t rc = create_from_host(n, m, from, to, w, directed, &h);
     if (rc != PRG_OK) return rc;
     prg::SolveOpts so;
     so.damping = damping;
+    so.precision = precision;
     try {
         rc = solve_host(h, so, norm_reset, nullptr, out, nullptr);
     } catch (...) {
@@ -315,6 +328,7 @@ void prg_default_options(prg_options *o) {
     o->stop = PRG_STOP_SUCCESSIVE;
     o->normalise = 1;
     o->start = nullptr;
+    o->inner = PRG_INNER_KRYLOV;
 }
 
 const char *prg_last_error(void) { return g_err.c_str(); }
@@ -329,6 +343,19 @@ int32_t prg_pagerank(uint32_t n, uint64_t m, const uint32_t *from, const uint32_
         return PRG_OK;
     }
     return dropin(n, m, from, to, directed, nullptr, nullptr, 0.85, out);
+    PRG_GUARD_END
+}
+
+int32_t prg_pagerank_linsys(uint32_t n, uint64_t m, const uint32_t *from, const uint32_t *to, int32_t directed,
+                            double *out) {
+    g_err.clear();
+    PRG_GUARD_BEGIN
+    if (n == 0) return PRG_OK;  // pagerank_linsys.rs:102-104
+    if (n == 1) {               // pagerank_linsys.rs:105-107
+        out[0] = 1.0;
+        return PRG_OK;
+    }
+    return dropin(n, m, from, to, directed, nullptr, nullptr, 0.85, out, PRG_PRECISION_LINSYS);
     PRG_GUARD_END
 }
 
@@ -500,6 +527,7 @@ int32_t prg_solve(prg_graph *h, const prg_options *opt, const double *reset, dou
     prg_options o;
     prg_default_options(&o);
     if (opt) o = *opt;
+    if (int32_t rc = check_options(o)) return rc;
     const uint32_t n = h->g.n;
     if (n == 0) return PRG_OK;
     if (reset) {
@@ -531,6 +559,7 @@ int32_t prg_solve_device(prg_graph *h, const prg_options *opt, const double *d_r
     prg_options o;
     prg_default_options(&o);
     if (opt) o = *opt;
+    if (int32_t rc = check_options(o)) return rc;
     if (!(o.damping > 0.0 && o.damping < 1.0))
         return fail(PRG_ERR_INVALID_ARGUMENT, "damping (" + rust_f64(o.damping) + ") must be in (0, 1)");
     if (h->g.n < 2) return fail(PRG_ERR_INVALID_ARGUMENT, "device solve needs vcount >= 2");
@@ -788,6 +817,8 @@ int32_t prg_set_tuning(const char *key, int64_t value) {
         t.batch_vec = (uint32_t)value;
     } else if (k == "refine_switch_e12") {
         t.refine_switch = (double)value * 1e-12;
+    } else if (k == "krylov_rel_e12") {
+        t.krylov_rel = (double)value * 1e-12;
     } else if (k == "hot_cache") {
         t.hot_cache = value != 0;
     } else if (k == "unroll") {

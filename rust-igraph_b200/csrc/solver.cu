@@ -39,6 +39,7 @@ constexpr uint32_t kPrepParts = 148u * 4u;
 void workspace_free(Workspace &ws, cudaStream_t s) {
     for (auto &kv : ws.graphs) cudaGraphExecDestroy(kv.second);
     ws.graphs.clear();
+    krylov_free(ws.kry, s);
     for (int i = 0; i < 2; i++) {
         wfree(ws.x64[i], s);
         wfree(ws.xt64[i], s);
@@ -77,7 +78,7 @@ void workspace_ensure(Workspace &ws, const DeviceGraph &g, cudaStream_t s) {
     ws.nhub = g.nhub;
     unsigned gmax = kPrepParts;
     const bool hot = g.perm != nullptr && g.hot_cache;
-    for (int m = 0; m < 4; m++) {
+    for (int m = 0; m < kModes; m++) {
         ws.cfg[m] = iteration_config(m, g.weighted, hot, g.blocks_per_sm, g.n);
         gmax = std::max(gmax, ws.cfg[m].grid);
     }
@@ -108,7 +109,7 @@ void workspace_ensure(Workspace &ws, const DeviceGraph &g, cudaStream_t s) {
     ws.ready = true;
 }
 
-static IterArgs base_args(const DeviceGraph &g, Workspace &ws, double damping) {
+IterArgs base_args(const DeviceGraph &g, Workspace &ws, double damping) {
     IterArgs a;
     std::memset(&a, 0, sizeof(a));
     a.row_ptr = g.row_ptr;
@@ -178,7 +179,7 @@ static void run_loop(Workspace &ws, cudaGraphExec_t exec, uint32_t max_iter, cud
     }
 }
 
-static void read_ctl(Workspace &ws, cudaStream_t s) {
+void read_ctl(Workspace &ws, cudaStream_t s) {
     PRG_CUDA(cudaMemcpyAsync(ws.h_ctl, ws.ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, s));
     PRG_CUDA(cudaStreamSynchronize(s));
 }
@@ -187,14 +188,23 @@ __global__ void to_f32_kernel(const double *a, float *b, uint32_t n) {
     for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) b[v] = (float)a[v];
 }
 
+void to_f32(const double *a, float *b, uint32_t n, cudaStream_t s) {
+    to_f32_kernel<<<148 * 4, kThreads, 0, s>>>(a, b, n);
+    PRG_CUDA(cudaGetLastError());
+}
+
 // FP64 power iteration (PLAIN64 / PPR64) from the start vector until the
 // successive L1 change is < thr or max_iter iterations ran.  Returns the
 // buffer holding the newest iterate.
-static const double *fp64_loop(const DeviceGraph &g, Workspace &ws, const SolveOpts &o, const double *d_t, double thr,
-                               uint32_t max_iter, SolveStats &st, cudaStream_t s) {
+const double *fp64_loop(const DeviceGraph &g, Workspace &ws, const SolveOpts &o, const double *d_t, double thr,
+                        uint32_t max_iter, SolveStats &st, cudaStream_t s) {
     const bool ppr = d_t != nullptr;
-    if (o.d_start) PRG_CUDA(cudaMemcpyAsync(ws.x64[0], o.d_start, (uint64_t)g.n * 8, cudaMemcpyDeviceToDevice, s));
-    else launch_fill_start(ws.x64[0], d_t, g.n, s);
+    if (o.d_start) {
+        if (o.d_start != ws.x64[0])
+            PRG_CUDA(cudaMemcpyAsync(ws.x64[0], o.d_start, (uint64_t)g.n * 8, cudaMemcpyDeviceToDevice, s));
+    } else {
+        launch_fill_start(ws.x64[0], d_t, g.n, s);
+    }
     Ctl c;
     std::memset(&c, 0, sizeof(c));
     c.thr = thr;
@@ -408,7 +418,10 @@ void solve(const DeviceGraph &g, Workspace &ws, const SolveOpts &o_in, const dou
         }
     }
     double *out = g.perm ? ws.out_tmp : d_out;
-    if (o.precision == 1) solve_refined(g, ws, o, t, out, st, s);
+    if (o.precision == 1 && o.inner == 1) solve_refined(g, ws, o, t, out, st, s);
+    else if (o.precision == 1) solve_krylov(g, ws, o, t, out, st, s, false, false);
+    else if (o.precision == 2) solve_krylov(g, ws, o, t, out, st, s, true, false);
+    else if (o.precision == 3) solve_krylov(g, ws, o, t, out, st, s, true, true);
     else solve_fp64(g, ws, o, t, out, st, s);
     if (g.perm) {
         gather_f64(d_out, ws.out_tmp, g.iperm, g.n, s);

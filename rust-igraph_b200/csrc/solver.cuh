@@ -14,12 +14,15 @@ struct SolveOpts {
     double damping = 0.85;
     double eps = 1e-10;
     uint32_t max_iter = 1000;
-    int precision = 0;      // 0 FP64, 1 FP32-refined
+    int precision = 0;      // 0 FP64 power, 1 FP32-refined, 2 FP64 Krylov, 3 pagerank_linsys
     int stop = 0;           // 0 successive (reference), 1 error bound
     int normalise = 1;
     const double *d_start = nullptr;  // device start vector (warm start) or null
-    double refine_switch = 5e-7;      // refined: FP64 steps until the successive change is below this
+    double refine_switch = 5e-7;      // refined (Richardson inner): FP64 steps until the successive change is below this
+    int inner = 0;                    // refined: 0 BiCGStab inner solve, 1 Richardson (power-style) correction
 };
+
+struct KrylovWs;  // krylov.cu
 
 struct SolveStats {
     uint32_t iterations = 0, fp64_passes = 0, fp32_passes = 0, residual_passes = 0;
@@ -32,7 +35,7 @@ struct SolveStats {
 struct Workspace {
     bool ready = false;
     uint32_t n = 0, nrb = 0, nhub = 0;
-    LaunchCfg cfg[4];  // persistent launch shape per iteration mode
+    LaunchCfg cfg[kModes];  // persistent launch shape per iteration mode
     double *x64[2] = {nullptr, nullptr};
     double *xt64[2] = {nullptr, nullptr};
     float *e32[2] = {nullptr, nullptr};
@@ -51,6 +54,7 @@ struct Workspace {
     std::map<uint64_t, cudaGraphExec_t> graphs;
     const void *graphs_rb = nullptr;  // row-block list the cached graphs were captured with
     int unroll = 8;  // iteration pairs per graph launch
+    KrylovWs *kry = nullptr;  // Krylov vectors, allocated on first use
 };
 
 void workspace_ensure(Workspace &ws, const DeviceGraph &g, cudaStream_t s);
@@ -64,5 +68,19 @@ void workspace_free(Workspace &ws, cudaStream_t s);
 // (null = uniform 1/n).  d_out: device double[n].
 void solve(const DeviceGraph &g, Workspace &ws, const SolveOpts &o, const double *d_t, double *d_out,
            SolveStats &st, cudaStream_t s);
+
+// Linear-system solve (krylov.cu): BiCGStab inner solves against FP64
+// residual passes.  fp64_inner = false is the FP32-refined form; linsys
+// applies pagerank_linsys()'s 2-norm stop rule and returns the iterate.
+void solve_krylov(const DeviceGraph &g, Workspace &ws, const SolveOpts &o, const double *d_t, double *d_out,
+                  SolveStats &st, cudaStream_t s, bool fp64_inner, bool linsys);
+void krylov_free(KrylovWs *&k, cudaStream_t s);
+
+// Pieces of the power-iteration driver the Krylov driver reuses (solver.cu).
+IterArgs base_args(const DeviceGraph &g, Workspace &ws, double damping);
+void read_ctl(Workspace &ws, cudaStream_t s);
+const double *fp64_loop(const DeviceGraph &g, Workspace &ws, const SolveOpts &o, const double *d_t, double thr,
+                        uint32_t max_iter, SolveStats &st, cudaStream_t s);
+void to_f32(const double *a, float *b, uint32_t n, cudaStream_t s);
 
 }  // namespace prg

@@ -43,6 +43,15 @@ template <>
 struct ModeT<MODE_CORR32> {
     using A = float;
 };
+template <>
+struct ModeT<MODE_KRY32> {
+    using A = float;
+};
+
+template <int MODE>
+constexpr bool kIs32 = MODE == MODE_CORR32 || MODE == MODE_KRY32;
+template <int MODE>
+constexpr bool kIsKry = MODE == MODE_KRY32 || MODE == MODE_KRY64;
 
 __device__ __forceinline__ void block_sum3(double &a, double &b, double &c, double *sh) {
     a = warp_sum(a);
@@ -88,11 +97,27 @@ template <>
 struct Pre<MODE_CORR32> {
     float old, t, iv, b;
 };
+template <>
+struct Pre<MODE_KRY32> {
+    float in, rh, t;
+};
+template <>
+struct Pre<MODE_KRY64> {
+    double in, rh, t;
+};
 
 template <int MODE>
 __device__ __forceinline__ Pre<MODE> epi_load(const IterArgs &a, uint32_t v) {
     Pre<MODE> p;
-    if constexpr (MODE == MODE_CORR32) {
+    if constexpr (MODE == MODE_KRY32) {
+        p.in = a.x32_in[v];
+        p.rh = a.rh32 ? a.rh32[v] : 0.0f;
+        p.t = a.t32 ? a.t32[v] : (float)a.inv_n;
+    } else if constexpr (MODE == MODE_KRY64) {
+        p.in = a.x64_in[v];
+        p.rh = a.rh64 ? a.rh64[v] : 0.0;
+        p.t = a.t64 ? a.t64[v] : a.inv_n;
+    } else if constexpr (MODE == MODE_CORR32) {
         p.old = a.x32_in[v];
         p.b = a.b32[v];
         p.iv = a.inv32[v];
@@ -110,7 +135,16 @@ __device__ __forceinline__ Pre<MODE> epi_load(const IterArgs &a, uint32_t v) {
 template <int MODE>
 __device__ __forceinline__ void epilogue(const IterArgs &a, const Uni &u, uint32_t v, typename ModeT<MODE>::A y,
                                          const Pre<MODE> &p, double &pd, double &pds, double &ps) {
-    if constexpr (MODE == MODE_CORR32) {
+    if constexpr (kIsKry<MODE>) {
+        // y = p - d*sum - d*dsum_p*t; Uni::dshare holds d*dsum_p
+        using A = typename ModeT<MODE>::A;
+        const A out = p.in - ((A)u.d * y + (A)u.dshare * p.t);
+        if constexpr (MODE == MODE_KRY32) a.x32_out[v] = out;
+        else a.x64_out[v] = out;
+        pd += (double)p.rh * (double)out;
+        pds += (double)out * (double)p.in;
+        ps += (double)out * (double)out;
+    } else if constexpr (MODE == MODE_CORR32) {
         const float df = (float)u.d;
         const float out = df * y + ((float)(u.d * u.dsum)) * p.t + p.b;
         a.x32_out[v] = out;
@@ -132,9 +166,12 @@ __device__ __forceinline__ void epilogue(const IterArgs &a, const Uni &u, uint32
             pd += fabs(r);
             ps += out;
             const float r32 = (float)r;
-            a.b32_out[v] = r32;
-            a.x32_out[v] = r32;  // the correction iteration starts from e0 = r
-            a.xt32_out[v] = r32 * p.iv;
+            if (a.b64_out) a.b64_out[v] = r;
+            if (a.b32_out) a.b32_out[v] = r32;
+            if (a.x32_out) {
+                a.x32_out[v] = r32;  // the correction iteration starts from e0 = r
+                a.xt32_out[v] = r32 * p.iv;
+            }
             if (p.dv == 0.0) pds += (double)r32;
         } else {
             pd += fabs(out - p.old);
@@ -150,7 +187,7 @@ __device__ __forceinline__ void epilogue(const IterArgs &a, const Uni &u, uint32
 
 template <int MODE>
 __device__ __forceinline__ const typename ModeT<MODE>::A *gather_src(const IterArgs &a) {
-    if constexpr (MODE == MODE_CORR32) return a.xt32_in;
+    if constexpr (kIs32<MODE>) return a.xt32_in;
     else return a.xt64_in;
 }
 
@@ -172,7 +209,7 @@ __device__ __forceinline__ void quad(const IterArgs &a, uint32_t base, uint32_t 
     const uint32_t cc[4] = {c.x, c.y, c.z, c.w};
     A wv[4] = {A(1), A(1), A(1), A(1)};
     if constexpr (W) {
-        if constexpr (MODE == MODE_CORR32) {
+        if constexpr (kIs32<MODE>) {
             const float4 q = ld_stream_f4(reinterpret_cast<const float4 *>(a.w32 + base), pol_s);
             wv[0] = q.x; wv[1] = q.y; wv[2] = q.z; wv[3] = q.w;
         } else {
@@ -263,7 +300,7 @@ __device__ __forceinline__ typename ModeT<MODE>::A warp_row_sum(const IterArgs &
 
 // Dynamic shared memory layout: [NT/32 warp buffers of kWarpBuf][hot prefix].
 template <int MODE, bool W, int NT>
-__global__ void __launch_bounds__(NT, NT == kThreads ? (MODE == MODE_CORR32 ? 5 : 4) : 1) iter_kernel(const IterArgs a) {
+__global__ void __launch_bounds__(NT, NT == kThreads ? (kIs32<MODE> ? 5 : 4) : 1) iter_kernel(const IterArgs a) {
     using A = typename ModeT<MODE>::A;
     constexpr int kW = NT / 32;
     constexpr bool HOT = NT == kThreadsBig;
@@ -274,7 +311,9 @@ __global__ void __launch_bounds__(NT, NT == kThreads ? (MODE == MODE_CORR32 ? 5 
     __shared__ int s_flag;
 
     Ctl *ctl = a.ctl;
-    if constexpr (MODE != MODE_RESID64) {
+    if constexpr (kIsKry<MODE>) {
+        if (*(volatile const int32_t *)a.kdone) return;
+    } else if constexpr (MODE != MODE_RESID64) {
         if (*(volatile int32_t *)&ctl->done) return;
     }
     const uint32_t hot = HOT ? a.hot : 0u;
@@ -290,8 +329,20 @@ __global__ void __launch_bounds__(NT, NT == kThreads ? (MODE == MODE_CORR32 ? 5 
     const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     Uni u;
     u.d = a.damping;
-    u.dsum = *(volatile double *)&ctl->dsum[a.parity];
-    {
+    if constexpr (kIsKry<MODE>) {
+        // dangling mass of the input vector: the producer's per-block
+        // records summed in a fixed order (identical in every block)
+        __shared__ double s_dz;
+        double dz = 0.0, z1 = 0.0, z2 = 0.0;
+        for (uint32_t i = threadIdx.x; i < a.kpart_n; i += NT) dz += a.kpart_in[i].x;
+        block_sum3(dz, z1, z2, s_red);
+        if (threadIdx.x == 0) s_dz = dz;
+        __syncthreads();
+        u.dsum = s_dz;
+        u.tele = 0.0;
+        u.dshare = u.d * u.dsum;
+    } else {
+        u.dsum = *(volatile double *)&ctl->dsum[a.parity];
         const double nf = (double)a.n;
         u.tele = __ddiv_rn(1.0 - u.d, nf);
         u.dshare = __ddiv_rn(__dmul_rn(u.d, u.dsum), nf);
@@ -372,6 +423,11 @@ __global__ void __launch_bounds__(NT, NT == kThreads ? (MODE == MODE_CORR32 ? 5 
     // ---- deterministic reduction of (diff, dangling, sum): block tree, then
     // the last block adds block and hub records in index order
     block_sum3(pd, pds, ps, s_red);
+    if constexpr (kIsKry<MODE>) {
+        // the consumer adds block and hub records itself
+        if (threadIdx.x == 0) a.kpart_out[blockIdx.x] = make_double4(pd, pds, ps, 0.0);
+        return;
+    }
     if (threadIdx.x == 0) {
         a.blk_part[blockIdx.x] = make_double4(pd, pds, ps, 0.0);
         __threadfence();
@@ -463,6 +519,15 @@ LaunchCfg iteration_config(int mode, bool weighted, bool hot_cache, uint32_t blo
         case MODE_PLAIN64: PRG_CFG(MODE_PLAIN64); break;
         case MODE_PPR64: PRG_CFG(MODE_PPR64); break;
         case MODE_RESID64: PRG_CFG(MODE_RESID64); break;
+        case MODE_KRY32:
+            // Krylov matvecs always run the 256-thread shape
+            if (weighted) kernel_config<MODE_KRY32, true, kThreads>(false, blocks_per_sm, n, c);
+            else kernel_config<MODE_KRY32, false, kThreads>(false, blocks_per_sm, n, c);
+            break;
+        case MODE_KRY64:
+            if (weighted) kernel_config<MODE_KRY64, true, kThreads>(false, blocks_per_sm, n, c);
+            else kernel_config<MODE_KRY64, false, kThreads>(false, blocks_per_sm, n, c);
+            break;
         default: PRG_CFG(MODE_CORR32); break;
     }
 #undef PRG_CFG
@@ -487,6 +552,14 @@ void launch_iteration(int mode, bool weighted, const IterArgs &a_in, const Launc
         case MODE_PPR64: PRG_LAUNCH(MODE_PPR64); break;
         case MODE_RESID64: PRG_LAUNCH(MODE_RESID64); break;
         case MODE_CORR32: PRG_LAUNCH(MODE_CORR32); break;
+        case MODE_KRY32:
+            if (weighted) iter_kernel<MODE_KRY32, true, kThreads><<<grid, block, c.smem, s>>>(a);
+            else iter_kernel<MODE_KRY32, false, kThreads><<<grid, block, c.smem, s>>>(a);
+            break;
+        case MODE_KRY64:
+            if (weighted) iter_kernel<MODE_KRY64, true, kThreads><<<grid, block, c.smem, s>>>(a);
+            else iter_kernel<MODE_KRY64, false, kThreads><<<grid, block, c.smem, s>>>(a);
+            break;
         default: break;
     }
 #undef PRG_LAUNCH

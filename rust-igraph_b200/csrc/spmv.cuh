@@ -21,7 +21,13 @@ enum IterMode : int {
     MODE_RESID64 = 2,
     // FP32 correction iteration  e' = d*P^T(e/s) + d*dsum_e*t + r
     MODE_CORR32 = 3,
+    // Krylov matvec y = A p of the PageRank linear system
+    //   A p = p - d*P^T(p/s) - d*dsum_p*t     (pagerank_linsys.rs:221-238)
+    // with the dot products (rh.y, y.p, y.y) reduced per block
+    MODE_KRY32 = 4,  // FP32 vectors and gathers
+    MODE_KRY64 = 5,  // FP64 vectors and gathers
 };
+constexpr int kModes = 6;
 
 struct IterArgs {
     // graph
@@ -48,6 +54,15 @@ struct IterArgs {
     const float *t32;
     const float *b32;   // CORR32: additive residual r
     float *b32_out;     // RESID64: residual r written here
+    double *b64_out;    // RESID64: residual r in FP64 (optional)
+    // Krylov matvec (MODE_KRY*): the input vector p is x*_in, its scaled copy
+    // p/s is xt*_in, y goes to x*_out; rh* (optional) is the shadow residual
+    const float *rh32;
+    const double *rh64;
+    const double4 *kpart_in;  // producer's per-block records; .x summed = dangling mass of p
+    uint32_t kpart_n;
+    double4 *kpart_out;       // per-block (rh.y, y.p, y.y)
+    const int32_t *kdone;     // nonzero: the Krylov solve has stopped, return at once
     // scalars
     double damping;
     double inv_n;

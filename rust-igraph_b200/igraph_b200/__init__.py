@@ -68,7 +68,7 @@ _ERRORS = {1: InvalidArgument, 2: VertexOutOfRange, 3: Internal, 4: Internal, 5:
 class prg_options(C.Structure):
     _fields_ = [("damping", C.c_double), ("eps", C.c_double), ("max_iter", C.c_uint32),
                 ("precision", C.c_int32), ("stop", C.c_int32), ("normalise", C.c_int32),
-                ("start", C.c_void_p)]
+                ("start", C.c_void_p), ("inner", C.c_int32)]
 
 
 class prg_stats(C.Structure):
@@ -112,6 +112,8 @@ def lib():
     L.prg_last_error.argtypes = []
     L.prg_pagerank.restype = C.c_int32
     L.prg_pagerank.argtypes = [C.c_uint32, C.c_uint64, u32p, u32p, C.c_int32, f64p]
+    L.prg_pagerank_linsys.restype = C.c_int32
+    L.prg_pagerank_linsys.argtypes = [C.c_uint32, C.c_uint64, u32p, u32p, C.c_int32, f64p]
     L.prg_pagerank_weighted.restype = C.c_int32
     L.prg_pagerank_weighted.argtypes = [C.c_uint32, C.c_uint64, u32p, u32p, C.c_int32, f64p, C.c_uint64, f64p]
     L.prg_personalized_pagerank.restype = C.c_int32
@@ -275,6 +277,16 @@ def pagerank(graph: Graph) -> np.ndarray:
     return out[:n]
 
 
+def pagerank_linsys(graph: Graph) -> np.ndarray:
+    """rust-igraph ``pagerank_linsys(&Graph)`` (pagerank_linsys.rs:99-160): the
+    linear-system form solved on the GPU to ||b - Ax||_2 < 1e-13 ||b||_2."""
+    n = graph.vcount()
+    f, t = graph.edge_arrays()
+    out = np.empty(max(n, 1), np.float64)
+    _check(lib().prg_pagerank_linsys(n, len(f), _ptr(f), _ptr(t), int(graph.is_directed()), _ptr(out)))
+    return out[:n]
+
+
 def pagerank_weighted(graph: Graph, weights) -> np.ndarray:
     """rust-igraph ``pagerank_weighted(&Graph, &[f64])`` (pagerank_weighted.rs:52-161)."""
     n = graph.vcount()
@@ -320,6 +332,10 @@ def personalized_pagerank_vs(graph: Graph, reset_vids, damping: float) -> np.nda
 
 PRECISION_FP64 = 0
 PRECISION_FP32_REFINED = 1
+PRECISION_FP64_KRYLOV = 2
+PRECISION_LINSYS = 3
+INNER_KRYLOV = 0
+INNER_RICHARDSON = 1
 STOP_SUCCESSIVE = 0
 STOP_ERROR_BOUND = 1
 
@@ -332,12 +348,14 @@ class Options:
     precision: int = PRECISION_FP64
     stop: int = STOP_SUCCESSIVE
     normalise: bool = True
+    inner: int = INNER_KRYLOV
 
     def to_c(self, start_ptr=None) -> prg_options:
         o = prg_options()
         o.damping, o.eps, o.max_iter = self.damping, self.eps, self.max_iter
         o.precision, o.stop, o.normalise = self.precision, self.stop, int(self.normalise)
         o.start = start_ptr
+        o.inner = self.inner
         return o
 
 
@@ -508,7 +526,7 @@ def set_tuning(key: str, value: int) -> None:
 
 
 TUNING_DEFAULTS = {"capw": 256, "shortmax": 256, "split": 8192, "blocks_per_sm": 0, "relabel": 2, "unroll": 8,
-                   "hot_cache": 0, "refine_switch_e12": 500000, "batch_vec": 1}
+                   "hot_cache": 0, "refine_switch_e12": 500000, "batch_vec": 1, "krylov_rel_e12": 10_000_000}
 
 
 def reset_tuning() -> None:

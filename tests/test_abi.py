@@ -37,6 +37,26 @@ def test_default_options_match_reference_constants():
     ig.lib().prg_default_options(C.byref(o))
     # pagerank.rs:23-25
     assert (o.damping, o.eps, o.max_iter, o.precision, o.stop, o.normalise) == (0.85, 1e-10, 1000, 0, 0, 1)
+    assert o.inner == ig.INNER_KRYLOV
+
+
+def test_linsys_trivial_graphs_need_no_device():
+    # pagerank_linsys.rs:102-107 and its tests :382-392
+    assert len(ig.pagerank_linsys(ig.Graph.with_vertices(0))) == 0
+    assert list(ig.pagerank_linsys(ig.Graph.with_vertices(1))) == [1.0]
+
+
+def test_unknown_options_are_rejected_before_device_work():
+    L = ig.lib()
+    for field, value, msg in (("precision", 7, "unknown precision 7"), ("inner", 5, "unknown inner solver 5"),
+                              ("stop", 3, "unknown stop rule 3")):
+        o = ig.prg_options()
+        L.prg_default_options(C.byref(o))
+        setattr(o, field, value)
+        out = np.empty(1)
+        rc = L.prg_solve(C.c_void_p(1), C.byref(o), None, out.ctypes.data_as(C.POINTER(C.c_double)), None)
+        assert rc == 1, field
+        assert L.prg_last_error().decode() == msg
 
 
 def test_trivial_graphs_need_no_device():
