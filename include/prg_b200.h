@@ -93,6 +93,9 @@ typedef struct prg_stats {
     uint32_t kernel_launches;  /* CUDA kernels this solve launched (graph nodes included) */
     double fp32_ms;            /* device time of the FP32 iteration graphs (CUDA events) */
     double fp64_ms;            /* device time of the FP64 iteration graphs / residual passes */
+    double spmv_ms;            /* device time of the SpMV launches that did work: the power iteration's
+                                  graphs, or the Krylov inner solve's matvec kernels (CUDA events) */
+    uint32_t spmv_launches;    /* the SpMV launches spmv_ms covers */
 } prg_stats;
 
 /* Fills the reference defaults: d = 0.85, eps = 1e-10, max_iter = 1000,

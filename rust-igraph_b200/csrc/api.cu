@@ -243,6 +243,8 @@ void fill_stats(prg_stats *st, const prg::SolveStats &s, const prg_graph *h) {
     st->kernel_launches = s.kernel_launches;
     st->fp32_ms = s.fp32_ms;
     st->fp64_ms = s.fp64_ms;
+    st->spmv_ms = s.spmv_ms;
+    st->spmv_launches = s.spmv_launches;
 }
 
 // Host-side solve: stages the (already normalised) reset and start vectors,

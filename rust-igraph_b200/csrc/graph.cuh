@@ -62,7 +62,7 @@ struct Tuning {
     bool hot_cache = false;
     double refine_switch = 5e-7;
     uint32_t batch_vec = 1;
-    double krylov_rel = 1e-5;  // refined Krylov: relative residual reduction per FP32 inner solve
+    double krylov_rel = 1e-4;  // refined Krylov: relative residual reduction per FP32 inner solve
 };
 Tuning &tuning();
 

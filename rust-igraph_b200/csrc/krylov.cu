@@ -32,6 +32,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <vector>
 
 #include "solver.cuh"
 
@@ -71,6 +72,7 @@ struct KrylovWs {
     KState *st = nullptr;
     KState *h_st = nullptr;  // pinned, two slots
     cudaEvent_t ev[2] = {nullptr, nullptr};
+    std::vector<cudaEvent_t> mv_ev;  // around each matvec launch: 4 per step
 };
 
 template <class T>
@@ -101,6 +103,7 @@ void krylov_free(KrylovWs *&k, cudaStream_t s) {
     if (k->h_st) cudaFreeHost(k->h_st);
     for (cudaEvent_t &e : k->ev)
         if (e) cudaEventDestroy(e);
+    for (cudaEvent_t e : k->mv_ev) cudaEventDestroy(e);
     delete k;
     k = nullptr;
 }
@@ -254,9 +257,9 @@ __global__ void __launch_bounds__(kVT) kv1(uint32_t n, int q, KState *st, const 
     const T tb = (T)beta, to = (T)om;
     double dz = 0.0;
     for (uint32_t i = blockIdx.x * kVT + threadIdx.x; i < n; i += gridDim.x * kVT) {
-        const T rv = r[i];
-        const T pv = restart ? rv : rv + tb * (p[i] - to * v[i]);
-        p[i] = pv;
+        const T rv = __ldcs(r + i);
+        const T pv = restart ? rv : rv + tb * (__ldcs(p + i) - to * __ldcs(v + i));
+        __stcs(p + i, pv);  // streamed: only p/s is gathered, keep that in L2
         bool dang;
         pt[i] = kscaled(pv, i, inv32, dval, dang);
         if (dang) dz += (double)pv;
@@ -288,8 +291,8 @@ __global__ void __launch_bounds__(kVT) kv2(uint32_t n, int q, KState *st, const 
     const T ta = (T)al;
     double dz = 0.0;
     for (uint32_t i = blockIdx.x * kVT + threadIdx.x; i < n; i += gridDim.x * kVT) {
-        const T sv = r[i] - ta * v[i];
-        s[i] = sv;
+        const T sv = __ldcs(r + i) - ta * __ldcs(v + i);
+        __stcs(s + i, sv);
         bool dang;
         sst[i] = kscaled(sv, i, inv32, dval, dang);
         if (dang) dz += (double)sv;
@@ -312,11 +315,11 @@ __global__ void __launch_bounds__(kVT) kv3(uint32_t n, int q, KState *st, const 
     const T ta = (T)st->alpha[q], to = (T)om;
     double a = 0.0, b = 0.0, c = 0.0;
     for (uint32_t i = blockIdx.x * kVT + threadIdx.x; i < n; i += gridDim.x * kVT) {
-        const T sv = s[i];
-        e[i] = e[i] + ta * p[i] + to * sv;
-        const T rv = sv - to * t[i];
-        r[i] = rv;
-        a += (double)rh[i] * (double)rv;
+        const T sv = __ldcs(s + i);
+        __stcs(e + i, __ldcs(e + i) + ta * __ldcs(p + i) + to * sv);
+        const T rv = sv - to * __ldcs(t + i);
+        __stcs(r + i, rv);
+        a += (double)__ldcs(rh + i) * (double)rv;
         b += fabs((double)rv);
         c += (double)rv * (double)rv;
     }
@@ -341,6 +344,7 @@ struct InnerResult {
     int32_t done = KRUN;
     double rnorm = 0.0;
     double ms = 0.0;
+    double matvec_ms = 0.0;  // the matvec launches of completed steps
     uint32_t launches = 0;
 };
 
@@ -391,15 +395,29 @@ static InnerResult bicgstab(const DeviceGraph &g, Workspace &ws, KrylovWs &k, KB
     const IterArgs m1 = matvec_args<T>(base, b.p, b.pt, b.v, b.rh, k.part1, kVB, k.part2, k.st);
     const IterArgs m2 = matvec_args<T>(base, b.s, b.st, b.t, (const T *)nullptr, k.part3, kVB, k.part4, k.st);
 
+    // the matvec launches are bracketed by events (4 per step) so their
+    // device time can be reported apart from the vector kernels
+    const uint32_t max_steps = (cap / 2u + 3u) * 2u + 2u;
     PRG_CUDA(cudaEventRecord(ws.eva, s));
     kv0<T><<<kVB, kVT, 0, s>>>(n, r, b.rh, b.e, k.part5);
     res.launches += 1u;
+    uint32_t it = 0;
     auto step = [&](int q) {
+        while (k.mv_ev.size() < 4u * (it + 1u)) {
+            cudaEvent_t e;
+            PRG_CUDA(cudaEventCreate(&e));
+            k.mv_ev.push_back(e);
+        }
+        cudaEvent_t *ev = &k.mv_ev[4u * it];
         kv1<T><<<kVB, kVT, 0, s>>>(n, q, k.st, k.part5, b.rh, r, b.p, b.pt, b.v, g.inv32, g.dval, k.part1);
+        PRG_CUDA(cudaEventRecord(ev[0], s));
         launch_iteration(mode, g.weighted, m1, cfg, s);
+        PRG_CUDA(cudaEventRecord(ev[1], s));
         kv2<T><<<kVB, kVT, 0, s>>>(n, q, k.st, k.part2, cfg.grid, ws.hub_rec, g.nhub, r, b.v, b.s, b.st, g.inv32,
                                     g.dval, k.part3);
+        PRG_CUDA(cudaEventRecord(ev[2], s));
         launch_iteration(mode, g.weighted, m2, cfg, s);
+        PRG_CUDA(cudaEventRecord(ev[3], s));
         kv3<T><<<kVB, kVT, 0, s>>>(n, q, k.st, k.part4, cfg.grid, ws.hub_rec, g.nhub, b.rh, b.p, b.s, b.t, b.e, r,
                                     k.part5);
         res.launches += 5u;
@@ -408,10 +426,13 @@ static InnerResult bicgstab(const DeviceGraph &g, Workspace &ws, KrylovWs &k, KB
     // j+1 runs (kernels of a finished solve return at once)
     const int per = 2;
     const uint32_t max_batches = cap / per + 3u;
-    uint32_t batch = 0, it = 0;
+    uint32_t batch = 0;
     bool stop = false;
     while (!stop) {
-        for (int i = 0; i < per; i++) step((int)(it++ & 1u));
+        for (int i = 0; i < per && it < max_steps; i++) {
+            step((int)(it & 1u));
+            it++;
+        }
         const int slot = (int)(batch & 1u);
         PRG_CUDA(cudaMemcpyAsync(&k.h_st[slot], k.st, sizeof(KState), cudaMemcpyDeviceToHost, s));
         PRG_CUDA(cudaEventRecord(k.ev[slot], s));
@@ -430,6 +451,12 @@ static InnerResult bicgstab(const DeviceGraph &g, Workspace &ws, KrylovWs &k, KB
     PRG_CUDA(cudaEventElapsedTime(&ms, ws.eva, ws.evb));
     res.ms = ms;
     res.steps = k.h_st[0].count;
+    for (uint32_t i = 0; i < res.steps && i < it; i++) {
+        float a = 0.f, b2 = 0.f;
+        PRG_CUDA(cudaEventElapsedTime(&a, k.mv_ev[4u * i], k.mv_ev[4u * i + 1u]));
+        PRG_CUDA(cudaEventElapsedTime(&b2, k.mv_ev[4u * i + 2u], k.mv_ev[4u * i + 3u]));
+        res.matvec_ms += (double)a + (double)b2;
+    }
     res.done = k.h_st[0].done;
     res.rnorm = k.h_st[0].rnorm;
     if (std::getenv("PRG_TRACE"))
@@ -520,6 +547,8 @@ void solve_krylov(const DeviceGraph &g, Workspace &ws, const SolveOpts &o, const
             ir = bicgstab<float>(g, ws, k, k.f, ws.b32, nullptr, ppr ? ws.t32 : nullptr, o.damping, rel, floor_abs,
                                  cap, false, s);
         mv += 2u * ir.steps;
+        st.spmv_ms += ir.matvec_ms;
+        st.spmv_launches += 2u * ir.steps;
         st.kernel_launches += ir.launches;
         st.fp32_ms += fp64_inner ? 0.0 : ir.ms;
         st.fp64_ms += fp64_inner ? ir.ms : 0.0;

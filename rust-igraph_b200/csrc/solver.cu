@@ -227,11 +227,14 @@ const double *fp64_loop(const DeviceGraph &g, Workspace &ws, const SolveOpts &o,
     const int mode = ppr ? MODE_PPR64 : MODE_PLAIN64;
     if (max_iter > 0) {
         cudaGraphExec_t ex = loop_graph(g, ws, mode, ppr, o.damping, a0, a1, s);
+        const double before = st.fp64_ms;
         run_loop(ws, ex, max_iter, s, &st.fp64_ms, &st.kernel_launches);
+        st.spmv_ms += st.fp64_ms - before;
     } else {
         read_ctl(ws, s);
     }
     const Ctl &h = *ws.h_ctl;
+    st.spmv_launches += h.iters;
     st.fp64_passes += h.iters;
     st.iterations += h.iters;
     st.last_diff = h.diff;
@@ -325,7 +328,10 @@ static void solve_refined(const DeviceGraph &g, Workspace &ws, const SolveOpts &
         if (std::getenv("PRG_TRACE"))
             std::fprintf(stderr, "[prg] residual pass %u: ||r||_1 = %.3e (after %u fp32 passes)\n", fp64, rn, fp32);
         if (!(rn > thr_final) || fp32 + fp64 >= pass_cap) break;
+        const double before = st.fp32_ms;
         run_loop(ws, ex, inner_cap, s, &st.fp32_ms, &st.kernel_launches);
+        st.spmv_ms += st.fp32_ms - before;
+        st.spmv_launches += ws.h_ctl->iters;
         fp32 += ws.h_ctl->iters;
         const float *e_fin = ws.h_ctl->parity_last == 0 ? ws.e32[1] : ws.e32[0];
         launch_prepare64(g, ws.x64[0], e_fin, ws.xt64[0], ws.ctl, 1, ws.blk_part, s);

@@ -29,6 +29,8 @@ struct SolveStats {
     double last_diff = 0, residual_l1 = 0, error_bound = 0, solve_ms = 0;
     uint32_t kernel_launches = 0;
     double fp32_ms = 0, fp64_ms = 0;
+    double spmv_ms = 0;          // SpMV launches that did work (power graphs / Krylov matvecs)
+    uint32_t spmv_launches = 0;
 };
 
 // Reusable per-handle solve buffers and captured CUDA graphs.

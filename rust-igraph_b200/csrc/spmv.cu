@@ -110,12 +110,12 @@ template <int MODE>
 __device__ __forceinline__ Pre<MODE> epi_load(const IterArgs &a, uint32_t v) {
     Pre<MODE> p;
     if constexpr (MODE == MODE_KRY32) {
-        p.in = a.x32_in[v];
-        p.rh = a.rh32 ? a.rh32[v] : 0.0f;
+        p.in = __ldcs(a.x32_in + v);
+        p.rh = a.rh32 ? __ldcs(a.rh32 + v) : 0.0f;
         p.t = a.t32 ? a.t32[v] : (float)a.inv_n;
     } else if constexpr (MODE == MODE_KRY64) {
-        p.in = a.x64_in[v];
-        p.rh = a.rh64 ? a.rh64[v] : 0.0;
+        p.in = __ldcs(a.x64_in + v);
+        p.rh = a.rh64 ? __ldcs(a.rh64 + v) : 0.0;
         p.t = a.t64 ? a.t64[v] : a.inv_n;
     } else if constexpr (MODE == MODE_CORR32) {
         p.old = a.x32_in[v];
@@ -139,8 +139,8 @@ __device__ __forceinline__ void epilogue(const IterArgs &a, const Uni &u, uint32
         // y = p - d*sum - d*dsum_p*t; Uni::dshare holds d*dsum_p
         using A = typename ModeT<MODE>::A;
         const A out = p.in - ((A)u.d * y + (A)u.dshare * p.t);
-        if constexpr (MODE == MODE_KRY32) a.x32_out[v] = out;
-        else a.x64_out[v] = out;
+        if constexpr (MODE == MODE_KRY32) __stcs(a.x32_out + v, out);
+        else __stcs(a.x64_out + v, out);
         pd += (double)p.rh * (double)out;
         pds += (double)out * (double)p.in;
         ps += (double)out * (double)out;

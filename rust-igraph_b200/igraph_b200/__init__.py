@@ -76,7 +76,8 @@ class prg_stats(C.Structure):
                 ("residual_passes", C.c_uint32), ("last_diff", C.c_double), ("residual_l1", C.c_double),
                 ("error_bound", C.c_double), ("solve_ms", C.c_double), ("build_ms", C.c_double),
                 ("arcs", C.c_uint64), ("n_dangling", C.c_uint32), ("kernel_launches", C.c_uint32),
-                ("fp32_ms", C.c_double), ("fp64_ms", C.c_double)]
+                ("fp32_ms", C.c_double), ("fp64_ms", C.c_double), ("spmv_ms", C.c_double),
+                ("spmv_launches", C.c_uint32)]
 
 
 class prg_batch_stats(C.Structure):
@@ -375,12 +376,14 @@ class Stats:
     kernel_launches: int
     fp32_ms: float
     fp64_ms: float
+    spmv_ms: float = 0.0
+    spmv_launches: int = 0
 
     @classmethod
     def from_c(cls, s: prg_stats) -> "Stats":
         return cls(s.iterations, s.fp64_passes, s.fp32_passes, s.residual_passes, s.last_diff, s.residual_l1,
                    s.error_bound, s.solve_ms, s.build_ms, s.arcs, s.n_dangling, s.kernel_launches, s.fp32_ms,
-                   s.fp64_ms)
+                   s.fp64_ms, s.spmv_ms, s.spmv_launches)
 
 
 class DeviceGraph:
@@ -526,7 +529,7 @@ def set_tuning(key: str, value: int) -> None:
 
 
 TUNING_DEFAULTS = {"capw": 256, "shortmax": 256, "split": 8192, "blocks_per_sm": 0, "relabel": 2, "unroll": 8,
-                   "hot_cache": 0, "refine_switch_e12": 500000, "batch_vec": 1, "krylov_rel_e12": 10_000_000}
+                   "hot_cache": 0, "refine_switch_e12": 500000, "batch_vec": 1, "krylov_rel_e12": 100_000_000}
 
 
 def reset_tuning() -> None:
