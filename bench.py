@@ -207,6 +207,24 @@ def _cpu_model():
 # ------------------------------------------------------------------ our arm
 
 
+def reduce_scalar(v, op, world_size, device):
+    """max or sum of one float over the ranks (NCCL on GPUs, gloo on CPUs);
+    every rank takes the same collective steps."""
+    if world_size == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([float(v)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX if op == "max" else dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def whole_job_value(units, ms, world_size, device):
+    """Whole-job throughput: units summed over ranks / the slowest rank's time."""
+    return reduce_scalar(units, "sum", world_size, device) / (reduce_scalar(ms, "max", world_size, device) / 1e3)
+
+
 def load_traffic():
     """DRAM traffic of the FP32 Krylov matvec from the committed ncu summary
     (profiles/ncu_traffic.txt, `key value` lines): bytes read + written per
@@ -249,11 +267,7 @@ def main():
             dist.barrier()
 
     def reduce(v, op):
-        if ws == 1:
-            return v
-        t = torch.tensor([float(v)], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX if op == "max" else dist.ReduceOp.SUM)
-        return float(t.item())
+        return reduce_scalar(v, op, ws, "cuda")
 
     scale, ef = args.scale, args.edge_factor
     n, m = 1 << scale, ef << scale

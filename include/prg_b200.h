@@ -215,7 +215,9 @@ int32_t prg_autotune(prg_graph *g, int32_t tune_batch, const char *cache_path, p
  * corrections; default 500000), "batch_vec" (batched columns per lane: 1, 2
  * or 4), "hot_cache" (1: relabelled graphs gather
  * their hot vertices from shared memory), "unroll" (iteration pairs per CUDA
- * graph). */
+ * graph), "krylov_rel_e12" (refined precision with the Krylov inner solver:
+ * each FP32 inner solve reduces the residual by value * 1e-12; default 1e8,
+ * i.e. 1e-4). */
 int32_t prg_set_tuning(const char *key, int64_t value);
 
 /* ---- batched personalized PageRank ---------------------------------- */
