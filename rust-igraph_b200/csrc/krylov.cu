@@ -4,8 +4,8 @@
 //   G(x) = d*P^T(x/s) + d*(sum_dangling x)*t + (1-d)*t
 // is the solution of the non-singular system A x = (1-d)*t with
 //   A x = x - d*P^T(x/s) - d*(sum_dangling x)*t            (pagerank_linsys.rs:221-238)
-// and b - A x = G(x) - x: the FP64 residual pass of the refined solver
-// (MODE_RESID64) already computes it.  Two solvers are built on that:
+// and b - A x = G(x) - x: an FP64 power step that also writes r = G(x) - x
+// (MODE_KRES64) computes it.  Two solvers are built on that:
 //
 //  * refined (FP32 Krylov, FP64 residual): repeat { r = G(x) - x in FP64;
 //    stop when ||r||_1 <= eps*(1-d)/d; solve A e = r with BiCGStab in FP32
@@ -514,7 +514,7 @@ void solve_krylov(const DeviceGraph &g, Workspace &ws, const SolveOpts &o, const
     bool fallback = false;
     for (int outer = 0; outer < 64; outer++) {
         PRG_CUDA(cudaEventRecord(ws.eva, s));
-        launch_iteration(MODE_RESID64, g.weighted, rp, ws.cfg[MODE_RESID64], s);
+        launch_iteration(MODE_KRES64, g.weighted, rp, ws.cfg[MODE_KRES64], s);
         PRG_CUDA(cudaEventRecord(ws.evb, s));
         fp64++;
         st.kernel_launches += 1u;

@@ -105,6 +105,10 @@ template <>
 struct Pre<MODE_KRY64> {
     double in, rh, t;
 };
+template <>
+struct Pre<MODE_KRES64> {
+    double old, t;
+};
 
 template <int MODE>
 __device__ __forceinline__ Pre<MODE> epi_load(const IterArgs &a, uint32_t v) {
@@ -117,6 +121,9 @@ __device__ __forceinline__ Pre<MODE> epi_load(const IterArgs &a, uint32_t v) {
         p.in = __ldcs(a.x64_in + v);
         p.rh = a.rh64 ? __ldcs(a.rh64 + v) : 0.0;
         p.t = a.t64 ? a.t64[v] : a.inv_n;
+    } else if constexpr (MODE == MODE_KRES64) {
+        p.old = __ldcs(a.x64_in + v);
+        p.t = a.t64 ? a.t64[v] : 0.0;
     } else if constexpr (MODE == MODE_CORR32) {
         p.old = a.x32_in[v];
         p.b = a.b32[v];
@@ -161,7 +168,13 @@ __device__ __forceinline__ void epilogue(const IterArgs &a, const Uni &u, uint32
             out = __dadd_rn(__dadd_rn(u.tele, u.dshare), __dmul_rn(u.d, y));
         }
         a.x64_out[v] = out;
-        if constexpr (MODE == MODE_RESID64) {
+        if constexpr (MODE == MODE_KRES64) {
+            const double r = out - p.old;
+            pd += fabs(r);
+            ps += out;
+            if (a.b64_out) __stcs(a.b64_out + v, r);
+            else __stcs(a.b32_out + v, (float)r);
+        } else if constexpr (MODE == MODE_RESID64) {
             const double r = out - p.old;
             pd += fabs(r);
             ps += out;
@@ -313,7 +326,7 @@ __global__ void __launch_bounds__(NT, NT == kThreads ? (kIs32<MODE> ? 5 : 4) : 1
     Ctl *ctl = a.ctl;
     if constexpr (kIsKry<MODE>) {
         if (*(volatile const int32_t *)a.kdone) return;
-    } else if constexpr (MODE != MODE_RESID64) {
+    } else if constexpr (MODE != MODE_RESID64 && MODE != MODE_KRES64) {
         if (*(volatile int32_t *)&ctl->done) return;
     }
     const uint32_t hot = HOT ? a.hot : 0u;
@@ -457,7 +470,7 @@ __global__ void __launch_bounds__(NT, NT == kThreads ? (kIs32<MODE> ? 5 : 4) : 1
         const double diff = x + hx, dsn = y + hy, sum = z + hz;
         ctl->groups_done = 0u;
         ctl->dsum[a.parity ^ 1] = dsn;
-        if constexpr (MODE == MODE_RESID64) {
+        if constexpr (MODE == MODE_RESID64 || MODE == MODE_KRES64) {
             ctl->rnorm = diff;
             ctl->gsum = sum;
             ctl->resid_passes += 1u;
@@ -528,6 +541,10 @@ LaunchCfg iteration_config(int mode, bool weighted, bool hot_cache, uint32_t blo
             if (weighted) kernel_config<MODE_KRY64, true, kThreads>(false, blocks_per_sm, n, c);
             else kernel_config<MODE_KRY64, false, kThreads>(false, blocks_per_sm, n, c);
             break;
+        case MODE_KRES64:
+            if (weighted) kernel_config<MODE_KRES64, true, kThreads>(false, blocks_per_sm, n, c);
+            else kernel_config<MODE_KRES64, false, kThreads>(false, blocks_per_sm, n, c);
+            break;
         default: PRG_CFG(MODE_CORR32); break;
     }
 #undef PRG_CFG
@@ -559,6 +576,10 @@ void launch_iteration(int mode, bool weighted, const IterArgs &a_in, const Launc
         case MODE_KRY64:
             if (weighted) iter_kernel<MODE_KRY64, true, kThreads><<<grid, block, c.smem, s>>>(a);
             else iter_kernel<MODE_KRY64, false, kThreads><<<grid, block, c.smem, s>>>(a);
+            break;
+        case MODE_KRES64:
+            if (weighted) iter_kernel<MODE_KRES64, true, kThreads><<<grid, block, c.smem, s>>>(a);
+            else iter_kernel<MODE_KRES64, false, kThreads><<<grid, block, c.smem, s>>>(a);
             break;
         default: break;
     }

@@ -26,8 +26,11 @@ enum IterMode : int {
     // with the dot products (rh.y, y.p, y.y) reduced per block
     MODE_KRY32 = 4,  // FP32 vectors and gathers
     MODE_KRY64 = 5,  // FP64 vectors and gathers
+    // FP64 residual pass of the Krylov solvers: g = G(x) and r = g - x
+    // (written FP32 to b32_out or FP64 to b64_out), ||r||_1 and sum(g)
+    MODE_KRES64 = 6,
 };
-constexpr int kModes = 6;
+constexpr int kModes = 7;
 
 struct IterArgs {
     // graph
