@@ -213,8 +213,9 @@ int32_t prg_autotune(prg_graph *g, int32_t tune_batch, const char *cache_path, p
  * skewed degree distributions), "refine_switch_e12" (refined precision: FP64
  * power steps until the successive change is below value * 1e-12, then FP32
  * corrections; default 500000), "batch_vec" (batched columns per lane: 1, 2
- * or 4), "hot_cache" (1: relabelled graphs gather
- * their hot vertices from shared memory), "unroll" (iteration pairs per CUDA
+ * or 4), "hot_cache" (relabelled graphs: each block of the iteration kernel
+ * keeps the first `value` entries of the gathered vector in shared memory,
+ * 0 = off, at most 65536), "unroll" (iteration pairs per CUDA
  * graph), "krylov_rel_e12" (refined precision with the Krylov inner solver:
  * each FP32 inner solve reduces the residual by value * 1e-12; default 1e8,
  * i.e. 1e-4). */

@@ -822,7 +822,8 @@ int32_t prg_set_tuning(const char *key, int64_t value) {
     } else if (k == "krylov_rel_e12") {
         t.krylov_rel = (double)value * 1e-12;
     } else if (k == "hot_cache") {
-        t.hot_cache = value != 0;
+        if (value > 65536) return fail(PRG_ERR_INVALID_ARGUMENT, "hot_cache must be at most 65536 entries");
+        t.hot_cache = (uint32_t)value;
     } else if (k == "unroll") {
         if (value < 1 || value > 64) return fail(PRG_ERR_INVALID_ARGUMENT, "unroll must be in 1..=64");
         t.unroll = (int)value;

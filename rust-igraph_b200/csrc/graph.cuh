@@ -39,7 +39,7 @@ struct DeviceGraph {
     uint32_t split = kSplit;
     uint32_t blocks_per_sm = 0;  // persistent grid = SMs x this (0 = occupancy maximum)
     int relabel = 2;             // 0 keep caller ids, 1 degree-sorted ids, 2 decide from the degree skew
-    bool hot_cache = false;      // relabelled graphs: cache the hot prefix of the rank vector in shared memory
+    uint32_t hot_cache = 0;      // relabelled graphs: entries of the rank vector's hot prefix each block keeps in shared memory (0 = off)
     uint32_t batch_vec = 0;      // batched tile width / 32 chosen by the autotuner (0 = process default)
 
     float build_ms = 0.f;
@@ -59,7 +59,7 @@ struct Tuning {
     uint32_t capw = kCapW, shortmax = kShortMax, split = kSplit, blocks_per_sm = 0;
     int relabel = 2;
     int unroll = 8;
-    bool hot_cache = false;
+    uint32_t hot_cache = 0;
     double refine_switch = 5e-7;
     uint32_t batch_vec = 1;
     double krylov_rel = 1e-4;  // refined Krylov: relative residual reduction per FP32 inner solve

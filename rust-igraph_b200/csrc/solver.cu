@@ -77,7 +77,7 @@ void workspace_ensure(Workspace &ws, const DeviceGraph &g, cudaStream_t s) {
     ws.nrb = g.nrb;
     ws.nhub = g.nhub;
     unsigned gmax = kPrepParts;
-    const bool hot = g.perm != nullptr && g.hot_cache;
+    const uint32_t hot = g.perm != nullptr ? g.hot_cache : 0u;
     for (int m = 0; m < kModes; m++) {
         ws.cfg[m] = iteration_config(m, g.weighted, hot, g.blocks_per_sm, g.n);
         gmax = std::max(gmax, ws.cfg[m].grid);

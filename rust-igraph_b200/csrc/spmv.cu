@@ -312,11 +312,11 @@ __device__ __forceinline__ typename ModeT<MODE>::A warp_row_sum(const IterArgs &
 }
 
 // Dynamic shared memory layout: [NT/32 warp buffers of kWarpBuf][hot prefix].
-template <int MODE, bool W, int NT>
-__global__ void __launch_bounds__(NT, NT == kThreads ? (kIs32<MODE> ? 5 : 4) : 1) iter_kernel(const IterArgs a) {
+template <int MODE, bool W, bool HOT>
+__global__ void __launch_bounds__(kThreads, HOT ? (kIs32<MODE> ? 4 : 3) : (kIs32<MODE> ? 5 : 4)) iter_kernel(const IterArgs a) {
     using A = typename ModeT<MODE>::A;
+    constexpr int NT = kThreads;
     constexpr int kW = NT / 32;
-    constexpr bool HOT = NT == kThreadsBig;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     A *s_buf = reinterpret_cast<A *>(smem_raw);
     A *s_hot = s_buf + kW * kWarpBuf;
@@ -490,8 +490,8 @@ __global__ void __launch_bounds__(NT, NT == kThreads ? (kIs32<MODE> ? 5 : 4) : 1
     }
 }
 
-template <int MODE, bool W, int NT>
-static void kernel_config(bool big, uint32_t blocks_per_sm, uint32_t n, LaunchCfg &c) {
+template <int MODE, bool W, bool HOT>
+static void kernel_config(uint32_t hot_entries, uint32_t blocks_per_sm, uint32_t n, LaunchCfg &c) {
     using A = typename ModeT<MODE>::A;
     static int sms = 0, smem_optin = 0;
     if (sms == 0) {
@@ -500,90 +500,74 @@ static void kernel_config(bool big, uint32_t blocks_per_sm, uint32_t n, LaunchCf
         PRG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
         PRG_CUDA(cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
     }
-    const size_t bufs = (size_t)(NT / 32) * kWarpBuf * sizeof(A);
+    const size_t bufs = (size_t)(kThreads / 32) * kWarpBuf * sizeof(A);
     size_t hot = 0;
-    if (big) {
+    if (HOT) {
         // leave room for the kernel's static shared memory (reduction scratch)
-        const size_t avail = (size_t)smem_optin - bufs - 2048;
-        hot = std::min<size_t>(avail / sizeof(A), n) & ~(size_t)3;
+        const size_t avail = ((size_t)smem_optin - bufs - 2048) / sizeof(A);
+        hot = std::min<size_t>(std::min<size_t>(hot_entries, avail), n) & ~(size_t)3;
     }
     c.smem = bufs + hot * sizeof(A);
     c.hot = (uint32_t)hot;
-    c.threads = NT;
-    PRG_CUDA(cudaFuncSetAttribute(iter_kernel<MODE, W, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c.smem));
+    c.threads = kThreads;
+    PRG_CUDA(cudaFuncSetAttribute(iter_kernel<MODE, W, HOT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c.smem));
     int occ = 0;
-    PRG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, iter_kernel<MODE, W, NT>, NT, c.smem));
+    PRG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, iter_kernel<MODE, W, HOT>, kThreads, c.smem));
     int per = occ > 0 ? occ : 1;
     if (blocks_per_sm > 0 && (int)blocks_per_sm < per) per = (int)blocks_per_sm;
     c.grid = (unsigned)(sms * per);
 }
 
-LaunchCfg iteration_config(int mode, bool weighted, bool hot_cache, uint32_t blocks_per_sm, uint32_t n) {
+template <int MODE>
+static void mode_config(bool weighted, uint32_t hot, uint32_t bps, uint32_t n, LaunchCfg &c) {
+    if (hot) {
+        if (weighted) kernel_config<MODE, true, true>(hot, bps, n, c);
+        else kernel_config<MODE, false, true>(hot, bps, n, c);
+    } else {
+        if (weighted) kernel_config<MODE, true, false>(0, bps, n, c);
+        else kernel_config<MODE, false, false>(0, bps, n, c);
+    }
+}
+
+LaunchCfg iteration_config(int mode, bool weighted, uint32_t hot_entries, uint32_t blocks_per_sm, uint32_t n) {
     LaunchCfg c;
-#define PRG_CFG(M)                                                                              \
-    if (hot_cache) {                                                                            \
-        if (weighted) kernel_config<M, true, kThreadsBig>(true, blocks_per_sm, n, c);           \
-        else kernel_config<M, false, kThreadsBig>(true, blocks_per_sm, n, c);                   \
-    } else {                                                                                    \
-        if (weighted) kernel_config<M, true, kThreads>(false, blocks_per_sm, n, c);             \
-        else kernel_config<M, false, kThreads>(false, blocks_per_sm, n, c);                     \
-    }
     switch (mode) {
-        case MODE_PLAIN64: PRG_CFG(MODE_PLAIN64); break;
-        case MODE_PPR64: PRG_CFG(MODE_PPR64); break;
-        case MODE_RESID64: PRG_CFG(MODE_RESID64); break;
-        case MODE_KRY32:
-            // Krylov matvecs always run the 256-thread shape
-            if (weighted) kernel_config<MODE_KRY32, true, kThreads>(false, blocks_per_sm, n, c);
-            else kernel_config<MODE_KRY32, false, kThreads>(false, blocks_per_sm, n, c);
-            break;
-        case MODE_KRY64:
-            if (weighted) kernel_config<MODE_KRY64, true, kThreads>(false, blocks_per_sm, n, c);
-            else kernel_config<MODE_KRY64, false, kThreads>(false, blocks_per_sm, n, c);
-            break;
-        case MODE_KRES64:
-            if (weighted) kernel_config<MODE_KRES64, true, kThreads>(false, blocks_per_sm, n, c);
-            else kernel_config<MODE_KRES64, false, kThreads>(false, blocks_per_sm, n, c);
-            break;
-        default: PRG_CFG(MODE_CORR32); break;
+        case MODE_PLAIN64: mode_config<MODE_PLAIN64>(weighted, hot_entries, blocks_per_sm, n, c); break;
+        case MODE_PPR64: mode_config<MODE_PPR64>(weighted, hot_entries, blocks_per_sm, n, c); break;
+        case MODE_RESID64: mode_config<MODE_RESID64>(weighted, hot_entries, blocks_per_sm, n, c); break;
+        case MODE_CORR32: mode_config<MODE_CORR32>(weighted, hot_entries, blocks_per_sm, n, c); break;
+        case MODE_KRY32: mode_config<MODE_KRY32>(weighted, hot_entries, blocks_per_sm, n, c); break;
+        case MODE_KRY64: mode_config<MODE_KRY64>(weighted, hot_entries, blocks_per_sm, n, c); break;
+        default: mode_config<MODE_KRES64>(weighted, hot_entries, blocks_per_sm, n, c); break;
     }
-#undef PRG_CFG
     return c;
+}
+
+template <int MODE>
+static void mode_launch(bool weighted, const IterArgs &a, const LaunchCfg &c, cudaStream_t s) {
+    const dim3 grid(c.grid), block(c.threads);
+    if (c.hot) {
+        if (weighted) iter_kernel<MODE, true, true><<<grid, block, c.smem, s>>>(a);
+        else iter_kernel<MODE, false, true><<<grid, block, c.smem, s>>>(a);
+    } else {
+        if (weighted) iter_kernel<MODE, true, false><<<grid, block, c.smem, s>>>(a);
+        else iter_kernel<MODE, false, false><<<grid, block, c.smem, s>>>(a);
+    }
 }
 
 void launch_iteration(int mode, bool weighted, const IterArgs &a_in, const LaunchCfg &c, cudaStream_t s) {
     IterArgs a = a_in;
     a.hot = c.hot;
-    const dim3 grid(c.grid), block(c.threads);
-    const bool big = c.threads == kThreadsBig;
-#define PRG_LAUNCH(M)                                                                          \
-    if (big) {                                                                                 \
-        if (weighted) iter_kernel<M, true, kThreadsBig><<<grid, block, c.smem, s>>>(a);        \
-        else iter_kernel<M, false, kThreadsBig><<<grid, block, c.smem, s>>>(a);                \
-    } else {                                                                                   \
-        if (weighted) iter_kernel<M, true, kThreads><<<grid, block, c.smem, s>>>(a);           \
-        else iter_kernel<M, false, kThreads><<<grid, block, c.smem, s>>>(a);                   \
-    }
     switch (mode) {
-        case MODE_PLAIN64: PRG_LAUNCH(MODE_PLAIN64); break;
-        case MODE_PPR64: PRG_LAUNCH(MODE_PPR64); break;
-        case MODE_RESID64: PRG_LAUNCH(MODE_RESID64); break;
-        case MODE_CORR32: PRG_LAUNCH(MODE_CORR32); break;
-        case MODE_KRY32:
-            if (weighted) iter_kernel<MODE_KRY32, true, kThreads><<<grid, block, c.smem, s>>>(a);
-            else iter_kernel<MODE_KRY32, false, kThreads><<<grid, block, c.smem, s>>>(a);
-            break;
-        case MODE_KRY64:
-            if (weighted) iter_kernel<MODE_KRY64, true, kThreads><<<grid, block, c.smem, s>>>(a);
-            else iter_kernel<MODE_KRY64, false, kThreads><<<grid, block, c.smem, s>>>(a);
-            break;
-        case MODE_KRES64:
-            if (weighted) iter_kernel<MODE_KRES64, true, kThreads><<<grid, block, c.smem, s>>>(a);
-            else iter_kernel<MODE_KRES64, false, kThreads><<<grid, block, c.smem, s>>>(a);
-            break;
+        case MODE_PLAIN64: mode_launch<MODE_PLAIN64>(weighted, a, c, s); break;
+        case MODE_PPR64: mode_launch<MODE_PPR64>(weighted, a, c, s); break;
+        case MODE_RESID64: mode_launch<MODE_RESID64>(weighted, a, c, s); break;
+        case MODE_CORR32: mode_launch<MODE_CORR32>(weighted, a, c, s); break;
+        case MODE_KRY32: mode_launch<MODE_KRY32>(weighted, a, c, s); break;
+        case MODE_KRY64: mode_launch<MODE_KRY64>(weighted, a, c, s); break;
+        case MODE_KRES64: mode_launch<MODE_KRES64>(weighted, a, c, s); break;
         default: break;
     }
-#undef PRG_LAUNCH
     PRG_CUDA(cudaGetLastError());
 }
 

@@ -78,8 +78,6 @@ struct IterArgs {
     int parity;
 };
 
-constexpr int kThreadsBig = 1024;  // one block per SM with the shared-memory hot prefix
-
 struct LaunchCfg {
     unsigned grid = 0;
     int threads = kThreads;
@@ -87,10 +85,10 @@ struct LaunchCfg {
     uint32_t hot = 0;  // hot-prefix length (vertices)
 };
 
-// Persistent launch shape of the iteration kernel on this device: either
-// 256-thread blocks at full occupancy, or (hot_cache) one 1024-thread block
-// per SM whose remaining shared memory caches the rank vector's hot prefix.
-LaunchCfg iteration_config(int mode, bool weighted, bool hot_cache, uint32_t blocks_per_sm, uint32_t n);
+// Persistent launch shape of the iteration kernel on this device: 256-thread
+// blocks, as many per SM as fit (or blocks_per_sm), each optionally holding
+// the first hot_entries values of the gathered vector in shared memory.
+LaunchCfg iteration_config(int mode, bool weighted, uint32_t hot_entries, uint32_t blocks_per_sm, uint32_t n);
 void launch_iteration(int mode, bool weighted, const IterArgs &a, const LaunchCfg &c, cudaStream_t s);
 
 // x <- x + e (e may be null), xt <- x / dval, dangling sum and total sum of

@@ -265,3 +265,25 @@ def test_rmat_auto_relabel(cuda_ok):
         assert dg.relabelled
         x, _ = dg.solve(ig.Options())
     assert maxabs(x, O.pagerank(n, f, t, True)) <= PARITY
+
+
+def test_shared_memory_hot_prefix_keeps_parity(cuda_ok):
+    # the optional per-block shared-memory copy of the hot prefix changes where
+    # gathers read from, never what they read
+    ig.set_tuning("hot_cache", 2048)
+    ig.set_tuning("relabel", 1)  # the hot prefix applies to degree-sorted ids
+    try:
+        n = 30_000
+        f, t = O.barabasi_game_bag(n, 5, False, True, 23)
+        g = G(n, f, t, True)
+        assert maxabs(ig.pagerank(g), O.pagerank(n, f, t, True)) <= PARITY
+        w = O.uniform_weights(len(f), 9)
+        assert maxabs(ig.pagerank_weighted(g, w), O.pagerank_weighted(n, f, t, True, w)) <= PARITY
+        with ig.DeviceGraph.from_host(n, f, t, True) as dg:
+            assert dg.relabelled
+            tight, _, _ = O.pagerank_tight(n, f, t, True, tol=1e-15)
+            for prec in (ig.PRECISION_FP32_REFINED, ig.PRECISION_FP64_KRYLOV):
+                x, st = dg.solve(ig.Options(precision=prec))
+                assert np.abs(x - tight).sum() <= L1_TOL and st.error_bound <= L1_TOL
+    finally:
+        ig.reset_tuning()
