@@ -218,7 +218,9 @@ int32_t prg_autotune(prg_graph *g, int32_t tune_batch, const char *cache_path, p
  * 0 = off, at most 65536), "unroll" (iteration pairs per CUDA
  * graph), "krylov_rel_e12" (refined precision with the Krylov inner solver:
  * each FP32 inner solve reduces the residual by value * 1e-12; default 1e8,
- * i.e. 1e-4). */
+ * i.e. 1e-4), "l1_hot32" / "l1_hot64" (relabelled graphs: FP32 / FP64
+ * passes gather sources with ids >= value without allocating in L1, so L1
+ * keeps the most-gathered prefix; defaults 16384 / 2048, 0 = all allocate). */
 int32_t prg_set_tuning(const char *key, int64_t value);
 
 /* ---- batched personalized PageRank ---------------------------------- */

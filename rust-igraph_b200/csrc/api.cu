@@ -129,6 +129,8 @@ int32_t create_from_device(uint32_t n, uint64_t m, const uint32_t *d_from, const
         h->g.blocks_per_sm = t.blocks_per_sm;
         h->g.relabel = t.relabel;
         h->g.hot_cache = t.hot_cache;
+        h->g.l1_hot32 = t.l1_hot32;
+        h->g.l1_hot64 = t.l1_hot64;
         h->ws.unroll = t.unroll;
     }
     PRG_CUDA(cudaGetDevice(&h->g.device));
@@ -819,6 +821,10 @@ int32_t prg_set_tuning(const char *key, int64_t value) {
         t.batch_vec = (uint32_t)value;
     } else if (k == "refine_switch_e12") {
         t.refine_switch = (double)value * 1e-12;
+    } else if (k == "l1_hot32") {
+        t.l1_hot32 = (uint32_t)std::min<int64_t>(value, 0xFFFFFFFFll);
+    } else if (k == "l1_hot64") {
+        t.l1_hot64 = (uint32_t)std::min<int64_t>(value, 0xFFFFFFFFll);
     } else if (k == "krylov_rel_e12") {
         t.krylov_rel = (double)value * 1e-12;
     } else if (k == "hot_cache") {

@@ -40,6 +40,9 @@ struct DeviceGraph {
     uint32_t blocks_per_sm = 0;  // persistent grid = SMs x this (0 = occupancy maximum)
     int relabel = 2;             // 0 keep caller ids, 1 degree-sorted ids, 2 decide from the degree skew
     uint32_t hot_cache = 0;      // relabelled graphs: entries of the rank vector's hot prefix each block keeps in shared memory (0 = off)
+    // relabelled graphs: gathers of ids >= l1_hot32 (FP32 passes) / l1_hot64
+    // (FP64 passes) bypass L1, keeping it for the hot prefix (0 = all allocate)
+    uint32_t l1_hot32 = 16384, l1_hot64 = 2048;
     uint32_t batch_vec = 0;      // batched tile width / 32 chosen by the autotuner (0 = process default)
 
     float build_ms = 0.f;
@@ -60,6 +63,7 @@ struct Tuning {
     int relabel = 2;
     int unroll = 8;
     uint32_t hot_cache = 0;
+    uint32_t l1_hot32 = 16384, l1_hot64 = 2048;
     double refine_switch = 5e-7;
     uint32_t batch_vec = 1;
     double krylov_rel = 1e-4;  // refined Krylov: relative residual reduction per FP32 inner solve

@@ -54,6 +54,17 @@ __device__ __forceinline__ float ld_gather(const float *p, uint64_t pol) {
     asm("ld.global.nc.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(p), "l"(pol));
     return v;
 }
+// Gather that does not allocate in L1 (cold sources: keeps L1 for the hot prefix).
+__device__ __forceinline__ float ld_gather_na(const float *p, uint64_t pol) {
+    float v;
+    asm("ld.global.nc.L1::no_allocate.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(p), "l"(pol));
+    return v;
+}
+__device__ __forceinline__ double ld_gather_na(const double *p, uint64_t pol) {
+    double v;
+    asm("ld.global.nc.L1::no_allocate.L2::cache_hint.f64 %0, [%1], %2;" : "=d"(v) : "l"(p), "l"(pol));
+    return v;
+}
 __device__ __forceinline__ double ld_gather(const double *p, uint64_t pol) {
     double v;
     asm("ld.global.nc.L2::cache_hint.f64 %0, [%1], %2;" : "=d"(v) : "l"(p), "l"(pol));

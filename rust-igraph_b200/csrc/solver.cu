@@ -80,6 +80,9 @@ void workspace_ensure(Workspace &ws, const DeviceGraph &g, cudaStream_t s) {
     const uint32_t hot = g.perm != nullptr ? g.hot_cache : 0u;
     for (int m = 0; m < kModes; m++) {
         ws.cfg[m] = iteration_config(m, g.weighted, hot, g.blocks_per_sm, g.n);
+        const bool fp32 = m == MODE_CORR32 || m == MODE_KRY32;
+        const uint32_t l1 = fp32 ? g.l1_hot32 : g.l1_hot64;
+        if (g.perm != nullptr && l1) ws.cfg[m].l1hot = l1;
         gmax = std::max(gmax, ws.cfg[m].grid);
     }
     const uint64_t n = g.n;

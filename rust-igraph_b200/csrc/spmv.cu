@@ -237,7 +237,7 @@ __device__ __forceinline__ void quad(const IterArgs &a, uint32_t base, uint32_t 
         A g = A(0);
         if (p >= lo && p < hi) {
             if constexpr (HOT) g = cc[k] < hot ? s_hot[cc[k]] : ld_gather(xt + cc[k], pol_g);
-            else g = ld_gather(xt + cc[k], pol_g);
+            else g = cc[k] < a.l1hot ? ld_gather(xt + cc[k], pol_g) : ld_gather_na(xt + cc[k], pol_g);
         }
         out[k] = W ? wv[k] * g : g;
     }
@@ -558,6 +558,7 @@ static void mode_launch(bool weighted, const IterArgs &a, const LaunchCfg &c, cu
 void launch_iteration(int mode, bool weighted, const IterArgs &a_in, const LaunchCfg &c, cudaStream_t s) {
     IterArgs a = a_in;
     a.hot = c.hot;
+    a.l1hot = c.l1hot;
     switch (mode) {
         case MODE_PLAIN64: mode_launch<MODE_PLAIN64>(weighted, a, c, s); break;
         case MODE_PPR64: mode_launch<MODE_PPR64>(weighted, a, c, s); break;

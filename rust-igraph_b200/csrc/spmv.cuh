@@ -44,6 +44,7 @@ struct IterArgs {
     const Hub *hubs;
     uint32_t nrb, nhub, n;
     uint32_t hot;  // sources below this id are gathered from the shared-memory hot prefix (set at launch)
+    uint32_t l1hot;  // sources at or above this id are gathered without L1 allocation (set at launch)
     // vectors (FP64 modes use the *64 pointers, CORR32 the *32 ones)
     const double *xt64_in;
     const double *x64_in;
@@ -83,6 +84,7 @@ struct LaunchCfg {
     int threads = kThreads;
     size_t smem = 0;   // dynamic shared memory (warp buffers + hot prefix)
     uint32_t hot = 0;  // hot-prefix length (vertices)
+    uint32_t l1hot = 0xFFFFFFFFu;  // gathers of ids >= l1hot bypass L1
 };
 
 // Persistent launch shape of the iteration kernel on this device: 256-thread
