@@ -220,7 +220,11 @@ int32_t prg_autotune(prg_graph *g, int32_t tune_batch, const char *cache_path, p
  * each FP32 inner solve reduces the residual by value * 1e-12; default 1e8,
  * i.e. 1e-4), "l1_hot32" / "l1_hot64" (relabelled graphs: FP32 / FP64
  * passes gather sources with ids >= value without allocating in L1, so L1
- * keeps the most-gathered prefix; defaults 16384 / 2048, 0 = all allocate). */
+ * keeps the most-gathered prefix; defaults 16384 / 2048, 0 = all allocate),
+ * "batch_barrier_extra" (failure-detection test hook, 0 or 1: with 1 every
+ * grid barrier of the batched solver waits for an arrival that never comes,
+ * so its bounded wait (about 1.5 s) expires and the call returns
+ * PRG_ERR_TIMEOUT with the context still usable; leave it 0). */
 int32_t prg_set_tuning(const char *key, int64_t value);
 
 /* ---- batched personalized PageRank ---------------------------------- */

@@ -821,6 +821,9 @@ int32_t prg_set_tuning(const char *key, int64_t value) {
         t.batch_vec = (uint32_t)value;
     } else if (k == "refine_switch_e12") {
         t.refine_switch = (double)value * 1e-12;
+    } else if (k == "batch_barrier_extra") {
+        if (value > 1) return fail(PRG_ERR_INVALID_ARGUMENT, "batch_barrier_extra must be 0 or 1");
+        t.batch_barrier_extra = (uint32_t)value;
     } else if (k == "l1_hot32") {
         t.l1_hot32 = (uint32_t)std::min<int64_t>(value, 0xFFFFFFFFll);
     } else if (k == "l1_hot64") {

@@ -66,7 +66,8 @@ struct Tuning {
     uint32_t l1_hot32 = 16384, l1_hot64 = 2048;
     double refine_switch = 5e-7;
     uint32_t batch_vec = 1;
-    double krylov_rel = 1e-4;  // refined Krylov: relative residual reduction per FP32 inner solve
+    double krylov_rel = 1e-4;
+    uint32_t batch_barrier_extra = 0;  // test hook: batched grid barriers wait for arrivals that never come  // refined Krylov: relative residual reduction per FP32 inner solve
 };
 Tuning &tuning();
 

@@ -19,7 +19,7 @@
 //
 // One cooperative persistent launch runs all iterations of a tile.  Phases
 // are separated by a grid barrier whose spin is bounded: if a barrier does
-// not complete within ~2 s the kernel records PRG_ERR_TIMEOUT in its status
+// not complete within ~1.5 s the kernel records PRG_ERR_TIMEOUT in its status
 // word and every block returns, so the host gets an error, not a hang.
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -65,6 +65,7 @@ struct TileArgs {
     int32_t *status;
     double damping;
     double tol;
+    uint32_t bar_extra;  // arrivals a barrier waits for beyond the grid (0; >0 only to exercise the timeout)
 };
 
 // Grid barrier with a bounded spin (co-residency is guaranteed by the
@@ -79,7 +80,7 @@ __device__ __forceinline__ bool grid_sync(const TileArgs &a) {
         __threadfence();
         const uint32_t arrived = atomicAdd(a.bar, 1u);
         int ok = 1;
-        if (arrived == gridDim.x - 1) {
+        if (arrived == gridDim.x - 1 + a.bar_extra) {
             a.bar[0] = 0u;
             __threadfence();
             atomicAdd(a.bar + 1, 1u);
@@ -87,7 +88,7 @@ __device__ __forceinline__ bool grid_sync(const TileArgs &a) {
             uint32_t spins = 0;
             while (*gen == g0) {
                 __nanosleep(64);
-                if (++spins > (1u << 25)) {  // ~2 s
+                if (++spins > (1u << 22)) {  // ~1.5 s (a phase takes milliseconds)
                     atomicExch(a.status, 7);  // PRG_ERR_TIMEOUT
                     ok = 0;
                     break;
@@ -487,6 +488,7 @@ int ppr_batch(const DeviceGraph &g, uint32_t K, const uint64_t *seed_offsets, co
         a.status = status;
         a.damping = damping;
         a.tol = tol;
+        a.bar_extra = tuning().batch_barrier_extra;
         if (vec == 4) run_tile<4>(a, grid, s);
         else if (vec == 2) run_tile<2>(a, grid, s);
         else run_tile<1>(a, grid, s);

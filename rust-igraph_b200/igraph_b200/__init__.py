@@ -530,7 +530,7 @@ def set_tuning(key: str, value: int) -> None:
 
 TUNING_DEFAULTS = {"capw": 256, "shortmax": 256, "split": 8192, "blocks_per_sm": 0, "relabel": 2, "unroll": 8,
                    "hot_cache": 0, "refine_switch_e12": 500000, "batch_vec": 1, "krylov_rel_e12": 100_000_000, "l1_hot32": 16384,
-                   "l1_hot64": 2048}
+                   "l1_hot64": 2048, "batch_barrier_extra": 0}
 
 
 def reset_tuning() -> None:

@@ -93,3 +93,24 @@ def test_batch_validation(cuda_ok):
             dg.ppr_batch([np.array([100], np.uint32)])
         with pytest.raises(ig.InvalidArgument, match="damping"):
             dg.ppr_batch([np.array([1], np.uint32)], damping=1.0)
+
+
+def test_barrier_timeout_is_reported_and_the_context_survives(cuda_ok):
+    # Failure detection without a fault: the test hook makes every grid
+    # barrier of the persistent batched kernel wait for one arrival that never
+    # comes.  The barrier's bounded wait (about 1.5 s) expires, the kernel
+    # records PRG_ERR_TIMEOUT and every block returns; the host raises, and
+    # the next call on the same graph and context succeeds.
+    n = 3000
+    f, t = O.barabasi_game_bag(n, 3, False, False, 5)
+    seeds = [np.array([1, 2, 3], np.uint32)]
+    with ig.DeviceGraph.from_host(n, f, t, False) as dg:
+        ig.set_tuning("batch_barrier_extra", 1)
+        try:
+            with pytest.raises(ig.DeviceTimeout, match="grid barrier timed out"):
+                dg.ppr_batch(seeds, 0.85, TOL_COL, 1000, 1)
+        finally:
+            ig.reset_tuning()
+        X, iters, st = dg.ppr_batch(seeds, 0.85, TOL_COL, 1000, 1)
+    ref = O.personalized_pagerank(n, f, t, False, reset_of(n, seeds[0]), 0.85)
+    assert np.abs(X[:, 0].astype(np.float64) - ref).sum() <= L1_COL
