@@ -47,7 +47,9 @@ enum prg_status {
     PRG_ERR_CUDA = 4,                 /* IgraphError::Internal("cuda: ...") */
     PRG_ERR_OUT_OF_MEMORY = 5,        /* IgraphError::Internal("cuda: out of memory") */
     PRG_ERR_DID_NOT_CONVERGE = 6,     /* IgraphError::DidNotConverge (never raised by the drop-ins) */
-    PRG_ERR_TIMEOUT = 7               /* a bounded device wait expired (batched solver) */
+    PRG_ERR_TIMEOUT = 7,              /* a bounded device wait expired (batched solver) */
+    PRG_ERR_PARSE = 8,                /* IgraphError::Parse { line, message } */
+    PRG_ERR_IO = 9                    /* IgraphError::Io (the text is not valid UTF-8) */
 };
 
 enum prg_precision {
@@ -271,8 +273,30 @@ int32_t prg_ppr_batch_device(prg_graph *g, uint32_t K, const uint64_t *seed_offs
 int32_t prg_solve_noalloc(prg_graph *g, const prg_options *opt, const double *d_reset, double *d_out,
                           prg_stats *stats);
 
+/* ---- edge-list reader ---------------------------------------------------- */
+
+/* rust-igraph read_edgelist() (src/algorithms/io/edgelist.rs:25-72) with the
+ * parsing on the GPU.  text: the file's bytes (len of them, host memory).
+ * One edge "u v" per line (u32 ids, whitespace-separated); after trimming,
+ * blank lines and lines starting with '#' are skipped; the graph is
+ * undirected with n = max id + 1.  On success from/to (capacity entries,
+ * host) receive the m edges in file order.  Errors, for the first failing
+ * line in file order: PRG_ERR_PARSE with *err_line (1-based) and the
+ * reference's message ("missing vertex id", "invalid vertex id `t`: ...",
+ * "expected exactly two vertex ids"); PRG_ERR_IO when a line is not valid
+ * UTF-8; PRG_ERR_INVALID_ARGUMENT when m exceeds capacity (*m is set). */
+int32_t prg_parse_edgelist(const char *text, uint64_t len, uint32_t *from, uint32_t *to, uint64_t capacity,
+                           uint64_t *m, uint32_t *n, uint64_t *err_line);
+/* Same, building the resident graph straight from the parsed edges (they
+ * never leave the GPU).  A text without edges gives *out = NULL, n = m = 0. */
+int32_t prg_read_edgelist(const char *text, uint64_t len, prg_graph **out, uint32_t *n, uint64_t *m,
+                          uint64_t *err_line);
+
 /* Message of the last error on this thread ("" if none). */
 const char *prg_last_error(void);
+/* Its length in bytes: a message that quotes input text (an edge-list token)
+ * may contain NUL bytes, so read prg_last_error_len() bytes, not up to NUL. */
+uint64_t prg_last_error_len(void);
 
 /* ---- device R-MAT generator (benchmark inputs) ------------------------ */
 /* Counter-based R-MAT (same edge stream as the CPU generator in the tests):

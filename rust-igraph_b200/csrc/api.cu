@@ -20,6 +20,7 @@
 #include "autotune.cuh"
 #include "gnn.cuh"
 #include "graph.cuh"
+#include "edgelist.cuh"
 #include "handle.cuh"
 #include "ppr_batch.cuh"
 #include "solver.cuh"
@@ -337,6 +338,8 @@ void prg_default_options(prg_options *o) {
 
 const char *prg_last_error(void) { return g_err.c_str(); }
 
+uint64_t prg_last_error_len(void) { return g_err.size(); }
+
 int32_t prg_pagerank(uint32_t n, uint64_t m, const uint32_t *from, const uint32_t *to, int32_t directed,
                      double *out) {
     g_err.clear();
@@ -487,6 +490,111 @@ int32_t prg_graph_create_device(uint32_t n, uint64_t m, const uint32_t *d_from, 
     PRG_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
     int32_t rc = create_from_device(n, m, d_from, d_to, d_weights, directed, s, out);
     if (rc != PRG_OK) cudaStreamDestroy(s);
+    return rc;
+    PRG_GUARD_END
+}
+
+// Copies the text to the device and parses it there (edgelist.cu).  On
+// success the result owns device edge arrays on stream s.
+static int32_t edgelist_common(const char *text, uint64_t len, cudaStream_t s, prg::el::ParseResult &r,
+                               uint64_t *err_line) {
+    if (err_line) *err_line = 0;
+    if (len && !text) return fail(PRG_ERR_INVALID_ARGUMENT, "null text");
+    uint8_t *d_text = nullptr;
+    if (len) {
+        PRG_CUDA(cudaMallocAsync((void **)&d_text, len, s));
+        PRG_CUDA(cudaMemcpyAsync(d_text, text, len, cudaMemcpyHostToDevice, s));
+    }
+    try {
+        r = prg::el::parse(d_text, reinterpret_cast<const uint8_t *>(text), len, s);
+    } catch (...) {
+        if (d_text) cudaFreeAsync(d_text, s);
+        throw;
+    }
+    if (d_text) cudaFreeAsync(d_text, s);
+    if (r.status != PRG_OK) {
+        if (err_line) *err_line = r.err_line;
+        return fail(r.status, r.message);
+    }
+    return PRG_OK;
+}
+
+int32_t prg_parse_edgelist(const char *text, uint64_t len, uint32_t *from, uint32_t *to, uint64_t capacity,
+                           uint64_t *m, uint32_t *n, uint64_t *err_line) {
+    g_err.clear();
+    PRG_GUARD_BEGIN
+    if (m) *m = 0;
+    if (n) *n = 0;
+    if (!ensure_pool_config()) return fail(PRG_ERR_CUDA, "cuda: no usable device");
+    cudaStream_t s;
+    PRG_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    prg::el::ParseResult r;
+    int32_t rc = PRG_OK;
+    try {
+        rc = edgelist_common(text, len, s, r, err_line);
+        if (rc == PRG_OK) {
+            if (m) *m = r.m;
+            if (n) *n = r.n;
+            if (r.m > capacity) {
+                rc = fail(PRG_ERR_INVALID_ARGUMENT, "edge arrays hold " + std::to_string(capacity) + " edges, the text has " +
+                                                        std::to_string(r.m));
+            } else if (r.m) {
+                if (!from || !to) {
+                    rc = fail(PRG_ERR_INVALID_ARGUMENT, "null edge arrays");
+                } else {
+                    PRG_CUDA(cudaMemcpyAsync(from, r.d_from, r.m * 4, cudaMemcpyDeviceToHost, s));
+                    PRG_CUDA(cudaMemcpyAsync(to, r.d_to, r.m * 4, cudaMemcpyDeviceToHost, s));
+                }
+            }
+        }
+        prg::el::free_result(r, s);
+        PRG_CUDA(cudaStreamSynchronize(s));
+    } catch (...) {
+        prg::el::free_result(r, s);
+        cudaStreamSynchronize(s);
+        cudaStreamDestroy(s);
+        throw;
+    }
+    cudaStreamDestroy(s);
+    return rc;
+    PRG_GUARD_END
+}
+
+int32_t prg_read_edgelist(const char *text, uint64_t len, prg_graph **out, uint32_t *n, uint64_t *m,
+                          uint64_t *err_line) {
+    g_err.clear();
+    PRG_GUARD_BEGIN
+    if (!out) return fail(PRG_ERR_INVALID_ARGUMENT, "null output handle");
+    *out = nullptr;
+    if (m) *m = 0;
+    if (n) *n = 0;
+    if (!ensure_pool_config()) return fail(PRG_ERR_CUDA, "cuda: no usable device");
+    cudaStream_t s;
+    PRG_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    prg::el::ParseResult r;
+    int32_t rc = PRG_OK;
+    try {
+        rc = edgelist_common(text, len, s, r, err_line);
+        if (rc == PRG_OK) {
+            if (m) *m = r.m;
+            if (n) *n = r.n;
+            if (r.m > 0) {
+                rc = create_from_device(r.n, r.m, r.d_from, r.d_to, nullptr, 0, s, out);
+                if (rc == PRG_OK) {
+                    prg::el::free_result(r, s);  // the graph owns the stream from here on
+                    return PRG_OK;
+                }
+            }
+        }
+        prg::el::free_result(r, s);
+        PRG_CUDA(cudaStreamSynchronize(s));
+    } catch (...) {
+        prg::el::free_result(r, s);
+        cudaStreamSynchronize(s);
+        cudaStreamDestroy(s);
+        throw;
+    }
+    cudaStreamDestroy(s);
     return rc;
     PRG_GUARD_END
 }

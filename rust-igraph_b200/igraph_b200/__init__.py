@@ -58,9 +58,22 @@ class DeviceTimeout(Internal):
     pass
 
 
+class ParseError(IgraphError):
+    """IgraphError::Parse { line, message } (displayed as the reference does)."""
+
+    def __init__(self, line: int, message: str):
+        super().__init__(f"parse error at line {line}: {message}")
+        self.line = line
+        self.message = message
+
+
+class IoError(IgraphError):
+    """IgraphError::Io."""
+
+
 PRG_OK = 0
 _ERRORS = {1: InvalidArgument, 2: VertexOutOfRange, 3: Internal, 4: Internal, 5: Internal, 6: DidNotConverge,
-           7: DeviceTimeout}
+           7: DeviceTimeout, 9: IoError}
 
 # ------------------------------------------------------------------ library
 
@@ -109,8 +122,10 @@ def lib():
     u32p, f64p, vp = C.c_void_p, C.c_void_p, C.c_void_p
     L.prg_default_options.restype = None
     L.prg_default_options.argtypes = [C.POINTER(prg_options)]
-    L.prg_last_error.restype = C.c_char_p
+    L.prg_last_error.restype = C.c_void_p
     L.prg_last_error.argtypes = []
+    L.prg_last_error_len.restype = C.c_uint64
+    L.prg_last_error_len.argtypes = []
     L.prg_pagerank.restype = C.c_int32
     L.prg_pagerank.argtypes = [C.c_uint32, C.c_uint64, u32p, u32p, C.c_int32, f64p]
     L.prg_pagerank_linsys.restype = C.c_int32
@@ -173,13 +188,28 @@ def lib():
     L.prg_rmat_device.restype = C.c_int32
     L.prg_rmat_device.argtypes = [C.c_uint32, C.c_uint64, C.c_double, C.c_double, C.c_double, C.c_uint64,
                                   vp, vp, vp]
+    L.prg_parse_edgelist.restype = C.c_int32
+    L.prg_parse_edgelist.argtypes = [C.c_char_p, C.c_uint64, vp, vp, C.c_uint64, C.POINTER(C.c_uint64),
+                                     C.POINTER(C.c_uint32), C.POINTER(C.c_uint64)]
+    L.prg_read_edgelist.restype = C.c_int32
+    L.prg_read_edgelist.argtypes = [C.c_char_p, C.c_uint64, C.POINTER(vp), C.POINTER(C.c_uint32),
+                                    C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]
     _lib = L
     return L
 
 
-def _check(rc: int) -> None:
+def last_error() -> str:
+    """The library's last error message on this thread (all of its bytes)."""
+    L = lib()
+    n = L.prg_last_error_len()
+    return C.string_at(L.prg_last_error(), n).decode("utf-8", "replace") if n else ""
+
+
+def _check(rc: int, err_line: int = 0) -> None:
     if rc != PRG_OK:
-        msg = lib().prg_last_error().decode("utf-8", "replace")
+        msg = last_error()
+        if rc == 8:
+            raise ParseError(err_line, msg)
         raise _ERRORS.get(rc, Internal)(msg)
 
 
@@ -286,6 +316,26 @@ def pagerank_linsys(graph: Graph) -> np.ndarray:
     out = np.empty(max(n, 1), np.float64)
     _check(lib().prg_pagerank_linsys(n, len(f), _ptr(f), _ptr(t), int(graph.is_directed()), _ptr(out)))
     return out[:n]
+
+
+def parse_edgelist(data: bytes):
+    """Edges of an edge-list text parsed on the GPU: (n, from, to) in file
+    order (read_edgelist's rules, io/edgelist.rs:25-72)."""
+    data = bytes(data)
+    cap = data.count(b"\n") + 1
+    f = np.empty(cap, np.uint32)
+    t = np.empty(cap, np.uint32)
+    m, n, line = C.c_uint64(), C.c_uint32(), C.c_uint64()
+    _check(lib().prg_parse_edgelist(data, len(data), _ptr(f), _ptr(t), cap, C.byref(m), C.byref(n), C.byref(line)),
+           line.value)
+    return n.value, f[:m.value].copy(), t[:m.value].copy()
+
+
+def read_edgelist(data: bytes) -> Graph:
+    """rust-igraph ``read_edgelist`` (io/edgelist.rs:25-61): an undirected
+    graph with n = max id + 1, parsed on the GPU."""
+    n, f, t = parse_edgelist(data)
+    return Graph.from_edge_arrays(n, f, t, False)
 
 
 def pagerank_weighted(graph: Graph, weights) -> np.ndarray:
@@ -411,6 +461,18 @@ class DeviceGraph:
     def from_graph(cls, g: Graph, weights=None) -> "DeviceGraph":
         f, t = g.edge_arrays()
         return cls.from_host(g.vcount(), f, t, g.is_directed(), weights)
+
+    @classmethod
+    def from_edgelist(cls, data: bytes) -> Optional["DeviceGraph"]:
+        """Resident graph straight from an edge-list text (prg_read_edgelist):
+        parsed on the GPU, the edges never leave it.  None when the text has
+        no edges."""
+        data = bytes(data)
+        h = C.c_void_p()
+        n, m, line = C.c_uint32(), C.c_uint64(), C.c_uint64()
+        _check(lib().prg_read_edgelist(data, len(data), C.byref(h), C.byref(n), C.byref(m), C.byref(line)),
+               line.value)
+        return cls(h) if h.value else None
 
     @classmethod
     def from_device(cls, n: int, m: int, d_from: int, d_to: int, directed: bool, d_weights: int = 0):

@@ -12,7 +12,10 @@ Run in a checkout that has the rust-igraph sources at REF (default
   generators the benchmark inputs are built with;
 * the golden 5-cycle personalized vector from the in-module test
   src/algorithms/properties/personalized_pagerank.rs:463-481 (parsed from
-  the source text, tolerance 1e-6 as that test uses).
+  the source text, tolerance 1e-6 as that test uses);
+* the edge-list fixture fixtures/karate.edges that the reference's tests read
+  with read_edgelist (tests/infomap.rs:11-15 and others), verbatim, with the
+  vertex and edge counts its header states.
 """
 import glob
 import json
@@ -71,7 +74,12 @@ def main():
             d = json.load(open(path))
             gens.append({"name": os.path.relpath(path, REF), "algo": d["algo"], "params": d["params"],
                          "expected": d["expected"]})
-    json.dump({"source": "rust-igraph v0.7.0 reference tree", "cases": cases, "generators": gens}, open(OUT, "w"), indent=1)
+    karate = open(os.path.join(REF, "fixtures/karate.edges")).read()
+    hm = re.search(r"(\d+) vertices.*?(\d+) edges", karate.splitlines()[0])
+    edgelists = [{"name": "fixtures/karate.edges", "text": karate, "vcount": int(hm.group(1)),
+                  "ecount": int(hm.group(2)), "used_by": "tests/infomap.rs:11-15, tests/label_propagation.rs"}]
+    json.dump({"source": "rust-igraph v0.7.0 reference tree", "cases": cases, "generators": gens,
+               "edgelists": edgelists}, open(OUT, "w"), indent=1)
     print(f"wrote {len(cases)} cases to {OUT}")
 
 

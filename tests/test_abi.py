@@ -56,7 +56,7 @@ def test_unknown_options_are_rejected_before_device_work():
         out = np.empty(1)
         rc = L.prg_solve(C.c_void_p(1), C.byref(o), None, out.ctypes.data_as(C.POINTER(C.c_double)), None)
         assert rc == 1, field
-        assert L.prg_last_error().decode() == msg
+        assert ig.last_error() == msg
 
 
 def test_trivial_graphs_need_no_device():
