@@ -1,4 +1,5 @@
-"""Timings of the five workload configurations on one GPU.
+"""Timings of the five workload configurations on one GPU, plus the
+edge-list ingest (text -> GPU parse -> resident CSR).
 
 Inputs are generated on the device with the shapes of each configuration
 (R-MAT; a Chung-Lu power law with the degree law of preferential attachment
@@ -9,7 +10,7 @@ to tolerance, GTEPS (in-CSR arcs x passes / time), algorithmic bytes of one
 SpMV pass, the SpMV launches' HBM rate against the measured copy peak, and
 the L1 distance to a tight FP64 solve of the same graph.
 
-    python -m igraph_b200.configs [--which 1,2,3,4,5] [--peak-gbs 6546]
+    python -m igraph_b200.configs [--which 1,2,3,4,5,6] [--peak-gbs 6546]
 """
 from __future__ import annotations
 
@@ -163,14 +164,87 @@ def config5(peak):
     net.close()
 
 
+def edgelist_text(u, v):
+    """An edge-list text ("u v" lines, ids without padding) from u32 arrays,
+    formatted with numpy (decimal digits gathered per line)."""
+    u = np.asarray(u, np.uint64)
+    v = np.asarray(v, np.uint64)
+    m = len(u)
+
+    def digits(x):
+        nd = np.ones(m, np.int64)
+        t = x.copy()
+        for k in range(1, 10):
+            nd += (x >= 10 ** k)
+        d = np.zeros((m, 10), np.uint8)
+        for k in range(10):
+            d[:, 9 - k] = (t % 10).astype(np.uint8) + 48
+            t //= 10
+        return d, nd
+
+    du, nu = digits(u)
+    dv, nv = digits(v)
+    width = nu + nv + 2
+    off = np.zeros(m + 1, np.int64)
+    np.cumsum(width, out=off[1:])
+    out = np.empty(int(off[-1]), np.uint8)
+    for k in range(10):  # digit k of u (from the left of its 10-digit field) goes to off + k - (10 - nu)
+        sel = k >= 10 - nu
+        out[off[:-1][sel] + k - (10 - nu[sel])] = du[sel, k]
+    out[off[:-1] + nu] = 32
+    for k in range(10):
+        sel = k >= 10 - nv
+        out[off[:-1][sel] + nu[sel] + 1 + k - (10 - nv[sel])] = dv[sel, k]
+    out[off[1:] - 1] = 10
+    return out.tobytes()
+
+
+def config6(peak):
+    # edge-list ingest: text -> GPU parse -> resident CSR (the edges never leave the GPU)
+    import time
+
+    import torch
+
+    for scale in (22,):
+        n, m = 1 << scale, 16 << scale
+        df = torch.empty(m, dtype=torch.int32, device="cuda")
+        dt = torch.empty(m, dtype=torch.int32, device="cuda")
+        generate_device(GEN_RMAT, n, m, df.data_ptr(), dt.data_ptr(), 0.57, 0.19, 0.19, seed=20241203)
+        u = df.cpu().numpy().view(np.uint32)
+        v = dt.cpu().numpy().view(np.uint32)
+        del df, dt
+        text = edgelist_text(u, v)
+        from . import parse_edgelist
+
+        res = {}
+        for name, fn in (("parse (H2D + parse + D2H of edges)", lambda: parse_edgelist(text)),
+                         ("read_edgelist to resident graph (H2D + parse + CSR build)",
+                          lambda: DeviceGraph.from_edgelist(text))):
+            r = fn()
+            if isinstance(r, DeviceGraph):
+                r.close()
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            r = fn()
+            torch.cuda.synchronize()
+            dt_s = time.perf_counter() - t0
+            if isinstance(r, DeviceGraph):
+                r.close()
+            else:
+                assert len(r[1]) == m and np.array_equal(r[1], u) and np.array_equal(r[2], v)
+            res[name] = {"s": round(dt_s, 4), "text_gb_per_s": len(text) / dt_s / 1e9}
+        print(json.dumps({"config": f"6 edge-list ingest R-MAT s{scale}", "lines": m, "text_bytes": len(text),
+                          **res}), flush=True)
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("--which", default="1,2,3,4,5")
+    ap.add_argument("--which", default="1,2,3,4,5,6")
     ap.add_argument("--peak-gbs", type=float, default=0.0)
     a = ap.parse_args(argv)
     peak = _peak(a.peak_gbs)
     for k in a.which.split(","):
-        {"1": config1, "2": config2, "3": config3, "4": config4, "5": config5}[k.strip()](peak)
+        {"1": config1, "2": config2, "3": config3, "4": config4, "5": config5, "6": config6}[k.strip()](peak)
 
 
 if __name__ == "__main__":
