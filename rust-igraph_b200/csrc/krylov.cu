@@ -32,6 +32,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <type_traits>
 #include <vector>
 
 #include "solver.cuh"
@@ -56,6 +57,7 @@ struct KState {
 enum : int32_t { KRUN = 0, KDONE_CONVERGED = 1, KDONE_BREAKDOWN = 2, KDONE_CAP = 3, KDONE_NONFINITE = 4 };
 
 constexpr unsigned kVB = 148u * 4u;  // blocks of the vector kernels
+constexpr uint32_t kEvStep = 6;       // events per BiCGStab step (around each of its five kernels)
 constexpr int kVT = 256;
 
 template <class T>
@@ -182,32 +184,100 @@ __device__ __forceinline__ double3 krecords(const double4 *a, uint32_t na, const
     return kblock3(x, y, z);
 }
 
-// p/s for the gather and whether v is dangling (out-degree or strength 0).
-__device__ __forceinline__ float kscaled(float x, uint32_t v, const float *inv32, const double *, bool &dang) {
-    const float iv = inv32[v];
-    dang = iv == 0.0f;
-    return x * iv;
-}
-__device__ __forceinline__ double kscaled(double x, uint32_t v, const float *, const double *dval, bool &dang) {
-    const double dv = dval[v];
-    dang = dv == 0.0;
-    return dang ? 0.0 : x / dv;
-}
-
 __device__ __forceinline__ bool kstopped(const KState *st) { return *(volatile const int32_t *)&st->done != KRUN; }
 __device__ __forceinline__ bool kleader() { return blockIdx.x == 0 && threadIdx.x == 0; }
+
+// W-wide loads and stores at an index that is a multiple of W (the vectors
+// come from the stream-ordered pool, 256-byte aligned): 16-byte accesses for
+// FP32 (W = 4), two 16-byte accesses for FP64; W = 1 for the tail.
+template <int W, bool CS, class T>
+__device__ __forceinline__ void ldv(const T *p, T (&o)[W]) {
+    if constexpr (W == 1) {
+        o[0] = CS ? __ldcs(p) : *p;
+    } else if constexpr (sizeof(T) == 4) {
+        const float4 q = CS ? __ldcs(reinterpret_cast<const float4 *>(p)) : *reinterpret_cast<const float4 *>(p);
+        o[0] = q.x; o[1] = q.y; o[2] = q.z; o[3] = q.w;
+    } else {
+        const double2 a = CS ? __ldcs(reinterpret_cast<const double2 *>(p)) : *reinterpret_cast<const double2 *>(p);
+        const double2 b = CS ? __ldcs(reinterpret_cast<const double2 *>(p) + 1)
+                             : *(reinterpret_cast<const double2 *>(p) + 1);
+        o[0] = a.x; o[1] = a.y; o[2] = b.x; o[3] = b.y;
+    }
+}
+template <int W, bool CS, class T>
+__device__ __forceinline__ void stv(T *p, const T (&x)[W]) {
+    if constexpr (W == 1) {
+        if (CS) __stcs(p, x[0]);
+        else *p = x[0];
+    } else if constexpr (sizeof(T) == 4) {
+        const float4 q = make_float4(x[0], x[1], x[2], x[3]);
+        if (CS) __stcs(reinterpret_cast<float4 *>(p), q);
+        else *reinterpret_cast<float4 *>(p) = q;
+    } else {
+        const double2 a = make_double2(x[0], x[1]), b = make_double2(x[2], x[3]);
+        if (CS) {
+            __stcs(reinterpret_cast<double2 *>(p), a);
+            __stcs(reinterpret_cast<double2 *>(p) + 1, b);
+        } else {
+            *reinterpret_cast<double2 *>(p) = a;
+            *(reinterpret_cast<double2 *>(p) + 1) = b;
+        }
+    }
+}
+
+// x / s for W elements at i (the gathered copy) and their dangling flags.
+template <int W>
+__device__ __forceinline__ void kscale(const float (&x)[W], uint32_t i, const float *inv32, const double *,
+                                       float (&o)[W], bool (&dang)[W]) {
+    float iv[W];
+    ldv<W, false>(inv32 + i, iv);
+#pragma unroll
+    for (int k = 0; k < W; k++) {
+        o[k] = x[k] * iv[k];
+        dang[k] = iv[k] == 0.0f;
+    }
+}
+template <int W>
+__device__ __forceinline__ void kscale(const double (&x)[W], uint32_t i, const float *, const double *dval,
+                                       double (&o)[W], bool (&dang)[W]) {
+    double dv[W];
+    ldv<W, false>(dval + i, dv);
+#pragma unroll
+    for (int k = 0; k < W; k++) {
+        dang[k] = dv[k] == 0.0;
+        o[k] = dang[k] ? 0.0 : x[k] / dv[k];
+    }
+}
+
+// Runs body<4>(i) over i = 0, 4, ... below n & ~3 (grid-stride), then
+// body<1>(i) over the tail.
+template <class F4, class F1>
+__device__ __forceinline__ void kfor(uint32_t n, F4 body4, F1 body1) {
+    const uint32_t tid = blockIdx.x * kVT + threadIdx.x, nt = gridDim.x * kVT;
+    const uint32_t n4 = n >> 2;
+    for (uint32_t j = tid; j < n4; j += nt) body4(j << 2);
+    for (uint32_t i = (n4 << 2) + tid; i < n; i += nt) body1(i);
+}
 
 // V0: rh = r, e = 0; records (rh.r, |r|_1, r.r).
 template <class T>
 __global__ void __launch_bounds__(kVT) kv0(uint32_t n, const T *r, T *rh, T *e, double4 *part5) {
     double a = 0.0, b = 0.0;
-    for (uint32_t v = blockIdx.x * kVT + threadIdx.x; v < n; v += gridDim.x * kVT) {
-        const T rv = r[v];
-        rh[v] = rv;
-        e[v] = T(0);
-        a += (double)rv * (double)rv;
-        b += fabs((double)rv);
-    }
+    auto body = [&](uint32_t i, auto w) {
+        constexpr int W = decltype(w)::value;
+        T rv[W], z[W];
+        ldv<W, true>(r + i, rv);
+#pragma unroll
+        for (int k = 0; k < W; k++) {
+            z[k] = T(0);
+            a += (double)rv[k] * (double)rv[k];
+            b += fabs((double)rv[k]);
+        }
+        stv<W, false>(rh + i, rv);
+        stv<W, true>(e + i, z);
+    };
+    kfor(n, [&](uint32_t i) { body(i, std::integral_constant<int, 4>()); },
+         [&](uint32_t i) { body(i, std::integral_constant<int, 1>()); });
     const double3 q = kblock3(a, b, 0.0);
     if (threadIdx.x == 0) part5[blockIdx.x] = make_double4(q.x, q.y, q.x, 0.0);
 }
@@ -256,15 +326,31 @@ __global__ void __launch_bounds__(kVT) kv1(uint32_t n, int q, KState *st, const 
     const double beta = restart ? 0.0 : (rhr / rho0) * (al / om);
     const T tb = (T)beta, to = (T)om;
     double dz = 0.0;
-    for (uint32_t i = blockIdx.x * kVT + threadIdx.x; i < n; i += gridDim.x * kVT) {
-        const T rv = __ldcs(r + i);
-        const T pv = restart ? rv : rv + tb * (__ldcs(p + i) - to * __ldcs(v + i));
-        __stcs(p + i, pv);  // streamed: only p/s is gathered, keep that in L2
-        bool dang;
-        pt[i] = kscaled(pv, i, inv32, dval, dang);
-        if (dang) dz += (double)pv;
-        if (write_rh) rh[i] = rv;
-    }
+    auto body = [&](uint32_t i, auto w) {
+        constexpr int W = decltype(w)::value;
+        T rv[W], pv[W], sc[W];
+        bool dang[W];
+        ldv<W, true>(r + i, rv);
+        if (restart) {
+#pragma unroll
+            for (int j = 0; j < W; j++) pv[j] = rv[j];
+        } else {
+            T po[W], vv[W];
+            ldv<W, true>(p + i, po);
+            ldv<W, true>(v + i, vv);
+#pragma unroll
+            for (int j = 0; j < W; j++) pv[j] = rv[j] + tb * (po[j] - to * vv[j]);
+        }
+        stv<W, true>(p + i, pv);  // streamed: only p/s is gathered, keep that in L2
+        kscale<W>(pv, i, inv32, dval, sc, dang);
+        stv<W, false>(pt + i, sc);
+#pragma unroll
+        for (int j = 0; j < W; j++)
+            if (dang[j]) dz += (double)pv[j];
+        if (write_rh) stv<W, false>(rh + i, rv);
+    };
+    kfor(n, [&](uint32_t i) { body(i, std::integral_constant<int, 4>()); },
+         [&](uint32_t i) { body(i, std::integral_constant<int, 1>()); });
     const double3 s3 = kblock3(dz, 0.0, 0.0);
     if (threadIdx.x == 0) part1[blockIdx.x] = make_double4(s3.x, 0.0, 0.0, 0.0);
     if (kleader()) {
@@ -290,13 +376,23 @@ __global__ void __launch_bounds__(kVT) kv2(uint32_t n, int q, KState *st, const 
     const double al = rho / sig;
     const T ta = (T)al;
     double dz = 0.0;
-    for (uint32_t i = blockIdx.x * kVT + threadIdx.x; i < n; i += gridDim.x * kVT) {
-        const T sv = __ldcs(r + i) - ta * __ldcs(v + i);
-        __stcs(s + i, sv);
-        bool dang;
-        sst[i] = kscaled(sv, i, inv32, dval, dang);
-        if (dang) dz += (double)sv;
-    }
+    auto body = [&](uint32_t i, auto w) {
+        constexpr int W = decltype(w)::value;
+        T rv[W], vv[W], sv[W], sc[W];
+        bool dang[W];
+        ldv<W, true>(r + i, rv);
+        ldv<W, true>(v + i, vv);
+#pragma unroll
+        for (int j = 0; j < W; j++) sv[j] = rv[j] - ta * vv[j];
+        stv<W, true>(s + i, sv);
+        kscale<W>(sv, i, inv32, dval, sc, dang);
+        stv<W, false>(sst + i, sc);
+#pragma unroll
+        for (int j = 0; j < W; j++)
+            if (dang[j]) dz += (double)sv[j];
+    };
+    kfor(n, [&](uint32_t i) { body(i, std::integral_constant<int, 4>()); },
+         [&](uint32_t i) { body(i, std::integral_constant<int, 1>()); });
     const double3 s3 = kblock3(dz, 0.0, 0.0);
     if (threadIdx.x == 0) part3[blockIdx.x] = make_double4(s3.x, 0.0, 0.0, 0.0);
     if (kleader()) st->alpha[q] = al;
@@ -314,15 +410,27 @@ __global__ void __launch_bounds__(kVT) kv3(uint32_t n, int q, KState *st, const 
     const double om = tt > 0.0 && isfinite(tt) ? ts / tt : 0.0;
     const T ta = (T)st->alpha[q], to = (T)om;
     double a = 0.0, b = 0.0, c = 0.0;
-    for (uint32_t i = blockIdx.x * kVT + threadIdx.x; i < n; i += gridDim.x * kVT) {
-        const T sv = __ldcs(s + i);
-        __stcs(e + i, __ldcs(e + i) + ta * __ldcs(p + i) + to * sv);
-        const T rv = sv - to * __ldcs(t + i);
-        __stcs(r + i, rv);
-        a += (double)__ldcs(rh + i) * (double)rv;
-        b += fabs((double)rv);
-        c += (double)rv * (double)rv;
-    }
+    auto body = [&](uint32_t i, auto w) {
+        constexpr int W = decltype(w)::value;
+        T sv[W], ev[W], pv[W], tv[W], hv[W], rv[W];
+        ldv<W, true>(s + i, sv);
+        ldv<W, true>(e + i, ev);
+        ldv<W, true>(p + i, pv);
+        ldv<W, true>(t + i, tv);
+        ldv<W, true>(rh + i, hv);
+#pragma unroll
+        for (int j = 0; j < W; j++) {
+            ev[j] = ev[j] + ta * pv[j] + to * sv[j];
+            rv[j] = sv[j] - to * tv[j];
+            a += (double)hv[j] * (double)rv[j];
+            b += fabs((double)rv[j]);
+            c += (double)rv[j] * (double)rv[j];
+        }
+        stv<W, true>(e + i, ev);
+        stv<W, true>(r + i, rv);
+    };
+    kfor(n, [&](uint32_t i) { body(i, std::integral_constant<int, 4>()); },
+         [&](uint32_t i) { body(i, std::integral_constant<int, 1>()); });
     const double3 s3 = kblock3(a, b, c);
     if (threadIdx.x == 0) part5[blockIdx.x] = make_double4(s3.x, s3.y, s3.z, 0.0);
     if (kleader()) {
@@ -403,23 +511,25 @@ static InnerResult bicgstab(const DeviceGraph &g, Workspace &ws, KrylovWs &k, KB
     res.launches += 1u;
     uint32_t it = 0;
     auto step = [&](int q) {
-        while (k.mv_ev.size() < 4u * (it + 1u)) {
+        while (k.mv_ev.size() < kEvStep * (it + 1u)) {
             cudaEvent_t e;
             PRG_CUDA(cudaEventCreate(&e));
             k.mv_ev.push_back(e);
         }
-        cudaEvent_t *ev = &k.mv_ev[4u * it];
-        kv1<T><<<kVB, kVT, 0, s>>>(n, q, k.st, k.part5, b.rh, r, b.p, b.pt, b.v, g.inv32, g.dval, k.part1);
+        cudaEvent_t *ev = &k.mv_ev[kEvStep * it];
         PRG_CUDA(cudaEventRecord(ev[0], s));
-        launch_iteration(mode, g.weighted, m1, cfg, s);
+        kv1<T><<<kVB, kVT, 0, s>>>(n, q, k.st, k.part5, b.rh, r, b.p, b.pt, b.v, g.inv32, g.dval, k.part1);
         PRG_CUDA(cudaEventRecord(ev[1], s));
+        launch_iteration(mode, g.weighted, m1, cfg, s);
+        PRG_CUDA(cudaEventRecord(ev[2], s));
         kv2<T><<<kVB, kVT, 0, s>>>(n, q, k.st, k.part2, cfg.grid, ws.hub_rec, g.nhub, r, b.v, b.s, b.st, g.inv32,
                                     g.dval, k.part3);
-        PRG_CUDA(cudaEventRecord(ev[2], s));
-        launch_iteration(mode, g.weighted, m2, cfg, s);
         PRG_CUDA(cudaEventRecord(ev[3], s));
+        launch_iteration(mode, g.weighted, m2, cfg, s);
+        PRG_CUDA(cudaEventRecord(ev[4], s));
         kv3<T><<<kVB, kVT, 0, s>>>(n, q, k.st, k.part4, cfg.grid, ws.hub_rec, g.nhub, b.rh, b.p, b.s, b.t, b.e, r,
                                     k.part5);
+        PRG_CUDA(cudaEventRecord(ev[5], s));
         res.launches += 5u;
     };
     // batches of `per` steps; the state copy of batch j is read while batch
@@ -451,18 +561,27 @@ static InnerResult bicgstab(const DeviceGraph &g, Workspace &ws, KrylovWs &k, KB
     PRG_CUDA(cudaEventElapsedTime(&ms, ws.eva, ws.evb));
     res.ms = ms;
     res.steps = k.h_st[0].count;
+    double vec_ms = 0.0, gap_ms = 0.0;
     for (uint32_t i = 0; i < res.steps && i < it; i++) {
-        float a = 0.f, b2 = 0.f;
-        PRG_CUDA(cudaEventElapsedTime(&a, k.mv_ev[4u * i], k.mv_ev[4u * i + 1u]));
-        PRG_CUDA(cudaEventElapsedTime(&b2, k.mv_ev[4u * i + 2u], k.mv_ev[4u * i + 3u]));
-        res.matvec_ms += (double)a + (double)b2;
+        const cudaEvent_t *ev = &k.mv_ev[kEvStep * i];
+        float t[5];
+        for (int j = 0; j < 5; j++) PRG_CUDA(cudaEventElapsedTime(&t[j], ev[j], ev[j + 1]));
+        res.matvec_ms += (double)t[1] + (double)t[3];
+        vec_ms += (double)t[0] + (double)t[2] + (double)t[4];
+        if (i + 1 < res.steps && i + 1 < it) {
+            float gp = 0.f;
+            PRG_CUDA(cudaEventElapsedTime(&gp, ev[5], k.mv_ev[kEvStep * (i + 1)]));
+            gap_ms += gp;
+        }
     }
     res.done = k.h_st[0].done;
     res.rnorm = k.h_st[0].rnorm;
     if (std::getenv("PRG_TRACE"))
-        std::fprintf(stderr, "[prg] bicgstab<%s>: %u steps, done=%d, ||r||=%.3e (r0 %.3e), restarts %u, %.3f ms\n",
+        std::fprintf(stderr,
+                     "[prg] bicgstab<%s>: %u steps, done=%d, ||r||=%.3e (r0 %.3e), restarts %u, %.3f ms "
+                     "(matvecs %.3f, vector kernels %.3f, between steps %.3f)\n",
                      sizeof(T) == 4 ? "f32" : "f64", res.steps, res.done, res.rnorm, k.h_st[0].r0norm,
-                     k.h_st[0].restarts, res.ms);
+                     k.h_st[0].restarts, res.ms, res.matvec_ms, vec_ms, gap_ms);
     return res;
 }
 
