@@ -43,6 +43,8 @@ struct KState {
     double rho[2], alpha[2], omega[2], rhh[2];  // by step parity
     double rel;        // inner stop: ||r|| <= max(rel * ||r0||, floor_abs)
     double floor_abs;
+    double near;       // rel * ||r0|| below near: aim for floor_abs in this solve
+    double best;       // smallest ||r|| so far (stagnation guard)
     double tol;        // set by the first V1 from ||r0||
     double rnorm;      // last residual norm V1 saw
     double r0norm;
@@ -51,10 +53,18 @@ struct KState {
     int32_t done;      // KDONE_*
     int32_t norm2;     // 0: L1 norms, 1: 2-norms
     uint32_t restarts;
-    uint32_t pad;
+    uint32_t stall;    // consecutive steps without a 2x gain over the best ||r||
 };
 
-enum : int32_t { KRUN = 0, KDONE_CONVERGED = 1, KDONE_BREAKDOWN = 2, KDONE_CAP = 3, KDONE_NONFINITE = 4 };
+enum : int32_t {
+    KRUN = 0,
+    KDONE_CONVERGED = 1,
+    KDONE_BREAKDOWN = 2,
+    KDONE_CAP = 3,
+    KDONE_NONFINITE = 4,
+    KDONE_STALLED = 5  // the residual stopped falling (precision limit of the inner type): keep e
+};
+constexpr uint32_t kStallSteps = 3;
 
 constexpr unsigned kVB = 148u * 4u;  // blocks of the vector kernels
 constexpr uint32_t kEvStep = 6;       // events per BiCGStab step (around each of its five kernels)
@@ -297,7 +307,10 @@ __global__ void __launch_bounds__(kVT) kv1(uint32_t n, int q, KState *st, const 
         if (kleader()) st->done = KDONE_NONFINITE;
         return;
     }
-    const double tol = k == 0 ? fmax(st->rel * norm, st->floor_abs) : st->tol;
+    // close to the final target already: finish it in this inner solve
+    // rather than pay for another outer cycle (residual pass + restart)
+    const double rt = st->rel * norm;
+    const double tol = k == 0 ? (rt < st->near ? st->floor_abs : fmax(rt, st->floor_abs)) : st->tol;
     if (k == 0 && kleader()) {
         st->tol = tol;
         st->r0norm = norm;
@@ -313,6 +326,16 @@ __global__ void __launch_bounds__(kVT) kv1(uint32_t n, int q, KState *st, const 
         if (kleader()) {
             st->rnorm = norm;
             st->done = KDONE_CAP;
+        }
+        return;
+    }
+    // stagnation: kStallSteps steps in a row without halving the best norm
+    const double best = k == 0 ? norm : st->best;
+    const uint32_t stall = k == 0 ? 0u : (norm < 0.5 * best ? 0u : st->stall + 1u);
+    if (stall >= kStallSteps) {
+        if (kleader()) {
+            st->rnorm = norm;
+            st->done = KDONE_STALLED;
         }
         return;
     }
@@ -357,6 +380,8 @@ __global__ void __launch_bounds__(kVT) kv1(uint32_t n, int q, KState *st, const 
         st->rho[q] = restart ? rr : rhr;
         st->rhh[q] = restart ? rr : rhh;
         st->rnorm = norm;
+        st->best = fmin(best, norm);
+        st->stall = stall;
         if (write_rh) st->restarts += 1u;
     }
 }
@@ -482,7 +507,7 @@ static IterArgs matvec_args(const IterArgs &base, const T *in, const T *in_scale
 template <class T>
 static InnerResult bicgstab(const DeviceGraph &g, Workspace &ws, KrylovWs &k, KBuf<T> &b, const T *r_in,
                             const double *t64, const float *t32, double damping, double rel, double floor_abs,
-                            uint32_t cap, bool norm2, cudaStream_t s) {
+                            double near, uint32_t cap, bool norm2, cudaStream_t s) {
     InnerResult res;
     constexpr int mode = sizeof(T) == 4 ? MODE_KRY32 : MODE_KRY64;
     const LaunchCfg &cfg = ws.cfg[mode];
@@ -493,6 +518,7 @@ static InnerResult bicgstab(const DeviceGraph &g, Workspace &ws, KrylovWs &k, KB
     std::memset(&init, 0, sizeof(init));
     init.rel = rel;
     init.floor_abs = floor_abs;
+    init.near = near;
     init.cap = cap;
     init.norm2 = norm2 ? 1 : 0;
     PRG_CUDA(cudaMemcpyAsync(k.st, &init, sizeof(KState), cudaMemcpyHostToDevice, s));
@@ -660,11 +686,14 @@ void solve_krylov(const DeviceGraph &g, Workspace &ws, const SolveOpts &o, const
         }
         const uint32_t cap = std::min<uint32_t>(500u, (pass_cap - mv - fp64) / 2u + 1u);
         InnerResult ir;
+        // a relative target within 100x of the final one is replaced by the floor
+        const double near = linsys ? 0.0 : 100.0 * thr_final;
         if (fp64_inner)
-            ir = bicgstab<double>(g, ws, k, k.d, k.d.r, d_t, nullptr, o.damping, rel, floor_abs, cap, linsys, s);
+            ir = bicgstab<double>(g, ws, k, k.d, k.d.r, d_t, nullptr, o.damping, rel, floor_abs, near, cap, linsys,
+                                  s);
         else
             ir = bicgstab<float>(g, ws, k, k.f, ws.b32, nullptr, ppr ? ws.t32 : nullptr, o.damping, rel, floor_abs,
-                                 cap, false, s);
+                                 near, cap, false, s);
         mv += 2u * ir.steps;
         st.spmv_ms += ir.matvec_ms;
         st.spmv_launches += 2u * ir.steps;

