@@ -49,7 +49,8 @@ enum prg_status {
     PRG_ERR_DID_NOT_CONVERGE = 6,     /* IgraphError::DidNotConverge (never raised by the drop-ins) */
     PRG_ERR_TIMEOUT = 7,              /* a bounded device wait expired (batched solver) */
     PRG_ERR_PARSE = 8,                /* IgraphError::Parse { line, message } */
-    PRG_ERR_IO = 9                    /* IgraphError::Io (the text is not valid UTF-8) */
+    PRG_ERR_IO = 9,                   /* IgraphError::Io (the text is not valid UTF-8) */
+    PRG_ERR_UNSUPPORTED = 10          /* IgraphError::Unsupported(&'static str) */
 };
 
 enum prg_precision {
@@ -115,6 +116,22 @@ int32_t prg_pagerank(uint32_t n, uint64_t m, const uint32_t *from, const uint32_
  * ||b - A x||_2 < 1e-13 ||b||_2 from the uniform start; unweighted. */
 int32_t prg_pagerank_linsys(uint32_t n, uint64_t m, const uint32_t *from, const uint32_t *to, int32_t directed,
                             double *out);
+
+/* rust-igraph eigenvector_centrality() (src/algorithms/properties/eigenvector.rs:118-125,
+ * 286-372): undirected, unweighted; the max-normalised shifted power
+ * iteration x' = (A + I) x to an L1 change < 1e-14 (at most 5000
+ * iterations), negatives clamped.  *eigenvalue (optional) receives the
+ * Rayleigh quotient x.Ax / x.x.  A directed graph gives PRG_ERR_UNSUPPORTED
+ * like the reference. */
+int32_t prg_eigenvector_centrality(uint32_t n, uint64_t m, const uint32_t *from, const uint32_t *to, int32_t directed,
+                                   double *out, double *eigenvalue);
+
+/* rust-igraph hub_and_authority_scores() (src/algorithms/properties/hits.rs:122-230),
+ * unweighted: hub[n], authority[n] (max element 1) and the dominant
+ * eigenvalue of A A^T.  Undirected graphs: both vectors are the eigenvector
+ * centrality and the eigenvalue its squared Rayleigh quotient. */
+int32_t prg_hub_and_authority_scores(uint32_t n, uint64_t m, const uint32_t *from, const uint32_t *to,
+                                     int32_t directed, double *hub, double *authority, double *eigenvalue);
 
 /* rust-igraph pagerank_weighted() (pagerank_weighted.rs:52-161).
  * weights_len is the caller's slice length (checked against m like :62-68). */

@@ -66,6 +66,10 @@ def lib():
         L.or_pagerank_tight.argtypes = [C.c_uint32, C.c_uint64, _u32p, _u32p, C.c_int, C.c_void_p, C.c_void_p,
                                         C.c_double, C.c_double, C.c_uint32, C.c_int, _f64p,
                                         C.POINTER(C.c_double), C.c_int]
+        L.or_eigenvector_centrality.restype = C.c_int
+        L.or_eigenvector_centrality.argtypes = [C.c_uint32, C.c_uint64, _u32p, _u32p, _f64p, C.POINTER(C.c_double)]
+        L.or_hits.restype = C.c_int
+        L.or_hits.argtypes = [C.c_uint32, C.c_uint64, _u32p, _u32p, C.c_int, _f64p, _f64p, C.POINTER(C.c_double)]
         L.or_adj_build.restype = C.c_void_p
         L.or_adj_build.argtypes = [C.c_uint32, C.c_uint64, _u32p, _u32p, C.c_int]
         L.or_adj_free.restype = None
@@ -173,6 +177,27 @@ def personalized_pagerank(n, frm, to, directed, reset, damping, return_iters=Fal
     lib().or_personalized_pagerank(n, len(f), f, t, int(directed), r, damping, out, C.byref(it))
     out = out[:n]
     return (out, it.value) if return_iters else out
+
+
+def eigenvector_centrality(n, frm, to):
+    """rust-igraph eigenvector_centrality (undirected, unweighted; eigenvector.rs:286-372):
+    (vector, eigenvalue, iterations)."""
+    f, t = _edges(frm, to)
+    out = np.zeros(max(n, 1), np.float64)
+    lam = C.c_double(0.0)
+    it = lib().or_eigenvector_centrality(n, len(f), f, t, out, C.byref(lam))
+    return out[:n], lam.value, it
+
+
+def hub_and_authority_scores(n, frm, to, directed):
+    """rust-igraph hub_and_authority_scores (unweighted; hits.rs:122-230):
+    (hub, authority, eigenvalue, iterations)."""
+    f, t = _edges(frm, to)
+    hub = np.zeros(max(n, 1), np.float64)
+    auth = np.zeros(max(n, 1), np.float64)
+    lam = C.c_double(0.0)
+    it = lib().or_hits(n, len(f), f, t, int(directed), hub, auth, C.byref(lam))
+    return hub[:n], auth[:n], lam.value, it
 
 
 def pagerank_tight(n, frm, to, directed, weights=None, reset=None, damping=0.85, tol=1e-14,

@@ -744,3 +744,180 @@ int64_t or_pagerank_tight(uint32_t n, uint64_t m, const uint32_t *from, const ui
     free(r); free(s); free(rp); free(src); free(val); free(x); free(xt); free(xn); free(part_d);
     return it;
 }
+
+/* ------------------------------------------------------------------------
+ * Eigenvector centrality and HITS (unweighted).  Neighbour lists are sorted
+ * ascending, the order the reference's index (rebuild_indexes sorts by
+ * (from, to) and (to, from), graph.rs:1708-1768) gives neighbors() /
+ * out_neighbors_vec() / in_neighbors_vec(), so the sums run in its order.
+ * ---------------------------------------------------------------------- */
+
+static int cmp_u32(const void *a, const void *b) {
+    const uint32_t x = *(const uint32_t *)a, y = *(const uint32_t *)b;
+    return x < y ? -1 : x > y;
+}
+
+/* rows[v] = sorted list of key->val pairs grouped by key (counting sort,
+ * then each row sorted ascending). */
+static void sorted_lists(uint32_t n, uint64_t cnt, const uint32_t *key, const uint32_t *val, uint64_t **rp_out,
+                         uint32_t **col_out) {
+    uint64_t *rp = (uint64_t *)calloc((size_t)n + 1, sizeof(uint64_t));
+    uint32_t *col = (uint32_t *)malloc((cnt ? cnt : 1) * sizeof(uint32_t));
+    for (uint64_t i = 0; i < cnt; i++) rp[key[i] + 1]++;
+    for (uint32_t v = 0; v < n; v++) rp[v + 1] += rp[v];
+    uint64_t *pos = (uint64_t *)malloc(((size_t)n + 1) * sizeof(uint64_t));
+    memcpy(pos, rp, ((size_t)n + 1) * sizeof(uint64_t));
+    for (uint64_t i = 0; i < cnt; i++) col[pos[key[i]]++] = val[i];
+    for (uint32_t v = 0; v < n; v++) qsort(col + rp[v], rp[v + 1] - rp[v], sizeof(uint32_t), cmp_u32);
+    free(pos);
+    *rp_out = rp;
+    *col_out = col;
+}
+
+/* Undirected neighbour lists: each edge in both rows, a loop twice. */
+static void undirected_lists(uint32_t n, uint64_t m, const uint32_t *from, const uint32_t *to, uint64_t **rp,
+                             uint32_t **col) {
+    uint32_t *k = (uint32_t *)malloc((2 * m + 1) * sizeof(uint32_t));
+    uint32_t *v = (uint32_t *)malloc((2 * m + 1) * sizeof(uint32_t));
+    for (uint64_t e = 0; e < m; e++) {
+        k[2 * e] = from[e];
+        v[2 * e] = to[e];
+        k[2 * e + 1] = to[e];
+        v[2 * e + 1] = from[e];
+    }
+    sorted_lists(n, 2 * m, k, v, rp, col);
+    free(k);
+    free(v);
+}
+
+static double rescale_max_abs(double *x, uint32_t n) {
+    double mx = 0.0;
+    for (uint32_t i = 0; i < n; i++) mx = fmax(mx, fabs(x[i]));
+    if (mx > 0.0)
+        for (uint32_t i = 0; i < n; i++) x[i] /= mx;
+    return mx;
+}
+
+/* eigenvector_centrality, undirected and unweighted (eigenvector.rs:286-372):
+ * x = 1; repeat x' = (A + I) x, x' /= max|x'|, until sum|x' - x| < 1e-14
+ * or 5000 iterations; eigenvalue = Rayleigh quotient x.Ax / x.x; negatives
+ * clamped to 0.  Returns the iterations run. */
+int or_eigenvector_centrality(uint32_t n, uint64_t m, const uint32_t *from, const uint32_t *to, double *out,
+                              double *eigval) {
+    if (n == 0) return 0;
+    if (m == 0 || n == 1) {
+        for (uint32_t i = 0; i < n; i++) out[i] = 1.0;
+        if (eigval) *eigval = 0.0;
+        return 0;
+    }
+    uint64_t *rp;
+    uint32_t *col;
+    undirected_lists(n, m, from, to, &rp, &col);
+    double *x = (double *)malloc(n * sizeof(double)), *xn = (double *)malloc(n * sizeof(double));
+    for (uint32_t i = 0; i < n; i++) x[i] = 1.0;
+    int it = 0;
+    for (; it < 5000;) {
+        it++;
+        for (uint32_t v = 0; v < n; v++) {
+            double s = x[v];
+            for (uint64_t p = rp[v]; p < rp[v + 1]; p++) s += x[col[p]];
+            xn[v] = s;
+        }
+        rescale_max_abs(xn, n);
+        double diff = 0.0;
+        for (uint32_t v = 0; v < n; v++) diff += fabs(xn[v] - x[v]);
+        double *t = x; x = xn; xn = t;
+        if (diff < 1e-14) break;
+    }
+    double num = 0.0, den = 0.0;
+    for (uint32_t v = 0; v < n; v++) {
+        double s = 0.0;
+        for (uint64_t p = rp[v]; p < rp[v + 1]; p++) s += x[col[p]];
+        num += x[v] * s;
+        den += x[v] * x[v];
+    }
+    if (eigval) *eigval = den > 0.0 ? num / den : 0.0;
+    for (uint32_t v = 0; v < n; v++) out[v] = x[v] < 0.0 ? 0.0 : x[v];
+    free(rp); free(col); free(x); free(xn);
+    return it;
+}
+
+/* hub_and_authority_scores, unweighted (hits.rs:122-230).  Directed: h = out-degrees
+ * max-normalised; repeat tmp = A^T h, h' = A tmp, eigenvalue = max|h'|, h' /= it,
+ * until sum|h' - h| < 1e-12 or 5000 iterations; then clamp, authority = A^T h
+ * rescaled and clamped.  Undirected: hub = authority = eigenvector
+ * centrality, eigenvalue = (Rayleigh quotient of A)^2 (hits.rs:131-141, 586-605). */
+int or_hits(uint32_t n, uint64_t m, const uint32_t *from, const uint32_t *to, int directed, double *hub,
+            double *auth, double *eigval) {
+    if (n == 0) return 0;
+    if (!directed) {
+        double lam = 0.0;
+        int it = or_eigenvector_centrality(n, m, from, to, hub, NULL);
+        memcpy(auth, hub, n * sizeof(double));
+        if (m > 0) {
+            uint64_t *rp;
+            uint32_t *col;
+            undirected_lists(n, m, from, to, &rp, &col);
+            double num = 0.0, den = 0.0;
+            for (uint32_t v = 0; v < n; v++) {
+                double s = 0.0;
+                for (uint64_t p = rp[v]; p < rp[v + 1]; p++) s += hub[col[p]];
+                den += hub[v] * hub[v];
+                num += hub[v] * s;
+            }
+            lam = den > 0.0 ? num / den : 0.0;
+            free(rp); free(col);
+        }
+        if (eigval) *eigval = lam * lam;
+        return it;
+    }
+    if (m == 0) {
+        for (uint32_t i = 0; i < n; i++) hub[i] = auth[i] = 1.0;
+        if (eigval) *eigval = 0.0;
+        return 0;
+    }
+    uint64_t *orp, *irp;
+    uint32_t *ocol, *icol;
+    sorted_lists(n, m, from, to, &orp, &ocol);  /* out_adj[u] = targets */
+    sorted_lists(n, m, to, from, &irp, &icol);  /* in_adj[v] = sources */
+    double *h = (double *)malloc(n * sizeof(double)), *hn = (double *)malloc(n * sizeof(double));
+    double *tmp = (double *)malloc(n * sizeof(double));
+    for (uint32_t u = 0; u < n; u++) h[u] = (double)(orp[u + 1] - orp[u]);
+    rescale_max_abs(h, n);
+    double lam = 0.0;
+    int it = 0;
+    for (; it < 5000;) {
+        it++;
+        for (uint32_t v = 0; v < n; v++) {
+            double s = 0.0;
+            for (uint64_t p = irp[v]; p < irp[v + 1]; p++) s += h[icol[p]];
+            tmp[v] = s;
+        }
+        for (uint32_t u = 0; u < n; u++) {
+            double s = 0.0;
+            for (uint64_t p = orp[u]; p < orp[u + 1]; p++) s += tmp[ocol[p]];
+            hn[u] = s;
+        }
+        double mx = 0.0;
+        for (uint32_t u = 0; u < n; u++) mx = fmax(mx, fabs(hn[u]));
+        if (mx > 0.0) {
+            lam = mx;
+            for (uint32_t u = 0; u < n; u++) hn[u] /= mx;
+        }
+        double diff = 0.0;
+        for (uint32_t u = 0; u < n; u++) diff += fabs(hn[u] - h[u]);
+        double *t = h; h = hn; hn = t;
+        if (diff < 1e-12) break;
+    }
+    for (uint32_t u = 0; u < n; u++) hub[u] = h[u] < 0.0 ? 0.0 : h[u];
+    for (uint32_t v = 0; v < n; v++) {
+        double s = 0.0;
+        for (uint64_t p = irp[v]; p < irp[v + 1]; p++) s += hub[icol[p]];
+        auth[v] = s;
+    }
+    rescale_max_abs(auth, n);
+    for (uint32_t v = 0; v < n; v++) if (auth[v] < 0.0) auth[v] = 0.0;
+    if (eigval) *eigval = lam;
+    free(orp); free(irp); free(ocol); free(icol); free(h); free(hn); free(tmp);
+    return it;
+}

@@ -21,6 +21,7 @@
 #include "gnn.cuh"
 #include "graph.cuh"
 #include "edgelist.cuh"
+#include "eigen.cuh"
 #include "handle.cuh"
 #include "ppr_batch.cuh"
 #include "solver.cuh"
@@ -111,7 +112,7 @@ __global__ void max_endpoint_kernel(const uint32_t *a, const uint32_t *b, uint64
 
 // Creates a handle from device edge arrays (copies nothing on the host).
 int32_t create_from_device(uint32_t n, uint64_t m, const uint32_t *d_from, const uint32_t *d_to, const double *d_w,
-                           int32_t directed, cudaStream_t s, prg_graph **out) {
+                           int32_t directed, cudaStream_t s, prg_graph **out, int relabel = -1) {
     if (m > 0xFFFFFFFFull) return fail(PRG_ERR_INTERNAL, "ecount overflows u32");
     const uint64_t arcs = directed ? m : 2 * m;
     if (arcs + prg::kColPad >= 0xFFFFFFFFull)
@@ -128,7 +129,7 @@ int32_t create_from_device(uint32_t n, uint64_t m, const uint32_t *d_from, const
         h->g.shortmax = t.shortmax;
         h->g.split = t.split;
         h->g.blocks_per_sm = t.blocks_per_sm;
-        h->g.relabel = t.relabel;
+        h->g.relabel = relabel >= 0 ? relabel : t.relabel;
         h->g.hot_cache = t.hot_cache;
         h->g.l1_hot32 = t.l1_hot32;
         h->g.l1_hot64 = t.l1_hot64;
@@ -156,7 +157,7 @@ int32_t create_from_device(uint32_t n, uint64_t m, const uint32_t *d_from, const
 }
 
 int32_t create_from_host(uint32_t n, uint64_t m, const uint32_t *from, const uint32_t *to, const double *w,
-                         int32_t directed, prg_graph **out) {
+                         int32_t directed, prg_graph **out, int relabel = -1) {
     if (!ensure_pool_config()) return fail(PRG_ERR_CUDA, "cuda: no usable device");
     cudaStream_t s;
     PRG_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
@@ -177,7 +178,7 @@ int32_t create_from_host(uint32_t n, uint64_t m, const uint32_t *from, const uin
         PRG_CUDA(cudaMallocAsync((void **)&d_w, mm * 8, s));
         if (m) PRG_CUDA(cudaMemcpyAsync(d_w, w, m * 8, cudaMemcpyHostToDevice, s));
     }
-    int32_t rc = create_from_device(n, m, d_f, d_t, w ? d_w : nullptr, directed, s, out);
+    int32_t rc = create_from_device(n, m, d_f, d_t, w ? d_w : nullptr, directed, s, out, relabel);
     cudaFreeAsync(d_f, s);
     cudaFreeAsync(d_t, s);
     if (d_w) cudaFreeAsync(d_w, s);
@@ -350,6 +351,90 @@ int32_t prg_pagerank(uint32_t n, uint64_t m, const uint32_t *from, const uint32_
         return PRG_OK;
     }
     return dropin(n, m, from, to, directed, nullptr, nullptr, 0.85, out);
+    PRG_GUARD_END
+}
+
+int32_t prg_eigenvector_centrality(uint32_t n, uint64_t m, const uint32_t *from, const uint32_t *to, int32_t directed,
+                                   double *out, double *eigenvalue) {
+    g_err.clear();
+    PRG_GUARD_BEGIN
+    if (eigenvalue) *eigenvalue = 0.0;
+    if (directed)  // eigenvector.rs:118-123
+        return fail(PRG_ERR_UNSUPPORTED,
+                    "directed eigenvector_centrality \xe2\x80\x94 use eigenvector_centrality_directed or _full");
+    if (n == 0) return PRG_OK;
+    if (m == 0 || n == 1) {  // eigenvector.rs:296-307: ones, eigenvalue 0
+        for (uint32_t i = 0; i < n; i++) out[i] = 1.0;
+        return PRG_OK;
+    }
+    prg_graph *h = nullptr;
+    int32_t rc = create_from_host(n, m, from, to, nullptr, 0, &h);
+    if (rc != PRG_OK) return rc;
+    try {
+        cudaStream_t s = h->stream;
+        if (!h->d_out) PRG_CUDA(cudaMallocAsync((void **)&h->d_out, (uint64_t)n * 8, s));
+        const prg::eig::Result r = prg::eig::eigenvector_centrality(h->g, h->ws, h->d_out, s);
+        PRG_CUDA(cudaMemcpyAsync(out, h->d_out, (uint64_t)n * 8, cudaMemcpyDeviceToHost, s));
+        PRG_CUDA(cudaStreamSynchronize(s));
+        if (eigenvalue) *eigenvalue = r.eigenvalue;
+    } catch (...) {
+        destroy(h);
+        throw;
+    }
+    destroy(h);
+    return PRG_OK;
+    PRG_GUARD_END
+}
+
+int32_t prg_hub_and_authority_scores(uint32_t n, uint64_t m, const uint32_t *from, const uint32_t *to,
+                                     int32_t directed, double *hub, double *authority, double *eigenvalue) {
+    g_err.clear();
+    PRG_GUARD_BEGIN
+    if (eigenvalue) *eigenvalue = 0.0;
+    if (n == 0) return PRG_OK;
+    if (!directed) {
+        // hits.rs:131-141: eigenvector centrality, eigenvalue = (x.Ax / x.x)^2
+        double lam = 0.0;
+        int32_t rc = prg_eigenvector_centrality(n, m, from, to, 0, hub, &lam);
+        if (rc != PRG_OK) return rc;
+        if (n == 1 && m > 0) lam = 2.0 * (double)m;  // x = [1]; every edge is a loop seen twice
+        for (uint32_t i = 0; i < n; i++) authority[i] = hub[i];
+        if (eigenvalue) *eigenvalue = lam * lam;
+        return PRG_OK;
+    }
+    if (m == 0) {  // hits.rs:144-150
+        for (uint32_t i = 0; i < n; i++) hub[i] = authority[i] = 1.0;
+        return PRG_OK;
+    }
+    prg_graph *g = nullptr, *rev = nullptr;
+    int32_t rc = create_from_host(n, m, from, to, nullptr, 1, &g, 0);
+    if (rc != PRG_OK) return rc;
+    rc = create_from_host(n, m, to, from, nullptr, 1, &rev, 0);
+    if (rc != PRG_OK) {
+        destroy(g);
+        return rc;
+    }
+    try {
+        cudaStream_t s = g->stream;
+        PRG_CUDA(cudaStreamSynchronize(rev->stream));  // rev's build runs on its own stream
+        double *d_h = nullptr, *d_a = nullptr;
+        PRG_CUDA(cudaMallocAsync((void **)&d_h, (uint64_t)n * 8, s));
+        PRG_CUDA(cudaMallocAsync((void **)&d_a, (uint64_t)n * 8, s));
+        const prg::eig::Result r = prg::eig::hits_directed(g->g, g->ws, rev->g, rev->ws, d_h, d_a, s);
+        PRG_CUDA(cudaMemcpyAsync(hub, d_h, (uint64_t)n * 8, cudaMemcpyDeviceToHost, s));
+        PRG_CUDA(cudaMemcpyAsync(authority, d_a, (uint64_t)n * 8, cudaMemcpyDeviceToHost, s));
+        cudaFreeAsync(d_h, s);
+        cudaFreeAsync(d_a, s);
+        PRG_CUDA(cudaStreamSynchronize(s));
+        if (eigenvalue) *eigenvalue = r.eigenvalue;
+    } catch (...) {
+        destroy(g);
+        destroy(rev);
+        throw;
+    }
+    destroy(g);
+    destroy(rev);
+    return PRG_OK;
     PRG_GUARD_END
 }
 

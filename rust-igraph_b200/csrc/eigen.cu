@@ -1,0 +1,371 @@
+// eigen.cu — eigenvector centrality and HITS hub/authority scores
+// (unweighted) as max-normalised power iterations over the resident CSR.
+//
+//   eigenvector_centrality (undirected; eigenvector.rs:286-372):
+//     x = 1; repeat x' = (A + I) x, x' /= max|x'| until sum|x' - x| < 1e-14
+//     or 5000 iterations; eigenvalue = x.Ax / x.x; negatives clamped.
+//   hub_and_authority_scores (hits.rs:122-230): directed graphs iterate
+//     h' = A (A^T h) from the out-degrees (max-normalised), the eigenvalue is
+//     max|h'|, until sum|h' - h| < 1e-12; authority = A^T h rescaled;
+//     undirected graphs take the eigenvector centrality and (x.Ax/x.x)^2.
+//
+// One iteration is the adjacency product (iter_kernel<MODE_EIG64>, which
+// also leaves per-block max |y| records), a normalise kernel (every block
+// reduces the records in the same order, divides, and records its part of
+// the L1 change) and a one-block check kernel that sums the parts and
+// raises `done`.  All kernels return at once once `done` is set, so the
+// host enqueues iterations ahead and polls a pinned copy of the state.
+// A^T products gather over the in-CSR of the graph; A products over the
+// in-CSR of the reversed graph (both built without relabelling, so they
+// share vertex ids).
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
+#include "eigen.cuh"
+#include "solver.cuh"
+
+namespace prg {
+namespace eig {
+
+struct State {
+    int32_t done;
+    uint32_t iters;
+    uint32_t max_iter;
+    int32_t final_buf;  // buffer index holding the newest normalised iterate
+    double diff, eps;
+    double maxv;        // max |y| of the newest product (HITS eigenvalue)
+    double pad;
+};
+
+constexpr unsigned kNB = 148u * 4u;
+constexpr int kNT = 256;
+
+__device__ __forceinline__ double3 recs3(const double4 *a, uint32_t na, const double4 *b, uint32_t nb) {
+    // (max .x, sum .y, sum .z) in a fixed order; result in every thread
+    __shared__ double sm[3][kNT / 32];
+    __shared__ double out[3];
+    double mx = 0.0, y = 0.0, z = 0.0;
+    for (uint32_t i = threadIdx.x; i < na; i += kNT) {
+        const double4 q = a[i];
+        mx = fmax(mx, q.x);
+        y += q.y;
+        z += q.z;
+    }
+    for (uint32_t i = threadIdx.x; i < nb; i += kNT) {
+        const double4 q = b[i];
+        mx = fmax(mx, q.x);
+        y += q.y;
+        z += q.z;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+        y += __shfl_xor_sync(0xffffffffu, y, o);
+        z += __shfl_xor_sync(0xffffffffu, z, o);
+    }
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    __syncthreads();
+    if (l == 0) {
+        sm[0][w] = mx;
+        sm[1][w] = y;
+        sm[2][w] = z;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int k = 1; k < kNT / 32; k++) {
+            mx = fmax(mx, sm[0][k]);
+            y += sm[1][k];
+            z += sm[2][k];
+        }
+        out[0] = mx;
+        out[1] = y;
+        out[2] = z;
+    }
+    __syncthreads();
+    return make_double3(out[0], out[1], out[2]);
+}
+
+// x /= max (records of the product that wrote x), sum |x - xold| per block.
+__global__ void __launch_bounds__(kNT) normalise_kernel(uint32_t n, const double4 *recs, uint32_t nrec,
+                                                        const double4 *hub_rec, uint32_t nhub, double *x,
+                                                        const double *xold, double4 *part, const State *st) {
+    if (st && *(volatile const int32_t *)&st->done) return;
+    const double mx = recs3(recs, nrec, hub_rec, nhub).x;
+    double d = 0.0;
+    for (uint32_t v = blockIdx.x * kNT + threadIdx.x; v < n; v += gridDim.x * kNT) {
+        double xv = x[v];
+        if (mx > 0.0) {
+            xv /= mx;
+            x[v] = xv;
+        }
+        if (xold) d += fabs(xv - xold[v]);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) d += __shfl_xor_sync(0xffffffffu, d, o);
+    __shared__ double sh[kNT / 32];
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    if (l == 0) sh[w] = d;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int k = 1; k < kNT / 32; k++) d += sh[k];
+        part[blockIdx.x] = make_double4(d, mx, 0.0, 0.0);
+    }
+}
+
+__global__ void check_kernel(const double4 *part, uint32_t nb, State *st, int32_t buf) {
+    if (st->done) return;
+    __shared__ double sh[32];
+    double d = 0.0;
+    for (uint32_t i = threadIdx.x; i < nb; i += blockDim.x) d += part[i].x;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) d += __shfl_xor_sync(0xffffffffu, d, o);
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    if (l == 0) sh[w] = d;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int k = 1; k < (int)(blockDim.x >> 5); k++) d += sh[k];
+        const double mx = part[0].y;
+        st->iters += 1u;
+        st->diff = d;
+        if (mx > 0.0) st->maxv = mx;
+        st->final_buf = buf;
+        if (d < st->eps || st->iters >= st->max_iter) st->done = 1;
+    }
+}
+
+__global__ void fill_kernel(double *x, uint32_t n, double v) {
+    for (uint32_t i = blockIdx.x * kNT + threadIdx.x; i < n; i += gridDim.x * kNT) x[i] = v;
+}
+
+// x = out-degree and block records (max, 0, 0) for the normalisation
+__global__ void degree_seed_kernel(const uint32_t *deg, uint32_t n, double *x, double4 *recs) {
+    double mx = 0.0;
+    for (uint32_t i = blockIdx.x * kNT + threadIdx.x; i < n; i += gridDim.x * kNT) {
+        x[i] = (double)deg[i];
+        mx = fmax(mx, x[i]);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    __shared__ double sh[kNT / 32];
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    if (l == 0) sh[w] = mx;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int k = 1; k < kNT / 32; k++) mx = fmax(mx, sh[k]);
+        recs[blockIdx.x] = make_double4(mx, 0.0, 0.0, 0.0);
+    }
+}
+
+__global__ void clamp_kernel(double *x, uint32_t n) {
+    for (uint32_t i = blockIdx.x * kNT + threadIdx.x; i < n; i += gridDim.x * kNT)
+        if (x[i] < 0.0) x[i] = 0.0;
+}
+
+// ---------------------------------------------------------------- host side
+
+struct Product {
+    const DeviceGraph *g;
+    Workspace *ws;
+};
+
+static IterArgs product_args(const Product &pr, const double *x, double *y, double shift, double4 *recs,
+                             const int32_t *done) {
+    IterArgs a = base_args(*pr.g, *pr.ws, 0.0);
+    a.x64_in = x;
+    a.xt64_in = x;
+    a.x64_out = y;
+    a.shift = shift;
+    a.kpart_out = recs;
+    a.kdone = done;
+    return a;
+}
+
+static void product(const Product &pr, const double *x, double *y, double shift, double4 *recs, const int32_t *done,
+                    cudaStream_t s) {
+    launch_iteration(MODE_EIG64, pr.g->weighted, product_args(pr, x, y, shift, recs, done), pr.ws->cfg[MODE_EIG64],
+                     s);
+}
+
+template <class T>
+static T *alloc(uint64_t count, cudaStream_t s) {
+    void *p = nullptr;
+    PRG_CUDA(cudaMallocAsync(&p, std::max<uint64_t>(count, 1) * sizeof(T), s));
+    return (T *)p;
+}
+template <class T>
+static void release(T *&p, cudaStream_t s) {
+    if (p) cudaFreeAsync(p, s);
+    p = nullptr;
+}
+
+// Runs iterations of `one(it)` (which enqueues one iteration ending in
+// check_kernel) until st->done, polling one batch behind.
+template <class F>
+static void run_until_done(State *d_st, State *h_st, uint32_t max_iter, cudaStream_t s, F one) {
+    cudaEvent_t ev[2];
+    for (cudaEvent_t &e : ev) PRG_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    const uint32_t per = 8;
+    uint32_t it = 0, batch = 0;
+    const uint32_t max_batches = max_iter / per + 3u;
+    bool stop = false;
+    try {
+        while (!stop) {
+            for (uint32_t i = 0; i < per && it < max_iter + per; i++) one(it++);
+            const int slot = (int)(batch & 1u);
+            PRG_CUDA(cudaMemcpyAsync(&h_st[slot], d_st, sizeof(State), cudaMemcpyDeviceToHost, s));
+            PRG_CUDA(cudaEventRecord(ev[slot], s));
+            if (batch > 0) {
+                PRG_CUDA(cudaEventSynchronize(ev[slot ^ 1]));
+                if (h_st[slot ^ 1].done) stop = true;
+            }
+            if (++batch >= max_batches) stop = true;
+        }
+        PRG_CUDA(cudaMemcpyAsync(&h_st[0], d_st, sizeof(State), cudaMemcpyDeviceToHost, s));
+        PRG_CUDA(cudaStreamSynchronize(s));
+    } catch (...) {
+        for (cudaEvent_t &e : ev) cudaEventDestroy(e);
+        throw;
+    }
+    for (cudaEvent_t &e : ev) cudaEventDestroy(e);
+}
+
+static double rayleigh(const Product &pr, const double *x, double *tmp, double4 *recs, cudaStream_t s) {
+    product(pr, x, tmp, 0.0, recs, nullptr, s);
+    const unsigned nb = pr.ws->cfg[MODE_EIG64].grid;
+    std::vector<double4> h(nb), hh(std::max<uint32_t>(pr.g->nhub, 1));
+    PRG_CUDA(cudaMemcpyAsync(h.data(), recs, nb * sizeof(double4), cudaMemcpyDeviceToHost, s));
+    if (pr.g->nhub)
+        PRG_CUDA(cudaMemcpyAsync(hh.data(), pr.ws->hub_rec, pr.g->nhub * sizeof(double4), cudaMemcpyDeviceToHost, s));
+    PRG_CUDA(cudaStreamSynchronize(s));
+    double num = 0.0, den = 0.0;
+    for (const double4 &q : h) {
+        num += q.y;
+        den += q.z;
+    }
+    for (uint32_t i = 0; i < pr.g->nhub; i++) {
+        num += hh[i].y;
+        den += hh[i].z;
+    }
+    return den > 0.0 ? num / den : 0.0;
+}
+
+Result eigenvector_centrality(const DeviceGraph &g, Workspace &ws, double *d_out, cudaStream_t s) {
+    Result r;
+    const uint32_t n = g.n;
+    workspace_ensure(ws, g, s);
+    PRG_CUDA(cudaMemsetAsync(ws.hub_ticket, 0, std::max<uint64_t>(g.nhub, 1) * 4, s));
+    const Product pr{&g, &ws};
+    const unsigned grid = ws.cfg[MODE_EIG64].grid;
+    double *x[2] = {alloc<double>(n, s), alloc<double>(n, s)};
+    double4 *recs = alloc<double4>(grid, s), *part = alloc<double4>(kNB, s);
+    State *d_st = alloc<State>(1, s), *h_st = nullptr;
+    PRG_CUDA(cudaMallocHost((void **)&h_st, 2 * sizeof(State)));
+    try {
+        State init;
+        std::memset(&init, 0, sizeof(init));
+        init.max_iter = 5000;
+        init.eps = 1e-14;
+        PRG_CUDA(cudaMemcpyAsync(d_st, &init, sizeof(State), cudaMemcpyHostToDevice, s));
+        fill_kernel<<<kNB, kNT, 0, s>>>(x[0], n, 1.0);
+        PRG_CUDA(cudaGetLastError());
+        run_until_done(d_st, h_st, init.max_iter, s, [&](uint32_t it) {
+            const int q = (int)(it & 1u);
+            product(pr, x[q], x[q ^ 1], 1.0, recs, &d_st->done, s);
+            normalise_kernel<<<kNB, kNT, 0, s>>>(n, recs, grid, ws.hub_rec, g.nhub, x[q ^ 1], x[q], part, d_st);
+            check_kernel<<<1, 256, 0, s>>>(part, kNB, d_st, q ^ 1);
+            PRG_CUDA(cudaGetLastError());
+        });
+        r.iterations = h_st[0].iters;
+        const double *xf = h_st[0].iters ? x[h_st[0].final_buf] : x[0];
+        double *other = xf == x[0] ? x[1] : x[0];
+        r.eigenvalue = rayleigh(pr, xf, other, recs, s);
+        clamp_kernel<<<kNB, kNT, 0, s>>>(const_cast<double *>(xf), n);
+        PRG_CUDA(cudaGetLastError());
+        if (g.perm) gather_f64(d_out, xf, g.iperm, n, s);
+        else PRG_CUDA(cudaMemcpyAsync(d_out, xf, (uint64_t)n * 8, cudaMemcpyDeviceToDevice, s));
+        PRG_CUDA(cudaStreamSynchronize(s));
+    } catch (...) {
+        cudaStreamSynchronize(s);
+        cudaFreeHost(h_st);
+        throw;
+    }
+    cudaFreeHost(h_st);
+    release(x[0], s);
+    release(x[1], s);
+    release(recs, s);
+    release(part, s);
+    release(d_st, s);
+    PRG_CUDA(cudaStreamSynchronize(s));
+    return r;
+}
+
+Result hits_directed(const DeviceGraph &g, Workspace &ws, const DeviceGraph &rev, Workspace &wsr, double *d_hub,
+                     double *d_auth, cudaStream_t s) {
+    Result r;
+    const uint32_t n = g.n;
+    workspace_ensure(ws, g, s);
+    workspace_ensure(wsr, rev, s);
+    PRG_CUDA(cudaMemsetAsync(ws.hub_ticket, 0, std::max<uint64_t>(g.nhub, 1) * 4, s));
+    PRG_CUDA(cudaMemsetAsync(wsr.hub_ticket, 0, std::max<uint64_t>(rev.nhub, 1) * 4, s));
+    const Product pin{&g, &ws};     // A^T h: tmp[v] = sum over in-neighbours u of h[u]
+    const Product pout{&rev, &wsr};  // A tmp: h[u] = sum over out-neighbours v of tmp[v]
+    const unsigned gin = ws.cfg[MODE_EIG64].grid, gout = wsr.cfg[MODE_EIG64].grid;
+    double *h[2] = {alloc<double>(n, s), alloc<double>(n, s)};
+    double *tmp = alloc<double>(n, s);
+    double4 *rin = alloc<double4>(std::max(gin, kNB), s), *rout = alloc<double4>(std::max(gout, kNB), s);
+    double4 *part = alloc<double4>(kNB, s);
+    State *d_st = alloc<State>(1, s), *h_st = nullptr;
+    PRG_CUDA(cudaMallocHost((void **)&h_st, 2 * sizeof(State)));
+    try {
+        State init;
+        std::memset(&init, 0, sizeof(init));
+        init.max_iter = 5000;
+        init.eps = 1e-12;
+        PRG_CUDA(cudaMemcpyAsync(d_st, &init, sizeof(State), cudaMemcpyHostToDevice, s));
+        // h = out-degree / max out-degree (the graph's deg is its out-degree)
+        degree_seed_kernel<<<kNB, kNT, 0, s>>>(g.deg, n, h[0], rout);
+        normalise_kernel<<<kNB, kNT, 0, s>>>(n, rout, kNB, nullptr, 0, h[0], nullptr, part, nullptr);
+        PRG_CUDA(cudaGetLastError());
+        run_until_done(d_st, h_st, init.max_iter, s, [&](uint32_t it) {
+            const int q = (int)(it & 1u);
+            product(pin, h[q], tmp, 0.0, rin, &d_st->done, s);
+            product(pout, tmp, h[q ^ 1], 0.0, rout, &d_st->done, s);
+            normalise_kernel<<<kNB, kNT, 0, s>>>(n, rout, gout, wsr.hub_rec, rev.nhub, h[q ^ 1], h[q], part, d_st);
+            check_kernel<<<1, 256, 0, s>>>(part, kNB, d_st, q ^ 1);
+            PRG_CUDA(cudaGetLastError());
+        });
+        r.iterations = h_st[0].iters;
+        r.eigenvalue = h_st[0].maxv;
+        double *hf = h_st[0].iters ? h[h_st[0].final_buf] : h[0];
+        clamp_kernel<<<kNB, kNT, 0, s>>>(hf, n);
+        // authority = A^T h, rescaled by its max, clamped
+        product(pin, hf, tmp, 0.0, rin, nullptr, s);
+        normalise_kernel<<<kNB, kNT, 0, s>>>(n, rin, gin, ws.hub_rec, g.nhub, tmp, nullptr, part, nullptr);
+        clamp_kernel<<<kNB, kNT, 0, s>>>(tmp, n);
+        PRG_CUDA(cudaGetLastError());
+        PRG_CUDA(cudaMemcpyAsync(d_hub, hf, (uint64_t)n * 8, cudaMemcpyDeviceToDevice, s));
+        PRG_CUDA(cudaMemcpyAsync(d_auth, tmp, (uint64_t)n * 8, cudaMemcpyDeviceToDevice, s));
+        PRG_CUDA(cudaStreamSynchronize(s));
+    } catch (...) {
+        cudaStreamSynchronize(s);
+        cudaFreeHost(h_st);
+        throw;
+    }
+    cudaFreeHost(h_st);
+    release(h[0], s);
+    release(h[1], s);
+    release(tmp, s);
+    release(rin, s);
+    release(rout, s);
+    release(part, s);
+    release(d_st, s);
+    PRG_CUDA(cudaStreamSynchronize(s));
+    return r;
+}
+
+}  // namespace eig
+}  // namespace prg

@@ -109,6 +109,10 @@ template <>
 struct Pre<MODE_KRES64> {
     double old, t;
 };
+template <>
+struct Pre<MODE_EIG64> {
+    double in;
+};
 
 template <int MODE>
 __device__ __forceinline__ Pre<MODE> epi_load(const IterArgs &a, uint32_t v) {
@@ -124,6 +128,8 @@ __device__ __forceinline__ Pre<MODE> epi_load(const IterArgs &a, uint32_t v) {
     } else if constexpr (MODE == MODE_KRES64) {
         p.old = __ldcs(a.x64_in + v);
         p.t = a.t64 ? a.t64[v] : 0.0;
+    } else if constexpr (MODE == MODE_EIG64) {
+        p.in = a.x64_in[v];
     } else if constexpr (MODE == MODE_CORR32) {
         p.old = a.x32_in[v];
         p.b = a.b32[v];
@@ -142,7 +148,13 @@ __device__ __forceinline__ Pre<MODE> epi_load(const IterArgs &a, uint32_t v) {
 template <int MODE>
 __device__ __forceinline__ void epilogue(const IterArgs &a, const Uni &u, uint32_t v, typename ModeT<MODE>::A y,
                                          const Pre<MODE> &p, double &pd, double &pds, double &ps) {
-    if constexpr (kIsKry<MODE>) {
+    if constexpr (MODE == MODE_EIG64) {
+        const double out = a.shift * p.in + y;
+        a.x64_out[v] = out;
+        pd = fmax(pd, fabs(out));
+        pds += p.in * out;
+        ps += p.in * p.in;
+    } else if constexpr (kIsKry<MODE>) {
         // y = p - d*sum - d*dsum_p*t; Uni::dshare holds d*dsum_p
         using A = typename ModeT<MODE>::A;
         const A out = p.in - ((A)u.d * y + (A)u.dshare * p.t);
@@ -324,7 +336,9 @@ __global__ void __launch_bounds__(kThreads, HOT ? (kIs32<MODE> ? 4 : 3) : (kIs32
     __shared__ int s_flag;
 
     Ctl *ctl = a.ctl;
-    if constexpr (kIsKry<MODE>) {
+    if constexpr (MODE == MODE_EIG64) {
+        if (a.kdone && *(volatile const int32_t *)a.kdone) return;
+    } else if constexpr (kIsKry<MODE>) {
         if (*(volatile const int32_t *)a.kdone) return;
     } else if constexpr (MODE != MODE_RESID64 && MODE != MODE_KRES64) {
         if (*(volatile int32_t *)&ctl->done) return;
@@ -354,6 +368,8 @@ __global__ void __launch_bounds__(kThreads, HOT ? (kIs32<MODE> ? 4 : 3) : (kIs32
         u.dsum = s_dz;
         u.tele = 0.0;
         u.dshare = u.d * u.dsum;
+    } else if constexpr (MODE == MODE_EIG64) {
+        u.dsum = u.tele = u.dshare = 0.0;
     } else {
         u.dsum = *(volatile double *)&ctl->dsum[a.parity];
         const double nf = (double)a.n;
@@ -435,6 +451,22 @@ __global__ void __launch_bounds__(kThreads, HOT ? (kIs32<MODE> ? 4 : 3) : (kIs32
 
     // ---- deterministic reduction of (diff, dangling, sum): block tree, then
     // the last block adds block and hub records in index order
+    if constexpr (MODE == MODE_EIG64) {
+        // (max |y|, x.y, x.x): a max tree for the first, sums for the others
+        double mx = pd;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+        double z = 0.0;
+        block_sum3(z, pds, ps, s_red);
+        __syncthreads();
+        if (lane == 0) s_red[warp] = mx;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            for (int w = 1; w < kW; w++) mx = fmax(mx, s_red[w]);
+            a.kpart_out[blockIdx.x] = make_double4(mx, pds, ps, 0.0);
+        }
+        return;
+    }
     block_sum3(pd, pds, ps, s_red);
     if constexpr (kIsKry<MODE>) {
         // the consumer adds block and hub records itself
@@ -538,6 +570,7 @@ LaunchCfg iteration_config(int mode, bool weighted, uint32_t hot_entries, uint32
         case MODE_CORR32: mode_config<MODE_CORR32>(weighted, hot_entries, blocks_per_sm, n, c); break;
         case MODE_KRY32: mode_config<MODE_KRY32>(weighted, hot_entries, blocks_per_sm, n, c); break;
         case MODE_KRY64: mode_config<MODE_KRY64>(weighted, hot_entries, blocks_per_sm, n, c); break;
+        case MODE_EIG64: mode_config<MODE_EIG64>(weighted, hot_entries, blocks_per_sm, n, c); break;
         default: mode_config<MODE_KRES64>(weighted, hot_entries, blocks_per_sm, n, c); break;
     }
     return c;
@@ -567,6 +600,7 @@ void launch_iteration(int mode, bool weighted, const IterArgs &a_in, const Launc
         case MODE_KRY32: mode_launch<MODE_KRY32>(weighted, a, c, s); break;
         case MODE_KRY64: mode_launch<MODE_KRY64>(weighted, a, c, s); break;
         case MODE_KRES64: mode_launch<MODE_KRES64>(weighted, a, c, s); break;
+        case MODE_EIG64: mode_launch<MODE_EIG64>(weighted, a, c, s); break;
         default: break;
     }
     PRG_CUDA(cudaGetLastError());

@@ -29,8 +29,12 @@ enum IterMode : int {
     // FP64 residual pass of the Krylov solvers: g = G(x) and r = g - x
     // (written FP32 to b32_out or FP64 to b64_out), ||r||_1 and sum(g)
     MODE_KRES64 = 6,
+    // adjacency product for eigenvector centrality / HITS:
+    //   y = shift * x + A x  (plain sums of gathered x, no degree scaling)
+    // with per-block records (max |y|, x.y, x.x)
+    MODE_EIG64 = 7,
 };
-constexpr int kModes = 7;
+constexpr int kModes = 8;
 
 struct IterArgs {
     // graph
@@ -66,7 +70,8 @@ struct IterArgs {
     const double4 *kpart_in;  // producer's per-block records; .x summed = dangling mass of p
     uint32_t kpart_n;
     double4 *kpart_out;       // per-block (rh.y, y.p, y.y)
-    const int32_t *kdone;     // nonzero: the Krylov solve has stopped, return at once
+    const int32_t *kdone;     // nonzero: the Krylov solve has stopped, return at once (may be null for EIG64)
+    double shift;             // MODE_EIG64: weight of the diagonal term
     // scalars
     double damping;
     double inv_n;

@@ -71,9 +71,13 @@ class IoError(IgraphError):
     """IgraphError::Io."""
 
 
+class Unsupported(IgraphError):
+    """IgraphError::Unsupported."""
+
+
 PRG_OK = 0
 _ERRORS = {1: InvalidArgument, 2: VertexOutOfRange, 3: Internal, 4: Internal, 5: Internal, 6: DidNotConverge,
-           7: DeviceTimeout, 9: IoError}
+           7: DeviceTimeout, 9: IoError, 10: Unsupported}
 
 # ------------------------------------------------------------------ library
 
@@ -188,6 +192,12 @@ def lib():
     L.prg_rmat_device.restype = C.c_int32
     L.prg_rmat_device.argtypes = [C.c_uint32, C.c_uint64, C.c_double, C.c_double, C.c_double, C.c_uint64,
                                   vp, vp, vp]
+    L.prg_eigenvector_centrality.restype = C.c_int32
+    L.prg_eigenvector_centrality.argtypes = [C.c_uint32, C.c_uint64, u32p, u32p, C.c_int32, f64p,
+                                             C.POINTER(C.c_double)]
+    L.prg_hub_and_authority_scores.restype = C.c_int32
+    L.prg_hub_and_authority_scores.argtypes = [C.c_uint32, C.c_uint64, u32p, u32p, C.c_int32, f64p, f64p,
+                                               C.POINTER(C.c_double)]
     L.prg_parse_edgelist.restype = C.c_int32
     L.prg_parse_edgelist.argtypes = [C.c_char_p, C.c_uint64, vp, vp, C.c_uint64, C.POINTER(C.c_uint64),
                                      C.POINTER(C.c_uint32), C.POINTER(C.c_uint64)]
@@ -316,6 +326,38 @@ def pagerank_linsys(graph: Graph) -> np.ndarray:
     out = np.empty(max(n, 1), np.float64)
     _check(lib().prg_pagerank_linsys(n, len(f), _ptr(f), _ptr(t), int(graph.is_directed()), _ptr(out)))
     return out[:n]
+
+
+def eigenvector_centrality(graph: Graph, with_eigenvalue: bool = False):
+    """rust-igraph ``eigenvector_centrality`` (eigenvector.rs:118-125, 286-372),
+    undirected and unweighted, on the GPU.  with_eigenvalue: also return the
+    Rayleigh quotient."""
+    n = graph.vcount()
+    f, t = graph.edge_arrays()
+    out = np.empty(max(n, 1), np.float64)
+    lam = C.c_double()
+    _check(lib().prg_eigenvector_centrality(n, len(f), _ptr(f), _ptr(t), int(graph.is_directed()), _ptr(out),
+                                            C.byref(lam)))
+    return (out[:n], lam.value) if with_eigenvalue else out[:n]
+
+
+@dataclass
+class HitsScores:
+    hub: np.ndarray
+    authority: np.ndarray
+    eigenvalue: float
+
+
+def hub_and_authority_scores(graph: Graph) -> HitsScores:
+    """rust-igraph ``hub_and_authority_scores`` (hits.rs:122-230), unweighted, on the GPU."""
+    n = graph.vcount()
+    f, t = graph.edge_arrays()
+    hub = np.empty(max(n, 1), np.float64)
+    auth = np.empty(max(n, 1), np.float64)
+    lam = C.c_double()
+    _check(lib().prg_hub_and_authority_scores(n, len(f), _ptr(f), _ptr(t), int(graph.is_directed()), _ptr(hub),
+                                              _ptr(auth), C.byref(lam)))
+    return HitsScores(hub[:n], auth[:n], lam.value)
 
 
 def parse_edgelist(data: bytes):

@@ -1,0 +1,49 @@
+"""The CPU restatements of eigenvector_centrality and hub_and_authority_scores
+(unweighted; oracle/prg_oracle.c) pinned to the reference's own unit tests
+(src/algorithms/properties/eigenvector.rs:770-829, hits.rs:627-760)."""
+import numpy as np
+
+import oracle as O
+
+
+def E(pairs):
+    a = np.array(pairs, np.uint32).reshape(-1, 2)
+    return a[:, 0].copy(), a[:, 1].copy()
+
+
+def test_eigenvector_reference_cases():
+    assert len(O.eigenvector_centrality(0, *E([]))[0]) == 0
+    assert list(O.eigenvector_centrality(1, *E([]))[0]) == [1.0]
+    assert np.allclose(O.eigenvector_centrality(3, *E([]))[0], 1.0, atol=1e-9)
+    assert np.allclose(O.eigenvector_centrality(3, *E([(0, 1), (1, 2), (2, 0)]))[0], 1.0, atol=1e-9)
+    x, lam, _ = O.eigenvector_centrality(4, *E([(0, 1), (0, 2), (0, 3)]))
+    assert np.allclose(x, [1.0] + [1 / np.sqrt(3)] * 3, atol=1e-9)
+    assert abs(lam - np.sqrt(3)) < 1e-9
+    k4 = [(u, v) for u in range(4) for v in range(u + 1, 4)]
+    assert np.allclose(O.eigenvector_centrality(4, *E(k4))[0], 1.0, atol=1e-9)
+
+
+def test_hits_reference_cases():
+    h, a, lam, _ = O.hub_and_authority_scores(3, *E([]), True)
+    assert np.all(h == 1.0) and np.all(a == 1.0) and lam == 0.0
+    h, a, lam, _ = O.hub_and_authority_scores(2, *E([(0, 1)]), True)
+    assert abs(lam - 1.0) < 1e-6
+    h, a, lam, _ = O.hub_and_authority_scores(4, *E([(0, 2), (0, 3), (1, 2), (1, 3)]), True)
+    assert np.allclose(h, [1, 1, 0, 0], atol=1e-9) and np.allclose(a, [0, 0, 1, 1], atol=1e-9)
+    assert abs(lam - 4.0) < 1e-6
+    h, a, lam, _ = O.hub_and_authority_scores(3, *E([(0, 1), (1, 2), (2, 0)]), True)
+    assert np.allclose(h, 1.0, atol=1e-9) and abs(lam - 1.0) < 1e-6
+    h, a, _, _ = O.hub_and_authority_scores(3, *E([(0, 2), (1, 2)]), True)  # sink
+    assert abs(h[2]) < 1e-9 and abs(a[2] - 1) < 1e-9 and abs(a[0]) < 1e-9 and abs(a[1]) < 1e-9
+    h, a, _, _ = O.hub_and_authority_scores(3, *E([(0, 1), (0, 2)]), True)  # source
+    assert abs(a[0]) < 1e-9 and abs(h[0] - 1) < 1e-9
+    # undirected: hub = authority = eigenvector centrality, eigenvalue = lambda^2
+    ec, lam1, _ = O.eigenvector_centrality(4, *E([(0, 1), (0, 2), (0, 3)]))
+    h, a, lam, _ = O.hub_and_authority_scores(4, *E([(0, 1), (0, 2), (0, 3)]), False)
+    assert np.array_equal(h, ec) and np.array_equal(a, ec) and abs(lam - lam1 ** 2) < 1e-12
+    # h proportional to A a after convergence (hits.rs doc example)
+    f, t = E([(0, 1), (0, 3), (1, 2), (1, 3), (2, 0), (2, 4), (3, 2), (4, 0), (4, 1)])
+    h, a, _, _ = O.hub_and_authority_scores(5, f, t, True)
+    ha = np.zeros(5)
+    np.add.at(ha, f, a[t])
+    assert np.allclose(ha / ha.max(), h, atol=1e-6)
