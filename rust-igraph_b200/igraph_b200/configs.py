@@ -237,6 +237,33 @@ def config6(peak):
                           **res}), flush=True)
 
 
+def config7(peak):
+    # eigenvector centrality (undirected) and HITS (directed) on R-MAT graphs
+    import time
+
+    import torch
+
+    from . import Graph, eigenvector_centrality, hub_and_authority_scores
+
+    for scale in (16, 20, 22):
+        n, m = 1 << scale, 16 << scale
+        df = torch.empty(m, dtype=torch.int32, device="cuda")
+        dt = torch.empty(m, dtype=torch.int32, device="cuda")
+        generate_device(GEN_RMAT, n, m, df.data_ptr(), dt.data_ptr(), 0.57, 0.19, 0.19, seed=7)
+        f = df.cpu().numpy().view(np.uint32).copy()
+        t = dt.cpu().numpy().view(np.uint32).copy()
+        del df, dt
+        for name, directed, fn in (("eigenvector_centrality (undirected)", False, eigenvector_centrality),
+                                   ("hub_and_authority_scores (directed)", True, hub_and_authority_scores)):
+            g = Graph.from_edge_arrays(n, f, t, directed)
+            fn(g)
+            t0 = time.perf_counter()
+            fn(g)
+            dt_s = time.perf_counter() - t0
+            print(json.dumps({"config": f"7 {name} R-MAT s{scale}", "n": n, "m": m,
+                              "seconds_incl_upload_and_build": round(dt_s, 4)}), flush=True)
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--which", default="1,2,3,4,5,6")
@@ -244,7 +271,8 @@ def main(argv=None):
     a = ap.parse_args(argv)
     peak = _peak(a.peak_gbs)
     for k in a.which.split(","):
-        {"1": config1, "2": config2, "3": config3, "4": config4, "5": config5, "6": config6}[k.strip()](peak)
+        {"1": config1, "2": config2, "3": config3, "4": config4, "5": config5, "6": config6,
+         "7": config7}[k.strip()](peak)
 
 
 if __name__ == "__main__":
