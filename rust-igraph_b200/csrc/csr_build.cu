@@ -327,16 +327,38 @@ __global__ void make_arcs(const uint32_t *from, const uint32_t *to, uint64_t m, 
     }
 }
 
-__global__ void histogram_u32(const uint32_t *key, uint64_t N, uint32_t *hist) {
-    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < N; i += (uint64_t)gridDim.x * blockDim.x)
-        atomicAdd(&hist[key[i]], 1u);
+// Out-degree by atomics.  Degree-heavy vertices usually have small ids (the
+// generators, and any degree-sorted numbering, put them there); their counts
+// are first gathered in a per-block shared-memory histogram so thousands of
+// updates to one hub do not serialise on a single L2 address.
+constexpr uint32_t kDegBins = 12288;
+constexpr int kDegThreads = 1024;
+
+__global__ void __launch_bounds__(kDegThreads) out_degree_kernel(const uint32_t *from, const uint32_t *to, uint64_t m,
+                                                                 bool directed, uint32_t n, uint32_t *deg) {
+    __shared__ uint32_t bins[kDegBins];
+    for (uint32_t i = threadIdx.x; i < kDegBins; i += kDegThreads) bins[i] = 0u;
+    __syncthreads();
+    auto add = [&](uint32_t v) {
+        if (v < kDegBins) atomicAdd_block(&bins[v], 1u);
+        else atomicAdd(&deg[v], 1u);
+    };
+    for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e < m; e += (uint64_t)gridDim.x * blockDim.x) {
+        add(from[e]);
+        if (!directed) add(to[e]);
+    }
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < kDegBins && i < n; i += kDegThreads)
+        if (bins[i]) atomicAdd(&deg[i], bins[i]);
 }
 
-__global__ void out_degree_kernel(const uint32_t *from, const uint32_t *to, uint64_t m, bool directed,
-                                  uint32_t *deg) {
-    for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e < m; e += (uint64_t)gridDim.x * blockDim.x) {
-        atomicAdd(&deg[from[e]], 1u);
-        if (!directed) atomicAdd(&deg[to[e]], 1u);
+// row_ptr of a CSR from its sorted row keys: rows (key[i-1], key[i]] start at
+// arc i (every entry of row_ptr[0..n] is written exactly once).
+__global__ void row_ptr_from_sorted(const uint32_t *key, uint64_t N, uint32_t n, uint32_t *row_ptr) {
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i <= N; i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t lo = i == 0 ? 0 : (uint64_t)key[i - 1] + 1;
+        const uint64_t hi = i == N ? n : key[i];
+        for (uint64_t r = lo; r <= hi; r++) row_ptr[r] = (uint32_t)i;
     }
 }
 
@@ -517,7 +539,7 @@ void build_graph(DeviceGraph &g, const uint32_t *d_from, const uint32_t *d_to, c
     // out-degree (unweighted divisor; also kept for weighted graphs)
     PRG_CUDA(cudaMallocAsync((void **)&g.deg, std::max<uint64_t>(n, 1) * 4, s));
     PRG_CUDA(cudaMemsetAsync(g.deg, 0, std::max<uint64_t>(n, 1) * 4, s));
-    if (m) out_degree_kernel<<<ge, kThreads, 0, s>>>(d_from, d_to, m, directed, g.deg);
+    if (m) out_degree_kernel<<<148 * 2, kDegThreads, 0, s>>>(d_from, d_to, m, directed, n, g.deg);
 
     // optional degree-sorted relabelling (internal ids); the edge list the CSR
     // is built from becomes (ef, et)
@@ -561,15 +583,12 @@ void build_graph(DeviceGraph &g, const uint32_t *d_from, const uint32_t *d_to, c
     uint32_t *k1 = dalloc<uint32_t>(arcs, s), *v1 = dalloc<uint32_t>(arcs, s);
     if (m) make_arcs<<<ge, kThreads, 0, s>>>(ef, et, m, directed, weighted, k0, v0);
 
-    // row_ptr from the in-degree histogram
-    uint32_t *indeg = dalloc<uint32_t>(n + 1, s);
-    PRG_CUDA(cudaMemsetAsync(indeg, 0, (uint64_t)(n + 1) * 4, s));
-    if (arcs) histogram_u32<<<ga, kThreads, 0, s>>>(k0, arcs, indeg);
-    PRG_CUDA(cudaMallocAsync((void **)&g.row_ptr, (uint64_t)(n + 1) * 4, s));
-    exclusive_scan_u32(indeg, g.row_ptr, n, s);
-    dfree(indeg, s);
-
     radix_sort_pairs(&k0, &v0, &k1, &v1, arcs, bits_for(n ? n - 1 : 0), s);
+
+    // row_ptr from the boundaries of the sorted destinations
+    PRG_CUDA(cudaMallocAsync((void **)&g.row_ptr, (uint64_t)(n + 1) * 4, s));
+    row_ptr_from_sorted<<<grid_for(arcs + 1, kThreads), kThreads, 0, s>>>(k0, arcs, n, g.row_ptr);
+    PRG_CUDA(cudaGetLastError());
 
     const uint64_t padded = arcs + kColPad;
     PRG_CUDA(cudaMallocAsync((void **)&g.col, padded * 4, s));
@@ -592,22 +611,19 @@ void build_graph(DeviceGraph &g, const uint32_t *d_from, const uint32_t *d_to, c
             // directed: group edge ids by source with a second stable sort
             uint32_t *sk = dalloc<uint32_t>(m, s), *sv = dalloc<uint32_t>(m, s);
             uint32_t *sk1 = dalloc<uint32_t>(m, s), *sv1 = dalloc<uint32_t>(m, s);
-            uint32_t *optr = dalloc<uint32_t>(n + 1, s), *oh = dalloc<uint32_t>(n + 1, s);
+            uint32_t *optr = dalloc<uint32_t>(n + 1, s);
             if (m) {
                 PRG_CUDA(cudaMemcpyAsync(sk, ef, m * 4, cudaMemcpyDeviceToDevice, s));
                 make_arcs<<<ge, kThreads, 0, s>>>(ef, et, m, true, true, sk1, sv);  // sv = edge ids
             }
-            PRG_CUDA(cudaMemsetAsync(oh, 0, (uint64_t)(n + 1) * 4, s));
-            if (m) histogram_u32<<<ge, kThreads, 0, s>>>(sk, m, oh);
-            exclusive_scan_u32(oh, optr, n, s);
             radix_sort_pairs(&sk, &sv, &sk1, &sv1, m, bits_for(n ? n - 1 : 0), s);
+            row_ptr_from_sorted<<<grid_for(m + 1, kThreads), kThreads, 0, s>>>(sk, m, n, optr);
             row_weight_sums<<<grid_for((uint64_t)n * 32, kThreads), kThreads, 0, s>>>(optr, d_w, sv, n, strength);
             dfree(sk, s);
             dfree(sv, s);
             dfree(sk1, s);
             dfree(sv1, s);
             dfree(optr, s);
-            dfree(oh, s);
         }
     }
     dfree(k0, s);
