@@ -133,6 +133,22 @@ int32_t prg_eigenvector_centrality(uint32_t n, uint64_t m, const uint32_t *from,
 int32_t prg_hub_and_authority_scores(uint32_t n, uint64_t m, const uint32_t *from, const uint32_t *to,
                                      int32_t directed, double *hub, double *authority, double *eigenvalue);
 
+/* rust-igraph eigenvector_centrality_weighted() (eigenvector.rs:157-168, 375-538):
+ * undirected, weights[e] per edge (weights_len must equal m); shifted power
+ * iteration x' = (W + I) x from the vertex strengths, L1 stop 1e-12.
+ * Negative weights (which the reference follows with a signed pivot) give
+ * PRG_ERR_UNSUPPORTED on this GPU path. */
+int32_t prg_eigenvector_centrality_weighted(uint32_t n, uint64_t m, const uint32_t *from, const uint32_t *to,
+                                            int32_t directed, const double *weights, uint64_t weights_len,
+                                            double *out, double *eigenvalue);
+
+/* rust-igraph hub_and_authority_scores_weighted() (hits.rs:245-585), non-negative
+ * weights: W W^T power iteration from the out-strengths (directed) or the
+ * weighted eigenvector centrality with the squared eigenvalue (undirected). */
+int32_t prg_hub_and_authority_scores_weighted(uint32_t n, uint64_t m, const uint32_t *from, const uint32_t *to,
+                                              int32_t directed, const double *weights, uint64_t weights_len,
+                                              double *hub, double *authority, double *eigenvalue);
+
 /* rust-igraph pagerank_weighted() (pagerank_weighted.rs:52-161).
  * weights_len is the caller's slice length (checked against m like :62-68). */
 int32_t prg_pagerank_weighted(uint32_t n, uint64_t m, const uint32_t *from, const uint32_t *to,

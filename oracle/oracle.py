@@ -70,6 +70,12 @@ def lib():
         L.or_eigenvector_centrality.argtypes = [C.c_uint32, C.c_uint64, _u32p, _u32p, _f64p, C.POINTER(C.c_double)]
         L.or_hits.restype = C.c_int
         L.or_hits.argtypes = [C.c_uint32, C.c_uint64, _u32p, _u32p, C.c_int, _f64p, _f64p, C.POINTER(C.c_double)]
+        L.or_eigenvector_weighted.restype = C.c_int
+        L.or_eigenvector_weighted.argtypes = [C.c_uint32, C.c_uint64, _u32p, _u32p, _f64p, _f64p,
+                                              C.POINTER(C.c_double)]
+        L.or_hits_weighted.restype = C.c_int
+        L.or_hits_weighted.argtypes = [C.c_uint32, C.c_uint64, _u32p, _u32p, _f64p, C.c_int, _f64p, _f64p,
+                                       C.POINTER(C.c_double)]
         L.or_adj_build.restype = C.c_void_p
         L.or_adj_build.argtypes = [C.c_uint32, C.c_uint64, _u32p, _u32p, C.c_int]
         L.or_adj_free.restype = None
@@ -197,6 +203,30 @@ def hub_and_authority_scores(n, frm, to, directed):
     auth = np.zeros(max(n, 1), np.float64)
     lam = C.c_double(0.0)
     it = lib().or_hits(n, len(f), f, t, int(directed), hub, auth, C.byref(lam))
+    return hub[:n], auth[:n], lam.value, it
+
+
+def eigenvector_centrality_weighted(n, frm, to, weights):
+    """rust-igraph eigenvector_centrality_weighted, non-negative weights
+    (eigenvector.rs:375-538): (vector, eigenvalue, iterations)."""
+    f, t = _edges(frm, to)
+    w = np.ascontiguousarray(weights, dtype=np.float64)
+    out = np.zeros(max(n, 1), np.float64)
+    lam = C.c_double(0.0)
+    it = lib().or_eigenvector_weighted(n, len(f), f, t, w if len(w) else np.zeros(1), out, C.byref(lam))
+    return out[:n], lam.value, it
+
+
+def hub_and_authority_scores_weighted(n, frm, to, weights, directed):
+    """rust-igraph hub_and_authority_scores_weighted, non-negative weights
+    (hits.rs:245-470): (hub, authority, eigenvalue, iterations)."""
+    f, t = _edges(frm, to)
+    w = np.ascontiguousarray(weights, dtype=np.float64)
+    hub = np.zeros(max(n, 1), np.float64)
+    auth = np.zeros(max(n, 1), np.float64)
+    lam = C.c_double(0.0)
+    it = lib().or_hits_weighted(n, len(f), f, t, w if len(w) else np.zeros(1), int(directed), hub, auth,
+                                C.byref(lam))
     return hub[:n], auth[:n], lam.value, it
 
 

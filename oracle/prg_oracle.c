@@ -921,3 +921,168 @@ int or_hits(uint32_t n, uint64_t m, const uint32_t *from, const uint32_t *to, in
     free(orp); free(irp); free(ocol); free(icol); free(h); free(hn); free(tmp);
     return it;
 }
+
+/* ---- weighted variants: incident-edge lists in the reference's order ----
+ * Undirected incident(v) = the out-range (edges with from == v, sorted by
+ * to) followed by the in-range (edges with to == v, sorted by from); a loop
+ * is in both (graph.rs:1212-1225).  Directed: out-range / in-range only.
+ * Ties (parallel edges) keep edge-id order. */
+
+typedef struct { uint32_t key, other, e; } kev;
+static int cmp_kev(const void *a, const void *b) {
+    const kev *x = (const kev *)a, *y = (const kev *)b;
+    if (x->key != y->key) return x->key < y->key ? -1 : 1;
+    if (x->other != y->other) return x->other < y->other ? -1 : 1;
+    return x->e < y->e ? -1 : x->e > y->e;
+}
+
+/* rows of (other endpoint, edge) pairs grouped by key, sorted by other */
+static void edge_rows(uint32_t n, uint64_t m, const uint32_t *key, const uint32_t *other, uint64_t **rp_out,
+                      uint32_t **oth_out, uint32_t **eid_out) {
+    kev *t = (kev *)malloc((m ? m : 1) * sizeof(kev));
+    for (uint64_t e = 0; e < m; e++) t[e] = (kev){key[e], other[e], (uint32_t)e};
+    qsort(t, m, sizeof(kev), cmp_kev);
+    uint64_t *rp = (uint64_t *)calloc((size_t)n + 1, sizeof(uint64_t));
+    uint32_t *oth = (uint32_t *)malloc((m ? m : 1) * sizeof(uint32_t)), *eid = (uint32_t *)malloc((m ? m : 1) * 4);
+    for (uint64_t i = 0; i < m; i++) {
+        rp[t[i].key + 1]++;
+        oth[i] = t[i].other;
+        eid[i] = t[i].e;
+    }
+    for (uint32_t v = 0; v < n; v++) rp[v + 1] += rp[v];
+    free(t);
+    *rp_out = rp;
+    *oth_out = oth;
+    *eid_out = eid;
+}
+
+/* (W + I) x over undirected incidence: out-range then in-range of v */
+static double winc(uint32_t v, const uint64_t *orp, const uint32_t *ooth, const uint32_t *oeid, const uint64_t *irp,
+                   const uint32_t *ioth, const uint32_t *ieid, const double *w, const double *x) {
+    double s = 0.0;
+    for (uint64_t p = orp[v]; p < orp[v + 1]; p++) s += w[oeid[p]] * x[ooth[p]];
+    for (uint64_t p = irp[v]; p < irp[v + 1]; p++) s += w[ieid[p]] * x[ioth[p]];
+    return s;
+}
+
+/* Weighted undirected shifted power iteration with a strength seed
+ * (eigenvector.rs:375-538 = hits.rs:470-553 for non-negative weights):
+ * returns iterations; eps 1e-12, 5000 iterations; *eigval = x.Wx / x.x. */
+int or_eigenvector_weighted(uint32_t n, uint64_t m, const uint32_t *from, const uint32_t *to, const double *w,
+                            double *out, double *eigval) {
+    if (eigval) *eigval = 0.0;
+    if (n == 0) return 0;
+    int allzero = 1;
+    for (uint64_t e = 0; e < m; e++) allzero &= w[e] == 0.0;
+    if (m == 0 || allzero) {
+        for (uint32_t i = 0; i < n; i++) out[i] = 1.0;
+        return 0;
+    }
+    uint64_t *orp, *irp;
+    uint32_t *ooth, *oeid, *ioth, *ieid;
+    edge_rows(n, m, from, to, &orp, &ooth, &oeid);
+    edge_rows(n, m, to, from, &irp, &ioth, &ieid);
+    double *x = (double *)malloc(n * sizeof(double)), *xn = (double *)malloc(n * sizeof(double));
+    int any = 0;
+    for (uint32_t v = 0; v < n; v++) {
+        double s = 0.0;
+        for (uint64_t p = orp[v]; p < orp[v + 1]; p++) s += w[oeid[p]];
+        for (uint64_t p = irp[v]; p < irp[v + 1]; p++) s += w[ieid[p]];
+        x[v] = s != 0.0 ? fabs(s) : 0.0;
+        any |= x[v] != 0.0;
+    }
+    if (!any)
+        for (uint32_t v = 0; v < n; v++) x[v] = 1.0;
+    rescale_max_abs(x, n);
+    int it = 0;
+    for (; it < 5000;) {
+        it++;
+        for (uint32_t v = 0; v < n; v++) xn[v] = x[v] + winc(v, orp, ooth, oeid, irp, ioth, ieid, w, x);
+        rescale_max_abs(xn, n);
+        double diff = 0.0;
+        for (uint32_t v = 0; v < n; v++) diff += fabs(xn[v] - x[v]);
+        double *t = x; x = xn; xn = t;
+        if (diff < 1e-12) break;
+    }
+    double num = 0.0, den = 0.0;
+    for (uint32_t v = 0; v < n; v++) {
+        num += x[v] * winc(v, orp, ooth, oeid, irp, ioth, ieid, w, x);
+        den += x[v] * x[v];
+    }
+    if (eigval) *eigval = den > 0.0 ? num / den : 0.0;
+    rescale_max_abs(x, n);
+    for (uint32_t v = 0; v < n; v++) out[v] = x[v] < 0.0 ? 0.0 : x[v];
+    free(orp); free(irp); free(ooth); free(oeid); free(ioth); free(ieid); free(x); free(xn);
+    return it;
+}
+
+/* hub_and_authority_scores_weighted, non-negative weights (hits.rs:245-470):
+ * directed: h = out-strength, tmp = W^T h, h' = W tmp, eigenvalue max|h'|,
+ * eps 1e-12; authority = W^T h rescaled; undirected: the weighted
+ * eigenvector and (x.Wx/x.x)^2. */
+int or_hits_weighted(uint32_t n, uint64_t m, const uint32_t *from, const uint32_t *to, const double *w, int directed,
+                     double *hub, double *auth, double *eigval) {
+    if (eigval) *eigval = 0.0;
+    if (n == 0) return 0;
+    int allzero = 1;
+    for (uint64_t e = 0; e < m; e++) allzero &= w[e] == 0.0;
+    if (m == 0 || allzero) {
+        for (uint32_t i = 0; i < n; i++) hub[i] = auth[i] = 1.0;
+        return 0;
+    }
+    if (!directed) {
+        double lam = 0.0;
+        int it = or_eigenvector_weighted(n, m, from, to, w, hub, &lam);
+        memcpy(auth, hub, n * sizeof(double));
+        if (eigval) *eigval = lam * lam;
+        return it;
+    }
+    uint64_t *orp, *irp;
+    uint32_t *ooth, *oeid, *ioth, *ieid;
+    edge_rows(n, m, from, to, &orp, &ooth, &oeid);  /* out_inc[u]: targets */
+    edge_rows(n, m, to, from, &irp, &ioth, &ieid);  /* in_inc[v]: sources */
+    double *h = (double *)malloc(n * sizeof(double)), *hn = (double *)malloc(n * sizeof(double));
+    double *tmp = (double *)malloc(n * sizeof(double));
+    for (uint32_t u = 0; u < n; u++) {
+        double s = 0.0;
+        for (uint64_t p = orp[u]; p < orp[u + 1]; p++) s += w[oeid[p]];
+        h[u] = s;
+    }
+    rescale_max_abs(h, n);
+    double lam = 0.0;
+    int it = 0;
+    for (; it < 5000;) {
+        it++;
+        for (uint32_t v = 0; v < n; v++) {
+            double s = 0.0;
+            for (uint64_t p = irp[v]; p < irp[v + 1]; p++) s += w[ieid[p]] * h[ioth[p]];
+            tmp[v] = s;
+        }
+        for (uint32_t u = 0; u < n; u++) {
+            double s = 0.0;
+            for (uint64_t p = orp[u]; p < orp[u + 1]; p++) s += w[oeid[p]] * tmp[ooth[p]];
+            hn[u] = s;
+        }
+        double mx = 0.0;
+        for (uint32_t u = 0; u < n; u++) mx = fmax(mx, fabs(hn[u]));
+        if (mx != 0.0) {
+            lam = mx;
+            for (uint32_t u = 0; u < n; u++) hn[u] /= mx;
+        }
+        double diff = 0.0;
+        for (uint32_t u = 0; u < n; u++) diff += fabs(hn[u] - h[u]);
+        double *t = h; h = hn; hn = t;
+        if (diff < 1e-12) break;
+    }
+    for (uint32_t u = 0; u < n; u++) hub[u] = h[u] < 0.0 ? 0.0 : h[u];
+    for (uint32_t v = 0; v < n; v++) {
+        double s = 0.0;
+        for (uint64_t p = irp[v]; p < irp[v + 1]; p++) s += w[ieid[p]] * hub[ioth[p]];
+        auth[v] = s;
+    }
+    rescale_max_abs(auth, n);
+    for (uint32_t v = 0; v < n; v++) if (auth[v] < 0.0) auth[v] = 0.0;
+    if (eigval) *eigval = lam;
+    free(orp); free(irp); free(ooth); free(oeid); free(ioth); free(ieid); free(h); free(hn); free(tmp);
+    return it;
+}

@@ -438,6 +438,125 @@ int32_t prg_hub_and_authority_scores(uint32_t n, uint64_t m, const uint32_t *fro
     PRG_GUARD_END
 }
 
+// Weighted variants: non-negative weights only (a signed pivot would be
+// needed otherwise); the checks come in the reference's order.
+static bool any_negative(const double *w, uint64_t m) {
+    for (uint64_t e = 0; e < m; e++)
+        if (w[e] < 0.0) return true;
+    return false;
+}
+static bool all_zero(const double *w, uint64_t m) {
+    for (uint64_t e = 0; e < m; e++)
+        if (w[e] != 0.0) return false;
+    return true;
+}
+
+int32_t prg_eigenvector_centrality_weighted(uint32_t n, uint64_t m, const uint32_t *from, const uint32_t *to,
+                                            int32_t directed, const double *weights, uint64_t weights_len,
+                                            double *out, double *eigenvalue) {
+    g_err.clear();
+    PRG_GUARD_BEGIN
+    if (eigenvalue) *eigenvalue = 0.0;
+    if (directed)  // eigenvector.rs:157-168
+        return fail(PRG_ERR_UNSUPPORTED, "directed eigenvector_centrality_weighted \xe2\x80\x94 use "
+                                         "eigenvector_centrality_directed_weighted");
+    if (weights_len != m)  // eigenvector.rs:272-283
+        return fail(PRG_ERR_INVALID_ARGUMENT, "weights vector length (" + std::to_string(weights_len) +
+                                                  ") not equal to number of edges (" + std::to_string(m) + ")");
+    if (n == 0) return PRG_OK;
+    if (m == 0 || all_zero(weights, m) || n == 1) {  // eigenvector.rs:379-405
+        for (uint32_t i = 0; i < n; i++) out[i] = 1.0;
+        return PRG_OK;
+    }
+    if (any_negative(weights, m))
+        return fail(PRG_ERR_UNSUPPORTED, "negative weights are not supported by the GPU eigenvector centrality");
+    prg_graph *h = nullptr;
+    int32_t rc = create_from_host(n, m, from, to, weights, 0, &h);
+    if (rc != PRG_OK) return rc;
+    try {
+        cudaStream_t s = h->stream;
+        if (!h->d_out) PRG_CUDA(cudaMallocAsync((void **)&h->d_out, (uint64_t)n * 8, s));
+        const prg::eig::Result r = prg::eig::eigenvector_centrality(h->g, h->ws, h->d_out, s, true, 1e-12);
+        PRG_CUDA(cudaMemcpyAsync(out, h->d_out, (uint64_t)n * 8, cudaMemcpyDeviceToHost, s));
+        PRG_CUDA(cudaStreamSynchronize(s));
+        if (eigenvalue) *eigenvalue = r.eigenvalue;
+    } catch (...) {
+        destroy(h);
+        throw;
+    }
+    destroy(h);
+    return PRG_OK;
+    PRG_GUARD_END
+}
+
+int32_t prg_hub_and_authority_scores_weighted(uint32_t n, uint64_t m, const uint32_t *from, const uint32_t *to,
+                                              int32_t directed, const double *weights, uint64_t weights_len,
+                                              double *hub, double *authority, double *eigenvalue) {
+    g_err.clear();
+    PRG_GUARD_BEGIN
+    if (eigenvalue) *eigenvalue = 0.0;
+    if (weights_len != m)  // hits.rs:294-300
+        return fail(PRG_ERR_INVALID_ARGUMENT, "weights length " + std::to_string(weights_len) +
+                                                  " does not match edge count " + std::to_string(m));
+    if (n == 0) return PRG_OK;
+    if (m == 0 || all_zero(weights, m)) {  // hits.rs:310-332
+        for (uint32_t i = 0; i < n; i++) hub[i] = authority[i] = 1.0;
+        return PRG_OK;
+    }
+    if (any_negative(weights, m))
+        return fail(PRG_ERR_UNSUPPORTED, "negative weights are not supported by the GPU hub and authority scores");
+    if (!directed) {
+        // hits.rs:334-341: weighted eigenvector centrality, eigenvalue (x.Wx / x.x)^2
+        prg_graph *h = nullptr;
+        int32_t rc = create_from_host(n, m, from, to, weights, 0, &h);
+        if (rc != PRG_OK) return rc;
+        try {
+            cudaStream_t s = h->stream;
+            if (!h->d_out) PRG_CUDA(cudaMallocAsync((void **)&h->d_out, (uint64_t)n * 8, s));
+            const prg::eig::Result r = prg::eig::eigenvector_centrality(h->g, h->ws, h->d_out, s, true, 1e-12);
+            PRG_CUDA(cudaMemcpyAsync(hub, h->d_out, (uint64_t)n * 8, cudaMemcpyDeviceToHost, s));
+            PRG_CUDA(cudaStreamSynchronize(s));
+            for (uint32_t i = 0; i < n; i++) authority[i] = hub[i];
+            if (eigenvalue) *eigenvalue = r.eigenvalue * r.eigenvalue;
+        } catch (...) {
+            destroy(h);
+            throw;
+        }
+        destroy(h);
+        return PRG_OK;
+    }
+    prg_graph *g = nullptr, *rev = nullptr;
+    int32_t rc = create_from_host(n, m, from, to, weights, 1, &g, 0);
+    if (rc != PRG_OK) return rc;
+    rc = create_from_host(n, m, to, from, weights, 1, &rev, 0);
+    if (rc != PRG_OK) {
+        destroy(g);
+        return rc;
+    }
+    try {
+        cudaStream_t s = g->stream;
+        PRG_CUDA(cudaStreamSynchronize(rev->stream));
+        double *d_h = nullptr, *d_a = nullptr;
+        PRG_CUDA(cudaMallocAsync((void **)&d_h, (uint64_t)n * 8, s));
+        PRG_CUDA(cudaMallocAsync((void **)&d_a, (uint64_t)n * 8, s));
+        const prg::eig::Result r = prg::eig::hits_directed(g->g, g->ws, rev->g, rev->ws, d_h, d_a, s);
+        PRG_CUDA(cudaMemcpyAsync(hub, d_h, (uint64_t)n * 8, cudaMemcpyDeviceToHost, s));
+        PRG_CUDA(cudaMemcpyAsync(authority, d_a, (uint64_t)n * 8, cudaMemcpyDeviceToHost, s));
+        cudaFreeAsync(d_h, s);
+        cudaFreeAsync(d_a, s);
+        PRG_CUDA(cudaStreamSynchronize(s));
+        if (eigenvalue) *eigenvalue = r.eigenvalue;
+    } catch (...) {
+        destroy(g);
+        destroy(rev);
+        throw;
+    }
+    destroy(g);
+    destroy(rev);
+    return PRG_OK;
+    PRG_GUARD_END
+}
+
 int32_t prg_pagerank_linsys(uint32_t n, uint64_t m, const uint32_t *from, const uint32_t *to, int32_t directed,
                             double *out) {
     g_err.clear();

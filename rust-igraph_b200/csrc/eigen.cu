@@ -141,11 +141,12 @@ __global__ void fill_kernel(double *x, uint32_t n, double v) {
     for (uint32_t i = blockIdx.x * kNT + threadIdx.x; i < n; i += gridDim.x * kNT) x[i] = v;
 }
 
-// x = out-degree and block records (max, 0, 0) for the normalisation
-__global__ void degree_seed_kernel(const uint32_t *deg, uint32_t n, double *x, double4 *recs) {
+// x = out-degree (deg) or |strength| (dval) and block records (max, 0, 0)
+// for the normalisation
+__global__ void degree_seed_kernel(const uint32_t *deg, const double *dval, uint32_t n, double *x, double4 *recs) {
     double mx = 0.0;
     for (uint32_t i = blockIdx.x * kNT + threadIdx.x; i < n; i += gridDim.x * kNT) {
-        x[i] = (double)deg[i];
+        x[i] = dval ? fabs(dval[i]) : (double)deg[i];
         mx = fmax(mx, x[i]);
     }
 #pragma unroll
@@ -253,7 +254,23 @@ static double rayleigh(const Product &pr, const double *x, double *tmp, double4 
     return den > 0.0 ? num / den : 0.0;
 }
 
-Result eigenvector_centrality(const DeviceGraph &g, Workspace &ws, double *d_out, cudaStream_t s) {
+// Seeds x from degrees or strengths and max-normalises it; an all-zero seed
+// becomes all ones.
+static void seed(const DeviceGraph &g, bool strength, double *x, double4 *recs, double4 *part, cudaStream_t s) {
+    degree_seed_kernel<<<kNB, kNT, 0, s>>>(g.deg, strength ? g.dval : nullptr, g.n, x, recs);
+    PRG_CUDA(cudaGetLastError());
+    std::vector<double4> h(kNB);
+    PRG_CUDA(cudaMemcpyAsync(h.data(), recs, kNB * sizeof(double4), cudaMemcpyDeviceToHost, s));
+    PRG_CUDA(cudaStreamSynchronize(s));
+    double mx = 0.0;
+    for (const double4 &q : h) mx = std::max(mx, q.x);
+    if (mx == 0.0) fill_kernel<<<kNB, kNT, 0, s>>>(x, g.n, 1.0);
+    else normalise_kernel<<<kNB, kNT, 0, s>>>(g.n, recs, kNB, nullptr, 0, x, nullptr, part, nullptr);
+    PRG_CUDA(cudaGetLastError());
+}
+
+Result eigenvector_centrality(const DeviceGraph &g, Workspace &ws, double *d_out, cudaStream_t s,
+                              bool strength_seed, double eps) {
     Result r;
     const uint32_t n = g.n;
     workspace_ensure(ws, g, s);
@@ -261,17 +278,21 @@ Result eigenvector_centrality(const DeviceGraph &g, Workspace &ws, double *d_out
     const Product pr{&g, &ws};
     const unsigned grid = ws.cfg[MODE_EIG64].grid;
     double *x[2] = {alloc<double>(n, s), alloc<double>(n, s)};
-    double4 *recs = alloc<double4>(grid, s), *part = alloc<double4>(kNB, s);
+    double4 *recs = alloc<double4>(std::max(grid, kNB), s), *part = alloc<double4>(kNB, s);
     State *d_st = alloc<State>(1, s), *h_st = nullptr;
     PRG_CUDA(cudaMallocHost((void **)&h_st, 2 * sizeof(State)));
     try {
         State init;
         std::memset(&init, 0, sizeof(init));
         init.max_iter = 5000;
-        init.eps = 1e-14;
+        init.eps = eps;
         PRG_CUDA(cudaMemcpyAsync(d_st, &init, sizeof(State), cudaMemcpyHostToDevice, s));
-        fill_kernel<<<kNB, kNT, 0, s>>>(x[0], n, 1.0);
-        PRG_CUDA(cudaGetLastError());
+        if (strength_seed) {
+            seed(g, true, x[0], recs, part, s);
+        } else {
+            fill_kernel<<<kNB, kNT, 0, s>>>(x[0], n, 1.0);
+            PRG_CUDA(cudaGetLastError());
+        }
         run_until_done(d_st, h_st, init.max_iter, s, [&](uint32_t it) {
             const int q = (int)(it & 1u);
             product(pr, x[q], x[q ^ 1], 1.0, recs, &d_st->done, s);
@@ -326,8 +347,9 @@ Result hits_directed(const DeviceGraph &g, Workspace &ws, const DeviceGraph &rev
         init.max_iter = 5000;
         init.eps = 1e-12;
         PRG_CUDA(cudaMemcpyAsync(d_st, &init, sizeof(State), cudaMemcpyHostToDevice, s));
-        // h = out-degree / max out-degree (the graph's deg is its out-degree)
-        degree_seed_kernel<<<kNB, kNT, 0, s>>>(g.deg, n, h[0], rout);
+        // h = out-degree (out-strength when weighted) / its max: the graph's
+        // deg / dval hold out-degree / out-strength
+        degree_seed_kernel<<<kNB, kNT, 0, s>>>(g.deg, g.weighted ? g.dval : nullptr, n, h[0], rout);
         normalise_kernel<<<kNB, kNT, 0, s>>>(n, rout, kNB, nullptr, 0, h[0], nullptr, part, nullptr);
         PRG_CUDA(cudaGetLastError());
         run_until_done(d_st, h_st, init.max_iter, s, [&](uint32_t it) {

@@ -14,11 +14,15 @@ struct Result {
     double eigenvalue = 0.0;
 };
 
-// Undirected graph g: x (caller ids) into d_out[n]; eigenvalue = x.Ax / x.x.
-Result eigenvector_centrality(const DeviceGraph &g, Workspace &ws, double *d_out, cudaStream_t s);
+// Undirected graph g: x (caller ids) into d_out[n]; eigenvalue = x.Ax / x.x
+// (A weighted when g is).  strength_seed: start from the vertex strengths
+// (all ones when they are all zero) instead of ones; eps: L1 stop.
+Result eigenvector_centrality(const DeviceGraph &g, Workspace &ws, double *d_out, cudaStream_t s,
+                              bool strength_seed = false, double eps = 1e-14);
 
 // Directed graph g and its reverse rev (both without relabelling):
 // hub and authority vectors into d_hub / d_auth; eigenvalue of A A^T.
+// The seed is the out-degree, or the out-strength when g is weighted.
 Result hits_directed(const DeviceGraph &g, Workspace &ws, const DeviceGraph &rev, Workspace &wsr, double *d_hub,
                      double *d_auth, cudaStream_t s);
 

@@ -195,6 +195,12 @@ def lib():
     L.prg_eigenvector_centrality.restype = C.c_int32
     L.prg_eigenvector_centrality.argtypes = [C.c_uint32, C.c_uint64, u32p, u32p, C.c_int32, f64p,
                                              C.POINTER(C.c_double)]
+    L.prg_eigenvector_centrality_weighted.restype = C.c_int32
+    L.prg_eigenvector_centrality_weighted.argtypes = [C.c_uint32, C.c_uint64, u32p, u32p, C.c_int32, f64p,
+                                                      C.c_uint64, f64p, f64p]
+    L.prg_hub_and_authority_scores_weighted.restype = C.c_int32
+    L.prg_hub_and_authority_scores_weighted.argtypes = [C.c_uint32, C.c_uint64, u32p, u32p, C.c_int32, f64p,
+                                                        C.c_uint64, f64p, f64p, f64p]
     L.prg_hub_and_authority_scores.restype = C.c_int32
     L.prg_hub_and_authority_scores.argtypes = [C.c_uint32, C.c_uint64, u32p, u32p, C.c_int32, f64p, f64p,
                                                C.POINTER(C.c_double)]
@@ -357,6 +363,34 @@ def hub_and_authority_scores(graph: Graph) -> HitsScores:
     lam = C.c_double()
     _check(lib().prg_hub_and_authority_scores(n, len(f), _ptr(f), _ptr(t), int(graph.is_directed()), _ptr(hub),
                                               _ptr(auth), C.byref(lam)))
+    return HitsScores(hub[:n], auth[:n], lam.value)
+
+
+def eigenvector_centrality_weighted(graph: Graph, weights, with_eigenvalue: bool = False):
+    """rust-igraph ``eigenvector_centrality_weighted`` (eigenvector.rs:157-168,
+    375-538), undirected, weights[e] >= 0 per edge id, on the GPU."""
+    n = graph.vcount()
+    f, t = graph.edge_arrays()
+    w = np.ascontiguousarray(weights, dtype=np.float64)
+    out = np.empty(max(n, 1), np.float64)
+    lam = C.c_double()
+    _check(lib().prg_eigenvector_centrality_weighted(n, len(f), _ptr(f), _ptr(t), int(graph.is_directed()),
+                                                     _ptr(w) if len(w) else None, len(w), _ptr(out), C.byref(lam)))
+    return (out[:n], lam.value) if with_eigenvalue else out[:n]
+
+
+def hub_and_authority_scores_weighted(graph: Graph, weights) -> HitsScores:
+    """rust-igraph ``hub_and_authority_scores_weighted`` (hits.rs:245-470),
+    weights[e] >= 0 per edge id, on the GPU."""
+    n = graph.vcount()
+    f, t = graph.edge_arrays()
+    w = np.ascontiguousarray(weights, dtype=np.float64)
+    hub = np.empty(max(n, 1), np.float64)
+    auth = np.empty(max(n, 1), np.float64)
+    lam = C.c_double()
+    _check(lib().prg_hub_and_authority_scores_weighted(n, len(f), _ptr(f), _ptr(t), int(graph.is_directed()),
+                                                       _ptr(w) if len(w) else None, len(w), _ptr(hub), _ptr(auth),
+                                                       C.byref(lam)))
     return HitsScores(hub[:n], auth[:n], lam.value)
 
 

@@ -47,3 +47,51 @@ def test_hits_reference_cases():
     ha = np.zeros(5)
     np.add.at(ha, f, a[t])
     assert np.allclose(ha / ha.max(), h, atol=1e-6)
+
+
+def test_eigenvector_weighted_reference_cases():
+    # eigenvector.rs:830-878
+    x, lam, _ = O.eigenvector_centrality_weighted(5, *E([(0, v) for v in range(1, 5)]), np.ones(4))
+    assert np.allclose(x, [1.0, 0.5, 0.5, 0.5, 0.5], atol=1e-9) and abs(lam - 2.0) < 1e-6
+    k5 = [(u, v) for u in range(5) for v in range(u + 1, 5)]
+    x, lam, _ = O.eigenvector_centrality_weighted(5, *E(k5), np.ones(10))
+    assert np.allclose(x, 1.0, atol=1e-9) and abs(lam - 4.0) < 1e-6
+    x, lam, _ = O.eigenvector_centrality_weighted(4, *E([]), np.zeros(0))
+    assert np.all(x == 1.0) and lam == 0.0
+    x, lam, _ = O.eigenvector_centrality_weighted(3, *E([(0, 1), (1, 2)]), np.zeros(2))
+    assert np.all(x == 1.0) and lam == 0.0
+    # unit weights give the unweighted centrality (a different seed, same fixed point)
+    f, t = E([(0, 1), (1, 2), (2, 3), (3, 0), (0, 2), (4, 0)])
+    xw, lw, _ = O.eigenvector_centrality_weighted(5, f, t, np.ones(6))
+    xu, lu, _ = O.eigenvector_centrality(5, f, t)
+    assert np.allclose(xw, xu, atol=1e-9) and abs(lw - lu) < 1e-9
+
+
+def test_hits_weighted_reference_cases():
+    # hits.rs:763-880
+    h, a, lam, _ = O.hub_and_authority_scores_weighted(0, *E([]), np.zeros(0), True)
+    assert len(h) == 0 and len(a) == 0 and lam == 0.0
+    h, a, lam, _ = O.hub_and_authority_scores_weighted(3, *E([]), np.zeros(0), True)
+    assert np.all(h == 1.0) and np.all(a == 1.0) and lam == 0.0
+    h, a, lam, _ = O.hub_and_authority_scores_weighted(3, *E([(0, 1), (1, 2)]), np.zeros(2), True)
+    assert np.all(h == 1.0) and np.all(a == 1.0) and lam == 0.0
+    f, t = E([(0, 1), (0, 2), (1, 3), (2, 3), (3, 4), (1, 4)])
+    hw, aw, lw, _ = O.hub_and_authority_scores_weighted(5, f, t, np.ones(6), True)
+    hu, au, lu, _ = O.hub_and_authority_scores(5, f, t, True)
+    assert np.allclose(hw, hu, atol=1e-6) and np.allclose(aw, au, atol=1e-6) and abs(lw - lu) < 1e-6
+    h, a, _, _ = O.hub_and_authority_scores_weighted(4, *E([(0, 2), (0, 3), (1, 2), (1, 3)]),
+                                                     np.array([1.0, 4.0, 2.0, 3.0]), True)
+    assert abs(h[2]) < 1e-9 and abs(h[3]) < 1e-9 and abs(a[0]) < 1e-9 and abs(a[1]) < 1e-9
+    assert a[3] > a[2]
+    # hub proportional to W authority after convergence
+    f, t = E([(0, 1), (0, 2), (1, 3), (2, 3), (3, 4), (4, 0)])
+    w = np.array([1.5, 0.5, 2.0, 1.0, 0.75, 1.25])
+    h, a, _, _ = O.hub_and_authority_scores_weighted(5, f, t, w, True)
+    wa = np.zeros(5)
+    np.add.at(wa, f, w * a[t])
+    assert np.allclose(wa / np.abs(wa).max(), h, atol=1e-6)
+    # undirected: the weighted eigenvector and its eigenvalue squared
+    f, t = E([(0, 1), (1, 2), (2, 3), (0, 3)])
+    h, a, lam, _ = O.hub_and_authority_scores_weighted(4, f, t, np.ones(4), False)
+    hu, au, lu, _ = O.hub_and_authority_scores(4, f, t, False)
+    assert np.allclose(h, hu, atol=1e-6) and np.array_equal(h, a) and abs(lam - lu) < 1e-6

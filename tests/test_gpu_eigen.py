@@ -106,3 +106,89 @@ def test_hits_undirected_delegates(cuda_ok):
     x, lam = ig.eigenvector_centrality(g, with_eigenvalue=True)
     assert np.array_equal(s.hub, x) and np.array_equal(s.authority, x)
     assert abs(s.eigenvalue - lam * lam) <= 1e-12 * lam * lam
+
+
+def test_weighted_reference_unit_cases(cuda_ok):
+    # eigenvector.rs:830-878
+    star = G(5, [(0, v) for v in range(1, 5)], False)
+    x, lam = ig.eigenvector_centrality_weighted(star, np.ones(4), with_eigenvalue=True)
+    assert np.allclose(x, [1.0, 0.5, 0.5, 0.5, 0.5], atol=1e-9) and abs(lam - 2.0) < 1e-6
+    k5 = G(5, [(u, v) for u in range(5) for v in range(u + 1, 5)], False)
+    x, lam = ig.eigenvector_centrality_weighted(k5, np.ones(10), with_eigenvalue=True)
+    assert np.allclose(x, 1.0, atol=1e-9) and abs(lam - 4.0) < 1e-6
+    x, lam = ig.eigenvector_centrality_weighted(ig.Graph.with_vertices(4), [], with_eigenvalue=True)
+    assert np.all(x == 1.0) and lam == 0.0
+    path = G(3, [(0, 1), (1, 2)], False)
+    x, lam = ig.eigenvector_centrality_weighted(path, [0.0, 0.0], with_eigenvalue=True)
+    assert np.all(x == 1.0) and lam == 0.0
+    with pytest.raises(ig.InvalidArgument, match=r"weights vector length \(1\) not equal to number of edges \(2\)"):
+        ig.eigenvector_centrality_weighted(path, [1.0])
+    with pytest.raises(ig.Unsupported, match="directed eigenvector_centrality_weighted"):
+        ig.eigenvector_centrality_weighted(G(3, [(0, 1)], True), [1.0])
+    with pytest.raises(ig.Unsupported, match="negative weights"):
+        ig.eigenvector_centrality_weighted(path, [1.0, -1.0])
+    # hits.rs:763-880
+    s = ig.hub_and_authority_scores_weighted(G(0, [], True), [])
+    assert len(s.hub) == 0 and s.eigenvalue == 0.0
+    s = ig.hub_and_authority_scores_weighted(G(3, [], True), [])
+    assert np.all(s.hub == 1.0) and np.all(s.authority == 1.0) and s.eigenvalue == 0.0
+    dpath = G(3, [(0, 1), (1, 2)], True)
+    s = ig.hub_and_authority_scores_weighted(dpath, [0.0, 0.0])
+    assert np.all(s.hub == 1.0) and np.all(s.authority == 1.0) and s.eigenvalue == 0.0
+    with pytest.raises(ig.InvalidArgument, match="weights length 1 does not match edge count 2"):
+        ig.hub_and_authority_scores_weighted(dpath, [1.0])
+    g = G(5, [(0, 1), (0, 2), (1, 3), (2, 3), (3, 4), (1, 4)], True)
+    sw, su = ig.hub_and_authority_scores_weighted(g, np.ones(6)), ig.hub_and_authority_scores(g)
+    assert np.allclose(sw.hub, su.hub, atol=1e-9) and np.allclose(sw.authority, su.authority, atol=1e-9)
+    assert abs(sw.eigenvalue - su.eigenvalue) < 1e-9
+    s = ig.hub_and_authority_scores_weighted(G(4, [(0, 2), (0, 3), (1, 2), (1, 3)], True), [1.0, 4.0, 2.0, 3.0])
+    assert abs(s.hub[2]) < 1e-9 and abs(s.hub[3]) < 1e-9 and abs(s.authority[0]) < 1e-9
+    assert abs(s.authority[1]) < 1e-9 and s.authority[3] > s.authority[2]
+    u = G(4, [(0, 1), (1, 2), (2, 3), (0, 3)], False)
+    sw, su = ig.hub_and_authority_scores_weighted(u, np.ones(4)), ig.hub_and_authority_scores(u)
+    assert np.allclose(sw.hub, su.hub, atol=1e-9) and abs(sw.eigenvalue - su.eigenvalue) < 1e-9
+
+
+def _weighted_graph(kind, directed):
+    if kind == "er":
+        n = 20_000
+        f, t = O.erdos_renyi_gnm(n, 100_000, directed, False, 31)
+    elif kind == "ba":
+        n = 30_000
+        f, t = O.barabasi_game_bag(n, 4, False, directed, 32)
+    elif kind == "rmat":
+        n = 1 << 15
+        f, t = O.rmat(15, 8 * n, seed=33)
+    else:
+        rng = np.random.default_rng(34)
+        n = 5000
+        f = rng.integers(0, n, 30_000).astype(np.uint32)
+        t = rng.integers(0, n, 30_000).astype(np.uint32)
+        f[:200] = t[:200] = 7  # loops
+    g = ig.Graph.from_edge_arrays(n, f, t, directed)
+    gf, gt = edges(g)
+    w = O.uniform_weights(len(gf), 35, 0.0, 3.0)
+    w[::97] = 0.0  # zero-weight edges stay in the graph
+    return n, g, gf, gt, w
+
+
+@pytest.mark.parametrize("kind", ["er", "ba", "rmat", "loops"])
+def test_eigenvector_weighted_matches_restatement(cuda_ok, kind):
+    n, g, gf, gt, w = _weighted_graph(kind, False)
+    x, lam = ig.eigenvector_centrality_weighted(g, w, with_eigenvalue=True)
+    ref, rlam, _ = O.eigenvector_centrality_weighted(n, gf, gt, w)
+    assert np.max(np.abs(x - ref)) <= TOL, np.max(np.abs(x - ref))
+    assert abs(lam - rlam) <= TOL * abs(rlam)
+    s = ig.hub_and_authority_scores_weighted(g, w)
+    assert np.array_equal(s.hub, x) and np.array_equal(s.authority, x)
+    assert abs(s.eigenvalue - lam * lam) <= 1e-12 * lam * lam
+
+
+@pytest.mark.parametrize("kind", ["er", "ba", "rmat"])
+def test_hits_weighted_directed_matches_restatement(cuda_ok, kind):
+    n, g, gf, gt, w = _weighted_graph(kind, True)
+    s = ig.hub_and_authority_scores_weighted(g, w)
+    h, a, lam, _ = O.hub_and_authority_scores_weighted(n, gf, gt, w, True)
+    assert np.max(np.abs(s.hub - h)) <= TOL and np.max(np.abs(s.authority - a)) <= TOL
+    assert abs(s.eigenvalue - lam) <= TOL * abs(lam)
+    assert s.hub.max() == 1.0 and s.authority.max() == 1.0 and s.hub.min() >= 0.0
