@@ -149,6 +149,18 @@ int32_t prg_hub_and_authority_scores_weighted(uint32_t n, uint64_t m, const uint
                                               int32_t directed, const double *weights, uint64_t weights_len,
                                               double *hub, double *authority, double *eigenvalue);
 
+/* Node flows of rust-igraph's Infomap flow model (community/infomap.rs:
+ * 233-355, the private power_iteration_pagerank): tau = 0.15 teleportation
+ * to vertex_weights / sum (uniform 1/n when NULL), arc weights edge_weights
+ * (unit when NULL) normalised by the out-strength, the dangling mass sent
+ * back through the teleport weights undamped, each iterate renormalised to
+ * sum 1; stops at an L1 change < 1e-10 or after 1000 iterations.  Checks
+ * the weights as infomap_with_options does (infomap.rs:175-218), in its
+ * order and with its messages.  node_flow[n]; iterations (optional). */
+int32_t prg_infomap_flow(uint32_t n, uint64_t m, const uint32_t *from, const uint32_t *to, int32_t directed,
+                         const double *edge_weights, uint64_t edge_weights_len, const double *vertex_weights,
+                         uint64_t vertex_weights_len, double *node_flow, uint32_t *iterations);
+
 /* rust-igraph pagerank_weighted() (pagerank_weighted.rs:52-161).
  * weights_len is the caller's slice length (checked against m like :62-68). */
 int32_t prg_pagerank_weighted(uint32_t n, uint64_t m, const uint32_t *from, const uint32_t *to,

@@ -76,6 +76,9 @@ def lib():
         L.or_hits_weighted.restype = C.c_int
         L.or_hits_weighted.argtypes = [C.c_uint32, C.c_uint64, _u32p, _u32p, _f64p, C.c_int, _f64p, _f64p,
                                        C.POINTER(C.c_double)]
+        L.or_infomap_flow.restype = C.c_int
+        L.or_infomap_flow.argtypes = [C.c_uint32, C.c_uint64, _u32p, _u32p, C.c_int, C.c_void_p, C.c_void_p,
+                                      _f64p]
         L.or_adj_build.restype = C.c_void_p
         L.or_adj_build.argtypes = [C.c_uint32, C.c_uint64, _u32p, _u32p, C.c_int]
         L.or_adj_free.restype = None
@@ -228,6 +231,19 @@ def hub_and_authority_scores_weighted(n, frm, to, weights, directed):
     it = lib().or_hits_weighted(n, len(f), f, t, w if len(w) else np.zeros(1), int(directed), hub, auth,
                                 C.byref(lam))
     return hub[:n], auth[:n], lam.value, it
+
+
+def infomap_flow(n, frm, to, directed, edge_weights=None, vertex_weights=None):
+    """Node flows of rust-igraph's Infomap flow model (infomap.rs:233-355):
+    (flow, iterations)."""
+    f, t = _edges(frm, to)
+    ew = None if edge_weights is None else np.ascontiguousarray(edge_weights, dtype=np.float64)
+    vw = None if vertex_weights is None else np.ascontiguousarray(vertex_weights, dtype=np.float64)
+    out = np.zeros(max(n, 1), np.float64)
+    it = lib().or_infomap_flow(n, len(f), f, t, int(directed),
+                               None if ew is None else ew.ctypes.data_as(C.c_void_p),
+                               None if vw is None else vw.ctypes.data_as(C.c_void_p), out)
+    return out[:n], int(it)
 
 
 def pagerank_tight(n, frm, to, directed, weights=None, reset=None, damping=0.85, tol=1e-14,

@@ -12,6 +12,7 @@
 
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -553,6 +554,82 @@ int32_t prg_hub_and_authority_scores_weighted(uint32_t n, uint64_t m, const uint
     }
     destroy(g);
     destroy(rev);
+    return PRG_OK;
+    PRG_GUARD_END
+}
+
+int32_t prg_infomap_flow(uint32_t n, uint64_t m, const uint32_t *from, const uint32_t *to, int32_t directed,
+                         const double *edge_weights, uint64_t edge_weights_len, const double *vertex_weights,
+                         uint64_t vertex_weights_len, double *node_flow, uint32_t *iterations) {
+    g_err.clear();
+    PRG_GUARD_BEGIN
+    if (iterations) *iterations = 0;
+    if (edge_weights) {  // infomap.rs:175-193
+        if (edge_weights_len != m)
+            return fail(PRG_ERR_INVALID_ARGUMENT, "edge weight vector length " + std::to_string(edge_weights_len) +
+                                                      " does not match edge count " + std::to_string(m));
+        for (uint64_t e = 0; e < m; e++) {
+            const double w = edge_weights[e];
+            if (w < 0.0 || !std::isfinite(w))
+                return fail(PRG_ERR_INVALID_ARGUMENT, "edge weight[" + std::to_string(e) + "] = " + rust_f64(w) +
+                                                          " is invalid (must be non-negative and finite)");
+        }
+    }
+    std::vector<double> tele;
+    if (vertex_weights) {  // infomap.rs:195-218
+        if (vertex_weights_len != n)
+            return fail(PRG_ERR_INVALID_ARGUMENT, "vertex weight vector length " +
+                                                      std::to_string(vertex_weights_len) +
+                                                      " does not match vertex count " + std::to_string(n));
+        bool any = false;
+        for (uint32_t i = 0; i < n; i++) {
+            const double w = vertex_weights[i];
+            if (w < 0.0 || !std::isfinite(w))
+                return fail(PRG_ERR_INVALID_ARGUMENT,
+                            "vertex weight[" + std::to_string(i) + "] = " + rust_f64(w) + " is invalid");
+            any |= w > 0.0;
+        }
+        if (!any && n > 0) return fail(PRG_ERR_INVALID_ARGUMENT, "all vertex weights are zero");
+        // infomap.rs:261-270: tele = vw / sum(vw), summed in index order
+        double sum = 0.0;
+        for (uint32_t i = 0; i < n; i++) sum += vertex_weights[i];
+        tele.resize(n);
+        for (uint32_t i = 0; i < n; i++) tele[i] = vertex_weights[i] / sum;
+    }
+    if (n == 0) return PRG_OK;
+    if (n == 1) {  // infomap.rs:308-310
+        node_flow[0] = 1.0;
+        return PRG_OK;
+    }
+    prg_graph *h = nullptr;
+    int32_t rc = create_from_host(n, m, from, to, edge_weights, directed, &h);
+    if (rc != PRG_OK) return rc;
+    double *d_t = nullptr, *d_ti = nullptr;
+    try {
+        cudaStream_t s = h->stream;
+        if (!h->d_out) PRG_CUDA(cudaMallocAsync((void **)&h->d_out, (uint64_t)n * 8, s));
+        if (!tele.empty()) {
+            PRG_CUDA(cudaMallocAsync((void **)&d_t, (uint64_t)n * 8, s));
+            PRG_CUDA(cudaMemcpyAsync(d_t, tele.data(), (uint64_t)n * 8, cudaMemcpyHostToDevice, s));
+            if (h->g.perm) {
+                PRG_CUDA(cudaMallocAsync((void **)&d_ti, (uint64_t)n * 8, s));
+                prg::gather_f64(d_ti, d_t, h->g.perm, n, s);
+            }
+        }
+        const prg::eig::Result r = prg::eig::infomap_flow(h->g, h->ws, d_ti ? d_ti : d_t, h->d_out, s);
+        PRG_CUDA(cudaMemcpyAsync(node_flow, h->d_out, (uint64_t)n * 8, cudaMemcpyDeviceToHost, s));
+        if (d_t) cudaFreeAsync(d_t, s);
+        if (d_ti) cudaFreeAsync(d_ti, s);
+        d_t = d_ti = nullptr;
+        PRG_CUDA(cudaStreamSynchronize(s));
+        if (iterations) *iterations = r.iterations;
+    } catch (...) {
+        if (d_t) cudaFreeAsync(d_t, h->stream);
+        if (d_ti) cudaFreeAsync(d_ti, h->stream);
+        destroy(h);
+        throw;
+    }
+    destroy(h);
     return PRG_OK;
     PRG_GUARD_END
 }

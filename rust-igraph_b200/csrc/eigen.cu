@@ -26,6 +26,7 @@
 #include <vector>
 
 #include "eigen.cuh"
+#include "prims.cuh"
 #include "solver.cuh"
 
 namespace prg {
@@ -159,6 +160,77 @@ __global__ void degree_seed_kernel(const uint32_t *deg, const double *dval, uint
         for (int k = 1; k < kNT / 32; k++) mx = fmax(mx, sh[k]);
         recs[blockIdx.x] = make_double4(mx, 0.0, 0.0, 0.0);
     }
+}
+
+// ---- Infomap flow model (infomap.rs:299-355)
+constexpr double kTau = 0.15;
+
+__device__ __forceinline__ double block_total(double v, double *sh) {
+    v = warp_sum(v);
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    if (l == 0) sh[w] = v;
+    __syncthreads();
+    if (threadIdx.x == 0)
+        for (int k = 1; k < kNT / 32; k++) v += sh[k];
+    return v;  // valid in thread 0
+}
+
+// pr = 1/n, xt = pr / strength (0 for dangling), records (0, dangling sum).
+__global__ void flow_init_kernel(uint32_t n, const double *dval, double *pr, double *xt, double4 *part) {
+    __shared__ double sh[kNT / 32];
+    const double p = 1.0 / (double)n;
+    double ds = 0.0;
+    for (uint32_t v = blockIdx.x * kNT + threadIdx.x; v < n; v += gridDim.x * kNT) {
+        pr[v] = p;
+        const double s = dval[v];
+        xt[v] = s > 0.0 ? p / s : 0.0;
+        if (s <= 0.0) ds += p;
+    }
+    ds = block_total(ds, sh);
+    if (threadIdx.x == 0) part[blockIdx.x] = make_double4(0.0, ds, 0.0, 0.0);
+}
+
+// buf[v] = tau t[v] + (1 - tau) link[v] + dangling t[v] in place over the
+// product y = link, with the dangling sum from the last normalisation's
+// records; records (0, sum of buf).
+__global__ void __launch_bounds__(kNT) flow_epi_kernel(uint32_t n, double *y, const double *t, const double4 *dpart,
+                                                       uint32_t ndp, double4 *spart, const State *st) {
+    if (*(volatile const int32_t *)&st->done) return;
+    __shared__ double sh[kNT / 32];
+    const double ds = recs3(dpart, ndp, nullptr, 0).y;
+    const double inv_n = 1.0 / (double)n;
+    double sum = 0.0;
+    for (uint32_t v = blockIdx.x * kNT + threadIdx.x; v < n; v += gridDim.x * kNT) {
+        const double tv = t ? t[v] : inv_n;
+        const double b = __dadd_rn(__dadd_rn(__dmul_rn(kTau, tv), __dmul_rn(1.0 - kTau, y[v])), __dmul_rn(ds, tv));
+        y[v] = b;
+        sum += b;
+    }
+    sum = block_total(sum, sh);
+    if (threadIdx.x == 0) spart[blockIdx.x] = make_double4(0.0, sum, 0.0, 0.0);
+}
+
+// pr_new = buf / sum(buf) (unscaled when the sum is not positive), the L1
+// change from pr_old, xt = pr_new / strength; records (change, dangling sum).
+__global__ void __launch_bounds__(kNT) flow_norm_kernel(uint32_t n, const double *buf, const double4 *spart,
+                                                        uint32_t nsp, const double *pr_old, double *pr_new, double *xt,
+                                                        const double *dval, double4 *dpart, const State *st) {
+    if (*(volatile const int32_t *)&st->done) return;
+    __shared__ double sh[kNT / 32];
+    const double s = recs3(spart, nsp, nullptr, 0).y;
+    double d = 0.0, ds = 0.0;
+    for (uint32_t v = blockIdx.x * kNT + threadIdx.x; v < n; v += gridDim.x * kNT) {
+        const double p = s > 0.0 ? __ddiv_rn(buf[v], s) : buf[v];
+        d += fabs(pr_old[v] - p);
+        pr_new[v] = p;
+        const double sv = dval[v];
+        xt[v] = sv > 0.0 ? __ddiv_rn(p, sv) : 0.0;
+        if (sv <= 0.0) ds += p;
+    }
+    d = block_total(d, sh);
+    __syncthreads();
+    ds = block_total(ds, sh);
+    if (threadIdx.x == 0) dpart[blockIdx.x] = make_double4(d, ds, 0.0, 0.0);
 }
 
 __global__ void clamp_kernel(double *x, uint32_t n) {
@@ -319,6 +391,58 @@ Result eigenvector_centrality(const DeviceGraph &g, Workspace &ws, double *d_out
     release(x[1], s);
     release(recs, s);
     release(part, s);
+    release(d_st, s);
+    PRG_CUDA(cudaStreamSynchronize(s));
+    return r;
+}
+
+Result infomap_flow(const DeviceGraph &g, Workspace &ws, const double *d_t, double *d_out, cudaStream_t s) {
+    Result r;
+    const uint32_t n = g.n;
+    workspace_ensure(ws, g, s);
+    PRG_CUDA(cudaMemsetAsync(ws.hub_ticket, 0, std::max<uint64_t>(g.nhub, 1) * 4, s));
+    const Product pr_{&g, &ws};
+    const unsigned grid = ws.cfg[MODE_EIG64].grid;
+    double *pr[2] = {alloc<double>(n, s), alloc<double>(n, s)};
+    double *xt = alloc<double>(n, s), *y = alloc<double>(n, s);
+    double4 *recs = alloc<double4>(std::max(grid, kNB), s), *spart = alloc<double4>(kNB, s);
+    double4 *dpart = alloc<double4>(kNB, s);
+    State *d_st = alloc<State>(1, s), *h_st = nullptr;
+    PRG_CUDA(cudaMallocHost((void **)&h_st, 2 * sizeof(State)));
+    try {
+        State init;
+        std::memset(&init, 0, sizeof(init));
+        init.max_iter = 1000;
+        init.eps = 1e-10;
+        PRG_CUDA(cudaMemcpyAsync(d_st, &init, sizeof(State), cudaMemcpyHostToDevice, s));
+        flow_init_kernel<<<kNB, kNT, 0, s>>>(n, g.dval, pr[0], xt, dpart);
+        PRG_CUDA(cudaGetLastError());
+        run_until_done(d_st, h_st, init.max_iter, s, [&](uint32_t it) {
+            const int q = (int)(it & 1u);
+            product(pr_, xt, y, 0.0, recs, &d_st->done, s);
+            flow_epi_kernel<<<kNB, kNT, 0, s>>>(n, y, d_t, dpart, kNB, spart, d_st);
+            flow_norm_kernel<<<kNB, kNT, 0, s>>>(n, y, spart, kNB, pr[q], pr[q ^ 1], xt, g.dval, dpart, d_st);
+            check_kernel<<<1, 256, 0, s>>>(dpart, kNB, d_st, q ^ 1);
+            PRG_CUDA(cudaGetLastError());
+        });
+        r.iterations = h_st[0].iters;
+        const double *pf = h_st[0].iters ? pr[h_st[0].final_buf] : pr[0];
+        if (g.perm) gather_f64(d_out, pf, g.iperm, n, s);
+        else PRG_CUDA(cudaMemcpyAsync(d_out, pf, (uint64_t)n * 8, cudaMemcpyDeviceToDevice, s));
+        PRG_CUDA(cudaStreamSynchronize(s));
+    } catch (...) {
+        cudaStreamSynchronize(s);
+        cudaFreeHost(h_st);
+        throw;
+    }
+    cudaFreeHost(h_st);
+    release(pr[0], s);
+    release(pr[1], s);
+    release(xt, s);
+    release(y, s);
+    release(recs, s);
+    release(spart, s);
+    release(dpart, s);
     release(d_st, s);
     PRG_CUDA(cudaStreamSynchronize(s));
     return r;

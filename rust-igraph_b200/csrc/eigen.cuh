@@ -26,5 +26,11 @@ Result eigenvector_centrality(const DeviceGraph &g, Workspace &ws, double *d_out
 Result hits_directed(const DeviceGraph &g, Workspace &ws, const DeviceGraph &rev, Workspace &wsr, double *d_hub,
                      double *d_auth, cudaStream_t s);
 
+// Infomap's flow model (infomap.rs:299-355) on g (directed or undirected,
+// arc weights when g is weighted): node flows into d_out[n] (caller ids).
+// d_t: teleport weights in g's internal ids, summing to 1 (null = 1/n).
+// Requires n >= 2.
+Result infomap_flow(const DeviceGraph &g, Workspace &ws, const double *d_t, double *d_out, cudaStream_t s);
+
 }  // namespace eig
 }  // namespace prg

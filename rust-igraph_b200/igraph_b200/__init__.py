@@ -201,6 +201,9 @@ def lib():
     L.prg_hub_and_authority_scores_weighted.restype = C.c_int32
     L.prg_hub_and_authority_scores_weighted.argtypes = [C.c_uint32, C.c_uint64, u32p, u32p, C.c_int32, f64p,
                                                         C.c_uint64, f64p, f64p, f64p]
+    L.prg_infomap_flow.restype = C.c_int32
+    L.prg_infomap_flow.argtypes = [C.c_uint32, C.c_uint64, u32p, u32p, C.c_int32, f64p, C.c_uint64, f64p,
+                                   C.c_uint64, f64p, C.POINTER(C.c_uint32)]
     L.prg_hub_and_authority_scores.restype = C.c_int32
     L.prg_hub_and_authority_scores.argtypes = [C.c_uint32, C.c_uint64, u32p, u32p, C.c_int32, f64p, f64p,
                                                C.POINTER(C.c_double)]
@@ -392,6 +395,24 @@ def hub_and_authority_scores_weighted(graph: Graph, weights) -> HitsScores:
                                                        _ptr(w) if len(w) else None, len(w), _ptr(hub), _ptr(auth),
                                                        C.byref(lam)))
     return HitsScores(hub[:n], auth[:n], lam.value)
+
+
+def infomap_flow(graph: Graph, edge_weights=None, vertex_weights=None, with_iterations: bool = False):
+    """Node flows of rust-igraph's Infomap flow model (community/infomap.rs:
+    233-355) on the GPU: tau = 0.15 teleportation to vertex_weights (uniform
+    when None), arc weights edge_weights (unit when None)."""
+    n = graph.vcount()
+    f, t = graph.edge_arrays()
+    ew = None if edge_weights is None else np.ascontiguousarray(edge_weights, dtype=np.float64)
+    vw = None if vertex_weights is None else np.ascontiguousarray(vertex_weights, dtype=np.float64)
+    out = np.empty(max(n, 1), np.float64)
+    it = C.c_uint32()
+    _check(lib().prg_infomap_flow(n, len(f), _ptr(f), _ptr(t), int(graph.is_directed()),
+                                  None if ew is None else (_ptr(ew) if len(ew) else _ptr(np.zeros(1))),
+                                  0 if ew is None else len(ew),
+                                  None if vw is None else (_ptr(vw) if len(vw) else _ptr(np.zeros(1))),
+                                  0 if vw is None else len(vw), _ptr(out), C.byref(it)))
+    return (out[:n], it.value) if with_iterations else out[:n]
 
 
 def parse_edgelist(data: bytes):

@@ -1,5 +1,6 @@
 """Timings of the five workload configurations on one GPU, plus the
-edge-list ingest (text -> GPU parse -> resident CSR).
+edge-list ingest (text -> GPU parse -> resident CSR), eigenvector
+centrality / HITS (7) and Infomap's flow model (8).
 
 Inputs are generated on the device with the shapes of each configuration
 (R-MAT; a Chung-Lu power law with the degree law of preferential attachment
@@ -10,7 +11,7 @@ to tolerance, GTEPS (in-CSR arcs x passes / time), algorithmic bytes of one
 SpMV pass, the SpMV launches' HBM rate against the measured copy peak, and
 the L1 distance to a tight FP64 solve of the same graph.
 
-    python -m igraph_b200.configs [--which 1,2,3,4,5,6] [--peak-gbs 6546]
+    python -m igraph_b200.configs [--which 1,2,3,4,5,6,7,8] [--peak-gbs 6546]
 """
 from __future__ import annotations
 
@@ -264,6 +265,32 @@ def config7(peak):
                               "seconds_incl_upload_and_build": round(dt_s, 4)}), flush=True)
 
 
+def config8(peak):
+    # Infomap's flow model (node flows) on directed R-MAT graphs
+    import time
+
+    import torch
+
+    from . import Graph, infomap_flow
+
+    for scale in (16, 20, 22):
+        n, m = 1 << scale, 16 << scale
+        df = torch.empty(m, dtype=torch.int32, device="cuda")
+        dt = torch.empty(m, dtype=torch.int32, device="cuda")
+        generate_device(GEN_RMAT, n, m, df.data_ptr(), dt.data_ptr(), 0.57, 0.19, 0.19, seed=8)
+        f = df.cpu().numpy().view(np.uint32).copy()
+        t = dt.cpu().numpy().view(np.uint32).copy()
+        del df, dt
+        g = Graph.from_edge_arrays(n, f, t, True)
+        infomap_flow(g)
+        t0 = time.perf_counter()
+        _, it = infomap_flow(g, with_iterations=True)
+        dt_s = time.perf_counter() - t0
+        print(json.dumps({"config": f"8 infomap_flow (directed) R-MAT s{scale}", "n": n, "m": m, "iterations": it,
+                          "seconds_incl_upload_and_build": round(dt_s, 4),
+                          "gteps_incl_upload_and_build": round(m * it / dt_s / 1e9, 2)}), flush=True)
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--which", default="1,2,3,4,5,6")
@@ -272,7 +299,7 @@ def main(argv=None):
     peak = _peak(a.peak_gbs)
     for k in a.which.split(","):
         {"1": config1, "2": config2, "3": config3, "4": config4, "5": config5, "6": config6,
-         "7": config7}[k.strip()](peak)
+         "7": config7, "8": config8}[k.strip()](peak)
 
 
 if __name__ == "__main__":

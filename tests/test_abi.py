@@ -135,3 +135,26 @@ def test_rust_float_display():
         ig.pagerank_weighted(g2(), [-1e-7])
     with pytest.raises(ig.InvalidArgument, match=r"\(got -12345678901234567000\)$"):
         ig.pagerank_weighted(g2(), [-1.2345678901234567e19])
+
+
+def test_infomap_flow_validation_and_trivial_graphs():
+    # infomap.rs:175-218 (checked before n == 0), 299-310
+    g = g2()
+    with pytest.raises(ig.InvalidArgument, match=r"^edge weight vector length 2 does not match edge count 1$"):
+        ig.infomap_flow(g, edge_weights=[1.0, 1.0])
+    with pytest.raises(ig.InvalidArgument,
+                       match=r"^edge weight\[0\] = -1 is invalid \(must be non-negative and finite\)$"):
+        ig.infomap_flow(g, edge_weights=[-1.0])
+    with pytest.raises(ig.InvalidArgument, match=r"^edge weight\[0\] = NaN is invalid"):
+        ig.infomap_flow(g, edge_weights=[math.nan])
+    with pytest.raises(ig.InvalidArgument, match=r"^vertex weight vector length 1 does not match vertex count 2$"):
+        ig.infomap_flow(g, vertex_weights=[1.0])
+    with pytest.raises(ig.InvalidArgument, match=r"^vertex weight\[1\] = inf is invalid$"):
+        ig.infomap_flow(g, vertex_weights=[1.0, math.inf])
+    with pytest.raises(ig.InvalidArgument, match=r"^all vertex weights are zero$"):
+        ig.infomap_flow(g, vertex_weights=[0.0, 0.0])
+    with pytest.raises(ig.InvalidArgument, match="edge weight vector length 1 does not match edge count 0"):
+        ig.infomap_flow(ig.Graph.with_vertices(0), edge_weights=[1.0])
+    assert len(ig.infomap_flow(ig.Graph.with_vertices(0))) == 0
+    assert list(ig.infomap_flow(ig.Graph.with_vertices(1))) == [1.0]
+    assert list(ig.infomap_flow(ig.Graph.with_vertices(1), vertex_weights=[3.0])) == [1.0]
