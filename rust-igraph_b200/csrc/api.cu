@@ -111,32 +111,47 @@ __global__ void max_endpoint_kernel(const uint32_t *a, const uint32_t *b, uint64
     if ((threadIdx.x & 31) == 0) atomicMax(out, mx);
 }
 
-// Creates a handle from device edge arrays (copies nothing on the host).
-int32_t create_from_device(uint32_t n, uint64_t m, const uint32_t *d_from, const uint32_t *d_to, const double *d_w,
-                           int32_t directed, cudaStream_t s, prg_graph **out, int relabel = -1) {
+// Size checks shared by both ways of creating a handle.
+static int32_t check_sizes(uint32_t n, uint64_t m, int32_t directed) {
     if (m > 0xFFFFFFFFull) return fail(PRG_ERR_INTERNAL, "ecount overflows u32");
     const uint64_t arcs = directed ? m : 2 * m;
     if (arcs + prg::kColPad >= 0xFFFFFFFFull)
         return fail(PRG_ERR_INTERNAL, "arc count exceeds the u32 CSR index range");
     if (n >= prg::kChunkFlag) return fail(PRG_ERR_INTERNAL, "vertex count exceeds 2^31 - 1");
+    return PRG_OK;
+}
+
+// A handle with the process-wide tuning applied and nothing built yet.
+static prg_graph *new_handle(uint32_t n, uint64_t m, int32_t directed, cudaStream_t s, int relabel) {
     prg_graph *h = new prg_graph();
     h->stream = s;
     h->g.n = n;
     h->g.m = m;
     h->g.directed = directed != 0;
-    {
-        const prg::Tuning &t = prg::tuning();
-        h->g.capw = t.capw;
-        h->g.shortmax = t.shortmax;
-        h->g.split = t.split;
-        h->g.blocks_per_sm = t.blocks_per_sm;
-        h->g.relabel = relabel >= 0 ? relabel : t.relabel;
-        h->g.hot_cache = t.hot_cache;
-        h->g.l1_hot32 = t.l1_hot32;
-        h->g.l1_hot64 = t.l1_hot64;
-        h->ws.unroll = t.unroll;
-    }
+    const prg::Tuning &t = prg::tuning();
+    h->g.capw = t.capw;
+    h->g.shortmax = t.shortmax;
+    h->g.split = t.split;
+    h->g.blocks_per_sm = t.blocks_per_sm;
+    h->g.relabel = relabel >= 0 ? relabel : t.relabel;
+    h->g.hot_cache = t.hot_cache;
+    h->g.l1_hot32 = t.l1_hot32;
+    h->g.l1_hot64 = t.l1_hot64;
+    h->ws.unroll = t.unroll;
     PRG_CUDA(cudaGetDevice(&h->g.device));
+    return h;
+}
+
+static std::string range_message(uint32_t mx, uint32_t n) {
+    return "vertex id " + std::to_string(mx) + " out of range (vcount = " + std::to_string(n) + ")";
+}
+
+// Creates a handle from device edge arrays (copies nothing on the host).
+int32_t create_from_device(uint32_t n, uint64_t m, const uint32_t *d_from, const uint32_t *d_to, const double *d_w,
+                           int32_t directed, cudaStream_t s, prg_graph **out, int relabel = -1) {
+    const int32_t rc = check_sizes(n, m, directed);
+    if (rc != PRG_OK) return rc;
+    prg_graph *h = new_handle(n, m, directed, s, relabel);
     if (m > 0) {
         uint32_t *d_mx = nullptr, mx = 0;
         PRG_CUDA(cudaMallocAsync((void **)&d_mx, 4, s));
@@ -148,14 +163,15 @@ int32_t create_from_device(uint32_t n, uint64_t m, const uint32_t *d_from, const
         PRG_CUDA(cudaStreamSynchronize(s));
         if (mx >= n) {
             delete h;
-            return fail(PRG_ERR_VERTEX_OUT_OF_RANGE, "vertex id " + std::to_string(mx) +
-                                                         " out of range (vcount = " + std::to_string(n) + ")");
+            return fail(PRG_ERR_VERTEX_OUT_OF_RANGE, range_message(mx, n));
         }
     }
     prg::build_graph(h->g, d_from, d_to, d_w, s);
     *out = h;
     return PRG_OK;
 }
+
+void destroy(prg_graph *h);
 
 int32_t create_from_host(uint32_t n, uint64_t m, const uint32_t *from, const uint32_t *to, const double *w,
                          int32_t directed, prg_graph **out, int relabel = -1) {
@@ -165,6 +181,30 @@ int32_t create_from_host(uint32_t n, uint64_t m, const uint32_t *from, const uin
     if (m > 0xFFFFFFFFull) {
         cudaStreamDestroy(s);
         return fail(PRG_ERR_INTERNAL, "ecount overflows u32");
+    }
+    if (m >= prg::kStreamMinEdges && !(w && directed)) {
+        // large edge lists: chunked copies overlapped with the build
+        int32_t rc = check_sizes(n, m, directed);
+        if (rc == PRG_OK) {
+            prg_graph *h = new_handle(n, m, directed, s, relabel);
+            uint32_t mx = 0;
+            bool ok = false;
+            try {
+                ok = prg::build_graph_host(h->g, from, to, w, s, &mx);
+            } catch (...) {
+                destroy(h);
+                throw;
+            }
+            if (ok) {
+                *out = h;
+                return PRG_OK;
+            }
+            destroy(h);  // what was built, and the stream
+            return fail(PRG_ERR_VERTEX_OUT_OF_RANGE, range_message(mx, n));
+        }
+        cudaStreamSynchronize(s);
+        cudaStreamDestroy(s);
+        return rc;
     }
     uint32_t *d_f = nullptr, *d_t = nullptr;
     double *d_w = nullptr;

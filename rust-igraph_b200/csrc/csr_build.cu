@@ -20,6 +20,8 @@
 
 #include <algorithm>
 #include <cstdio>
+#include <cstdlib>
+#include <vector>
 
 #include "graph.cuh"
 #include "prims.cuh"
@@ -233,16 +235,18 @@ __global__ void __launch_bounds__(kThreads) rs_downsweep(const uint32_t *kin, co
     }
 }
 
-void radix_sort_pairs(uint32_t **keys, uint32_t **vals, uint32_t **keys_alt, uint32_t **vals_alt, uint64_t N,
-                      int key_bits, cudaStream_t s) {
-    if (N <= 1 || key_bits <= 0) return;
+// Stable passes over the 8-bit digits at shifts first_shift, +8, ... below
+// key_bits; the result ends in *keys / *vals.
+static void radix_passes(uint32_t **keys, uint32_t **vals, uint32_t **keys_alt, uint32_t **vals_alt, uint64_t N,
+                         int first_shift, int key_bits, cudaStream_t s) {
+    if (N <= 1 || key_bits <= first_shift) return;
     uint64_t tiles = (N + kRsTile - 1) / kRsTile;
     uint64_t G = std::min<uint64_t>(tiles, 148u * 8u);
     uint64_t chunk_tiles = (tiles + G - 1) / G;
     uint64_t chunk = chunk_tiles * kRsTile;
     G = (N + chunk - 1) / chunk;
     uint32_t *counts = dalloc<uint32_t>(256 * G, s);
-    for (int shift = 0; shift < key_bits; shift += 8) {
+    for (int shift = first_shift; shift < key_bits; shift += 8) {
         rs_upsweep<<<(unsigned)G, kThreads, 0, s>>>(*keys, N, chunk, shift, counts, (uint32_t)G);
         scan_single_block<<<1, 1024, 0, s>>>(counts, 256 * G, nullptr);
         rs_downsweep<<<(unsigned)G, kThreads, 0, s>>>(*keys, *vals, *keys_alt, *vals_alt, N, chunk, shift, counts,
@@ -252,6 +256,25 @@ void radix_sort_pairs(uint32_t **keys, uint32_t **vals, uint32_t **keys_alt, uin
         std::swap(*vals, *vals_alt);
     }
     dfree(counts, s);
+}
+
+void radix_sort_pairs(uint32_t **keys, uint32_t **vals, uint32_t **keys_alt, uint32_t **vals_alt, uint64_t N,
+                      int key_bits, cudaStream_t s) {
+    radix_passes(keys, vals, keys_alt, vals_alt, N, 0, key_bits, s);
+}
+
+// One stable pass on the 8-bit digit at `shift`: (keys, vals) -> (keys_out,
+// vals_out).
+static void radix_pass_pairs(uint32_t *keys, uint32_t *vals, uint32_t *keys_out, uint32_t *vals_out, uint64_t N,
+                             int shift, cudaStream_t s) {
+    if (N <= 1) {
+        if (N == 1) {
+            PRG_CUDA(cudaMemcpyAsync(keys_out, keys, 4, cudaMemcpyDeviceToDevice, s));
+            PRG_CUDA(cudaMemcpyAsync(vals_out, vals, 4, cudaMemcpyDeviceToDevice, s));
+        }
+        return;
+    }
+    radix_passes(&keys, &vals, &keys_out, &vals_out, N, shift, shift + 8, s);
 }
 
 // ------------------------------------------------------------------ CSR
@@ -340,6 +363,7 @@ __global__ void __launch_bounds__(kDegThreads) out_degree_kernel(const uint32_t 
     for (uint32_t i = threadIdx.x; i < kDegBins; i += kDegThreads) bins[i] = 0u;
     __syncthreads();
     auto add = [&](uint32_t v) {
+        if (v >= n) return;  // out-of-range ids are reported by the caller's range check
         if (v < kDegBins) atomicAdd_block(&bins[v], 1u);
         else atomicAdd(&deg[v], 1u);
     };
@@ -523,6 +547,64 @@ static int bits_for(uint32_t maxkey) {
     return b;
 }
 
+// Divisors, dangling count, maximum in-degree and row-blocks of a graph whose
+// row_ptr / col (/ weights) and deg are built; strength (weighted graphs, n
+// entries, freed here) holds the out-strengths.
+static void finish_graph(DeviceGraph &g, double *&strength, cudaStream_t s) {
+    const uint32_t n = g.n;
+    const unsigned gn = grid_for(n, kThreads);
+    PRG_CUDA(cudaMallocAsync((void **)&g.dval, std::max<uint64_t>(n, 1) * 8, s));
+    PRG_CUDA(cudaMallocAsync((void **)&g.inv32, std::max<uint64_t>(n, 1) * 4, s));
+    uint32_t *d_nd = dalloc<uint32_t>(2, s);
+    PRG_CUDA(cudaMemsetAsync(d_nd, 0, 8, s));
+    finish_degrees<<<gn, kThreads, 0, s>>>(n, g.deg, strength, g.weighted, g.dval, g.inv32, d_nd);
+    max_degree_kernel<<<gn, kThreads, 0, s>>>(g.row_ptr, n, d_nd + 1);
+    PRG_CUDA(cudaGetLastError());
+    uint32_t hnd[2];
+    PRG_CUDA(cudaMemcpyAsync(hnd, d_nd, 8, cudaMemcpyDeviceToHost, s));
+    dfree(strength, s);
+    dfree(d_nd, s);
+    PRG_CUDA(cudaStreamSynchronize(s));
+    g.n_dangling = hnd[0];
+    g.max_in_degree = hnd[1];
+    build_row_blocks(g, g.capw, g.shortmax, g.split, s);
+}
+
+// Degree-sorted relabelling of the vertices when g.relabel asks for it (1) or
+// the degree distribution is skewed (2: max degree >= 32 x mean, n >= 4096):
+// g.perm (new -> old), g.iperm (old -> new) and g.deg in new ids.  Needs
+// g.deg (out-degree) and g.arcs.  Returns whether it relabelled.
+static bool relabel_vertices(DeviceGraph &g, cudaStream_t s) {
+    const uint32_t n = g.n;
+    if (n < 2 || g.relabel == 0) return false;
+    const unsigned gn = grid_for(n, kThreads);
+    uint32_t *d_mx = dalloc<uint32_t>(1, s), maxdeg = 0;
+    PRG_CUDA(cudaMemsetAsync(d_mx, 0, 4, s));
+    max_u32_kernel<<<gn, kThreads, 0, s>>>(g.deg, n, d_mx);
+    PRG_CUDA(cudaMemcpyAsync(&maxdeg, d_mx, 4, cudaMemcpyDeviceToHost, s));
+    PRG_CUDA(cudaStreamSynchronize(s));
+    dfree(d_mx, s);
+    const double mean = (double)g.arcs / (double)n;
+    const bool skewed = n >= 4096 && (double)maxdeg >= 32.0 * (mean > 1.0 ? mean : 1.0);
+    if (g.relabel != 1 && !skewed) return false;
+    uint32_t *pk = dalloc<uint32_t>(n, s), *pv = dalloc<uint32_t>(n, s);
+    uint32_t *pk1 = dalloc<uint32_t>(n, s), *pv1 = dalloc<uint32_t>(n, s);
+    relabel_keys<<<gn, kThreads, 0, s>>>(g.deg, n, maxdeg, pk, pv);
+    radix_sort_pairs(&pk, &pv, &pk1, &pv1, n, bits_for(maxdeg), s);
+    PRG_CUDA(cudaMallocAsync((void **)&g.perm, (uint64_t)n * 4, s));
+    PRG_CUDA(cudaMallocAsync((void **)&g.iperm, (uint64_t)n * 4, s));
+    PRG_CUDA(cudaMemcpyAsync(g.perm, pv, (uint64_t)n * 4, cudaMemcpyDeviceToDevice, s));
+    uint32_t *deg_new = dalloc<uint32_t>(n, s);
+    relabel_finish<<<gn, kThreads, 0, s>>>(g.perm, g.deg, n, g.iperm, deg_new);
+    cudaFreeAsync(g.deg, s);
+    g.deg = deg_new;
+    dfree(pk, s);
+    dfree(pv, s);
+    dfree(pk1, s);
+    dfree(pv1, s);
+    return true;
+}
+
 void build_graph(DeviceGraph &g, const uint32_t *d_from, const uint32_t *d_to, const double *d_w, cudaStream_t s) {
     cudaEvent_t e0, e1;
     PRG_CUDA(cudaEventCreate(&e0));
@@ -545,37 +627,12 @@ void build_graph(DeviceGraph &g, const uint32_t *d_from, const uint32_t *d_to, c
     // is built from becomes (ef, et)
     const uint32_t *ef = d_from, *et = d_to;
     uint32_t *rf = nullptr, *rt = nullptr;
-    if (n >= 2 && g.relabel != 0) {
-        uint32_t *d_mx = dalloc<uint32_t>(1, s), maxdeg = 0;
-        PRG_CUDA(cudaMemsetAsync(d_mx, 0, 4, s));
-        max_u32_kernel<<<gn, kThreads, 0, s>>>(g.deg, n, d_mx);
-        PRG_CUDA(cudaMemcpyAsync(&maxdeg, d_mx, 4, cudaMemcpyDeviceToHost, s));
-        PRG_CUDA(cudaStreamSynchronize(s));
-        dfree(d_mx, s);
-        const double mean = (double)arcs / (double)n;
-        const bool skewed = n >= 4096 && (double)maxdeg >= 32.0 * (mean > 1.0 ? mean : 1.0);
-        if (g.relabel == 1 || skewed) {
-            uint32_t *pk = dalloc<uint32_t>(n, s), *pv = dalloc<uint32_t>(n, s);
-            uint32_t *pk1 = dalloc<uint32_t>(n, s), *pv1 = dalloc<uint32_t>(n, s);
-            relabel_keys<<<gn, kThreads, 0, s>>>(g.deg, n, maxdeg, pk, pv);
-            radix_sort_pairs(&pk, &pv, &pk1, &pv1, n, bits_for(maxdeg), s);
-            PRG_CUDA(cudaMallocAsync((void **)&g.perm, (uint64_t)n * 4, s));
-            PRG_CUDA(cudaMallocAsync((void **)&g.iperm, (uint64_t)n * 4, s));
-            PRG_CUDA(cudaMemcpyAsync(g.perm, pv, (uint64_t)n * 4, cudaMemcpyDeviceToDevice, s));
-            uint32_t *deg_new = dalloc<uint32_t>(n, s);
-            relabel_finish<<<gn, kThreads, 0, s>>>(g.perm, g.deg, n, g.iperm, deg_new);
-            cudaFreeAsync(g.deg, s);
-            g.deg = deg_new;
-            rf = dalloc<uint32_t>(m, s);
-            rt = dalloc<uint32_t>(m, s);
-            if (m) relabel_edges<<<ge, kThreads, 0, s>>>(d_from, d_to, m, g.iperm, rf, rt);
-            ef = rf;
-            et = rt;
-            dfree(pk, s);
-            dfree(pv, s);
-            dfree(pk1, s);
-            dfree(pv1, s);
-        }
+    if (relabel_vertices(g, s)) {
+        rf = dalloc<uint32_t>(m, s);
+        rt = dalloc<uint32_t>(m, s);
+        if (m) relabel_edges<<<ge, kThreads, 0, s>>>(d_from, d_to, m, g.iperm, rf, rt);
+        ef = rf;
+        et = rt;
     }
 
     // arcs in edge order, then stable sort by destination
@@ -633,27 +690,264 @@ void build_graph(DeviceGraph &g, const uint32_t *d_from, const uint32_t *d_to, c
     dfree(rf, s);
     dfree(rt, s);
 
-    PRG_CUDA(cudaMallocAsync((void **)&g.dval, std::max<uint64_t>(n, 1) * 8, s));
-    PRG_CUDA(cudaMallocAsync((void **)&g.inv32, std::max<uint64_t>(n, 1) * 4, s));
-    uint32_t *d_nd = dalloc<uint32_t>(2, s);
-    PRG_CUDA(cudaMemsetAsync(d_nd, 0, 8, s));
-    finish_degrees<<<gn, kThreads, 0, s>>>(n, g.deg, strength, weighted, g.dval, g.inv32, d_nd);
-    max_degree_kernel<<<gn, kThreads, 0, s>>>(g.row_ptr, n, d_nd + 1);
-    PRG_CUDA(cudaGetLastError());
-    uint32_t hnd[2];
-    PRG_CUDA(cudaMemcpyAsync(hnd, d_nd, 8, cudaMemcpyDeviceToHost, s));
-    dfree(strength, s);
-    dfree(d_nd, s);
-    PRG_CUDA(cudaStreamSynchronize(s));
-    g.n_dangling = hnd[0];
-    g.max_in_degree = hnd[1];
-
-    build_row_blocks(g, g.capw, g.shortmax, g.split, s);
+    finish_graph(g, strength, s);
     PRG_CUDA(cudaEventRecord(e1, s));
     PRG_CUDA(cudaEventSynchronize(e1));
     PRG_CUDA(cudaEventElapsedTime(&g.build_ms, e0, e1));
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
+}
+
+// ------------------------------------------------------------------ streamed build from host edges
+//
+// The edge list arrives in chunks (host -> device copies on a side stream);
+// each chunk is processed while the next one is in flight.  An arc's final
+// CSR position is
+//     row_ptr[dst] + (arcs into dst in earlier chunks) + (rank among the
+//                                                          chunk's arcs into dst)
+// and only row_ptr needs the whole list.  So every chunk is stably sorted by
+// destination on arrival, its ranks are added to the running per-destination
+// counts (off[arc], cnt[dst]), and after the last chunk one scan of the
+// counts and one scatter place every arc.  Within a row the arcs keep their
+// arc order, exactly as the sort of the whole list in build_graph leaves
+// them, so both builds produce the same CSR.
+
+// Start of each destination's run in the sorted chunk: base = cnt - i.
+__global__ void chunk_ranks_begin(const uint32_t *keys, uint64_t N, uint32_t n, const uint32_t *cnt, uint32_t *base) {
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < N; i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t k = keys[i];
+        if (k < n && (i == 0 || keys[i - 1] != k)) base[k] = cnt[k] - (uint32_t)i;
+    }
+}
+
+// off[arc] = arcs into its destination before it; the run's last arc
+// advances cnt.  (u32 arithmetic: base + i is the true count.)
+__global__ void chunk_ranks_end(const uint32_t *keys, const uint32_t *vals, uint64_t N, uint32_t n,
+                                const uint32_t *base, uint32_t *cnt, uint32_t *off) {
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < N; i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t k = keys[i];
+        if (k >= n) continue;
+        const uint32_t b = base[k];
+        off[vals[i]] = b + (uint32_t)i;
+        if (i + 1 == N || keys[i + 1] != k) cnt[k] = b + (uint32_t)i + 1u;
+    }
+}
+
+__global__ void gather_u32_kernel(uint32_t *dst, const uint32_t *src, const uint32_t *idx, uint32_t n) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) dst[i] = src[idx[i]];
+}
+
+// The arcs' final positions, row_ptr[dst] + off[arc], are a permutation of
+// [0, arcs).  Writing each arc straight to its position would be one random
+// 4-byte HBM write per arc.  Instead: (1) arc_positions writes (position,
+// value) pairs in arc order; (2) one stable radix pass on the position's top
+// 8 bits groups them into 256 windows of consecutive positions; (3)
+// place_arcs writes each window while its slice of col sits in L2.
+// value = the relabelled source (unweighted) or the arc id (weighted: the
+// source and the edge weight are fetched when placing).
+__global__ void arc_positions(const uint32_t *from, const uint32_t *to, uint64_t arcs, bool directed, bool weighted,
+                              const uint32_t *iperm, const uint32_t *row_ptr, const uint32_t *off, uint32_t *pos,
+                              uint32_t *val) {
+    for (uint64_t a = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; a < arcs;
+         a += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t e = directed ? a : (a >> 1);
+        uint32_t dst = to[e], src = from[e];
+        if (!directed && (a & 1u) == 0u) {
+            dst = from[e];
+            src = to[e];
+        }
+        if (iperm) {
+            dst = iperm[dst];
+            src = iperm[src];
+        }
+        pos[a] = row_ptr[dst] + off[a];
+        val[a] = weighted ? (uint32_t)a : src;
+    }
+}
+
+__global__ void place_arcs(const uint32_t *pos, const uint32_t *val, uint64_t arcs, bool directed,
+                           const uint32_t *from, const uint32_t *to, const double *w, const uint32_t *iperm,
+                           uint32_t *col, double *w64, float *w32) {
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < arcs; i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t p = pos[i];
+        if (p >= arcs) continue;  // never for a consistent build
+        if (!w) {
+            col[p] = val[i];
+            continue;
+        }
+        const uint32_t a = val[i];
+        const uint64_t e = directed ? a : (a >> 1);
+        uint32_t src = (directed || (a & 1u)) ? from[e] : to[e];
+        if (iperm) src = iperm[src];
+        col[p] = src;
+        const double we = w[e];
+        w64[p] = we;
+        w32[p] = (float)we;
+    }
+}
+
+bool build_graph_host(DeviceGraph &g, const uint32_t *h_from, const uint32_t *h_to, const double *h_w, cudaStream_t s,
+                      uint32_t *max_endpoint) {
+    cudaEvent_t e0, e1;
+    PRG_CUDA(cudaEventCreate(&e0));
+    PRG_CUDA(cudaEventCreate(&e1));
+    PRG_CUDA(cudaEventRecord(e0, s));
+    const uint32_t n = g.n;
+    const uint64_t m = g.m;
+    const bool directed = g.directed, weighted = h_w != nullptr;
+    g.weighted = weighted;
+    const uint64_t arcs = directed ? m : 2 * m;
+    g.arcs = arcs;
+    const uint64_t chunk = std::max<uint64_t>(kStreamChunkMin, (m + kStreamChunks - 1) / kStreamChunks);
+    const uint64_t nchunks = (m + chunk - 1) / chunk;
+    const uint64_t chunk_arcs = directed ? chunk : 2 * chunk;
+    const int key_bits = bits_for(n ? n - 1 : 0);
+
+    uint32_t *d_from = dalloc<uint32_t>(m, s), *d_to = dalloc<uint32_t>(m, s);
+    double *d_w = weighted ? dalloc<double>(m, s) : nullptr;
+    PRG_CUDA(cudaMallocAsync((void **)&g.deg, std::max<uint64_t>(n, 1) * 4, s));
+    PRG_CUDA(cudaMemsetAsync(g.deg, 0, std::max<uint64_t>(n, 1) * 4, s));
+    uint32_t *cnt = dalloc<uint32_t>(n, s), *base = dalloc<uint32_t>(n, s), *off = dalloc<uint32_t>(arcs, s);
+    PRG_CUDA(cudaMemsetAsync(cnt, 0, std::max<uint64_t>(n, 1) * 4, s));
+    uint32_t *d_mx = dalloc<uint32_t>(1, s);
+    PRG_CUDA(cudaMemsetAsync(d_mx, 0, 4, s));
+    uint32_t *ka = dalloc<uint32_t>(chunk_arcs, s), *va = dalloc<uint32_t>(chunk_arcs, s);
+    uint32_t *kb = dalloc<uint32_t>(chunk_arcs, s), *vb = dalloc<uint32_t>(chunk_arcs, s);
+
+    cudaStream_t cs;
+    PRG_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+    std::vector<cudaEvent_t> ev(nchunks + 1);
+    for (cudaEvent_t &e : ev) PRG_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    // the copy stream starts once the allocations above are usable
+    PRG_CUDA(cudaEventRecord(ev[nchunks], s));
+    PRG_CUDA(cudaStreamWaitEvent(cs, ev[nchunks], 0));
+    for (uint64_t c = 0; c < nchunks; c++) {
+        const uint64_t b = c * chunk, len = std::min(chunk, m - b);
+        const uint64_t a0 = directed ? b : 2 * b, la = directed ? len : 2 * len;
+        PRG_CUDA(cudaMemcpyAsync(d_from + b, h_from + b, len * 4, cudaMemcpyHostToDevice, cs));
+        PRG_CUDA(cudaMemcpyAsync(d_to + b, h_to + b, len * 4, cudaMemcpyHostToDevice, cs));
+        if (weighted) PRG_CUDA(cudaMemcpyAsync(d_w + b, h_w + b, len * 8, cudaMemcpyHostToDevice, cs));
+        PRG_CUDA(cudaEventRecord(ev[c], cs));
+        PRG_CUDA(cudaStreamWaitEvent(s, ev[c], 0));
+        const unsigned gl = grid_for(len, kThreads), gla = grid_for(la, kThreads);
+        max_u32_kernel<<<gl, kThreads, 0, s>>>(d_from + b, (uint32_t)len, d_mx);
+        max_u32_kernel<<<gl, kThreads, 0, s>>>(d_to + b, (uint32_t)len, d_mx);
+        out_degree_kernel<<<148 * 2, kDegThreads, 0, s>>>(d_from + b, d_to + b, len, directed, n, g.deg);
+        make_arcs<<<gl, kThreads, 0, s>>>(d_from + b, d_to + b, len, directed, true, ka, va);
+        uint32_t *k0 = ka, *v0 = va, *k1 = kb, *v1 = vb;
+        radix_sort_pairs(&k0, &v0, &k1, &v1, la, key_bits, s);
+        chunk_ranks_begin<<<gla, kThreads, 0, s>>>(k0, la, n, cnt, base);
+        chunk_ranks_end<<<gla, kThreads, 0, s>>>(k0, v0, la, n, base, cnt, off + a0);
+        PRG_CUDA(cudaGetLastError());
+    }
+    const bool trace = std::getenv("PRG_TRACE") != nullptr;
+    cudaEvent_t t_copy = nullptr, t_loop = nullptr, t_tail[4] = {};
+    if (trace) {
+        PRG_CUDA(cudaEventCreate(&t_copy));
+        PRG_CUDA(cudaEventCreate(&t_loop));
+        for (cudaEvent_t &e : t_tail) PRG_CUDA(cudaEventCreate(&e));
+        PRG_CUDA(cudaEventRecord(t_copy, cs));
+        PRG_CUDA(cudaEventRecord(t_loop, s));
+    }
+    uint32_t mx = 0;
+    PRG_CUDA(cudaMemcpyAsync(&mx, d_mx, 4, cudaMemcpyDeviceToHost, s));
+    PRG_CUDA(cudaStreamSynchronize(s));
+    PRG_CUDA(cudaStreamSynchronize(cs));
+    for (cudaEvent_t &e : ev) cudaEventDestroy(e);
+    cudaStreamDestroy(cs);
+    dfree(ka, s);
+    dfree(va, s);
+    dfree(kb, s);
+    dfree(vb, s);
+    dfree(d_mx, s);
+    *max_endpoint = mx;
+    if (m > 0 && mx >= n) {
+        dfree(d_from, s);
+        dfree(d_to, s);
+        dfree(d_w, s);
+        dfree(cnt, s);
+        dfree(base, s);
+        dfree(off, s);
+        if (trace) {
+            cudaEventDestroy(t_copy);
+            cudaEventDestroy(t_loop);
+            for (cudaEvent_t &e : t_tail) cudaEventDestroy(e);
+        }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        return false;
+    }
+
+    const unsigned gn = grid_for(n, kThreads), ga = grid_for(arcs, kThreads);
+    const bool relabelled = relabel_vertices(g, s);
+    if (trace) PRG_CUDA(cudaEventRecord(t_tail[0], s));
+    uint32_t *rows = cnt;
+    if (relabelled) {
+        gather_u32_kernel<<<gn, kThreads, 0, s>>>(base, cnt, g.perm, n);  // base is free now
+        rows = base;
+    }
+    PRG_CUDA(cudaMallocAsync((void **)&g.row_ptr, (uint64_t)(n + 1) * 4, s));
+    exclusive_scan_u32(rows, g.row_ptr, n, s);
+    const uint64_t padded = arcs + kColPad;
+    PRG_CUDA(cudaMallocAsync((void **)&g.col, padded * 4, s));
+    PRG_CUDA(cudaMemsetAsync(g.col, 0, padded * 4, s));
+    if (weighted) {
+        PRG_CUDA(cudaMallocAsync((void **)&g.w64, padded * 8, s));
+        PRG_CUDA(cudaMallocAsync((void **)&g.w32, padded * 4, s));
+        PRG_CUDA(cudaMemsetAsync(g.w64, 0, padded * 8, s));
+        PRG_CUDA(cudaMemsetAsync(g.w32, 0, padded * 4, s));
+    }
+    if (trace) PRG_CUDA(cudaEventRecord(t_tail[1], s));
+    if (arcs) {
+        const uint32_t *ip = relabelled ? g.iperm : nullptr;
+        uint32_t *pk = dalloc<uint32_t>(arcs, s), *pv = dalloc<uint32_t>(arcs, s);
+        uint32_t *pk1 = dalloc<uint32_t>(arcs, s), *pv1 = dalloc<uint32_t>(arcs, s);
+        arc_positions<<<ga, kThreads, 0, s>>>(d_from, d_to, arcs, directed, weighted, ip, g.row_ptr, off, pk, pv);
+        const int pbits = bits_for((uint32_t)(arcs - 1));
+        radix_pass_pairs(pk, pv, pk1, pv1, arcs, std::max(0, pbits - 8), s);
+        place_arcs<<<ga, kThreads, 0, s>>>(pk1, pv1, arcs, directed, d_from, d_to, d_w, ip, g.col, g.w64, g.w32);
+        dfree(pk, s);
+        dfree(pv, s);
+        dfree(pk1, s);
+        dfree(pv1, s);
+    }
+    PRG_CUDA(cudaGetLastError());
+    if (trace) PRG_CUDA(cudaEventRecord(t_tail[2], s));
+    double *strength = nullptr;
+    if (weighted) {
+        // undirected only: arcs out of u are exactly the arcs into u (same weights)
+        strength = dalloc<double>(n, s);
+        row_weight_sums<<<grid_for((uint64_t)n * 32, kThreads), kThreads, 0, s>>>(g.row_ptr, g.w64, nullptr, n,
+                                                                               strength);
+    }
+    dfree(d_from, s);
+    dfree(d_to, s);
+    dfree(d_w, s);
+    dfree(cnt, s);
+    dfree(base, s);
+    dfree(off, s);
+    finish_graph(g, strength, s);
+    PRG_CUDA(cudaEventRecord(e1, s));
+    PRG_CUDA(cudaEventSynchronize(e1));
+    PRG_CUDA(cudaEventElapsedTime(&g.build_ms, e0, e1));
+    if (trace) {
+        float c = 0, l = 0, r = 0, sc = 0, sca = 0;
+        cudaEventElapsedTime(&c, e0, t_copy);
+        cudaEventElapsedTime(&l, e0, t_loop);
+        cudaEventElapsedTime(&r, t_loop, t_tail[0]);
+        cudaEventElapsedTime(&sc, t_tail[0], t_tail[1]);
+        cudaEventElapsedTime(&sca, t_tail[1], t_tail[2]);
+        std::fprintf(stderr,
+                     "[prg] streamed build: %llu chunks, copies done %.2f ms, chunk work done %.2f ms, relabel %.2f, "
+                     "scan+alloc %.2f, scatter %.2f, finish %.2f, total %.2f ms\n",
+                     (unsigned long long)nchunks, c, l, r, sc, sca, g.build_ms - l - r - sc - sca, g.build_ms);
+        cudaEventDestroy(t_copy);
+        cudaEventDestroy(t_loop);
+        for (cudaEvent_t &e : t_tail) cudaEventDestroy(e);
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return true;
 }
 
 void free_graph(DeviceGraph &g) {

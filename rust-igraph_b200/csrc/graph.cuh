@@ -53,6 +53,18 @@ struct DeviceGraph {
 // stream-ordered allocator.
 void build_graph(DeviceGraph &g, const uint32_t *d_from, const uint32_t *d_to, const double *d_w,
                  cudaStream_t s);
+// The same graph from HOST edge arrays, streamed: chunks of the edge list are
+// copied on a side stream and sorted on arrival while the next chunk is in
+// flight, then one scan and one scatter finish the CSR (identical to
+// build_graph's).  Not for directed weighted graphs (their out-strengths
+// need a second sort by source).  Returns false, with nothing built, when
+// an endpoint is >= n (its maximum in *max_endpoint).
+bool build_graph_host(DeviceGraph &g, const uint32_t *h_from, const uint32_t *h_to, const double *h_w, cudaStream_t s,
+                      uint32_t *max_endpoint);
+constexpr uint64_t kStreamChunks = 16;             // chunks of the streamed build
+constexpr uint64_t kStreamChunkMin = 1ull << 22;   // smallest chunk (edges)
+constexpr uint64_t kStreamMinEdges = 1ull << 23;   // smaller edge lists take the one-shot build
+
 // Rebuilds only the row-blocks with new tuning (autotuner).
 void build_row_blocks(DeviceGraph &g, uint32_t capw, uint32_t shortmax, uint32_t split, cudaStream_t s);
 void free_graph(DeviceGraph &g);
