@@ -142,6 +142,24 @@ int32_t prg_eigenvector_centrality_weighted(uint32_t n, uint64_t m, const uint32
                                             int32_t directed, const double *weights, uint64_t weights_len,
                                             double *out, double *eigenvalue);
 
+/* EigenvectorMode (eigenvector.rs:63-76). */
+enum prg_eig_mode { PRG_EIG_OUT = 0, PRG_EIG_IN = 1, PRG_EIG_ALL = 2 };
+
+/* rust-igraph eigenvector_centrality_full() (eigenvector.rs:238-285), with
+ * eigenvector_centrality_directed / _directed_weighted as its cases;
+ * weights may be NULL (unweighted), else weights_len must equal m, and
+ * negative weights give PRG_ERR_UNSUPPORTED.  Undirected graphs take the
+ * symmetric path whatever the mode.  On directed graphs, Out / In walk the
+ * in- / out-edges of each vertex (directed_path, eigenvector.rs:539-720):
+ * a DAG gives 1 on vertices with zero out- / in-strength and eigenvalue 0;
+ * otherwise a power iteration shifted by the largest row sum + 1 from the
+ * in- / out-strengths, L1 stop 1e-12, and an eigenvalue <= 1e-12 gives the
+ * zero vector.  All on a directed graph iterates over the out-edges, as the
+ * reference's symmetric routines see a directed graph there. */
+int32_t prg_eigenvector_centrality_full(uint32_t n, uint64_t m, const uint32_t *from, const uint32_t *to,
+                                        int32_t directed, int32_t mode, const double *weights, uint64_t weights_len,
+                                        double *out, double *eigenvalue);
+
 /* rust-igraph hub_and_authority_scores_weighted() (hits.rs:245-585), non-negative
  * weights: W W^T power iteration from the out-strengths (directed) or the
  * weighted eigenvector centrality with the squared eigenvalue (undirected). */

@@ -76,6 +76,9 @@ def lib():
         L.or_hits_weighted.restype = C.c_int
         L.or_hits_weighted.argtypes = [C.c_uint32, C.c_uint64, _u32p, _u32p, _f64p, C.c_int, _f64p, _f64p,
                                        C.POINTER(C.c_double)]
+        L.or_eigenvector_full.restype = C.c_int
+        L.or_eigenvector_full.argtypes = [C.c_uint32, C.c_uint64, _u32p, _u32p, C.c_int, C.c_int, C.c_void_p,
+                                          _f64p, C.POINTER(C.c_double)]
         L.or_infomap_flow.restype = C.c_int
         L.or_infomap_flow.argtypes = [C.c_uint32, C.c_uint64, _u32p, _u32p, C.c_int, C.c_void_p, C.c_void_p,
                                       _f64p]
@@ -231,6 +234,21 @@ def hub_and_authority_scores_weighted(n, frm, to, weights, directed):
     it = lib().or_hits_weighted(n, len(f), f, t, w if len(w) else np.zeros(1), int(directed), hub, auth,
                                 C.byref(lam))
     return hub[:n], auth[:n], lam.value, it
+
+
+EIG_OUT, EIG_IN, EIG_ALL = 0, 1, 2
+
+
+def eigenvector_centrality_full(n, frm, to, directed, mode, weights=None):
+    """rust-igraph eigenvector_centrality_full (eigenvector.rs:238-285,
+    539-756), non-negative weights: (vector, eigenvalue, iterations)."""
+    f, t = _edges(frm, to)
+    w = None if weights is None else np.ascontiguousarray(weights, dtype=np.float64)
+    out = np.zeros(max(n, 1), np.float64)
+    lam = C.c_double(0.0)
+    it = lib().or_eigenvector_full(n, len(f), f, t, int(directed), int(mode),
+                                   None if w is None else w.ctypes.data_as(C.c_void_p), out, C.byref(lam))
+    return out[:n], lam.value, it
 
 
 def infomap_flow(n, frm, to, directed, edge_weights=None, vertex_weights=None):

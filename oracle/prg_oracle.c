@@ -1177,3 +1177,190 @@ int or_infomap_flow(uint32_t n, uint64_t m, const uint32_t *from, const uint32_t
     free(orp); free(ov); free(ow); free(str); free(cur); free(t); free(irp); free(iu); free(iw); free(pr); free(buf);
     return it;
 }
+
+/* Kahn's algorithm: 1 when the directed graph has no cycle (a loop is one). */
+static int is_dag(uint32_t n, uint64_t m, const uint32_t *from, const uint32_t *to) {
+    uint64_t *orp = (uint64_t *)calloc((size_t)n + 1, sizeof(uint64_t));
+    uint32_t *oc = (uint32_t *)malloc((m ? m : 1) * sizeof(uint32_t));
+    uint32_t *indeg = (uint32_t *)calloc(n ? n : 1, sizeof(uint32_t));
+    uint32_t *queue = (uint32_t *)malloc((n ? n : 1) * sizeof(uint32_t));
+    for (uint64_t e = 0; e < m; e++) {
+        orp[from[e] + 1]++;
+        indeg[to[e]]++;
+    }
+    for (uint32_t v = 0; v < n; v++) orp[v + 1] += orp[v];
+    uint64_t *cur = (uint64_t *)malloc(((size_t)n + 1) * sizeof(uint64_t));
+    memcpy(cur, orp, ((size_t)n + 1) * sizeof(uint64_t));
+    for (uint64_t e = 0; e < m; e++) oc[cur[from[e]]++] = to[e];
+    uint32_t head = 0, tail = 0;
+    for (uint32_t v = 0; v < n; v++)
+        if (indeg[v] == 0) queue[tail++] = v;
+    while (head < tail) {
+        const uint32_t u = queue[head++];
+        for (uint64_t p = orp[u]; p < orp[u + 1]; p++)
+            if (--indeg[oc[p]] == 0) queue[tail++] = oc[p];
+    }
+    free(orp); free(oc); free(indeg); free(queue); free(cur);
+    return tail == n;
+}
+
+/* eigenvector_centrality_full (eigenvector.rs:238-285), non-negative weights
+ * (w may be NULL = unit): mode 0 = Out, 1 = In, 2 = All.
+ * Undirected graphs take All.  All on a directed graph runs the "undirected"
+ * routines over what graph.neighbors / graph.incident return there, the
+ * out-edges only (graph.rs:808-819, 1212-1217): unweighted x' = x + sum over
+ * ascending out-neighbours (eps 1e-14); weighted x' = x + sum over out-edges
+ * in (target, edge id) order with an out-strength seed (eps 1e-12).
+ * Out / In (directed_path, eigenvector.rs:539-720): m == 0 or all-zero
+ * weights -> ones; a DAG -> 1 on vertices with zero out-strength (Out) / zero
+ * in-strength (In), 0 elsewhere, eigenvalue 0; else walk the in-edges (Out)
+ * / out-edges (In) of v in edge order, seed |strength| of that walk
+ * (all-zero -> ones) max-normalised, shift = max(max walk strength, 1) + 1,
+ * x' = shift x + M x max-normalised until the L1 change < 1e-12 (5000
+ * iterations); eigenvalue = x.Mx / x.x, and <= 1e-12 gives zeros. */
+int or_eigenvector_full(uint32_t n, uint64_t m, const uint32_t *from, const uint32_t *to, int directed, int mode,
+                        const double *w, double *out, double *eigval) {
+    if (eigval) *eigval = 0.0;
+    if (!directed) {
+        if (w) return or_eigenvector_weighted(n, m, from, to, w, out, eigval);
+        return or_eigenvector_centrality(n, m, from, to, out, eigval);
+    }
+    if (n == 0) return 0;
+    if (mode == 2) {
+        if (m == 0 || n == 1) {
+            for (uint32_t i = 0; i < n; i++) out[i] = 1.0;
+            return 0;
+        }
+        int allzero = 1;
+        if (w)
+            for (uint64_t e = 0; e < m; e++) allzero &= w[e] == 0.0;
+        if (w && allzero) {
+            for (uint32_t i = 0; i < n; i++) out[i] = 1.0;
+            return 0;
+        }
+        uint64_t *rp;
+        uint32_t *oth, *eid;
+        edge_rows(n, m, from, to, &rp, &oth, &eid); /* out-edges by (source, target, id) */
+        double *x = (double *)malloc(n * sizeof(double)), *xn = (double *)malloc(n * sizeof(double));
+        int any = 0;
+        for (uint32_t v = 0; v < n; v++) {
+            if (!w) {
+                x[v] = 1.0;
+                continue;
+            }
+            double s = 0.0;
+            for (uint64_t p = rp[v]; p < rp[v + 1]; p++) s += w[eid[p]];
+            x[v] = s != 0.0 ? fabs(s) : 0.0;
+            any |= x[v] != 0.0;
+        }
+        if (w) {
+            if (!any)
+                for (uint32_t v = 0; v < n; v++) x[v] = 1.0;
+            rescale_max_abs(x, n);
+        }
+        const double eps = w ? 1e-12 : 1e-14;
+        int it = 0;
+        while (it < 5000) {
+            it++;
+            for (uint32_t v = 0; v < n; v++) {
+                double s = x[v];
+                for (uint64_t p = rp[v]; p < rp[v + 1]; p++) s += (w ? w[eid[p]] : 1.0) * x[oth[p]];
+                xn[v] = s;
+            }
+            rescale_max_abs(xn, n);
+            double diff = 0.0;
+            for (uint32_t v = 0; v < n; v++) diff += fabs(xn[v] - x[v]);
+            double *t = x; x = xn; xn = t;
+            if (diff < eps) break;
+        }
+        double num = 0.0, den = 0.0;
+        for (uint32_t v = 0; v < n; v++) {
+            double s = 0.0;
+            for (uint64_t p = rp[v]; p < rp[v + 1]; p++) s += (w ? w[eid[p]] : 1.0) * x[oth[p]];
+            num += x[v] * s;
+            den += x[v] * x[v];
+        }
+        if (eigval) *eigval = den > 0.0 ? num / den : 0.0;
+        rescale_max_abs(x, n);
+        for (uint32_t v = 0; v < n; v++) out[v] = x[v] < 0.0 ? 0.0 : x[v];
+        free(rp); free(oth); free(eid); free(x); free(xn);
+        return it;
+    }
+    /* Out / In */
+    int allzero = 1;
+    if (w)
+        for (uint64_t e = 0; e < m; e++) allzero &= w[e] == 0.0;
+    if (m == 0 || (w && allzero)) {
+        for (uint32_t i = 0; i < n; i++) out[i] = 1.0;
+        return 0;
+    }
+    if (is_dag(n, m, from, to)) {
+        double *st = (double *)calloc(n, sizeof(double));
+        for (uint64_t e = 0; e < m; e++) st[mode == 0 ? from[e] : to[e]] += w ? w[e] : 1.0;
+        for (uint32_t v = 0; v < n; v++) out[v] = st[v] == 0.0 ? 1.0 : 0.0;
+        free(st);
+        return 0;
+    }
+    /* walk[v]: (edge, neighbour) in edge order; Out: in-edges u->v, In: out-edges v->u */
+    const uint32_t *key = mode == 0 ? to : from, *nbr = mode == 0 ? from : to;
+    uint64_t *rp = (uint64_t *)calloc((size_t)n + 1, sizeof(uint64_t));
+    uint32_t *wn = (uint32_t *)malloc(m * sizeof(uint32_t)), *we = (uint32_t *)malloc(m * sizeof(uint32_t));
+    for (uint64_t e = 0; e < m; e++) rp[key[e] + 1]++;
+    for (uint32_t v = 0; v < n; v++) rp[v + 1] += rp[v];
+    uint64_t *cur = (uint64_t *)malloc(((size_t)n + 1) * sizeof(uint64_t));
+    memcpy(cur, rp, ((size_t)n + 1) * sizeof(uint64_t));
+    for (uint64_t e = 0; e < m; e++) {
+        wn[cur[key[e]]] = nbr[e];
+        we[cur[key[e]]++] = (uint32_t)e;
+    }
+    double *x = (double *)malloc(n * sizeof(double)), *xn = (double *)malloc(n * sizeof(double));
+    double row_norm = 0.0;
+    int any = 0;
+    for (uint32_t v = 0; v < n; v++) {
+        double s = 0.0, sa = 0.0;
+        for (uint64_t p = rp[v]; p < rp[v + 1]; p++) {
+            const double wv = w ? w[we[p]] : 1.0;
+            s += wv;
+            sa += fabs(wv);
+        }
+        x[v] = s != 0.0 ? fabs(s) : 0.0;
+        any |= x[v] != 0.0;
+        if (sa > row_norm) row_norm = sa;
+    }
+    if (!any)
+        for (uint32_t v = 0; v < n; v++) x[v] = 1.0;
+    rescale_max_abs(x, n);
+    const double shift = (row_norm > 1.0 ? row_norm : 1.0) + 1.0;
+    int it = 0;
+    while (it < 5000) {
+        it++;
+        for (uint32_t v = 0; v < n; v++) {
+            double s = shift * x[v];
+            for (uint64_t p = rp[v]; p < rp[v + 1]; p++) s += (w ? w[we[p]] : 1.0) * x[wn[p]];
+            xn[v] = s;
+        }
+        rescale_max_abs(xn, n);
+        double diff = 0.0;
+        for (uint32_t v = 0; v < n; v++) diff += fabs(xn[v] - x[v]);
+        double *t = x; x = xn; xn = t;
+        if (diff < 1e-12) break;
+    }
+    double num = 0.0, den = 0.0;
+    for (uint32_t v = 0; v < n; v++) {
+        double s = 0.0;
+        for (uint64_t p = rp[v]; p < rp[v + 1]; p++) s += (w ? w[we[p]] : 1.0) * x[wn[p]];
+        num += x[v] * s;
+        den += x[v] * x[v];
+    }
+    double lam = den > 0.0 ? num / den : 0.0;
+    if (lam <= 1e-12) {
+        lam = 0.0;
+        for (uint32_t v = 0; v < n; v++) out[v] = 0.0;
+    } else {
+        rescale_max_abs(x, n);
+        for (uint32_t v = 0; v < n; v++) out[v] = x[v] < 0.0 ? 0.0 : x[v];
+    }
+    if (eigval) *eigval = lam;
+    free(rp); free(wn); free(we); free(cur); free(x); free(xn);
+    return it;
+}

@@ -530,6 +530,58 @@ int32_t prg_eigenvector_centrality_weighted(uint32_t n, uint64_t m, const uint32
     PRG_GUARD_END
 }
 
+int32_t prg_eigenvector_centrality_full(uint32_t n, uint64_t m, const uint32_t *from, const uint32_t *to,
+                                        int32_t directed, int32_t mode, const double *weights, uint64_t weights_len,
+                                        double *out, double *eigenvalue) {
+    g_err.clear();
+    PRG_GUARD_BEGIN
+    if (eigenvalue) *eigenvalue = 0.0;
+    if (weights && weights_len != m)  // eigenvector.rs:272-283
+        return fail(PRG_ERR_INVALID_ARGUMENT, "weights vector length (" + std::to_string(weights_len) +
+                                                  ") not equal to number of edges (" + std::to_string(m) + ")");
+    if (mode < PRG_EIG_OUT || mode > PRG_EIG_ALL) return fail(PRG_ERR_INVALID_ARGUMENT, "unknown eigenvector mode");
+    if (!directed) {  // eigenvector.rs:252-264: undirected input takes the symmetric path
+        if (weights) return prg_eigenvector_centrality_weighted(n, m, from, to, 0, weights, m, out, eigenvalue);
+        return prg_eigenvector_centrality(n, m, from, to, 0, out, eigenvalue);
+    }
+    if (n == 0) return PRG_OK;
+    const bool all = mode == PRG_EIG_ALL;
+    if (m == 0 || (all && n == 1) || (weights && all_zero(weights, m))) {
+        for (uint32_t i = 0; i < n; i++) out[i] = 1.0;
+        return PRG_OK;
+    }
+    if (weights && any_negative(weights, m))
+        return fail(PRG_ERR_UNSUPPORTED, "negative weights are not supported by the GPU eigenvector centrality");
+    // Out walks the in-edges of v: the graph's own in-CSR.  In, and All on a
+    // directed graph (graph.neighbors / incident give out-edges there), walk
+    // the out-edges: the in-CSR of the reversed graph.
+    const bool reverse = mode != PRG_EIG_OUT;
+    prg_graph *h = nullptr;
+    int32_t rc = create_from_host(n, m, reverse ? to : from, reverse ? from : to, weights, 1, &h);
+    if (rc != PRG_OK) return rc;
+    try {
+        cudaStream_t s = h->stream;
+        if (!h->d_out) PRG_CUDA(cudaMallocAsync((void **)&h->d_out, (uint64_t)n * 8, s));
+        prg::eig::Result r;
+        if (!all) {
+            r = prg::eig::eigenvector_directed(h->g, h->ws, h->d_out, s);
+        } else if (weights) {
+            r = prg::eig::eigenvector_centrality(h->g, h->ws, h->d_out, s, true, 1e-12);  // eigenvector.rs:375-538
+        } else {
+            r = prg::eig::eigenvector_centrality(h->g, h->ws, h->d_out, s);  // eigenvector.rs:286-372
+        }
+        PRG_CUDA(cudaMemcpyAsync(out, h->d_out, (uint64_t)n * 8, cudaMemcpyDeviceToHost, s));
+        PRG_CUDA(cudaStreamSynchronize(s));
+        if (eigenvalue) *eigenvalue = r.eigenvalue;
+    } catch (...) {
+        destroy(h);
+        throw;
+    }
+    destroy(h);
+    return PRG_OK;
+    PRG_GUARD_END
+}
+
 int32_t prg_hub_and_authority_scores_weighted(uint32_t n, uint64_t m, const uint32_t *from, const uint32_t *to,
                                               int32_t directed, const double *weights, uint64_t weights_len,
                                               double *hub, double *authority, double *eigenvalue) {

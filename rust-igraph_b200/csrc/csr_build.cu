@@ -245,10 +245,10 @@ static void radix_passes(uint32_t **keys, uint32_t **vals, uint32_t **keys_alt, 
     uint64_t chunk_tiles = (tiles + G - 1) / G;
     uint64_t chunk = chunk_tiles * kRsTile;
     G = (N + chunk - 1) / chunk;
-    uint32_t *counts = dalloc<uint32_t>(256 * G, s);
+    uint32_t *counts = dalloc<uint32_t>(256 * G + 1, s);  // + the scan's total
     for (int shift = first_shift; shift < key_bits; shift += 8) {
         rs_upsweep<<<(unsigned)G, kThreads, 0, s>>>(*keys, N, chunk, shift, counts, (uint32_t)G);
-        scan_single_block<<<1, 1024, 0, s>>>(counts, 256 * G, nullptr);
+        exclusive_scan_u32(counts, counts, 256 * G, s);  // in place: each tile is loaded before it is written
         rs_downsweep<<<(unsigned)G, kThreads, 0, s>>>(*keys, *vals, *keys_alt, *vals_alt, N, chunk, shift, counts,
                                                      (uint32_t)G);
         PRG_CUDA(cudaGetLastError());

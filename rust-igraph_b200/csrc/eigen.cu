@@ -162,6 +162,82 @@ __global__ void degree_seed_kernel(const uint32_t *deg, const double *dval, uint
     }
 }
 
+// ---- directed eigenvector centrality (eigenvector.rs:539-756)
+
+// x[v] = |sum of row v's arc weights| (row length when unweighted), one warp
+// per row; records (max x, max sum of |w| over a row, 0, 0).
+__global__ void __launch_bounds__(kNT) rowsum_seed_kernel(const uint32_t *row_ptr, const double *w64, uint32_t n,
+                                                          double *x, double4 *recs) {
+    __shared__ double sm[2][kNT / 32];
+    const uint32_t lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    double mx = 0.0, mnorm = 0.0;
+    for (uint32_t v = (blockIdx.x * kNT + threadIdx.x) >> 5; v < n; v += (gridDim.x * kNT) >> 5) {
+        const uint32_t lo = row_ptr[v], hi = row_ptr[v + 1];
+        double s = 0.0, sa = 0.0;
+        if (w64) {
+            for (uint32_t p = lo + lane; p < hi; p += 32) {
+                s += w64[p];
+                sa += fabs(w64[p]);
+            }
+            s = warp_sum(s);
+            sa = warp_sum(sa);
+        } else {
+            s = sa = (double)(hi - lo);
+        }
+        if (lane == 0) {
+            x[v] = fabs(s);
+            mx = fmax(mx, fabs(s));
+            mnorm = fmax(mnorm, sa);
+        }
+    }
+    if (lane == 0) {
+        sm[0][wid] = mx;
+        sm[1][wid] = mnorm;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int k = 1; k < kNT / 32; k++) {
+            mx = fmax(mx, sm[0][k]);
+            mnorm = fmax(mnorm, sm[1][k]);
+        }
+        recs[blockIdx.x] = make_double4(mx, mnorm, 0.0, 0.0);
+    }
+}
+
+// DAG test: sinks are peeled round by round over the in-CSR (a vertex whose
+// remaining out-degree reaches 0 joins the next frontier); every vertex is
+// peeled exactly when the graph has no cycle.  A self-loop keeps its vertex.
+__global__ void peel_init(const uint32_t *deg, uint32_t n, uint32_t *odeg, uint32_t *front, uint32_t *cnt) {
+    for (uint32_t v = blockIdx.x * kNT + threadIdx.x; v < n; v += gridDim.x * kNT) {
+        odeg[v] = deg[v];
+        if (deg[v] == 0u) front[atomicAdd(cnt, 1u)] = v;
+    }
+}
+
+__global__ void peel_round(const uint32_t *row_ptr, const uint32_t *col, uint32_t n, uint32_t *odeg,
+                           const uint32_t *front_in, const uint32_t *cnt_in, uint32_t *front_out, uint32_t *cnt_out,
+                           unsigned long long *removed) {
+    const uint32_t k = *cnt_in;
+    if (blockIdx.x == 0 && threadIdx.x == 0) *removed += k;
+    for (uint32_t i = blockIdx.x * kNT + threadIdx.x; i < k; i += gridDim.x * kNT) {
+        const uint32_t v = front_in[i];
+        for (uint32_t p = row_ptr[v]; p < row_ptr[v + 1]; p++) {
+            const uint32_t u = col[p];
+            if (atomicSub(&odeg[u], 1u) == 1u) {
+                const uint32_t slot = atomicAdd(cnt_out, 1u);
+                if (slot < n) front_out[slot] = u;
+            }
+        }
+    }
+}
+
+__global__ void zero_u32_kernel(uint32_t *p) { *p = 0u; }
+
+// x[v] = 1 where the graph's own out-strength (dval) is 0, else 0.
+__global__ void sentinel_kernel(const double *dval, uint32_t n, double *x) {
+    for (uint32_t v = blockIdx.x * kNT + threadIdx.x; v < n; v += gridDim.x * kNT) x[v] = dval[v] == 0.0 ? 1.0 : 0.0;
+}
+
 // ---- Infomap flow model (infomap.rs:299-355)
 constexpr double kTau = 0.15;
 
@@ -326,23 +402,37 @@ static double rayleigh(const Product &pr, const double *x, double *tmp, double4 
     return den > 0.0 ? num / den : 0.0;
 }
 
-// Seeds x from degrees or strengths and max-normalises it; an all-zero seed
-// becomes all ones.
-static void seed(const DeviceGraph &g, bool strength, double *x, double4 *recs, double4 *part, cudaStream_t s) {
-    degree_seed_kernel<<<kNB, kNT, 0, s>>>(g.deg, strength ? g.dval : nullptr, g.n, x, recs);
+// Seeds x with the absolute row sums of g's in-CSR (the strength the walk
+// over each row sees) and max-normalises it; an all-zero seed becomes all
+// ones.  Returns the largest row sum of |w| (the shift's row norm).
+static double seed(const DeviceGraph &g, double *x, double4 *recs, double4 *part, cudaStream_t s) {
+    rowsum_seed_kernel<<<kNB, kNT, 0, s>>>(g.row_ptr, g.weighted ? g.w64 : nullptr, g.n, x, recs);
     PRG_CUDA(cudaGetLastError());
     std::vector<double4> h(kNB);
     PRG_CUDA(cudaMemcpyAsync(h.data(), recs, kNB * sizeof(double4), cudaMemcpyDeviceToHost, s));
     PRG_CUDA(cudaStreamSynchronize(s));
-    double mx = 0.0;
-    for (const double4 &q : h) mx = std::max(mx, q.x);
+    double mx = 0.0, norm = 0.0;
+    for (const double4 &q : h) {
+        mx = std::max(mx, q.x);
+        norm = std::max(norm, q.y);
+    }
     if (mx == 0.0) fill_kernel<<<kNB, kNT, 0, s>>>(x, g.n, 1.0);
     else normalise_kernel<<<kNB, kNT, 0, s>>>(g.n, recs, kNB, nullptr, 0, x, nullptr, part, nullptr);
     PRG_CUDA(cudaGetLastError());
+    return norm;
 }
 
 Result eigenvector_centrality(const DeviceGraph &g, Workspace &ws, double *d_out, cudaStream_t s,
                               bool strength_seed, double eps) {
+    EigOpts o;
+    o.rowsum_seed = strength_seed;
+    o.eps = eps;
+    return eigenvector_centrality(g, ws, d_out, s, o);
+}
+
+Result eigenvector_centrality(const DeviceGraph &g, Workspace &ws, double *d_out, cudaStream_t s, const EigOpts &o) {
+    const bool strength_seed = o.rowsum_seed;
+    const double eps = o.eps;
     Result r;
     const uint32_t n = g.n;
     workspace_ensure(ws, g, s);
@@ -359,15 +449,17 @@ Result eigenvector_centrality(const DeviceGraph &g, Workspace &ws, double *d_out
         init.max_iter = 5000;
         init.eps = eps;
         PRG_CUDA(cudaMemcpyAsync(d_st, &init, sizeof(State), cudaMemcpyHostToDevice, s));
+        double shift = 1.0;
         if (strength_seed) {
-            seed(g, true, x[0], recs, part, s);
+            const double norm = seed(g, x[0], recs, part, s);
+            if (o.auto_shift) shift = std::max(norm, 1.0) + 1.0;  // eigenvector.rs:627-643
         } else {
             fill_kernel<<<kNB, kNT, 0, s>>>(x[0], n, 1.0);
             PRG_CUDA(cudaGetLastError());
         }
         run_until_done(d_st, h_st, init.max_iter, s, [&](uint32_t it) {
             const int q = (int)(it & 1u);
-            product(pr, x[q], x[q ^ 1], 1.0, recs, &d_st->done, s);
+            product(pr, x[q], x[q ^ 1], shift, recs, &d_st->done, s);
             normalise_kernel<<<kNB, kNT, 0, s>>>(n, recs, grid, ws.hub_rec, g.nhub, x[q ^ 1], x[q], part, d_st);
             check_kernel<<<1, 256, 0, s>>>(part, kNB, d_st, q ^ 1);
             PRG_CUDA(cudaGetLastError());
@@ -376,6 +468,11 @@ Result eigenvector_centrality(const DeviceGraph &g, Workspace &ws, double *d_out
         const double *xf = h_st[0].iters ? x[h_st[0].final_buf] : x[0];
         double *other = xf == x[0] ? x[1] : x[0];
         r.eigenvalue = rayleigh(pr, xf, other, recs, s);
+        if (o.zero_fallback && r.eigenvalue <= 1e-12) {
+            // eigenvector.rs:695-699: a (numerically) nilpotent matrix gives zeros
+            r.eigenvalue = 0.0;
+            fill_kernel<<<kNB, kNT, 0, s>>>(const_cast<double *>(xf), n, 0.0);
+        }
         clamp_kernel<<<kNB, kNT, 0, s>>>(const_cast<double *>(xf), n);
         PRG_CUDA(cudaGetLastError());
         if (g.perm) gather_f64(d_out, xf, g.iperm, n, s);
@@ -394,6 +491,59 @@ Result eigenvector_centrality(const DeviceGraph &g, Workspace &ws, double *d_out
     release(d_st, s);
     PRG_CUDA(cudaStreamSynchronize(s));
     return r;
+}
+
+bool is_dag(const DeviceGraph &g, cudaStream_t s) {
+    const uint32_t n = g.n;
+    if (n == 0) return true;
+    uint32_t *odeg = alloc<uint32_t>(n, s), *front[2] = {alloc<uint32_t>(n, s), alloc<uint32_t>(n, s)};
+    uint32_t *cnt = alloc<uint32_t>(2, s);
+    unsigned long long *removed = alloc<unsigned long long>(1, s);
+    PRG_CUDA(cudaMemsetAsync(cnt, 0, 8, s));
+    PRG_CUDA(cudaMemsetAsync(removed, 0, 8, s));
+    peel_init<<<kNB, kNT, 0, s>>>(g.deg, n, odeg, front[0], cnt);
+    PRG_CUDA(cudaGetLastError());
+    uint32_t h_next = 0;
+    unsigned long long h_removed = 0;
+    for (uint32_t r = 0;; r++) {
+        const int c = (int)(r & 1u);
+        peel_round<<<kNB, kNT, 0, s>>>(g.row_ptr, g.col, n, odeg, front[c], cnt + c, front[c ^ 1], cnt + (c ^ 1),
+                                       removed);
+        zero_u32_kernel<<<1, 1, 0, s>>>(cnt + c);
+        PRG_CUDA(cudaGetLastError());
+        if ((r & 15u) == 15u) {  // poll: empty frontier -> done
+            PRG_CUDA(cudaMemcpyAsync(&h_next, cnt + (c ^ 1), 4, cudaMemcpyDeviceToHost, s));
+            PRG_CUDA(cudaStreamSynchronize(s));
+            if (h_next == 0u) break;
+        }
+    }
+    PRG_CUDA(cudaMemcpyAsync(&h_removed, removed, 8, cudaMemcpyDeviceToHost, s));
+    PRG_CUDA(cudaStreamSynchronize(s));
+    release(odeg, s);
+    release(front[0], s);
+    release(front[1], s);
+    release(cnt, s);
+    release(removed, s);
+    return h_removed == (unsigned long long)n;
+}
+
+Result eigenvector_directed(const DeviceGraph &g, Workspace &ws, double *d_out, cudaStream_t s) {
+    if (is_dag(g, s)) {  // eigenvector.rs:570-575, 721-756
+        double *x = alloc<double>(g.n, s);
+        sentinel_kernel<<<kNB, kNT, 0, s>>>(g.dval, g.n, x);
+        PRG_CUDA(cudaGetLastError());
+        if (g.perm) gather_f64(d_out, x, g.iperm, g.n, s);
+        else PRG_CUDA(cudaMemcpyAsync(d_out, x, (uint64_t)g.n * 8, cudaMemcpyDeviceToDevice, s));
+        release(x, s);
+        PRG_CUDA(cudaStreamSynchronize(s));
+        return Result{};
+    }
+    EigOpts o;
+    o.rowsum_seed = true;
+    o.eps = 1e-12;
+    o.auto_shift = true;
+    o.zero_fallback = true;
+    return eigenvector_centrality(g, ws, d_out, s, o);
 }
 
 Result infomap_flow(const DeviceGraph &g, Workspace &ws, const double *d_t, double *d_out, cudaStream_t s) {

@@ -14,11 +14,28 @@ struct Result {
     double eigenvalue = 0.0;
 };
 
-// Undirected graph g: x (caller ids) into d_out[n]; eigenvalue = x.Ax / x.x
-// (A weighted when g is).  strength_seed: start from the vertex strengths
-// (all ones when they are all zero) instead of ones; eps: L1 stop.
+// Options of the shifted power iteration x' = shift x + A x over g's in-CSR.
+struct EigOpts {
+    bool rowsum_seed = false;    // start from |row sums| of A (all ones when zero) instead of ones
+    double eps = 1e-14;          // L1 stop
+    bool auto_shift = false;     // shift = max(max row sum of |A|, 1) + 1 (else 1)
+    bool zero_fallback = false;  // eigenvalue <= 1e-12 -> zero vector, eigenvalue 0
+};
+
+// Power iteration on g: x (caller ids) into d_out[n]; eigenvalue = x.Ax / x.x
+// (A weighted when g is), negatives clamped.  For an undirected g the row
+// sums are the vertex strengths.
+Result eigenvector_centrality(const DeviceGraph &g, Workspace &ws, double *d_out, cudaStream_t s, const EigOpts &o);
 Result eigenvector_centrality(const DeviceGraph &g, Workspace &ws, double *d_out, cudaStream_t s,
                               bool strength_seed = false, double eps = 1e-14);
+
+// True when the directed graph g has no cycle.
+bool is_dag(const DeviceGraph &g, cudaStream_t s);
+
+// Directed eigenvector centrality over g's in-CSR (eigenvector.rs:539-756,
+// non-negative weights): Out mode on a graph is this on the graph itself, In
+// mode this on its reverse.  A DAG gives 1 where g's out-strength is 0.
+Result eigenvector_directed(const DeviceGraph &g, Workspace &ws, double *d_out, cudaStream_t s);
 
 // Directed graph g and its reverse rev (both without relabelling):
 // hub and authority vectors into d_hub / d_auth; eigenvalue of A A^T.

@@ -201,6 +201,9 @@ def lib():
     L.prg_hub_and_authority_scores_weighted.restype = C.c_int32
     L.prg_hub_and_authority_scores_weighted.argtypes = [C.c_uint32, C.c_uint64, u32p, u32p, C.c_int32, f64p,
                                                         C.c_uint64, f64p, f64p, f64p]
+    L.prg_eigenvector_centrality_full.restype = C.c_int32
+    L.prg_eigenvector_centrality_full.argtypes = [C.c_uint32, C.c_uint64, u32p, u32p, C.c_int32, C.c_int32, f64p,
+                                                  C.c_uint64, f64p, f64p]
     L.prg_infomap_flow.restype = C.c_int32
     L.prg_infomap_flow.argtypes = [C.c_uint32, C.c_uint64, u32p, u32p, C.c_int32, f64p, C.c_uint64, f64p,
                                    C.c_uint64, f64p, C.POINTER(C.c_uint32)]
@@ -380,6 +383,39 @@ def eigenvector_centrality_weighted(graph: Graph, weights, with_eigenvalue: bool
     _check(lib().prg_eigenvector_centrality_weighted(n, len(f), _ptr(f), _ptr(t), int(graph.is_directed()),
                                                      _ptr(w) if len(w) else None, len(w), _ptr(out), C.byref(lam)))
     return (out[:n], lam.value) if with_eigenvalue else out[:n]
+
+
+EIG_OUT, EIG_IN, EIG_ALL = 0, 1, 2  # EigenvectorMode (eigenvector.rs:63-76)
+
+
+@dataclass
+class EigenvectorScores:
+    vector: np.ndarray
+    eigenvalue: float
+
+
+def eigenvector_centrality_full(graph: Graph, mode: int, weights=None) -> EigenvectorScores:
+    """rust-igraph ``eigenvector_centrality_full`` (eigenvector.rs:238-285) on
+    the GPU; non-negative weights."""
+    n = graph.vcount()
+    f, t = graph.edge_arrays()
+    w = None if weights is None else np.ascontiguousarray(weights, dtype=np.float64)
+    out = np.empty(max(n, 1), np.float64)
+    lam = C.c_double()
+    _check(lib().prg_eigenvector_centrality_full(n, len(f), _ptr(f), _ptr(t), int(graph.is_directed()), int(mode),
+                                                 None if w is None else (_ptr(w) if len(w) else _ptr(np.zeros(1))),
+                                                 0 if w is None else len(w), _ptr(out), C.byref(lam)))
+    return EigenvectorScores(out[:n], lam.value)
+
+
+def eigenvector_centrality_directed(graph: Graph, mode: int) -> EigenvectorScores:
+    """rust-igraph ``eigenvector_centrality_directed`` (eigenvector.rs:189-194)."""
+    return eigenvector_centrality_full(graph, mode)
+
+
+def eigenvector_centrality_directed_weighted(graph: Graph, mode: int, weights) -> EigenvectorScores:
+    """rust-igraph ``eigenvector_centrality_directed_weighted`` (eigenvector.rs:218-224)."""
+    return eigenvector_centrality_full(graph, mode, weights)
 
 
 def hub_and_authority_scores_weighted(graph: Graph, weights) -> HitsScores:

@@ -95,3 +95,42 @@ def test_hits_weighted_reference_cases():
     h, a, lam, _ = O.hub_and_authority_scores_weighted(4, f, t, np.ones(4), False)
     hu, au, lu, _ = O.hub_and_authority_scores(4, f, t, False)
     assert np.allclose(h, hu, atol=1e-6) and np.array_equal(h, a) and abs(lam - lu) < 1e-6
+
+
+def test_eigenvector_directed_reference_cases():
+    # eigenvector.rs:880-1052 (directed) and :960-985 (dispatch)
+    full = O.eigenvector_centrality_full
+    k5 = [(u, v) for u in range(5) for v in range(5) if u != v]
+    x, lam, _ = full(5, *E(k5), True, O.EIG_OUT)
+    assert np.allclose(x, 1.0, atol=1e-9) and abs(lam - 4.0) < 1e-6
+    k10 = [(u, v) for u in range(10) for v in range(10) if u != v]
+    x, lam, _ = full(10, *E(k10), True, O.EIG_OUT)
+    assert np.allclose(x, 1.0, atol=1e-9) and abs(lam - 9.0) < 1e-9
+    x, lam, _ = full(5, *E([(0, v) for v in range(1, 5)]), True, O.EIG_OUT)  # DAG: sinks
+    assert list(x) == [0.0, 1.0, 1.0, 1.0, 1.0] and lam == 0.0
+    x, lam, _ = full(5, *E([(v, 0) for v in range(1, 5)]), True, O.EIG_IN)  # DAG, In: sources
+    assert list(x) == [0.0, 1.0, 1.0, 1.0, 1.0] and lam == 0.0
+    x, lam, _ = full(5, *E([(v, 0) for v in range(1, 5)]), True, O.EIG_OUT)
+    assert list(x) == [1.0, 0.0, 0.0, 0.0, 0.0] and lam == 0.0
+    x, lam, _ = full(4, *E([(0, 1), (1, 2), (2, 3), (3, 0), (1, 3)]), True, O.EIG_OUT)
+    assert abs(lam - 1.220744) < 1e-4 and np.allclose(x, [0.819173, 0.671044, 0.549700, 1.0], atol=1e-3)
+    x, lam, _ = full(5, *E([]), True, O.EIG_OUT)
+    assert np.all(x == 1.0) and lam == 0.0
+    x, lam, _ = full(50, *E([(i, (i + 1) % 50) for i in range(50)]), True, O.EIG_OUT)
+    assert abs(lam - 1.0) < 1e-9 and x.max() - x.min() < 1e-9
+    # undirected input takes the symmetric path whatever the mode
+    tri = E([(0, 1), (1, 2), (2, 0)])
+    a = full(3, *tri, False, O.EIG_OUT)
+    b = full(3, *tri, False, O.EIG_ALL)
+    assert np.allclose(a[0], 1.0, atol=1e-9) and np.array_equal(a[0], b[0]) and a[1] == b[1]
+    # In mode on G is Out mode on the reversed graph
+    rng = np.random.default_rng(4)
+    f = rng.integers(0, 300, 3000).astype(np.uint32)
+    t = rng.integers(0, 300, 3000).astype(np.uint32)
+    xi, li, _ = full(300, f, t, True, O.EIG_IN)
+    xo, lo, _ = full(300, t, f, True, O.EIG_OUT)
+    assert np.array_equal(xi, xo) and li == lo
+    # unit weights are the unweighted iteration
+    xw, lw, _ = full(300, f, t, True, O.EIG_OUT, weights=np.ones(3000))
+    xu, lu, _ = full(300, f, t, True, O.EIG_OUT)
+    assert np.array_equal(xw, xu) and lw == lu

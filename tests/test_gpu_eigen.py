@@ -192,3 +192,83 @@ def test_hits_weighted_directed_matches_restatement(cuda_ok, kind):
     assert np.max(np.abs(s.hub - h)) <= TOL and np.max(np.abs(s.authority - a)) <= TOL
     assert abs(s.eigenvalue - lam) <= TOL * abs(lam)
     assert s.hub.max() == 1.0 and s.authority.max() == 1.0 and s.hub.min() >= 0.0
+
+
+def test_directed_reference_unit_cases(cuda_ok):
+    # eigenvector.rs:880-1052, through the GPU entry point
+    full = ig.eigenvector_centrality_full
+    k5 = G(5, [(u, v) for u in range(5) for v in range(5) if u != v], True)
+    s = ig.eigenvector_centrality_directed(k5, ig.EIG_OUT)
+    assert np.allclose(s.vector, 1.0, atol=1e-9) and abs(s.eigenvalue - 4.0) < 1e-6
+    k10 = G(10, [(u, v) for u in range(10) for v in range(10) if u != v], True)
+    s = ig.eigenvector_centrality_directed(k10, ig.EIG_OUT)
+    assert np.allclose(s.vector, 1.0, atol=1e-9) and abs(s.eigenvalue - 9.0) < 1e-9
+    out_star, in_star = G(5, [(0, v) for v in range(1, 5)], True), G(5, [(v, 0) for v in range(1, 5)], True)
+    s = ig.eigenvector_centrality_directed(out_star, ig.EIG_OUT)
+    assert list(s.vector) == [0.0, 1.0, 1.0, 1.0, 1.0] and s.eigenvalue == 0.0
+    s = ig.eigenvector_centrality_directed(in_star, ig.EIG_IN)
+    assert list(s.vector) == [0.0, 1.0, 1.0, 1.0, 1.0] and s.eigenvalue == 0.0
+    s = ig.eigenvector_centrality_directed(in_star, ig.EIG_OUT)
+    assert list(s.vector) == [1.0, 0.0, 0.0, 0.0, 0.0] and s.eigenvalue == 0.0
+    chord = G(4, [(0, 1), (1, 2), (2, 3), (3, 0), (1, 3)], True)
+    s = ig.eigenvector_centrality_directed(chord, ig.EIG_OUT)
+    assert abs(s.eigenvalue - 1.220744) < 1e-4
+    assert np.allclose(s.vector, [0.819173, 0.671044, 0.549700, 1.0], atol=1e-3)
+    s = ig.eigenvector_centrality_directed(G(5, [], True), ig.EIG_OUT)
+    assert np.all(s.vector == 1.0) and s.eigenvalue == 0.0
+    cyc = G(50, [(i, (i + 1) % 50) for i in range(50)], True)
+    s = ig.eigenvector_centrality_directed(cyc, ig.EIG_OUT)
+    assert abs(s.eigenvalue - 1.0) < 1e-9 and s.vector.max() - s.vector.min() < 1e-9
+    tri = G(3, [(0, 1), (1, 2), (2, 0)], False)
+    a, b = full(tri, ig.EIG_OUT), full(tri, ig.EIG_ALL)
+    assert np.allclose(a.vector, 1.0, atol=1e-9) and np.array_equal(a.vector, b.vector)
+    r = ig.eigenvector_centrality_directed_weighted(G(3, [(0, 1), (1, 2), (2, 0)], True), ig.EIG_ALL, [1.0] * 3)
+    assert len(r.vector) == 3
+    with pytest.raises(ig.InvalidArgument, match=r"weights vector length \(1\) not equal to number of edges \(3\)"):
+        ig.eigenvector_centrality_directed_weighted(G(3, [(0, 1), (1, 2), (2, 0)], True), ig.EIG_OUT, [1.0])
+    with pytest.raises(ig.Unsupported, match="negative weights"):
+        ig.eigenvector_centrality_directed_weighted(G(3, [(0, 1), (1, 2), (2, 0)], True), ig.EIG_OUT,
+                                                    [1.0, -1.0, 1.0])
+
+
+def _directed_case(kind):
+    if kind == "rmat":
+        n = 1 << 13
+        f, t = O.rmat(13, 8 * n, seed=51)
+    elif kind == "er":
+        n = 6000
+        f, t = O.erdos_renyi_gnm(n, 24_000, True, False, 52)
+    elif kind == "dag":  # edges from lower to higher ids: a DAG with many sinks and sources
+        rng = np.random.default_rng(53)
+        n = 20_000
+        a = rng.integers(0, n, 80_000)
+        b = rng.integers(0, n, 80_000)
+        keep = a != b
+        f = np.minimum(a, b)[keep].astype(np.uint32)
+        t = np.maximum(a, b)[keep].astype(np.uint32)
+    else:  # cycles through a hub plus loops
+        rng = np.random.default_rng(54)
+        n = 4000
+        f = rng.integers(0, n, 16_000).astype(np.uint32)
+        t = rng.integers(0, n, 16_000).astype(np.uint32)
+        f[:100] = t[:100] = 9
+    return n, f, t
+
+
+@pytest.mark.parametrize("kind", ["rmat", "er", "dag", "loops"])
+@pytest.mark.parametrize("mode", [0, 1, 2])
+@pytest.mark.parametrize("weighted", [False, True])
+def test_directed_matches_restatement(cuda_ok, kind, mode, weighted):
+    n, f, t = _directed_case(kind)
+    g = ig.Graph.from_edge_arrays(n, f, t, True)
+    gf, gt = g.edge_arrays()
+    w = None
+    if weighted:
+        w = O.uniform_weights(len(gf), 55, 0.0, 2.0)
+        w[::11] = 0.0
+    s = ig.eigenvector_centrality_full(g, mode, w)
+    ref, lam, _ = O.eigenvector_centrality_full(n, gf, gt, True, mode, weights=w)
+    assert np.max(np.abs(s.vector - ref)) <= TOL, np.max(np.abs(s.vector - ref))
+    assert abs(s.eigenvalue - lam) <= TOL * max(abs(lam), 1.0)
+    if kind == "dag" and mode != 2:
+        assert s.eigenvalue == 0.0 and set(np.unique(s.vector)) <= {0.0, 1.0}
