@@ -679,6 +679,9 @@ void Net::alloc(cudaStream_t s) {
     PRG_CUDA(cudaMallocAsync((void **)&m, kParams * 4, s));
     PRG_CUDA(cudaMallocAsync((void **)&v, kParams * 4, s));
     PRG_CUDA(cudaMallocAsync((void **)&w, sizeof(Ws), s));
+    // loss_grad writes only the used rows of W3 / entries of B3, so the
+    // gradient's other slots must start (and stay) zero
+    PRG_CUDA(cudaMemsetAsync(G, 0, kParams * 4, s));
     PRG_CUDA(cudaMemsetAsync(m, 0, kParams * 4, s));
     PRG_CUDA(cudaMemsetAsync(v, 0, kParams * 4, s));
     PRG_CUDA(cudaMemsetAsync(w, 0, sizeof(Ws), s));
