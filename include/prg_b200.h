@@ -136,8 +136,10 @@ int32_t prg_hub_and_authority_scores(uint32_t n, uint64_t m, const uint32_t *fro
 /* rust-igraph eigenvector_centrality_weighted() (eigenvector.rs:157-168, 375-538):
  * undirected, weights[e] per edge (weights_len must equal m); shifted power
  * iteration x' = (W + I) x from the vertex strengths, L1 stop 1e-12.
- * Negative weights (which the reference follows with a signed pivot) give
- * PRG_ERR_UNSUPPORTED on this GPU path. */
+ * With a negative weight the iteration follows the reference's signed rules:
+ * each iterate is divided by its component of greatest magnitude with its
+ * sign (the lowest vertex id on ties), a zero strength on a vertex with
+ * edges seeds 1, and nothing is clamped. */
 int32_t prg_eigenvector_centrality_weighted(uint32_t n, uint64_t m, const uint32_t *from, const uint32_t *to,
                                             int32_t directed, const double *weights, uint64_t weights_len,
                                             double *out, double *eigenvalue);
@@ -147,8 +149,10 @@ enum prg_eig_mode { PRG_EIG_OUT = 0, PRG_EIG_IN = 1, PRG_EIG_ALL = 2 };
 
 /* rust-igraph eigenvector_centrality_full() (eigenvector.rs:238-285), with
  * eigenvector_centrality_directed / _directed_weighted as its cases;
- * weights may be NULL (unweighted), else weights_len must equal m, and
- * negative weights give PRG_ERR_UNSUPPORTED.  Undirected graphs take the
+ * weights may be NULL (unweighted), else weights_len must equal m; with a
+ * negative weight the reference's signed rules apply as in
+ * prg_eigenvector_centrality_weighted, and there is no DAG or zero-eigenvalue
+ * shortcut.  Undirected graphs take the
  * symmetric path whatever the mode.  On directed graphs, Out / In walk the
  * in- / out-edges of each vertex (directed_path, eigenvector.rs:539-720):
  * a DAG gives 1 on vertices with zero out- / in-strength and eigenvalue 0;
@@ -160,9 +164,12 @@ int32_t prg_eigenvector_centrality_full(uint32_t n, uint64_t m, const uint32_t *
                                         int32_t directed, int32_t mode, const double *weights, uint64_t weights_len,
                                         double *out, double *eigenvalue);
 
-/* rust-igraph hub_and_authority_scores_weighted() (hits.rs:245-585), non-negative
- * weights: W W^T power iteration from the out-strengths (directed) or the
- * weighted eigenvector centrality with the squared eigenvalue (undirected). */
+/* rust-igraph hub_and_authority_scores_weighted() (hits.rs:245-585): W W^T
+ * power iteration from the out-strengths (directed) or the weighted shifted
+ * iteration from the signed strengths with the squared Rayleigh quotient
+ * (undirected).  With a negative weight each iterate is divided by its
+ * signed component of greatest magnitude, which is then the eigenvalue
+ * estimate, and nothing is clamped. */
 int32_t prg_hub_and_authority_scores_weighted(uint32_t n, uint64_t m, const uint32_t *from, const uint32_t *to,
                                               int32_t directed, const double *weights, uint64_t weights_len,
                                               double *hub, double *authority, double *eigenvalue);

@@ -956,70 +956,131 @@ static void edge_rows(uint32_t n, uint64_t m, const uint32_t *key, const uint32_
     *eid_out = eid;
 }
 
-/* (W + I) x over undirected incidence: out-range then in-range of v */
-static double winc(uint32_t v, const uint64_t *orp, const uint32_t *ooth, const uint32_t *oeid, const uint64_t *irp,
-                   const uint32_t *ioth, const uint32_t *ieid, const double *w, const double *x) {
-    double s = 0.0;
-    for (uint64_t p = orp[v]; p < orp[v + 1]; p++) s += w[oeid[p]] * x[ooth[p]];
-    for (uint64_t p = irp[v]; p < irp[v + 1]; p++) s += w[ieid[p]] * x[ioth[p]];
-    return s;
+/* The signed component of greatest magnitude, the first in index order on
+ * ties (eigenvector.rs:464-476, hits.rs:399-411): the pivot with negative
+ * weights. */
+static double signed_pivot(const double *x, uint32_t n) {
+    double best = 0.0, sg = 0.0;
+    for (uint32_t i = 0; i < n; i++)
+        if (fabs(x[i]) > best) {
+            best = fabs(x[i]);
+            sg = x[i];
+        }
+    return sg;
 }
 
-/* Weighted undirected shifted power iteration with a strength seed
- * (eigenvector.rs:375-538 = hits.rs:470-553 for non-negative weights):
- * returns iterations; eps 1e-12, 5000 iterations; *eigval = x.Wx / x.x. */
+static int any_negative_w(const double *w, uint64_t m) {
+    for (uint64_t e = 0; e < m; e++)
+        if (w[e] < 0.0) return 1;
+    return 0;
+}
+
+/* The reference's "symmetric" weighted iteration over incident edges:
+ * undirected graphs walk the out-range then the in-range of v (a loop twice);
+ * out_only walks the out-edges alone, which is what graph.incident gives on a
+ * directed graph.  Seed: the strength s of v's incident edges, |s| for
+ * eigenvector centrality (eigenvector.rs:413-443) or s itself for HITS
+ * (hits.rs:483-503); with negative weights a zero strength on a non-empty
+ * list seeds 1; all zero -> ones; max-abs rescaled.  x' = x + W x, divided by
+ * the max |x'| (the signed pivot with negative weights), until the L1 change
+ * < 1e-12 or 5000 iterations.  Eigenvector form: eigenvalue = x.Wx / x.x,
+ * then rescale and (non-negative weights) clamp.  HITS form: clamp
+ * (non-negative weights), then eigenvalue = x.Wx / x.x of the result. */
+static int weighted_core(uint32_t n, uint64_t m, const uint32_t *from, const uint32_t *to, const double *w,
+                         int out_only, int hits_form, double *out, double *eigval) {
+    const int neg = any_negative_w(w, m);
+    uint64_t *orp, *irp = NULL;
+    uint32_t *ooth, *oeid, *ioth = NULL, *ieid = NULL;
+    edge_rows(n, m, from, to, &orp, &ooth, &oeid);
+    if (!out_only) edge_rows(n, m, to, from, &irp, &ioth, &ieid);
+    double *x = (double *)malloc(n * sizeof(double)), *xn = (double *)malloc(n * sizeof(double));
+    int any = 0;
+    for (uint32_t v = 0; v < n; v++) {
+        double s = 0.0;
+        uint64_t deg = orp[v + 1] - orp[v];
+        for (uint64_t p = orp[v]; p < orp[v + 1]; p++) s += w[oeid[p]];
+        if (!out_only) {
+            for (uint64_t p = irp[v]; p < irp[v + 1]; p++) s += w[ieid[p]];
+            deg += irp[v + 1] - irp[v];
+        }
+        if (s != 0.0) x[v] = hits_form ? s : fabs(s);
+        else x[v] = (neg && deg > 0) ? 1.0 : 0.0;
+        any |= x[v] != 0.0;
+    }
+    if (!any)
+        for (uint32_t v = 0; v < n; v++) x[v] = 1.0;
+    rescale_max_abs(x, n);
+#define WX(v, vec) ({                                                               \
+        double s_ = 0.0;                                                            \
+        for (uint64_t p = orp[v]; p < orp[v + 1]; p++) s_ += w[oeid[p]] * vec[ooth[p]];  \
+        if (!out_only)                                                              \
+            for (uint64_t p = irp[v]; p < irp[v + 1]; p++) s_ += w[ieid[p]] * vec[ioth[p]]; \
+        s_; })
+    int it = 0;
+    while (it < 5000) {
+        it++;
+        for (uint32_t v = 0; v < n; v++) xn[v] = x[v] + WX(v, x);
+        if (neg) {
+            const double pv = signed_pivot(xn, n);
+            if (pv != 0.0)
+                for (uint32_t v = 0; v < n; v++) xn[v] /= pv;
+        } else {
+            rescale_max_abs(xn, n);
+        }
+        double diff = 0.0;
+        for (uint32_t v = 0; v < n; v++) diff += fabs(xn[v] - x[v]);
+        double *t = x; x = xn; xn = t;
+        if (diff < 1e-12) break;
+    }
+    if (!hits_form) {
+        double num = 0.0, den = 0.0;
+        for (uint32_t v = 0; v < n; v++) {
+            num += x[v] * WX(v, x);
+            den += x[v] * x[v];
+        }
+        if (eigval) *eigval = den > 0.0 ? num / den : 0.0;
+        rescale_max_abs(x, n);
+    }
+    if (!neg)
+        for (uint32_t v = 0; v < n; v++) if (x[v] < 0.0) x[v] = 0.0;
+    if (hits_form) {
+        double num = 0.0, den = 0.0;
+        for (uint32_t v = 0; v < n; v++) {
+            num += x[v] * WX(v, x);
+            den += x[v] * x[v];
+        }
+        if (eigval) *eigval = den > 0.0 ? num / den : 0.0;
+    }
+#undef WX
+    memcpy(out, x, n * sizeof(double));
+    free(orp); free(ooth); free(oeid); free(irp); free(ioth); free(ieid); free(x); free(xn);
+    return it;
+}
+
+/* eigenvector_centrality_weighted (eigenvector.rs:375-538): n == 0 -> empty;
+ * m == 0, all-zero weights or n == 1 -> ones, eigenvalue 0; otherwise the
+ * weighted core in its eigenvector form.  Returns iterations. */
 int or_eigenvector_weighted(uint32_t n, uint64_t m, const uint32_t *from, const uint32_t *to, const double *w,
                             double *out, double *eigval) {
     if (eigval) *eigval = 0.0;
     if (n == 0) return 0;
     int allzero = 1;
     for (uint64_t e = 0; e < m; e++) allzero &= w[e] == 0.0;
-    if (m == 0 || allzero) {
+    if (m == 0 || allzero || n == 1) {
         for (uint32_t i = 0; i < n; i++) out[i] = 1.0;
         return 0;
     }
-    uint64_t *orp, *irp;
-    uint32_t *ooth, *oeid, *ioth, *ieid;
-    edge_rows(n, m, from, to, &orp, &ooth, &oeid);
-    edge_rows(n, m, to, from, &irp, &ioth, &ieid);
-    double *x = (double *)malloc(n * sizeof(double)), *xn = (double *)malloc(n * sizeof(double));
-    int any = 0;
-    for (uint32_t v = 0; v < n; v++) {
-        double s = 0.0;
-        for (uint64_t p = orp[v]; p < orp[v + 1]; p++) s += w[oeid[p]];
-        for (uint64_t p = irp[v]; p < irp[v + 1]; p++) s += w[ieid[p]];
-        x[v] = s != 0.0 ? fabs(s) : 0.0;
-        any |= x[v] != 0.0;
-    }
-    if (!any)
-        for (uint32_t v = 0; v < n; v++) x[v] = 1.0;
-    rescale_max_abs(x, n);
-    int it = 0;
-    for (; it < 5000;) {
-        it++;
-        for (uint32_t v = 0; v < n; v++) xn[v] = x[v] + winc(v, orp, ooth, oeid, irp, ioth, ieid, w, x);
-        rescale_max_abs(xn, n);
-        double diff = 0.0;
-        for (uint32_t v = 0; v < n; v++) diff += fabs(xn[v] - x[v]);
-        double *t = x; x = xn; xn = t;
-        if (diff < 1e-12) break;
-    }
-    double num = 0.0, den = 0.0;
-    for (uint32_t v = 0; v < n; v++) {
-        num += x[v] * winc(v, orp, ooth, oeid, irp, ioth, ieid, w, x);
-        den += x[v] * x[v];
-    }
-    if (eigval) *eigval = den > 0.0 ? num / den : 0.0;
-    rescale_max_abs(x, n);
-    for (uint32_t v = 0; v < n; v++) out[v] = x[v] < 0.0 ? 0.0 : x[v];
-    free(orp); free(irp); free(ooth); free(oeid); free(ioth); free(ieid); free(x); free(xn);
-    return it;
+    return weighted_core(n, m, from, to, w, 0, 0, out, eigval);
 }
 
-/* hub_and_authority_scores_weighted, non-negative weights (hits.rs:245-470):
- * directed: h = out-strength, tmp = W^T h, h' = W tmp, eigenvalue max|h'|,
- * eps 1e-12; authority = W^T h rescaled; undirected: the weighted
- * eigenvector and (x.Wx/x.x)^2. */
+/* hub_and_authority_scores_weighted (hits.rs:288-470).  m == 0 or all-zero
+ * weights -> ones.  Undirected: the weighted core in its HITS form, hub =
+ * authority, eigenvalue = (x.Wx / x.x)^2.  Directed: h = out-strength (with
+ * negative weights a zero strength on a non-empty out-list seeds 1), max-abs
+ * rescaled; tmp = W^T h, h' = W tmp, divided by max |h'| (the signed pivot
+ * with negative weights), which is the eigenvalue estimate; L1 stop 1e-12;
+ * clamp (non-negative weights); authority = W^T h, max-abs rescaled, clamped
+ * likewise. */
 int or_hits_weighted(uint32_t n, uint64_t m, const uint32_t *from, const uint32_t *to, const double *w, int directed,
                      double *hub, double *auth, double *eigval) {
     if (eigval) *eigval = 0.0;
@@ -1032,11 +1093,12 @@ int or_hits_weighted(uint32_t n, uint64_t m, const uint32_t *from, const uint32_
     }
     if (!directed) {
         double lam = 0.0;
-        int it = or_eigenvector_weighted(n, m, from, to, w, hub, &lam);
+        int it = weighted_core(n, m, from, to, w, 0, 1, hub, &lam);
         memcpy(auth, hub, n * sizeof(double));
         if (eigval) *eigval = lam * lam;
         return it;
     }
+    const int neg = any_negative_w(w, m);
     uint64_t *orp, *irp;
     uint32_t *ooth, *oeid, *ioth, *ieid;
     edge_rows(n, m, from, to, &orp, &ooth, &oeid);  /* out_inc[u]: targets */
@@ -1046,7 +1108,7 @@ int or_hits_weighted(uint32_t n, uint64_t m, const uint32_t *from, const uint32_
     for (uint32_t u = 0; u < n; u++) {
         double s = 0.0;
         for (uint64_t p = orp[u]; p < orp[u + 1]; p++) s += w[oeid[p]];
-        h[u] = s;
+        h[u] = s != 0.0 ? s : ((neg && orp[u + 1] > orp[u]) ? 1.0 : 0.0);
     }
     rescale_max_abs(h, n);
     double lam = 0.0;
@@ -1063,25 +1125,31 @@ int or_hits_weighted(uint32_t n, uint64_t m, const uint32_t *from, const uint32_
             for (uint64_t p = orp[u]; p < orp[u + 1]; p++) s += w[oeid[p]] * tmp[ooth[p]];
             hn[u] = s;
         }
-        double mx = 0.0;
-        for (uint32_t u = 0; u < n; u++) mx = fmax(mx, fabs(hn[u]));
-        if (mx != 0.0) {
-            lam = mx;
-            for (uint32_t u = 0; u < n; u++) hn[u] /= mx;
+        double scale;
+        if (neg) {
+            scale = signed_pivot(hn, n);
+        } else {
+            scale = 0.0;
+            for (uint32_t u = 0; u < n; u++) scale = fmax(scale, fabs(hn[u]));
+        }
+        if (scale != 0.0) {
+            lam = scale;
+            for (uint32_t u = 0; u < n; u++) hn[u] /= scale;
         }
         double diff = 0.0;
         for (uint32_t u = 0; u < n; u++) diff += fabs(hn[u] - h[u]);
         double *t = h; h = hn; hn = t;
         if (diff < 1e-12) break;
     }
-    for (uint32_t u = 0; u < n; u++) hub[u] = h[u] < 0.0 ? 0.0 : h[u];
+    for (uint32_t u = 0; u < n; u++) hub[u] = (!neg && h[u] < 0.0) ? 0.0 : h[u];
     for (uint32_t v = 0; v < n; v++) {
         double s = 0.0;
         for (uint64_t p = irp[v]; p < irp[v + 1]; p++) s += w[ieid[p]] * hub[ioth[p]];
         auth[v] = s;
     }
     rescale_max_abs(auth, n);
-    for (uint32_t v = 0; v < n; v++) if (auth[v] < 0.0) auth[v] = 0.0;
+    if (!neg)
+        for (uint32_t v = 0; v < n; v++) if (auth[v] < 0.0) auth[v] = 0.0;
     if (eigval) *eigval = lam;
     free(orp); free(irp); free(ooth); free(oeid); free(ioth); free(ieid); free(h); free(hn); free(tmp);
     return it;
@@ -1204,8 +1272,8 @@ static int is_dag(uint32_t n, uint64_t m, const uint32_t *from, const uint32_t *
     return tail == n;
 }
 
-/* eigenvector_centrality_full (eigenvector.rs:238-285), non-negative weights
- * (w may be NULL = unit): mode 0 = Out, 1 = In, 2 = All.
+/* eigenvector_centrality_full (eigenvector.rs:238-285), weights of either
+ * sign (w may be NULL = unit): mode 0 = Out, 1 = In, 2 = All.
  * Undirected graphs take All.  All on a directed graph runs the "undirected"
  * routines over what graph.neighbors / graph.incident return there, the
  * out-edges only (graph.rs:808-819, 1212-1217): unweighted x' = x + sum over
@@ -1217,7 +1285,10 @@ static int is_dag(uint32_t n, uint64_t m, const uint32_t *from, const uint32_t *
  * / out-edges (In) of v in edge order, seed |strength| of that walk
  * (all-zero -> ones) max-normalised, shift = max(max walk strength, 1) + 1,
  * x' = shift x + M x max-normalised until the L1 change < 1e-12 (5000
- * iterations); eigenvalue = x.Mx / x.x, and <= 1e-12 gives zeros. */
+ * iterations); eigenvalue = x.Mx / x.x, and <= 1e-12 gives zeros.  With a
+ * negative weight: no DAG short-circuit, a zero strength on a non-empty walk
+ * seeds 1, the signed pivot normalises, and neither the zero rule nor the
+ * clamp applies. */
 int or_eigenvector_full(uint32_t n, uint64_t m, const uint32_t *from, const uint32_t *to, int directed, int mode,
                         const double *w, double *out, double *eigval) {
     if (eigval) *eigval = 0.0;
@@ -1238,50 +1309,35 @@ int or_eigenvector_full(uint32_t n, uint64_t m, const uint32_t *from, const uint
             for (uint32_t i = 0; i < n; i++) out[i] = 1.0;
             return 0;
         }
+        if (w) return weighted_core(n, m, from, to, w, 1, 0, out, eigval);
+        /* unweighted: ascending out-neighbours, x' = x + sum, eps 1e-14 */
         uint64_t *rp;
         uint32_t *oth, *eid;
         edge_rows(n, m, from, to, &rp, &oth, &eid); /* out-edges by (source, target, id) */
         double *x = (double *)malloc(n * sizeof(double)), *xn = (double *)malloc(n * sizeof(double));
-        int any = 0;
-        for (uint32_t v = 0; v < n; v++) {
-            if (!w) {
-                x[v] = 1.0;
-                continue;
-            }
-            double s = 0.0;
-            for (uint64_t p = rp[v]; p < rp[v + 1]; p++) s += w[eid[p]];
-            x[v] = s != 0.0 ? fabs(s) : 0.0;
-            any |= x[v] != 0.0;
-        }
-        if (w) {
-            if (!any)
-                for (uint32_t v = 0; v < n; v++) x[v] = 1.0;
-            rescale_max_abs(x, n);
-        }
-        const double eps = w ? 1e-12 : 1e-14;
+        for (uint32_t v = 0; v < n; v++) x[v] = 1.0;
         int it = 0;
         while (it < 5000) {
             it++;
             for (uint32_t v = 0; v < n; v++) {
                 double s = x[v];
-                for (uint64_t p = rp[v]; p < rp[v + 1]; p++) s += (w ? w[eid[p]] : 1.0) * x[oth[p]];
+                for (uint64_t p = rp[v]; p < rp[v + 1]; p++) s += x[oth[p]];
                 xn[v] = s;
             }
             rescale_max_abs(xn, n);
             double diff = 0.0;
             for (uint32_t v = 0; v < n; v++) diff += fabs(xn[v] - x[v]);
             double *t = x; x = xn; xn = t;
-            if (diff < eps) break;
+            if (diff < 1e-14) break;
         }
         double num = 0.0, den = 0.0;
         for (uint32_t v = 0; v < n; v++) {
             double s = 0.0;
-            for (uint64_t p = rp[v]; p < rp[v + 1]; p++) s += (w ? w[eid[p]] : 1.0) * x[oth[p]];
+            for (uint64_t p = rp[v]; p < rp[v + 1]; p++) s += x[oth[p]];
             num += x[v] * s;
             den += x[v] * x[v];
         }
         if (eigval) *eigval = den > 0.0 ? num / den : 0.0;
-        rescale_max_abs(x, n);
         for (uint32_t v = 0; v < n; v++) out[v] = x[v] < 0.0 ? 0.0 : x[v];
         free(rp); free(oth); free(eid); free(x); free(xn);
         return it;
@@ -1294,7 +1350,8 @@ int or_eigenvector_full(uint32_t n, uint64_t m, const uint32_t *from, const uint
         for (uint32_t i = 0; i < n; i++) out[i] = 1.0;
         return 0;
     }
-    if (is_dag(n, m, from, to)) {
+    const int neg = w ? any_negative_w(w, m) : 0;
+    if (!neg && is_dag(n, m, from, to)) {
         double *st = (double *)calloc(n, sizeof(double));
         for (uint64_t e = 0; e < m; e++) st[mode == 0 ? from[e] : to[e]] += w ? w[e] : 1.0;
         for (uint32_t v = 0; v < n; v++) out[v] = st[v] == 0.0 ? 1.0 : 0.0;
@@ -1323,7 +1380,8 @@ int or_eigenvector_full(uint32_t n, uint64_t m, const uint32_t *from, const uint
             s += wv;
             sa += fabs(wv);
         }
-        x[v] = s != 0.0 ? fabs(s) : 0.0;
+        if (s != 0.0) x[v] = fabs(s);
+        else x[v] = (neg && rp[v + 1] > rp[v]) ? 1.0 : 0.0;
         any |= x[v] != 0.0;
         if (sa > row_norm) row_norm = sa;
     }
@@ -1339,7 +1397,13 @@ int or_eigenvector_full(uint32_t n, uint64_t m, const uint32_t *from, const uint
             for (uint64_t p = rp[v]; p < rp[v + 1]; p++) s += (w ? w[we[p]] : 1.0) * x[wn[p]];
             xn[v] = s;
         }
-        rescale_max_abs(xn, n);
+        if (neg) {
+            const double pv = signed_pivot(xn, n);
+            if (pv != 0.0)
+                for (uint32_t v = 0; v < n; v++) xn[v] /= pv;
+        } else {
+            rescale_max_abs(xn, n);
+        }
         double diff = 0.0;
         for (uint32_t v = 0; v < n; v++) diff += fabs(xn[v] - x[v]);
         double *t = x; x = xn; xn = t;
@@ -1353,12 +1417,12 @@ int or_eigenvector_full(uint32_t n, uint64_t m, const uint32_t *from, const uint
         den += x[v] * x[v];
     }
     double lam = den > 0.0 ? num / den : 0.0;
-    if (lam <= 1e-12) {
+    if (!neg && lam <= 1e-12) {
         lam = 0.0;
         for (uint32_t v = 0; v < n; v++) out[v] = 0.0;
     } else {
         rescale_max_abs(x, n);
-        for (uint32_t v = 0; v < n; v++) out[v] = x[v] < 0.0 ? 0.0 : x[v];
+        for (uint32_t v = 0; v < n; v++) out[v] = (!neg && x[v] < 0.0) ? 0.0 : x[v];
     }
     if (eigval) *eigval = lam;
     free(rp); free(wn); free(we); free(cur); free(x); free(xn);

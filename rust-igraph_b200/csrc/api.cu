@@ -479,8 +479,9 @@ int32_t prg_hub_and_authority_scores(uint32_t n, uint64_t m, const uint32_t *fro
     PRG_GUARD_END
 }
 
-// Weighted variants: non-negative weights only (a signed pivot would be
-// needed otherwise); the checks come in the reference's order.
+// Weighted eigen variants; the checks come in the reference's order.  A
+// negative weight switches the iterations to the reference's signed rules
+// (signed pivot, no clamping, no DAG or zero-eigenvalue shortcut).
 static bool any_negative(const double *w, uint64_t m) {
     for (uint64_t e = 0; e < m; e++)
         if (w[e] < 0.0) return true;
@@ -509,15 +510,17 @@ int32_t prg_eigenvector_centrality_weighted(uint32_t n, uint64_t m, const uint32
         for (uint32_t i = 0; i < n; i++) out[i] = 1.0;
         return PRG_OK;
     }
-    if (any_negative(weights, m))
-        return fail(PRG_ERR_UNSUPPORTED, "negative weights are not supported by the GPU eigenvector centrality");
+    prg::eig::EigOpts o;  // eigenvector.rs:375-538
+    o.rowsum_seed = true;
+    o.eps = 1e-12;
+    o.negative = any_negative(weights, m);
     prg_graph *h = nullptr;
     int32_t rc = create_from_host(n, m, from, to, weights, 0, &h);
     if (rc != PRG_OK) return rc;
     try {
         cudaStream_t s = h->stream;
         if (!h->d_out) PRG_CUDA(cudaMallocAsync((void **)&h->d_out, (uint64_t)n * 8, s));
-        const prg::eig::Result r = prg::eig::eigenvector_centrality(h->g, h->ws, h->d_out, s, true, 1e-12);
+        const prg::eig::Result r = prg::eig::eigenvector_centrality(h->g, h->ws, h->d_out, s, o);
         PRG_CUDA(cudaMemcpyAsync(out, h->d_out, (uint64_t)n * 8, cudaMemcpyDeviceToHost, s));
         PRG_CUDA(cudaStreamSynchronize(s));
         if (eigenvalue) *eigenvalue = r.eigenvalue;
@@ -550,8 +553,7 @@ int32_t prg_eigenvector_centrality_full(uint32_t n, uint64_t m, const uint32_t *
         for (uint32_t i = 0; i < n; i++) out[i] = 1.0;
         return PRG_OK;
     }
-    if (weights && any_negative(weights, m))
-        return fail(PRG_ERR_UNSUPPORTED, "negative weights are not supported by the GPU eigenvector centrality");
+    const bool neg = weights && any_negative(weights, m);
     // Out walks the in-edges of v: the graph's own in-CSR.  In, and All on a
     // directed graph (graph.neighbors / incident give out-edges there), walk
     // the out-edges: the in-CSR of the reversed graph.
@@ -564,9 +566,13 @@ int32_t prg_eigenvector_centrality_full(uint32_t n, uint64_t m, const uint32_t *
         if (!h->d_out) PRG_CUDA(cudaMallocAsync((void **)&h->d_out, (uint64_t)n * 8, s));
         prg::eig::Result r;
         if (!all) {
-            r = prg::eig::eigenvector_directed(h->g, h->ws, h->d_out, s);
+            r = prg::eig::eigenvector_directed(h->g, h->ws, h->d_out, s, neg);
         } else if (weights) {
-            r = prg::eig::eigenvector_centrality(h->g, h->ws, h->d_out, s, true, 1e-12);  // eigenvector.rs:375-538
+            prg::eig::EigOpts o;  // eigenvector.rs:375-538
+            o.rowsum_seed = true;
+            o.eps = 1e-12;
+            o.negative = neg;
+            r = prg::eig::eigenvector_centrality(h->g, h->ws, h->d_out, s, o);
         } else {
             r = prg::eig::eigenvector_centrality(h->g, h->ws, h->d_out, s);  // eigenvector.rs:286-372
         }
@@ -596,17 +602,22 @@ int32_t prg_hub_and_authority_scores_weighted(uint32_t n, uint64_t m, const uint
         for (uint32_t i = 0; i < n; i++) hub[i] = authority[i] = 1.0;
         return PRG_OK;
     }
-    if (any_negative(weights, m))
-        return fail(PRG_ERR_UNSUPPORTED, "negative weights are not supported by the GPU hub and authority scores");
+    const bool neg = any_negative(weights, m);
     if (!directed) {
-        // hits.rs:334-341: weighted eigenvector centrality, eigenvalue (x.Wx / x.x)^2
+        // hits.rs:334-341, 470-553: the weighted iteration with a signed
+        // strength seed, eigenvalue (x.Wx / x.x)^2
+        prg::eig::EigOpts o;
+        o.rowsum_seed = true;
+        o.signed_seed = true;
+        o.eps = 1e-12;
+        o.negative = neg;
         prg_graph *h = nullptr;
         int32_t rc = create_from_host(n, m, from, to, weights, 0, &h);
         if (rc != PRG_OK) return rc;
         try {
             cudaStream_t s = h->stream;
             if (!h->d_out) PRG_CUDA(cudaMallocAsync((void **)&h->d_out, (uint64_t)n * 8, s));
-            const prg::eig::Result r = prg::eig::eigenvector_centrality(h->g, h->ws, h->d_out, s, true, 1e-12);
+            const prg::eig::Result r = prg::eig::eigenvector_centrality(h->g, h->ws, h->d_out, s, o);
             PRG_CUDA(cudaMemcpyAsync(hub, h->d_out, (uint64_t)n * 8, cudaMemcpyDeviceToHost, s));
             PRG_CUDA(cudaStreamSynchronize(s));
             for (uint32_t i = 0; i < n; i++) authority[i] = hub[i];
@@ -632,7 +643,7 @@ int32_t prg_hub_and_authority_scores_weighted(uint32_t n, uint64_t m, const uint
         double *d_h = nullptr, *d_a = nullptr;
         PRG_CUDA(cudaMallocAsync((void **)&d_h, (uint64_t)n * 8, s));
         PRG_CUDA(cudaMallocAsync((void **)&d_a, (uint64_t)n * 8, s));
-        const prg::eig::Result r = prg::eig::hits_directed(g->g, g->ws, rev->g, rev->ws, d_h, d_a, s);
+        const prg::eig::Result r = prg::eig::hits_directed(g->g, g->ws, rev->g, rev->ws, d_h, d_a, s, neg);
         PRG_CUDA(cudaMemcpyAsync(hub, d_h, (uint64_t)n * 8, cudaMemcpyDeviceToHost, s));
         PRG_CUDA(cudaMemcpyAsync(authority, d_a, (uint64_t)n * 8, cudaMemcpyDeviceToHost, s));
         cudaFreeAsync(d_h, s);

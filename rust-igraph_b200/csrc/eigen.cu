@@ -132,7 +132,7 @@ __global__ void check_kernel(const double4 *part, uint32_t nb, State *st, int32_
         const double mx = part[0].y;
         st->iters += 1u;
         st->diff = d;
-        if (mx > 0.0) st->maxv = mx;
+        if (mx != 0.0) st->maxv = mx;  // the last non-zero scale (signed with negative weights)
         st->final_buf = buf;
         if (d < st->eps || st->iters >= st->max_iter) st->done = 1;
     }
@@ -142,13 +142,15 @@ __global__ void fill_kernel(double *x, uint32_t n, double v) {
     for (uint32_t i = blockIdx.x * kNT + threadIdx.x; i < n; i += gridDim.x * kNT) x[i] = v;
 }
 
-// x = out-degree (deg) or |strength| (dval) and block records (max, 0, 0)
-// for the normalisation
-__global__ void degree_seed_kernel(const uint32_t *deg, const double *dval, uint32_t n, double *x, double4 *recs) {
+// x = out-degree (deg) or out-strength (dval; with negative weights (neg) a
+// zero strength on a vertex with out-arcs gives 1) and block records
+// (max |x|, 0, 0) for the normalisation
+__global__ void degree_seed_kernel(const uint32_t *deg, const double *dval, uint32_t n, bool neg, double *x,
+                                   double4 *recs) {
     double mx = 0.0;
     for (uint32_t i = blockIdx.x * kNT + threadIdx.x; i < n; i += gridDim.x * kNT) {
-        x[i] = dval ? fabs(dval[i]) : (double)deg[i];
-        mx = fmax(mx, x[i]);
+        x[i] = dval ? (dval[i] != 0.0 ? dval[i] : ((neg && deg[i] > 0u) ? 1.0 : 0.0)) : (double)deg[i];
+        mx = fmax(mx, fabs(x[i]));
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
@@ -162,12 +164,109 @@ __global__ void degree_seed_kernel(const uint32_t *deg, const double *dval, uint
     }
 }
 
+// ---- signed pivot (negative weights; eigenvector.rs:464-476, hits.rs:399-411)
+// The component of greatest |y|, the one with the smallest caller id (perm[i],
+// or i) on ties, as the reference scans caller ids in order and keeps the
+// first strict maximum.  (mag, id, value) records: a total order, so any
+// reduction order gives the same pivot.
+__device__ __forceinline__ bool pv_better(double m1, double i1, double m2, double i2) {
+    return m1 > m2 || (m1 == m2 && i1 < i2);
+}
+
+__device__ __forceinline__ void pv_reduce_block(double &mag, double &id, double &val, double (*sm)[kNT / 32]) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const double m2 = __shfl_xor_sync(0xffffffffu, mag, o), i2 = __shfl_xor_sync(0xffffffffu, id, o);
+        const double v2 = __shfl_xor_sync(0xffffffffu, val, o);
+        if (pv_better(m2, i2, mag, id)) {
+            mag = m2;
+            id = i2;
+            val = v2;
+        }
+    }
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    __syncthreads();
+    if (l == 0) {
+        sm[0][w] = mag;
+        sm[1][w] = id;
+        sm[2][w] = val;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0)
+        for (int k = 1; k < kNT / 32; k++)
+            if (pv_better(sm[0][k], sm[1][k], mag, id)) {
+                mag = sm[0][k];
+                id = sm[1][k];
+                val = sm[2][k];
+            }
+}
+
+__global__ void __launch_bounds__(kNT) pivot_kernel(const double *y, uint32_t n, const uint32_t *perm, double4 *recs,
+                                                    const State *st) {
+    if (st && *(volatile const int32_t *)&st->done) return;
+    __shared__ double sm[3][kNT / 32];
+    double mag = -1.0, id = 4294967296.0, val = 0.0;
+    for (uint32_t i = blockIdx.x * kNT + threadIdx.x; i < n; i += gridDim.x * kNT) {
+        const double m = fabs(y[i]), c = (double)(perm ? perm[i] : i);
+        if (pv_better(m, c, mag, id)) {
+            mag = m;
+            id = c;
+            val = y[i];
+        }
+    }
+    pv_reduce_block(mag, id, val, sm);
+    if (threadIdx.x == 0) recs[blockIdx.x] = make_double4(mag, id, val, 0.0);
+}
+
+// x /= pivot (when the pivot is not 0), sum |x - xold| per block; records
+// (change, pivot, 0, 0) as normalise_kernel's.
+__global__ void __launch_bounds__(kNT) normalise_signed_kernel(uint32_t n, const double4 *recs, uint32_t nrec,
+                                                               double *x, const double *xold, double4 *part,
+                                                               const State *st) {
+    if (st && *(volatile const int32_t *)&st->done) return;
+    __shared__ double sm[3][kNT / 32];
+    __shared__ double s_piv;
+    double mag = -1.0, id = 4294967296.0, val = 0.0;
+    for (uint32_t i = threadIdx.x; i < nrec; i += kNT) {
+        const double4 q = recs[i];
+        if (pv_better(q.x, q.y, mag, id)) {
+            mag = q.x;
+            id = q.y;
+            val = q.z;
+        }
+    }
+    pv_reduce_block(mag, id, val, sm);
+    if (threadIdx.x == 0) s_piv = val;
+    __syncthreads();
+    const double piv = s_piv;
+    double d = 0.0;
+    for (uint32_t v = blockIdx.x * kNT + threadIdx.x; v < n; v += gridDim.x * kNT) {
+        double xv = x[v];
+        if (piv != 0.0) {
+            xv /= piv;
+            x[v] = xv;
+        }
+        if (xold) d += fabs(xv - xold[v]);
+    }
+    d = warp_sum(d);
+    __shared__ double sh[kNT / 32];
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    if (l == 0) sh[w] = d;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int k = 1; k < kNT / 32; k++) d += sh[k];
+        part[blockIdx.x] = make_double4(d, piv, 0.0, 0.0);
+    }
+}
+
 // ---- directed eigenvector centrality (eigenvector.rs:539-756)
 
-// x[v] = |sum of row v's arc weights| (row length when unweighted), one warp
-// per row; records (max x, max sum of |w| over a row, 0, 0).
+// x[v] = |sum of row v's arc weights| (row length when unweighted; the sum
+// itself when keep_sign), and with negative weights (neg) 1 for a zero sum
+// over a non-empty row; one warp per row; records (max |x|, max sum of |w|
+// over a row, 0, 0).
 __global__ void __launch_bounds__(kNT) rowsum_seed_kernel(const uint32_t *row_ptr, const double *w64, uint32_t n,
-                                                          double *x, double4 *recs) {
+                                                          bool keep_sign, bool neg, double *x, double4 *recs) {
     __shared__ double sm[2][kNT / 32];
     const uint32_t lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     double mx = 0.0, mnorm = 0.0;
@@ -185,8 +284,9 @@ __global__ void __launch_bounds__(kNT) rowsum_seed_kernel(const uint32_t *row_pt
             s = sa = (double)(hi - lo);
         }
         if (lane == 0) {
-            x[v] = fabs(s);
-            mx = fmax(mx, fabs(s));
+            const double xv = s != 0.0 ? (keep_sign ? s : fabs(s)) : ((neg && hi > lo) ? 1.0 : 0.0);
+            x[v] = xv;
+            mx = fmax(mx, fabs(xv));
             mnorm = fmax(mnorm, sa);
         }
     }
@@ -405,8 +505,9 @@ static double rayleigh(const Product &pr, const double *x, double *tmp, double4 
 // Seeds x with the absolute row sums of g's in-CSR (the strength the walk
 // over each row sees) and max-normalises it; an all-zero seed becomes all
 // ones.  Returns the largest row sum of |w| (the shift's row norm).
-static double seed(const DeviceGraph &g, double *x, double4 *recs, double4 *part, cudaStream_t s) {
-    rowsum_seed_kernel<<<kNB, kNT, 0, s>>>(g.row_ptr, g.weighted ? g.w64 : nullptr, g.n, x, recs);
+static double seed(const DeviceGraph &g, bool keep_sign, bool neg, double *x, double4 *recs, double4 *part,
+                   cudaStream_t s) {
+    rowsum_seed_kernel<<<kNB, kNT, 0, s>>>(g.row_ptr, g.weighted ? g.w64 : nullptr, g.n, keep_sign, neg, x, recs);
     PRG_CUDA(cudaGetLastError());
     std::vector<double4> h(kNB);
     PRG_CUDA(cudaMemcpyAsync(h.data(), recs, kNB * sizeof(double4), cudaMemcpyDeviceToHost, s));
@@ -441,6 +542,7 @@ Result eigenvector_centrality(const DeviceGraph &g, Workspace &ws, double *d_out
     const unsigned grid = ws.cfg[MODE_EIG64].grid;
     double *x[2] = {alloc<double>(n, s), alloc<double>(n, s)};
     double4 *recs = alloc<double4>(std::max(grid, kNB), s), *part = alloc<double4>(kNB, s);
+    double4 *pvrec = alloc<double4>(kNB, s);
     State *d_st = alloc<State>(1, s), *h_st = nullptr;
     PRG_CUDA(cudaMallocHost((void **)&h_st, 2 * sizeof(State)));
     try {
@@ -451,7 +553,7 @@ Result eigenvector_centrality(const DeviceGraph &g, Workspace &ws, double *d_out
         PRG_CUDA(cudaMemcpyAsync(d_st, &init, sizeof(State), cudaMemcpyHostToDevice, s));
         double shift = 1.0;
         if (strength_seed) {
-            const double norm = seed(g, x[0], recs, part, s);
+            const double norm = seed(g, o.signed_seed, o.negative, x[0], recs, part, s);
             if (o.auto_shift) shift = std::max(norm, 1.0) + 1.0;  // eigenvector.rs:627-643
         } else {
             fill_kernel<<<kNB, kNT, 0, s>>>(x[0], n, 1.0);
@@ -460,7 +562,12 @@ Result eigenvector_centrality(const DeviceGraph &g, Workspace &ws, double *d_out
         run_until_done(d_st, h_st, init.max_iter, s, [&](uint32_t it) {
             const int q = (int)(it & 1u);
             product(pr, x[q], x[q ^ 1], shift, recs, &d_st->done, s);
-            normalise_kernel<<<kNB, kNT, 0, s>>>(n, recs, grid, ws.hub_rec, g.nhub, x[q ^ 1], x[q], part, d_st);
+            if (o.negative) {
+                pivot_kernel<<<kNB, kNT, 0, s>>>(x[q ^ 1], n, g.perm, pvrec, d_st);
+                normalise_signed_kernel<<<kNB, kNT, 0, s>>>(n, pvrec, kNB, x[q ^ 1], x[q], part, d_st);
+            } else {
+                normalise_kernel<<<kNB, kNT, 0, s>>>(n, recs, grid, ws.hub_rec, g.nhub, x[q ^ 1], x[q], part, d_st);
+            }
             check_kernel<<<1, 256, 0, s>>>(part, kNB, d_st, q ^ 1);
             PRG_CUDA(cudaGetLastError());
         });
@@ -468,12 +575,13 @@ Result eigenvector_centrality(const DeviceGraph &g, Workspace &ws, double *d_out
         const double *xf = h_st[0].iters ? x[h_st[0].final_buf] : x[0];
         double *other = xf == x[0] ? x[1] : x[0];
         r.eigenvalue = rayleigh(pr, xf, other, recs, s);
-        if (o.zero_fallback && r.eigenvalue <= 1e-12) {
+        if (o.zero_fallback && !o.negative && r.eigenvalue <= 1e-12) {
             // eigenvector.rs:695-699: a (numerically) nilpotent matrix gives zeros
             r.eigenvalue = 0.0;
             fill_kernel<<<kNB, kNT, 0, s>>>(const_cast<double *>(xf), n, 0.0);
         }
-        clamp_kernel<<<kNB, kNT, 0, s>>>(const_cast<double *>(xf), n);
+        // negatives are numerical drift only with non-negative weights
+        if (!o.negative) clamp_kernel<<<kNB, kNT, 0, s>>>(const_cast<double *>(xf), n);
         PRG_CUDA(cudaGetLastError());
         if (g.perm) gather_f64(d_out, xf, g.iperm, n, s);
         else PRG_CUDA(cudaMemcpyAsync(d_out, xf, (uint64_t)n * 8, cudaMemcpyDeviceToDevice, s));
@@ -488,6 +596,7 @@ Result eigenvector_centrality(const DeviceGraph &g, Workspace &ws, double *d_out
     release(x[1], s);
     release(recs, s);
     release(part, s);
+    release(pvrec, s);
     release(d_st, s);
     PRG_CUDA(cudaStreamSynchronize(s));
     return r;
@@ -527,8 +636,8 @@ bool is_dag(const DeviceGraph &g, cudaStream_t s) {
     return h_removed == (unsigned long long)n;
 }
 
-Result eigenvector_directed(const DeviceGraph &g, Workspace &ws, double *d_out, cudaStream_t s) {
-    if (is_dag(g, s)) {  // eigenvector.rs:570-575, 721-756
+Result eigenvector_directed(const DeviceGraph &g, Workspace &ws, double *d_out, cudaStream_t s, bool negative) {
+    if (!negative && is_dag(g, s)) {  // eigenvector.rs:570-575, 721-756
         double *x = alloc<double>(g.n, s);
         sentinel_kernel<<<kNB, kNT, 0, s>>>(g.dval, g.n, x);
         PRG_CUDA(cudaGetLastError());
@@ -543,6 +652,7 @@ Result eigenvector_directed(const DeviceGraph &g, Workspace &ws, double *d_out, 
     o.eps = 1e-12;
     o.auto_shift = true;
     o.zero_fallback = true;
+    o.negative = negative;
     return eigenvector_centrality(g, ws, d_out, s, o);
 }
 
@@ -599,7 +709,7 @@ Result infomap_flow(const DeviceGraph &g, Workspace &ws, const double *d_t, doub
 }
 
 Result hits_directed(const DeviceGraph &g, Workspace &ws, const DeviceGraph &rev, Workspace &wsr, double *d_hub,
-                     double *d_auth, cudaStream_t s) {
+                     double *d_auth, cudaStream_t s, bool negative) {
     Result r;
     const uint32_t n = g.n;
     workspace_ensure(ws, g, s);
@@ -612,7 +722,7 @@ Result hits_directed(const DeviceGraph &g, Workspace &ws, const DeviceGraph &rev
     double *h[2] = {alloc<double>(n, s), alloc<double>(n, s)};
     double *tmp = alloc<double>(n, s);
     double4 *rin = alloc<double4>(std::max(gin, kNB), s), *rout = alloc<double4>(std::max(gout, kNB), s);
-    double4 *part = alloc<double4>(kNB, s);
+    double4 *part = alloc<double4>(kNB, s), *pvrec = alloc<double4>(kNB, s);
     State *d_st = alloc<State>(1, s), *h_st = nullptr;
     PRG_CUDA(cudaMallocHost((void **)&h_st, 2 * sizeof(State)));
     try {
@@ -623,25 +733,31 @@ Result hits_directed(const DeviceGraph &g, Workspace &ws, const DeviceGraph &rev
         PRG_CUDA(cudaMemcpyAsync(d_st, &init, sizeof(State), cudaMemcpyHostToDevice, s));
         // h = out-degree (out-strength when weighted) / its max: the graph's
         // deg / dval hold out-degree / out-strength
-        degree_seed_kernel<<<kNB, kNT, 0, s>>>(g.deg, g.weighted ? g.dval : nullptr, n, h[0], rout);
+        degree_seed_kernel<<<kNB, kNT, 0, s>>>(g.deg, g.weighted ? g.dval : nullptr, n, negative, h[0], rout);
         normalise_kernel<<<kNB, kNT, 0, s>>>(n, rout, kNB, nullptr, 0, h[0], nullptr, part, nullptr);
         PRG_CUDA(cudaGetLastError());
         run_until_done(d_st, h_st, init.max_iter, s, [&](uint32_t it) {
             const int q = (int)(it & 1u);
             product(pin, h[q], tmp, 0.0, rin, &d_st->done, s);
             product(pout, tmp, h[q ^ 1], 0.0, rout, &d_st->done, s);
-            normalise_kernel<<<kNB, kNT, 0, s>>>(n, rout, gout, wsr.hub_rec, rev.nhub, h[q ^ 1], h[q], part, d_st);
+            if (negative) {  // hits.rs:399-411: the signed pivot, also the eigenvalue estimate
+                pivot_kernel<<<kNB, kNT, 0, s>>>(h[q ^ 1], n, g.perm, pvrec, d_st);
+                normalise_signed_kernel<<<kNB, kNT, 0, s>>>(n, pvrec, kNB, h[q ^ 1], h[q], part, d_st);
+            } else {
+                normalise_kernel<<<kNB, kNT, 0, s>>>(n, rout, gout, wsr.hub_rec, rev.nhub, h[q ^ 1], h[q], part,
+                                                     d_st);
+            }
             check_kernel<<<1, 256, 0, s>>>(part, kNB, d_st, q ^ 1);
             PRG_CUDA(cudaGetLastError());
         });
         r.iterations = h_st[0].iters;
         r.eigenvalue = h_st[0].maxv;
         double *hf = h_st[0].iters ? h[h_st[0].final_buf] : h[0];
-        clamp_kernel<<<kNB, kNT, 0, s>>>(hf, n);
-        // authority = A^T h, rescaled by its max, clamped
+        if (!negative) clamp_kernel<<<kNB, kNT, 0, s>>>(hf, n);
+        // authority = A^T h, rescaled by its max |.|, clamped (non-negative weights)
         product(pin, hf, tmp, 0.0, rin, nullptr, s);
         normalise_kernel<<<kNB, kNT, 0, s>>>(n, rin, gin, ws.hub_rec, g.nhub, tmp, nullptr, part, nullptr);
-        clamp_kernel<<<kNB, kNT, 0, s>>>(tmp, n);
+        if (!negative) clamp_kernel<<<kNB, kNT, 0, s>>>(tmp, n);
         PRG_CUDA(cudaGetLastError());
         PRG_CUDA(cudaMemcpyAsync(d_hub, hf, (uint64_t)n * 8, cudaMemcpyDeviceToDevice, s));
         PRG_CUDA(cudaMemcpyAsync(d_auth, tmp, (uint64_t)n * 8, cudaMemcpyDeviceToDevice, s));
@@ -658,6 +774,7 @@ Result hits_directed(const DeviceGraph &g, Workspace &ws, const DeviceGraph &rev
     release(rin, s);
     release(rout, s);
     release(part, s);
+    release(pvrec, s);
     release(d_st, s);
     PRG_CUDA(cudaStreamSynchronize(s));
     return r;

@@ -20,6 +20,9 @@ struct EigOpts {
     double eps = 1e-14;          // L1 stop
     bool auto_shift = false;     // shift = max(max row sum of |A|, 1) + 1 (else 1)
     bool zero_fallback = false;  // eigenvalue <= 1e-12 -> zero vector, eigenvalue 0
+    bool negative = false;       // some weight < 0: signed pivot, a zero row sum over a non-empty row seeds 1,
+                                 // no clamping and no zero fallback
+    bool signed_seed = false;    // keep the sign of the row sums in the seed (the HITS form)
 };
 
 // Power iteration on g: x (caller ids) into d_out[n]; eigenvalue = x.Ax / x.x
@@ -35,13 +38,13 @@ bool is_dag(const DeviceGraph &g, cudaStream_t s);
 // Directed eigenvector centrality over g's in-CSR (eigenvector.rs:539-756,
 // non-negative weights): Out mode on a graph is this on the graph itself, In
 // mode this on its reverse.  A DAG gives 1 where g's out-strength is 0.
-Result eigenvector_directed(const DeviceGraph &g, Workspace &ws, double *d_out, cudaStream_t s);
+Result eigenvector_directed(const DeviceGraph &g, Workspace &ws, double *d_out, cudaStream_t s, bool negative = false);
 
 // Directed graph g and its reverse rev (both without relabelling):
 // hub and authority vectors into d_hub / d_auth; eigenvalue of A A^T.
 // The seed is the out-degree, or the out-strength when g is weighted.
 Result hits_directed(const DeviceGraph &g, Workspace &ws, const DeviceGraph &rev, Workspace &wsr, double *d_hub,
-                     double *d_auth, cudaStream_t s);
+                     double *d_auth, cudaStream_t s, bool negative = false);
 
 // Infomap's flow model (infomap.rs:299-355) on g (directed or undirected,
 // arc weights when g is weighted): node flows into d_out[n] (caller ids).

@@ -134,3 +134,33 @@ def test_eigenvector_directed_reference_cases():
     xw, lw, _ = full(300, f, t, True, O.EIG_OUT, weights=np.ones(3000))
     xu, lu, _ = full(300, f, t, True, O.EIG_OUT)
     assert np.array_equal(xw, xu) and lw == lu
+
+
+def test_negative_weight_rules():
+    # hits.rs:871-883: with negative weights nothing is clipped and the hub
+    # vector still reaches |1|
+    h, a, lam, _ = O.hub_and_authority_scores_weighted(3, *E([(0, 1), (1, 2), (2, 0)]), np.array([1.0, -1.0, 1.0]),
+                                                       True)
+    assert np.all(np.isfinite(h)) and np.all(np.isfinite(a)) and abs(np.abs(h).max() - 1.0) < 1e-6
+    # undirected path 0-1-2 with weights -1: the largest eigenvalue of W + I
+    # is 1 + sqrt 2, eigenvector [1, -sqrt 2, 1]; the signed pivot is vertex 1
+    x, lam, _ = O.eigenvector_centrality_weighted(3, *E([(0, 1), (1, 2)]), np.array([-1.0, -1.0]))
+    assert np.allclose(x, [-1 / np.sqrt(2), 1.0, -1 / np.sqrt(2)], atol=1e-9) and abs(lam - np.sqrt(2)) < 1e-9
+    # the same graph through HITS: hub = authority = x, eigenvalue lambda^2
+    h, a, lam2, _ = O.hub_and_authority_scores_weighted(3, *E([(0, 1), (1, 2)]), np.array([-1.0, -1.0]), False)
+    assert np.allclose(h, x, atol=1e-9) and np.array_equal(h, a) and abs(lam2 - 2.0) < 1e-9
+    # directed 2-cycle with weights -1, Out mode: the |strength| seed [1, 1] is
+    # the lambda = -1 eigenvector of M and the shifted iteration keeps it;
+    # negative weights skip the zero-eigenvalue rule
+    x, lam, _ = O.eigenvector_centrality_full(2, *E([(0, 1), (1, 0)]), True, O.EIG_OUT, weights=[-1.0, -1.0])
+    assert list(x) == [1.0, 1.0] and lam == -1.0
+    # an extra edge of weight -1e-9 (signed rules) against +1e-9 (unsigned)
+    rng = np.random.default_rng(7)
+    f = rng.integers(0, 200, 1500).astype(np.uint32)
+    t = rng.integers(0, 200, 1500).astype(np.uint32)
+    w = rng.random(1500) + 0.5
+    w[-1] = 1e-9
+    x0, l0, _ = O.eigenvector_centrality_weighted(200, f, t, w)
+    w[-1] = -1e-9
+    x1, l1, _ = O.eigenvector_centrality_weighted(200, f, t, w)
+    assert np.abs(x1 - x0).max() < 1e-6 and abs(l1 - l0) < 1e-6

@@ -125,8 +125,12 @@ def test_weighted_reference_unit_cases(cuda_ok):
         ig.eigenvector_centrality_weighted(path, [1.0])
     with pytest.raises(ig.Unsupported, match="directed eigenvector_centrality_weighted"):
         ig.eigenvector_centrality_weighted(G(3, [(0, 1)], True), [1.0])
-    with pytest.raises(ig.Unsupported, match="negative weights"):
-        ig.eigenvector_centrality_weighted(path, [1.0, -1.0])
+    # negative weights: the signed pivot (closed form: eigenvector [1, -sqrt 2, 1]
+    # of W = -A for the path, pivot on vertex 1)
+    x, lam = ig.eigenvector_centrality_weighted(path, [-1.0, -1.0], with_eigenvalue=True)
+    assert np.allclose(x, [-1 / np.sqrt(2), 1.0, -1 / np.sqrt(2)], atol=1e-9) and abs(lam - np.sqrt(2)) < 1e-9
+    s = ig.hub_and_authority_scores_weighted(path, [-1.0, -1.0])
+    assert np.allclose(s.hub, x, atol=1e-9) and abs(s.eigenvalue - 2.0) < 1e-9
     # hits.rs:763-880
     s = ig.hub_and_authority_scores_weighted(G(0, [], True), [])
     assert len(s.hub) == 0 and s.eigenvalue == 0.0
@@ -226,9 +230,14 @@ def test_directed_reference_unit_cases(cuda_ok):
     assert len(r.vector) == 3
     with pytest.raises(ig.InvalidArgument, match=r"weights vector length \(1\) not equal to number of edges \(3\)"):
         ig.eigenvector_centrality_directed_weighted(G(3, [(0, 1), (1, 2), (2, 0)], True), ig.EIG_OUT, [1.0])
-    with pytest.raises(ig.Unsupported, match="negative weights"):
-        ig.eigenvector_centrality_directed_weighted(G(3, [(0, 1), (1, 2), (2, 0)], True), ig.EIG_OUT,
-                                                    [1.0, -1.0, 1.0])
+    # hits.rs:871-883: negative weights are taken, nothing is clipped, and the
+    # hub vector still reaches |1|
+    s = ig.hub_and_authority_scores_weighted(G(3, [(0, 1), (1, 2), (2, 0)], True), [1.0, -1.0, 1.0])
+    assert np.all(np.isfinite(s.hub)) and np.all(np.isfinite(s.authority))
+    assert abs(np.abs(s.hub).max() - 1.0) < 1e-6
+    # directed 2-cycle with weights -1 (Out): the seed is the lambda = -1 eigenvector
+    s = ig.eigenvector_centrality_directed_weighted(G(2, [(0, 1), (1, 0)], True), ig.EIG_OUT, [-1.0, -1.0])
+    assert list(s.vector) == [1.0, 1.0] and s.eigenvalue == -1.0
 
 
 def _directed_case(kind):
@@ -272,3 +281,51 @@ def test_directed_matches_restatement(cuda_ok, kind, mode, weighted):
     assert abs(s.eigenvalue - lam) <= TOL * max(abs(lam), 1.0)
     if kind == "dag" and mode != 2:
         assert s.eigenvalue == 0.0 and set(np.unique(s.vector)) <= {0.0, 1.0}
+
+
+def _mixed_weights(m, seed):
+    # mostly positive, 5 % small negative weights: the dominant eigenvector is
+    # well separated, so the signed iterations converge well inside the cap
+    rng = np.random.default_rng(seed)
+    w = rng.uniform(0.2, 2.0, m)
+    neg = rng.random(m) < 0.05
+    w[neg] = -rng.uniform(0.05, 0.5, int(neg.sum()))
+    return w
+
+
+@pytest.mark.parametrize("kind", ["er", "ba", "rmat"])
+def test_negative_weights_match_restatement(cuda_ok, kind):
+    if kind == "er":
+        n = 20_000
+        f, t = O.erdos_renyi_gnm(n, 100_000, False, False, 61)
+    elif kind == "ba":  # degree-skewed: relabelled, so pivot ties go through the caller ids
+        n = 30_000
+        f, t = O.barabasi_game_bag(n, 4, False, False, 62)
+    else:
+        n = 1 << 13
+        f, t = O.rmat(13, 8 * n, seed=63)
+    g = ig.Graph.from_edge_arrays(n, f, t, False)
+    gf, gt = g.edge_arrays()
+    w = _mixed_weights(len(gf), 64)
+    x, lam = ig.eigenvector_centrality_weighted(g, w, with_eigenvalue=True)
+    ref, rlam, it = O.eigenvector_centrality_weighted(n, gf, gt, w)
+    assert it < 5000 and x.min() < 0.0  # signed: nothing clamped
+    assert np.max(np.abs(x - ref)) <= TOL and abs(lam - rlam) <= TOL * abs(rlam)
+    s = ig.hub_and_authority_scores_weighted(g, w)
+    h, _, hlam, _ = O.hub_and_authority_scores_weighted(n, gf, gt, w, False)
+    assert np.max(np.abs(s.hub - h)) <= TOL and abs(s.eigenvalue - hlam) <= TOL * abs(hlam)
+    gd = ig.Graph.from_edge_arrays(n, f, t, True)
+    df, dt = gd.edge_arrays()
+    wd = _mixed_weights(len(df), 65)
+    s = ig.hub_and_authority_scores_weighted(gd, wd)
+    h, a, hlam, it = O.hub_and_authority_scores_weighted(n, df, dt, wd, True)
+    assert it < 5000
+    assert np.max(np.abs(s.hub - h)) <= TOL and np.max(np.abs(s.authority - a)) <= TOL
+    assert abs(s.eigenvalue - hlam) <= TOL * abs(hlam)
+    if kind == "rmat":  # the directed shifted iterations converge on this graph
+        for mode in (ig.EIG_OUT, ig.EIG_IN, ig.EIG_ALL):
+            r = ig.eigenvector_centrality_full(gd, mode, wd)
+            ref, rlam, it = O.eigenvector_centrality_full(n, df, dt, True, mode, weights=wd)
+            assert it < 5000
+            assert np.max(np.abs(r.vector - ref)) <= TOL, (mode, np.max(np.abs(r.vector - ref)))
+            assert abs(r.eigenvalue - rlam) <= TOL * abs(rlam)
