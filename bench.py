@@ -383,6 +383,11 @@ def main():
                 "frac": achieved / peak if achieved else None, "traffic": traffic, "peak_source": peak_src,
                 "kernel": "iter_kernel<MODE_KRY32> (FP32 Krylov matvec y = A p with fused dot products)",
                 "bytes_per_launch": bytes_launch, "avg_launch_us": avg_launch_s * 1e6, "launches_timed": mv_n}
+    # the same index stream gathered once per arc and nothing else: the floor
+    # this access pattern sets (L1 wavefronts of random gathers), measured live
+    floor_ms = dg.gather_probe(20)
+    roofline["gather_floor_us"] = floor_ms * 1e3
+    roofline["frac_of_gather_floor"] = floor_ms * 1e3 / (avg_launch_s * 1e6) if mv_n else None
 
     # ---- end to end through the public API with host buffers
     e2e = None

@@ -234,6 +234,13 @@ int32_t prg_graph_relabelled(const prg_graph *g);
 int32_t prg_graph_device_csr(const prg_graph *g, const uint32_t **row_ptr, const uint32_t **col,
                              const uint32_t **perm, const float **inv32);
 
+/* Diagnostic with no counterpart in the reference: the average time (ms) of
+ * a pass that only streams the graph's column indices and gathers one FP32
+ * value per arc, with the FP32 matvec's load policies (reps timed passes after
+ * one warm-up).  It bounds from below any pass over this graph that gathers
+ * once per arc; bench.py reports the matvec against it. */
+int32_t prg_graph_gather_probe(prg_graph *g, int32_t reps, double *ms_per_pass);
+
 /* ---- learned warm start --------------------------------------------------- */
 /* A two-layer message-passing network (hidden 32, 8-channel messages scaled
  * by 1/out-degree, BF16 weights, FP32 accumulation on the tensor cores) that

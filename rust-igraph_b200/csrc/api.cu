@@ -1016,6 +1016,17 @@ int32_t prg_graph_info(const prg_graph *h, uint32_t *n, uint64_t *arcs, uint32_t
 
 void *prg_graph_stream(prg_graph *h) { return h ? (void *)h->stream : nullptr; }
 
+int32_t prg_graph_gather_probe(prg_graph *h, int32_t reps, double *ms_per_pass) {
+    g_err.clear();
+    PRG_GUARD_BEGIN
+    if (!h) return fail(PRG_ERR_INVALID_ARGUMENT, "null graph handle");
+    if (reps < 1 || reps > 10000) return fail(PRG_ERR_INVALID_ARGUMENT, "reps must be in 1..=10000");
+    const float ms = prg::gather_probe(h->g, reps, h->stream);
+    if (ms_per_pass) *ms_per_pass = (double)ms;
+    return PRG_OK;
+    PRG_GUARD_END
+}
+
 int32_t prg_solve(prg_graph *h, const prg_options *opt, const double *reset, double *out, prg_stats *st) {
     g_err.clear();
     PRG_GUARD_BEGIN

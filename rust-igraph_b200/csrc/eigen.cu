@@ -614,7 +614,10 @@ bool is_dag(const DeviceGraph &g, cudaStream_t s) {
     PRG_CUDA(cudaGetLastError());
     uint32_t h_next = 0;
     unsigned long long h_removed = 0;
-    for (uint32_t r = 0;; r++) {
+    // every vertex enters a frontier at most once, so the frontiers are empty
+    // after at most n + 1 rounds; the bound only guards against a broken count
+    const uint64_t max_rounds = (uint64_t)n + 32u;
+    for (uint64_t r = 0; r < max_rounds; r++) {
         const int c = (int)(r & 1u);
         peel_round<<<kNB, kNT, 0, s>>>(g.row_ptr, g.col, n, odeg, front[c], cnt + c, front[c ^ 1], cnt + (c ^ 1),
                                        removed);

@@ -606,6 +606,58 @@ void launch_iteration(int mode, bool weighted, const IterArgs &a_in, const Launc
     PRG_CUDA(cudaGetLastError());
 }
 
+// ------------------------------------------------------------------ gather probe
+
+// Diagnostic: the FP32 matvec's loads and nothing else.  Consecutive threads
+// stream consecutive 16-byte quads of col (evict-first, as the iteration
+// kernel does) and gather x at each source with the same L1 policy (ids >=
+// l1hot bypass L1); the sums go to out so nothing is optimised away.  No row
+// structure, staging, reduction or epilogue: the time is a floor for any pass
+// that reads this index stream and gathers once per arc.
+__global__ void __launch_bounds__(kThreads) gather_probe_kernel(const uint32_t *col, uint64_t arcs, const float *x,
+                                                                uint32_t l1hot, float *out) {
+    const uint64_t nq = (arcs + 3) >> 2;  // col carries kColPad slots past the last arc
+    const uint64_t pol_g = policy_evict_last();
+    float acc = 0.f;
+    for (uint64_t q = (uint64_t)blockIdx.x * kThreads + threadIdx.x; q < nq; q += (uint64_t)gridDim.x * kThreads) {
+        const uint4 c = ld_stream_u4(reinterpret_cast<const uint4 *>(col) + q, policy_evict_first());
+        auto g = [&](uint32_t v, uint64_t p) {
+            return p < arcs ? (v < l1hot ? ld_gather(x + v, pol_g) : ld_gather_na(x + v, pol_g)) : 0.f;
+        };
+        acc += (g(c.x, 4 * q) + g(c.y, 4 * q + 1)) + (g(c.z, 4 * q + 2) + g(c.w, 4 * q + 3));
+    }
+    out[(uint64_t)blockIdx.x * kThreads + threadIdx.x] = acc;
+}
+
+float gather_probe(const DeviceGraph &g, int reps, cudaStream_t s) {
+    int dev = 0, sms = 0;
+    PRG_CUDA(cudaGetDevice(&dev));
+    PRG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    const unsigned grid = (unsigned)sms * 8u;  // 2048 resident threads per SM
+    float *x = nullptr, *out = nullptr;
+    PRG_CUDA(cudaMallocAsync((void **)&x, std::max<uint64_t>(g.n, 1) * 4, s));
+    PRG_CUDA(cudaMallocAsync((void **)&out, (uint64_t)grid * kThreads * 4, s));
+    PRG_CUDA(cudaMemsetAsync(x, 0, std::max<uint64_t>(g.n, 1) * 4, s));
+    const uint32_t l1hot = g.perm != nullptr && g.l1_hot32 ? g.l1_hot32 : 0xFFFFFFFFu;
+    cudaEvent_t e0, e1;
+    PRG_CUDA(cudaEventCreate(&e0));
+    PRG_CUDA(cudaEventCreate(&e1));
+    gather_probe_kernel<<<grid, kThreads, 0, s>>>(g.col, g.arcs, x, l1hot, out);  // warm-up
+    PRG_CUDA(cudaEventRecord(e0, s));
+    for (int r = 0; r < reps; r++) gather_probe_kernel<<<grid, kThreads, 0, s>>>(g.col, g.arcs, x, l1hot, out);
+    PRG_CUDA(cudaEventRecord(e1, s));
+    PRG_CUDA(cudaGetLastError());
+    PRG_CUDA(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    PRG_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFreeAsync(x, s);
+    cudaFreeAsync(out, s);
+    PRG_CUDA(cudaStreamSynchronize(s));
+    return ms / (float)std::max(reps, 1);
+}
+
 // ------------------------------------------------------------------ elementwise
 
 constexpr unsigned kPrepBlocks = 148u * 4u;

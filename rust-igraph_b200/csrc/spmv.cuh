@@ -98,6 +98,11 @@ struct LaunchCfg {
 LaunchCfg iteration_config(int mode, bool weighted, uint32_t hot_entries, uint32_t blocks_per_sm, uint32_t n);
 void launch_iteration(int mode, bool weighted, const IterArgs &a, const LaunchCfg &c, cudaStream_t s);
 
+// Average time (ms) of a pass that only streams g's column indices and gathers
+// one FP32 value per arc with the FP32 matvec's load policies (reps timed
+// launches after one warm-up): the gather floor of g's index stream.
+float gather_probe(const DeviceGraph &g, int reps, cudaStream_t s);
+
 // x <- x + e (e may be null), xt <- x / dval, dangling sum and total sum of
 // x into ctl->dsum[parity] / ctl->gsum via a deterministic two-level tree.
 void launch_prepare64(const DeviceGraph &g, double *x, const float *e, double *xt, Ctl *ctl, int parity,

@@ -204,6 +204,8 @@ def lib():
     L.prg_eigenvector_centrality_full.restype = C.c_int32
     L.prg_eigenvector_centrality_full.argtypes = [C.c_uint32, C.c_uint64, u32p, u32p, C.c_int32, C.c_int32, f64p,
                                                   C.c_uint64, f64p, f64p]
+    L.prg_graph_gather_probe.restype = C.c_int32
+    L.prg_graph_gather_probe.argtypes = [vp, C.c_int32, C.POINTER(C.c_double)]
     L.prg_infomap_flow.restype = C.c_int32
     L.prg_infomap_flow.argtypes = [C.c_uint32, C.c_uint64, u32p, u32p, C.c_int32, f64p, C.c_uint64, f64p,
                                    C.c_uint64, f64p, C.POINTER(C.c_uint32)]
@@ -689,6 +691,13 @@ class DeviceGraph:
         stats = {"column_iterations": st.column_iterations, "max_iters": st.max_iters, "tiles": st.tiles,
                  "tile_width": st.tile_width, "kernel_launches": st.kernel_launches, "ms": st.ms}
         return X, iters[:K], stats
+
+    def gather_probe(self, reps: int = 20) -> float:
+        """Milliseconds of a gather-only pass over this graph's index stream
+        (the floor of the FP32 matvec's memory access pattern)."""
+        ms = C.c_double()
+        _check(lib().prg_graph_gather_probe(self._h, int(reps), C.byref(ms)))
+        return ms.value
 
     def close(self):
         if self._h:
