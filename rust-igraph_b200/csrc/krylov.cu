@@ -54,6 +54,7 @@ struct KState {
     int32_t norm2;     // 0: L1 norms, 1: 2-norms
     uint32_t restarts;
     uint32_t stall;    // consecutive steps without a 2x gain over the best ||r||
+    uint32_t half;     // 1: the solve ended at a half step (the last step ran one matvec)
 };
 
 enum : int32_t {
@@ -386,7 +387,8 @@ __global__ void __launch_bounds__(kVT) kv1(uint32_t n, int q, KState *st, const 
     }
 }
 
-// V2: alpha = rho / (rh.v); s = r - alpha v, s/s_deg, dangling mass of s.
+// V2: alpha = rho / (rh.v); s = r - alpha v, s/s_deg; records (dangling mass
+// of s, |s|_1, s.s), the norms for the half-step test in M2.
 template <class T>
 __global__ void __launch_bounds__(kVT) kv2(uint32_t n, int q, KState *st, const double4 *part2, uint32_t n2,
                                            const double4 *hub_rec, uint32_t nhub, const T *r, const T *v, T *s,
@@ -400,7 +402,7 @@ __global__ void __launch_bounds__(kVT) kv2(uint32_t n, int q, KState *st, const 
     }
     const double al = rho / sig;
     const T ta = (T)al;
-    double dz = 0.0;
+    double dz = 0.0, s1 = 0.0, s2 = 0.0;
     auto body = [&](uint32_t i, auto w) {
         constexpr int W = decltype(w)::value;
         T rv[W], vv[W], sv[W], sc[W];
@@ -408,7 +410,11 @@ __global__ void __launch_bounds__(kVT) kv2(uint32_t n, int q, KState *st, const 
         ldv<W, true>(r + i, rv);
         ldv<W, true>(v + i, vv);
 #pragma unroll
-        for (int j = 0; j < W; j++) sv[j] = rv[j] - ta * vv[j];
+        for (int j = 0; j < W; j++) {
+            sv[j] = rv[j] - ta * vv[j];
+            s1 += fabs((double)sv[j]);
+            s2 += (double)sv[j] * (double)sv[j];
+        }
         stv<W, true>(s + i, sv);
         kscale<W>(sv, i, inv32, dval, sc, dang);
         stv<W, false>(sst + i, sc);
@@ -418,18 +424,45 @@ __global__ void __launch_bounds__(kVT) kv2(uint32_t n, int q, KState *st, const 
     };
     kfor(n, [&](uint32_t i) { body(i, std::integral_constant<int, 4>()); },
          [&](uint32_t i) { body(i, std::integral_constant<int, 1>()); });
-    const double3 s3 = kblock3(dz, 0.0, 0.0);
-    if (threadIdx.x == 0) part3[blockIdx.x] = make_double4(s3.x, 0.0, 0.0, 0.0);
+    const double3 s3 = kblock3(dz, s1, s2);
+    if (threadIdx.x == 0) part3[blockIdx.x] = make_double4(s3.x, s3.y, s3.z, 0.0);
     if (kleader()) st->alpha[q] = al;
 }
 
 // V3: omega = (t.s)/(t.t); e += alpha p + omega s; r = s - omega t;
-// records (rh.r, |r|_1, r.r) for the next V1.
+// records (rh.r, |r|_1, r.r) for the next V1.  When M2 skipped (its marker
+// part4[0].w = 1: ||s|| met the target), the step ends at its half:
+// e += alpha p and the solve is converged.
 template <class T>
 __global__ void __launch_bounds__(kVT) kv3(uint32_t n, int q, KState *st, const double4 *part4, uint32_t n4,
-                                           const double4 *hub_rec, uint32_t nhub, const T *rh, const T *p,
-                                           const T *s, const T *t, T *e, T *r, double4 *part5) {
+                                           const double4 *hub_rec, uint32_t nhub, const double4 *part3,
+                                           const T *rh, const T *p, const T *s, const T *t, T *e, T *r,
+                                           double4 *part5) {
     if (kstopped(st)) return;
+    if (part4[0].w == 1.0) {
+        const T ta = (T)st->alpha[q];
+        auto half = [&](uint32_t i, auto w) {
+            constexpr int W = decltype(w)::value;
+            T ev[W], pv[W];
+            ldv<W, true>(e + i, ev);
+            ldv<W, true>(p + i, pv);
+#pragma unroll
+            for (int j = 0; j < W; j++) ev[j] = ev[j] + ta * pv[j];
+            stv<W, true>(e + i, ev);
+        };
+        kfor(n, [&](uint32_t i) { half(i, std::integral_constant<int, 4>()); },
+             [&](uint32_t i) { half(i, std::integral_constant<int, 1>()); });
+        if (blockIdx.x == 0) {  // the block-wide reduction runs in all of block 0's threads
+            const double3 sr = krecords(part3, gridDim.x, nullptr, 0);
+            if (threadIdx.x == 0) {
+                st->rnorm = st->norm2 ? sqrt(sr.z) : sr.y;
+                st->count += 1u;
+                st->half = 1u;
+                st->done = KDONE_CONVERGED;
+            }
+        }
+        return;
+    }
     const double3 red = krecords(part4, n4, hub_rec, nhub);
     const double ts = red.y, tt = red.z;
     const double om = tt > 0.0 && isfinite(tt) ? ts / tt : 0.0;
@@ -474,6 +507,7 @@ __global__ void __launch_bounds__(kVT) kadd64(uint32_t n, double *x, const doubl
 
 struct InnerResult {
     uint32_t steps = 0;
+    uint32_t half = 0;       // 1: the last step stopped after its first matvec
     int32_t done = KRUN;
     double rnorm = 0.0;
     double ms = 0.0;
@@ -527,7 +561,9 @@ static InnerResult bicgstab(const DeviceGraph &g, Workspace &ws, KrylovWs &k, KB
     if constexpr (sizeof(T) == 4) base.t32 = t32;
     else base.t64 = t64;
     const IterArgs m1 = matvec_args<T>(base, b.p, b.pt, b.v, b.rh, k.part1, kVB, k.part2, k.st);
-    const IterArgs m2 = matvec_args<T>(base, b.s, b.st, b.t, (const T *)nullptr, k.part3, kVB, k.part4, k.st);
+    IterArgs m2 = matvec_args<T>(base, b.s, b.st, b.t, (const T *)nullptr, k.part3, kVB, k.part4, k.st);
+    m2.ktol = &k.st->tol;  // skip t = A s when ||s|| already meets the target (half step)
+    m2.knorm2 = norm2 ? 1 : 0;
 
     // the matvec launches are bracketed by events (4 per step) so their
     // device time can be reported apart from the vector kernels
@@ -553,8 +589,8 @@ static InnerResult bicgstab(const DeviceGraph &g, Workspace &ws, KrylovWs &k, KB
         PRG_CUDA(cudaEventRecord(ev[3], s));
         launch_iteration(mode, g.weighted, m2, cfg, s);
         PRG_CUDA(cudaEventRecord(ev[4], s));
-        kv3<T><<<kVB, kVT, 0, s>>>(n, q, k.st, k.part4, cfg.grid, ws.hub_rec, g.nhub, b.rh, b.p, b.s, b.t, b.e, r,
-                                    k.part5);
+        kv3<T><<<kVB, kVT, 0, s>>>(n, q, k.st, k.part4, cfg.grid, ws.hub_rec, g.nhub, k.part3, b.rh, b.p, b.s, b.t,
+                                    b.e, r, k.part5);
         PRG_CUDA(cudaEventRecord(ev[5], s));
         res.launches += 5u;
     };
@@ -602,11 +638,12 @@ static InnerResult bicgstab(const DeviceGraph &g, Workspace &ws, KrylovWs &k, KB
     }
     res.done = k.h_st[0].done;
     res.rnorm = k.h_st[0].rnorm;
+    res.half = k.h_st[0].half;
     if (std::getenv("PRG_TRACE"))
         std::fprintf(stderr,
-                     "[prg] bicgstab<%s>: %u steps, done=%d, ||r||=%.3e (r0 %.3e), restarts %u, %.3f ms "
+                     "[prg] bicgstab<%s>: %u steps (half %u), done=%d, ||r||=%.3e (r0 %.3e), restarts %u, %.3f ms "
                      "(matvecs %.3f, vector kernels %.3f, between steps %.3f)\n",
-                     sizeof(T) == 4 ? "f32" : "f64", res.steps, res.done, res.rnorm, k.h_st[0].r0norm,
+                     sizeof(T) == 4 ? "f32" : "f64", res.steps, res.half, res.done, res.rnorm, k.h_st[0].r0norm,
                      k.h_st[0].restarts, res.ms, res.matvec_ms, vec_ms, gap_ms);
     return res;
 }
@@ -694,9 +731,9 @@ void solve_krylov(const DeviceGraph &g, Workspace &ws, const SolveOpts &o, const
         else
             ir = bicgstab<float>(g, ws, k, k.f, ws.b32, nullptr, ppr ? ws.t32 : nullptr, o.damping, rel, floor_abs,
                                  near, cap, false, s);
-        mv += 2u * ir.steps;
+        mv += 2u * ir.steps - ir.half;
         st.spmv_ms += ir.matvec_ms;
-        st.spmv_launches += 2u * ir.steps;
+        st.spmv_launches += 2u * ir.steps - ir.half;
         st.kernel_launches += ir.launches;
         st.fp32_ms += fp64_inner ? 0.0 : ir.ms;
         st.fp64_ms += fp64_inner ? ir.ms : 0.0;

@@ -360,11 +360,26 @@ __global__ void __launch_bounds__(kThreads, HOT ? (kIs32<MODE> ? 4 : 3) : (kIs32
         // dangling mass of the input vector: the producer's per-block
         // records summed in a fixed order (identical in every block)
         __shared__ double s_dz;
+        __shared__ int s_skip;
         double dz = 0.0, z1 = 0.0, z2 = 0.0;
-        for (uint32_t i = threadIdx.x; i < a.kpart_n; i += NT) dz += a.kpart_in[i].x;
+        for (uint32_t i = threadIdx.x; i < a.kpart_n; i += NT) {
+            const double4 q = a.kpart_in[i];
+            dz += q.x;
+            z1 += q.y;
+            z2 += q.z;
+        }
         block_sum3(dz, z1, z2, s_red);
-        if (threadIdx.x == 0) s_dz = dz;
+        if (threadIdx.x == 0) {
+            s_dz = dz;
+            // the BiCGStab half step already met the target: every block sums
+            // the same records in the same order, so all of them skip together
+            s_skip = a.ktol != nullptr && !((a.knorm2 ? sqrt(z2) : z1) > *a.ktol);
+        }
         __syncthreads();
+        if (s_skip) {
+            if (blockIdx.x == 0 && threadIdx.x == 0) a.kpart_out[0] = make_double4(0.0, 0.0, 0.0, 1.0);
+            return;
+        }
         u.dsum = s_dz;
         u.tele = 0.0;
         u.dshare = u.d * u.dsum;

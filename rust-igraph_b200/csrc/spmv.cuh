@@ -71,6 +71,9 @@ struct IterArgs {
     uint32_t kpart_n;
     double4 *kpart_out;       // per-block (rh.y, y.p, y.y)
     const int32_t *kdone;     // nonzero: the Krylov solve has stopped, return at once (may be null for EIG64)
+    const double *ktol;       // MODE_KRY*, optional: when the input's norm (kpart_in .y = L1 / .z = squares
+                              // summed) is <= *ktol the launch does nothing but mark kpart_out[0].w = 1
+    int32_t knorm2;           // with ktol: compare the 2-norm instead of the L1 norm
     double shift;             // MODE_EIG64: weight of the diagonal term
     // scalars
     double damping;
