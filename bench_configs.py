@@ -11,7 +11,7 @@ to tolerance, GTEPS (in-CSR arcs x passes / time), algorithmic bytes of one
 SpMV pass, the SpMV launches' HBM rate against the measured copy peak, and
 the L1 distance to a tight FP64 solve of the same graph.
 
-    python -m igraph_b200.configs [--which 1,2,3,4,5,6,7,8] [--peak-gbs 6546]
+    python bench_configs.py [--which 1,2,3,4,5,6,7,8] [--peak-gbs 6546]
 """
 from __future__ import annotations
 
@@ -20,9 +20,14 @@ import json
 import math
 import os
 
+import sys
+
 import numpy as np
 
-from . import (GEN_BLOCKS, GEN_POWERLAW, GEN_RMAT, PRECISION_FP32_REFINED, PRECISION_FP64, PRECISION_FP64_KRYLOV,
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "rust-igraph_b200"))
+
+from igraph_b200 import (GEN_BLOCKS, GEN_POWERLAW, GEN_RMAT, PRECISION_FP32_REFINED, PRECISION_FP64, PRECISION_FP64_KRYLOV,
                STOP_ERROR_BOUND, DeviceGraph, Options, generate_device)
 
 D = 0.85
@@ -31,8 +36,7 @@ D = 0.85
 def _peak(arg):
     if arg:
         return arg
-    path = os.path.join(os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__)))),
-                        "MEASURED_PEAKS.json")
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     try:
         return float(json.load(open(path))["hbm_gbs"])
     except Exception:
@@ -155,7 +159,7 @@ def config4(peak):
 
 
 def config5(peak):
-    from . import warmstart as ws
+    from igraph_b200 import warmstart as ws
 
     net = ws.WarmStartNet.load()
     for scale in (22, 23, 24):
@@ -215,7 +219,7 @@ def config6(peak):
         v = dt.cpu().numpy().view(np.uint32)
         del df, dt
         text = edgelist_text(u, v)
-        from . import parse_edgelist
+        from igraph_b200 import parse_edgelist
 
         res = {}
         for name, fn in (("parse (H2D + parse + D2H of edges)", lambda: parse_edgelist(text)),
@@ -244,7 +248,7 @@ def config7(peak):
 
     import torch
 
-    from . import Graph, eigenvector_centrality, hub_and_authority_scores
+    from igraph_b200 import Graph, eigenvector_centrality, hub_and_authority_scores
 
     for scale in (16, 20, 22):
         n, m = 1 << scale, 16 << scale
@@ -271,7 +275,7 @@ def config8(peak):
 
     import torch
 
-    from . import Graph, infomap_flow
+    from igraph_b200 import Graph, infomap_flow
 
     for scale in (16, 20, 22):
         n, m = 1 << scale, 16 << scale

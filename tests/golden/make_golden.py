@@ -1,7 +1,8 @@
 """Regenerates tests/golden/reference_fixtures.json from the reference tree.
 
-Run in a checkout that has the rust-igraph sources at REF (default
-/root/reference); the GPU box never runs this.  It collects, unchanged:
+Run in a checkout that has the rust-igraph sources, passing their path as
+the first argument (or in $RUST_IGRAPH_REF); the GPU box never runs this.
+It collects, unchanged:
 
 * the conformance fixtures the reference's own tests replay for this path
   (tests/conformance/{c,py,r}/{pagerank,pagerank_weighted,personalized_pagerank}/*.json,
@@ -23,7 +24,8 @@ import os
 import re
 import sys
 
-REF = os.environ.get("RUST_IGRAPH_REF", "/root/reference")
+# the reference checkout: first argument, else $RUST_IGRAPH_REF
+REF = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("RUST_IGRAPH_REF", "")
 OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "reference_fixtures.json")
 
 # tolerance rules of the reference drivers
@@ -35,6 +37,8 @@ TOL = {
 
 
 def main():
+    if not REF or not os.path.isdir(REF):
+        sys.exit("usage: make_golden.py <path of the rust-igraph checkout> (or set RUST_IGRAPH_REF)")
     cases = []
     for algo in ("pagerank", "pagerank_weighted", "personalized_pagerank"):
         for path in sorted(glob.glob(os.path.join(REF, "tests/conformance/*", algo, "*.json"))):

@@ -32,6 +32,19 @@ def test_library_loads_and_exports_all_symbols():
         assert hasattr(raw, n), f"missing export {n}"
 
 
+def test_rust_binding_declares_the_header():
+    """The Rust crate's FFI module (rust-igraph_b200/rust/src/ffi.rs, built
+    by cargo where a Rust toolchain exists) declares exactly the header's
+    entry points, and the status codes agree."""
+    src = open(os.path.join(ROOT, "rust-igraph_b200", "rust", "src", "ffi.rs")).read()
+    rust = sorted(set(re.findall(r"pub fn (prg_\w+)\s*\(", src)))
+    assert rust == declared_functions()
+    hdr = open(os.path.join(ROOT, "include", "prg_b200.h")).read()
+    for name, val in re.findall(r"pub const (PRG_\w+): i32 = (\d+);", src):
+        m = re.search(rf"\b{name}\s*=\s*(\d+)", hdr)
+        assert m and int(m.group(1)) == int(val), name
+
+
 def test_default_options_match_reference_constants():
     o = ig.prg_options()
     ig.lib().prg_default_options(C.byref(o))
