@@ -6,11 +6,13 @@ Workload (the precision-at-scale configuration): directed R-MAT, scale 24
 0.85.  One step = one full solve to a certified L1 error <= 1e-10 against the
 FP64 fixed point with FP32 SpMV (BiCGStab inner solves) + FP64 residual
 refinement, on a graph resident in HBM.  value = time-to-tolerance
-throughput in GTEPS: in-CSR arcs x the pass count the plain FP64 power
-iteration needs for the same certified tolerance on this graph / time to
-tolerance, summed over ranks, max time over ranks.  For the power iteration
-itself (the reference arm) that is its plain GTEPS, so the ratio of two arms
-is their ratio of time to tolerance.  The line also carries the plain FP64
+throughput in GTEPS: in-CSR arcs x the pass count of the reference's own
+loop on this graph (FP64 power iteration stopped at a successive L1 change
+< 1e-10, pagerank.rs:136-139, counted by the GPU FP64 drop-in) / our time to
+the stricter certified tolerance, summed over ranks, max time over ranks.
+For the power iteration itself (the reference arm) that is its plain GTEPS,
+so the ratio of two arms is their ratio of time to tolerance.  The line also
+gives the value normalised by the certified FP64 pass count.  The line also carries the plain FP64
 power iteration, the FP64 Krylov form and the learned warm start (inference
 included) measured in the same run.
 
@@ -285,6 +287,7 @@ def main():
     opt_ref = ig.Options(precision=ig.PRECISION_FP32_REFINED, eps=EPS, damping=D)
     opt_64 = ig.Options(precision=ig.PRECISION_FP64, stop=ig.STOP_ERROR_BOUND, eps=EPS, damping=D)
     opt_k64 = ig.Options(precision=ig.PRECISION_FP64_KRYLOV, eps=EPS, damping=D)
+    opt_succ = ig.Options(precision=ig.PRECISION_FP64, stop=ig.STOP_SUCCESSIVE, eps=EPS, damping=D)
 
     with torch.cuda.stream(stream):
         flush.fill_(0)  # first launch of the fill kernel (module load) stays out of the timed region
@@ -328,8 +331,19 @@ def main():
              "spmv_us": st64[-1].spmv_ms / max(st64[-1].spmv_launches, 1) * 1e3,
              "error_bound": st64[-1].error_bound,
              "l1_refined_vs_fp64": float((x_ref - x64).abs().sum().item())}
-    total_units = reduce(arcs * p_plain * args.steps, "sum")
+    # the reference's own stop rule (successive L1 change < 1e-10,
+    # pagerank.rs:136-139) on the same graph: the FP64 drop-in path, which the
+    # tests hold to the restatement's iteration count within 1
+    ms_succ, st_succ = timed(opt_succ, 1)
+    p_ref_rule = st_succ[-1].iterations
+    plain["ref_rule_passes"] = p_ref_rule
+    plain["ref_rule_ms"] = st_succ[-1].solve_ms
+    # value: arcs x the pass count the reference itself runs / our time to a
+    # certified L1 <= 1e-10 (the stricter target); the certified pass count
+    # gives the second normalisation
+    total_units = reduce(arcs * p_ref_rule * args.steps, "sum")
     value = total_units / (ms_max / 1e3) / 1e9
+    value_certified = reduce(arcs * p_plain * args.steps, "sum") / (ms_max / 1e3) / 1e9
 
     k64 = None
     if not args.no_plain:
@@ -412,7 +426,7 @@ def main():
         e2e_stats = [e2e_step() for _ in range(args.steps)]
         torch.cuda.synchronize()
         el = reduce(time.perf_counter() - t0, "max")
-        units = reduce(arcs * p_plain * args.steps, "sum")
+        units = reduce(arcs * p_ref_rule * args.steps, "sum")
         e2e = {"value": units / el / 1e9, "unit": "GTEPS", "h2d_bytes_per_step": 2 * 4 * m,
                "d2h_bytes_per_step": 8 * n, "ms_per_step": el / args.steps * 1e3,
                "includes": "H2D of the edge list from pinned memory, CSR build, refined solve, D2H of the result",
@@ -438,7 +452,8 @@ def main():
                "sample": f"{args.cpu_iters} iterations of the pagerank.rs:107-140 loop (C restatement) over the "
                          f"full graph, {it_s:.1f} s; in-adjacency build {b_s:.1f} s not counted; the power "
                          f"iteration's time-to-tolerance throughput equals its GTEPS",
-               "time_to_tol_s_estimate": it_s / args.cpu_iters * p_plain,
+               "time_to_tol_s_estimate": it_s / args.cpu_iters * p_ref_rule,
+               "time_to_tol_s_estimate_certified": it_s / args.cpu_iters * p_plain,
                "host_nproc": os.cpu_count(), "host_cpu": _cpu_model()}
         adj.close()
 
@@ -458,12 +473,16 @@ def main():
         "data": "synthetic",
         "config": {**workload(scale, ef), "arcs": arcs, "n_dangling": dg.n_dangling,
                    "precision": "FP32 SpMV (BiCGStab inner solves) + FP64 residual refinement",
-                   "value_definition": "time-to-tolerance throughput: in-CSR arcs x the plain FP64 power "
-                                       "iteration's pass count to the same certified tolerance / time to "
-                                       "tolerance (equals GTEPS for the power iteration)",
+                   "value_definition": "time-to-tolerance throughput: in-CSR arcs x the pass count of the "
+                                       "reference's own loop on this graph (FP64 power iteration, successive "
+                                       "L1 change < 1e-10) / our time to a certified L1 <= 1e-10 (equals GTEPS "
+                                       "for the power iteration itself)",
                    "l2": "inputs larger than L2 (CSR 1.07 GB) and a 256 MiB write between steps",
                    "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU"},
         "time_to_tol_ms": t_ref,
+        "ref_rule_passes": p_ref_rule,
+        "certified_fp64_passes": p_plain,
+        "value_certified_normalisation": value_certified,
         "solve_ms_each": [round(s.solve_ms, 2) for s in stats],
         "passes_per_solve": s0.iterations,
         "fp32_matvecs_per_solve": s0.fp32_passes,

@@ -339,13 +339,16 @@ int32_t prg_ppr_batch_device(prg_graph *g, uint32_t K, const uint64_t *seed_offs
  * for callers that must not allocate device memory at solve time, such as a
  * real-time loop that reserves memory up front or code running under another
  * framework's memory budget).  Same iteration and stop rule as prg_solve at
- * PRG_PRECISION_FP64 on a graph created earlier; d_reset: optional
- * normalised teleport vector, d_out: double[n], both device memory in caller
- * ids.  All solve scratch lives in one static device array (about 26.6 MiB
- * per GPU, held until exit); limits: n <= 524,288, <= 262,144 row-blocks,
- * <= 8,192 hub rows, FP64 only (else PRG_ERR_INVALID_ARGUMENT).  The first
- * call on a device looks up the array's address (cudaGetSymbolAddress):
- * make it before any stream capture.  Calls share the array, so calls that
+ * PRG_PRECISION_FP64 on a graph created earlier, with the same option checks;
+ * opt->start, when set, is a device start vector in caller ids.  d_reset:
+ * optional normalised teleport vector, d_out: double[n], both device memory
+ * in caller ids.  All solve scratch lives in one static device array (about
+ * 26.6 MiB per GPU, held until exit); limits: n <= 524,288, <= 262,144
+ * row-blocks, <= 8,192 hub rows, FP64 only (else PRG_ERR_INVALID_ARGUMENT).
+ * CUDA allocates that array (and loads the kernels) on first use, so
+ * creating a graph handle within those limits (prg_graph_create*,
+ * prg_read_edgelist) does it then; the solve itself, its first call
+ * included, allocates nothing.  Calls share the array, so calls that
  * overlap on the GPU race; run them one at a time. */
 int32_t prg_solve_noalloc(prg_graph *g, const prg_options *opt, const double *d_reset, double *d_out,
                           prg_stats *stats);

@@ -230,6 +230,20 @@ int32_t create_from_host(uint32_t n, uint64_t m, const uint32_t *from, const uin
     return rc;
 }
 
+// Set-up for a handle returned to the caller: the allocation-free solve's
+// scratch and kernels are loaded now, while allocating is allowed.  A
+// failure destroys the handle and propagates.
+static void prepare_handle(prg_graph *&h) {
+    try {
+        prg::noalloc_prepare(h->g);
+    } catch (...) {
+        cudaStreamSynchronize(h->stream);
+        destroy(h);
+        h = nullptr;
+        throw;
+    }
+}
+
 void destroy(prg_graph *h) {
     if (!h) return;
     cudaStream_t s = h->stream;
@@ -859,7 +873,9 @@ int32_t prg_graph_create(uint32_t n, uint64_t m, const uint32_t *from, const uin
                                                           ")");
         }
     }
-    return create_from_host(n, m, from, to, weights, directed, out);
+    const int32_t rc = create_from_host(n, m, from, to, weights, directed, out);
+    if (rc == PRG_OK) prepare_handle(*out);
+    return rc;
     PRG_GUARD_END
 }
 
@@ -874,6 +890,7 @@ int32_t prg_graph_create_device(uint32_t n, uint64_t m, const uint32_t *d_from, 
     PRG_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
     int32_t rc = create_from_device(n, m, d_from, d_to, d_weights, directed, s, out);
     if (rc != PRG_OK) cudaStreamDestroy(s);
+    else prepare_handle(*out);
     return rc;
     PRG_GUARD_END
 }
@@ -966,6 +983,7 @@ int32_t prg_read_edgelist(const char *text, uint64_t len, prg_graph **out, uint3
                 rc = create_from_device(r.n, r.m, r.d_from, r.d_to, nullptr, 0, s, out);
                 if (rc == PRG_OK) {
                     prg::el::free_result(r, s);  // the graph owns the stream from here on
+                    prepare_handle(*out);
                     return PRG_OK;
                 }
             }

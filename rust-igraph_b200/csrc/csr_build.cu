@@ -293,6 +293,11 @@ void gather_f64(double *dst, const double *src, const uint32_t *idx, uint32_t n,
     PRG_CUDA(cudaGetLastError());
 }
 
+void preload_gather_f64() {
+    cudaFuncAttributes fa;
+    PRG_CUDA(cudaFuncGetAttributes(&fa, gather_f64_kernel));
+}
+
 // ---- degree-sorted relabelling.  On skewed (power-law) graphs the vertices
 // that are gathered most often are those with the largest out-degree; giving
 // them the smallest internal ids packs the hot part of the rank vector into a

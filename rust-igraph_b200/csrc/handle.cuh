@@ -5,6 +5,12 @@
 #include "graph.cuh"
 #include "solver.cuh"
 
+namespace prg {
+// Loads the allocation-free solve's static scratch and kernels (noalloc.cu);
+// called when a handle is created, while allocating is allowed.
+void noalloc_prepare(const DeviceGraph &g);
+}  // namespace prg
+
 struct prg_graph {
     prg::DeviceGraph g;
     prg::Workspace ws;

@@ -17,18 +17,25 @@
 // and the FP64 path only; larger inputs are rejected with
 // PRG_ERR_INVALID_ARGUMENT.
 //
-// The first call on a device looks up the array's device address with
-// cudaGetSymbolAddress (host code cannot use the symbol itself: in host code
-// its name is only a stand-in); make that first call before any stream
-// capture.  All calls share the one array and it keeps the last call's
-// contents, so the parts that must start at zero (control block, hub
+// CUDA loads a module lazily, on the first use of anything in it, and that
+// load is when the device allocates the module's code and its __device__
+// arrays.  So the set-up happens when a graph within the limits below is
+// created (prg_graph_create*, prg_read_edgelist), a point where the caller
+// is allocating anyway: noalloc_prepare() looks up the array's device
+// address with cudaGetSymbolAddress (host code cannot use the symbol
+// itself: in host code its name is only a stand-in), which loads this
+// module and its array, and it loads every kernel the solve launches.  The
+// solve itself then allocates nothing, its first call on a device
+// included.  It still looks the address up on every call (cheap once the
+// module is loaded), so a context torn down and made again is never handed
+// a stale address.  All calls share the one array and it keeps the last
+// call's contents, so the parts that must start at zero (control block, hub
 // tickets) are cleared at the start of each call, and calls that overlap on
 // the GPU — on two streams, or from two threads — race on the array.
 #include <cuda_runtime.h>
 #include <stdint.h>
 
 #include <cstring>
-#include <mutex>
 #include <string>
 
 #include "../../include/prg_b200.h"
@@ -66,39 +73,54 @@ int32_t na_fail(int32_t code, const std::string &m) {
     return code;
 }
 
-// Device address of the scratch array on the current device (looked up once
-// per device; the host-side name is not a device pointer).
-void *scratch_on(int dev, cudaError_t *err) {
-    static std::mutex mu;
-    static void *ptr[256] = {};
-    std::lock_guard<std::mutex> lk(mu);
-    if (dev < 0 || dev >= 256) {
-        *err = cudaErrorInvalidDevice;
-        return nullptr;
-    }
-    if (!ptr[dev]) {
-        void *p = nullptr;
-        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (e != cudaSuccess) {
-            *err = e;
-            return nullptr;
-        }
-        ptr[dev] = p;
-    }
-    return ptr[dev];
+// Device address of the scratch array on the current device.  The host-side
+// name is not a device pointer; the lookup also loads this module (and so
+// the array) if nothing has loaded it yet.
+void *scratch_address(cudaError_t *err) {
+    void *p = nullptr;
+    *err = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    return *err == cudaSuccess ? p : nullptr;
+}
+
+bool within_limits(const prg::DeviceGraph &g) {
+    return g.n <= kNaMaxN && g.nrb <= kNaMaxRb && g.nhub <= kNaMaxHub;
 }
 
 }  // namespace
 
+namespace prg {
+
+// Called when a graph handle is created (api.cu), while allocating is
+// allowed: loads this module's scratch array and every kernel the
+// allocation-free solve launches, so that solve allocates nothing later.
+// Graphs beyond the limits skip it (the solve rejects them anyway).
+void noalloc_prepare(const DeviceGraph &g) {
+    if (!within_limits(g) || g.n < 2) return;
+    cudaError_t e = cudaSuccess;
+    if (!scratch_address(&e)) throw CudaError(e, "cudaGetSymbolAddress(g_noalloc_scratch)");
+    iteration_config(MODE_PLAIN64, g.weighted, 0, g.blocks_per_sm, g.n);
+    iteration_config(MODE_PPR64, g.weighted, 0, g.blocks_per_sm, g.n);
+    preload_fp64_support();
+}
+
+}  // namespace prg
+
 extern "C" int32_t prg_solve_noalloc(prg_graph *h, const prg_options *opt, const double *d_reset, double *d_out,
                                      prg_stats *st) {
     prg::set_last_error("");
+    if (st) std::memset(st, 0, sizeof(*st));
     if (!h) return na_fail(PRG_ERR_INVALID_ARGUMENT, "null graph handle");
     prg_options o;
     prg_default_options(&o);
     if (opt) o = *opt;
     const prg::DeviceGraph &g = h->g;
     const uint32_t n = g.n;
+    // the checks prg_solve_device makes, then this entry point's own limits
+    if (o.precision < PRG_PRECISION_FP64 || o.precision > PRG_PRECISION_LINSYS)
+        return na_fail(PRG_ERR_INVALID_ARGUMENT, "unknown precision " + std::to_string(o.precision));
+    if (o.stop != PRG_STOP_SUCCESSIVE && o.stop != PRG_STOP_ERROR_BOUND)
+        return na_fail(PRG_ERR_INVALID_ARGUMENT, "unknown stop rule " + std::to_string(o.stop));
+    if (!(o.eps > 0.0)) return na_fail(PRG_ERR_INVALID_ARGUMENT, "eps must be positive");
     if (o.precision != PRG_PRECISION_FP64)
         return na_fail(PRG_ERR_INVALID_ARGUMENT, "the allocation-free solve runs the FP64 path only");
     if (!(o.damping > 0.0 && o.damping < 1.0))
@@ -113,19 +135,21 @@ extern "C" int32_t prg_solve_noalloc(prg_graph *h, const prg_options *opt, const
                                                      " hub rows; the allocation-free solve supports at most " +
                                                      std::to_string(kNaMaxRb) + " and " + std::to_string(kNaMaxHub));
     cudaStream_t s = h->stream;
-    if (n == 0) return PRG_OK;
-    if (n == 1) {
-        const double one = 1.0;
-        if (cudaMemcpy(d_out, &one, 8, cudaMemcpyHostToDevice) != cudaSuccess)
-            return na_fail(PRG_ERR_CUDA, "cuda: copy failed");
-        return PRG_OK;
-    }
     try {
         int dev = 0;
         PRG_CUDA(cudaGetDevice(&dev));
         if (dev != g.device) return na_fail(PRG_ERR_INVALID_ARGUMENT, "the graph lives on another device");
+        if (n == 0) return PRG_OK;
+        if (n == 1) {
+            // a single vertex holds all the mass (pagerank.rs:62-64); the copy
+            // is ordered after earlier work on the graph's stream
+            static const double one = 1.0;
+            PRG_CUDA(cudaMemcpyAsync(d_out, &one, 8, cudaMemcpyHostToDevice, s));
+            PRG_CUDA(cudaStreamSynchronize(s));
+            return PRG_OK;
+        }
         cudaError_t e = cudaSuccess;
-        unsigned char *base = static_cast<unsigned char *>(scratch_on(dev, &e));
+        unsigned char *base = static_cast<unsigned char *>(scratch_address(&e));
         if (!base) return na_fail(PRG_ERR_CUDA, std::string("cuda: scratch lookup: ") + cudaGetErrorString(e));
         prg::Ctl *ctl = reinterpret_cast<prg::Ctl *>(base + kOffCtl);
         double4 *blk = reinterpret_cast<double4 *>(base + kOffBlk);
@@ -163,7 +187,14 @@ extern "C" int32_t prg_solve_noalloc(prg_graph *h, const prg_options *opt, const
                 t = d_reset;
             }
         }
-        prg::launch_fill_start(x0, t, n, s);
+        if (o.start) {
+            // a caller-supplied start vector in device memory, used as given
+            // (as prg_solve_device does), mapped to internal ids
+            if (g.perm) prg::gather_f64(x0, o.start, g.perm, n, s);
+            else PRG_CUDA(cudaMemcpyAsync(x0, o.start, (size_t)n * 8, cudaMemcpyDeviceToDevice, s));
+        } else {
+            prg::launch_fill_start(x0, t, n, s);
+        }
         prg::launch_prepare64(g, x0, nullptr, xt0, ctl, 0, blk, s);
 
         prg::IterArgs a0;

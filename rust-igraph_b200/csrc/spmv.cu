@@ -744,4 +744,14 @@ void launch_fill_start(double *x, const double *t, uint32_t n, cudaStream_t s) {
     PRG_CUDA(cudaGetLastError());
 }
 
+void preload_gather_f64();  // csr_build.cu
+
+void preload_fp64_support() {
+    cudaFuncAttributes fa;
+    PRG_CUDA(cudaFuncGetAttributes(&fa, fill_start_kernel));
+    PRG_CUDA(cudaFuncGetAttributes(&fa, prepare64_kernel));
+    PRG_CUDA(cudaFuncGetAttributes(&fa, prepare64_final));
+    preload_gather_f64();
+}
+
 }  // namespace prg

@@ -114,5 +114,8 @@ void launch_prepare64(const DeviceGraph &g, double *x, const float *e, double *x
 void launch_normalise(double *x, uint32_t n, const Ctl *ctl, cudaStream_t s);
 // x <- t (FP64 copy) or uniform 1/n when t is null.
 void launch_fill_start(double *x, const double *t, uint32_t n, cudaStream_t s);
+// Loads the start, prepare and id-gather kernels now (CUDA loads kernels
+// lazily, allocating device memory at that point).
+void preload_fp64_support();
 
 }  // namespace prg

@@ -322,6 +322,21 @@ class Graph:
 
 # ------------------------------------------------------------------ drop-ins
 
+    # Graph methods that delegate to the free functions, as the reference's
+    # do (src/core/graph.rs:1857-1859, 5454-5456, 6285-6289, 7002-7004).
+    def pagerank(self) -> np.ndarray:
+        return pagerank(self)
+
+    def pagerank_weighted(self, weights) -> np.ndarray:
+        return pagerank_weighted(self, weights)
+
+    def personalized_pagerank(self, reset) -> np.ndarray:
+        """personalized_pagerank_default: damping 0.85 (graph.rs:6285-6289)."""
+        return personalized_pagerank_default(self, reset)
+
+    def pagerank_linsys(self) -> np.ndarray:
+        return pagerank_linsys(self)
+
 
 def pagerank(graph: Graph) -> np.ndarray:
     """rust-igraph ``pagerank(&Graph)`` (pagerank.rs:52-143) on the GPU."""
@@ -658,12 +673,13 @@ class DeviceGraph:
         _check(lib().prg_autotune(self._h, int(batch), cache_path.encode() if cache_path else None, C.byref(r)))
         return {k: getattr(r, k) for k, _ in prg_tune_result._fields_ if k != "pad"}
 
-    def solve_noalloc(self, d_out: int, options: Optional[Options] = None, d_reset: int = 0):
+    def solve_noalloc(self, d_out: int, options: Optional[Options] = None, d_reset: int = 0, d_start: int = 0):
         """FP64 solve into a device buffer with no device allocation inside
-        the call (prg_solve_noalloc); d_reset: normalised teleport vector."""
+        the call (prg_solve_noalloc); d_reset: normalised teleport vector,
+        d_start: optional device start vector (caller ids)."""
         o = options or Options()
         st = prg_stats()
-        co = o.to_c(None)
+        co = o.to_c(C.c_void_p(d_start) if d_start else None)
         _check(lib().prg_solve_noalloc(self._h, C.byref(co), C.c_void_p(d_reset) if d_reset else None,
                                        C.c_void_p(d_out), C.byref(st)))
         return Stats.from_c(st)

@@ -287,3 +287,20 @@ def test_shared_memory_hot_prefix_keeps_parity(cuda_ok):
                 assert np.abs(x - tight).sum() <= L1_TOL and st.error_bound <= L1_TOL
     finally:
         ig.reset_tuning()
+
+
+def test_graph_methods_delegate(cuda_ok):
+    # Graph.pagerank / .pagerank_weighted / .personalized_pagerank /
+    # .pagerank_linsys call the free functions (graph.rs:1857-1859,
+    # 5454-5456, 6285-6289, 7002-7004); personalized uses damping 0.85
+    n = 2_000
+    f, t = O.erdos_renyi_gnm(n, 12_000, False, False, 41)
+    g = ig.Graph.from_edge_arrays(n, f, t, False)
+    w = O.uniform_weights(len(f), 42)
+    r = np.zeros(n)
+    r[[3, 7, 1999]] = [1.0, 0.5, 0.5]
+    assert np.abs(g.pagerank() - O.pagerank(n, f, t, False)).max() <= 1e-10
+    assert np.abs(g.pagerank_weighted(w) - O.pagerank_weighted(n, f, t, False, w)).max() <= 1e-10
+    assert np.abs(g.personalized_pagerank(r) - O.personalized_pagerank(n, f, t, False, r, 0.85)).max() \
+        <= 1e-10
+    assert np.array_equal(g.pagerank_linsys(), ig.pagerank_linsys(g))

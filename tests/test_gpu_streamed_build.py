@@ -1,7 +1,8 @@
 """The streamed build from host edge arrays (edge lists of >= 2^23 edges:
 chunked host -> device copies overlapped with per-chunk sorts, then one scan
 and one scatter) against the one-shot build from device arrays: the same
-row_ptr, col and vertex numbering, hence bit-identical solves."""
+row_ptr, col and vertex numbering, hence bit-identical solves; the weighted
+case is also checked against the restatement of pagerank_weighted()."""
 import ctypes as C
 
 import numpy as np
@@ -83,6 +84,11 @@ def test_undirected_weighted_matches_device_build(cuda_ok):
     # the drop-in goes through the streamed build as well
     got = ig.pagerank_weighted(ig.Graph.from_edge_arrays(n, f, t, False), w)
     assert np.max(np.abs(got - xa)) <= 1e-12
+    # and both agree with the restatement of pagerank_weighted() (the host
+    # sorts of graph.rs:1708-1768 that the streamed build replaces)
+    ref = O.pagerank_weighted(n, f, t, False, w)
+    assert np.max(np.abs(xb - ref)) <= 1e-10
+    assert np.max(np.abs(got - ref)) <= 1e-10
 
 
 def test_out_of_range_endpoint_is_reported(cuda_ok):
