@@ -300,6 +300,8 @@ int32_t prg_autotune(prg_graph *g, int32_t tune_batch, const char *cache_path, p
  * i.e. 1e-4), "l1_hot32" / "l1_hot64" (relabelled graphs: FP32 / FP64
  * passes gather sources with ids >= value without allocating in L1, so L1
  * keeps the most-gathered prefix; defaults 16384 / 2048, 0 = all allocate),
+ * "batch_cheb" (batched solver on undirected graphs: 1 Chebyshev steps, the
+ * default, 0 plain power steps),
  * "batch_barrier_extra" (failure-detection test hook, 0 or 1: with 1 every
  * grid barrier of the batched solver waits for an arrival that never comes,
  * so its bounded wait (about 1.5 s) expires and the call returns
@@ -315,6 +317,8 @@ typedef struct prg_batch_stats {
     uint32_t tile_width;        /* columns per tile (32 * vec) */
     uint32_t kernel_launches;
     double ms;                  /* device time (CUDA events) */
+    uint32_t chebyshev;         /* 1: Chebyshev steps (undirected graph), 0: plain power steps */
+    uint32_t pad;
 } prg_batch_stats;
 
 /* K personalized PageRank vectors at once (FP32 SpMM with FP32 accumulation).
@@ -322,7 +326,13 @@ typedef struct prg_batch_stats {
  * (personalized_pagerank.rs:241-268 building the reset, :65-182 iterating)
  * with seeds_k = seeds[seed_offsets[k] .. seed_offsets[k+1]) in caller ids,
  * stopped per column when its successive L1 change is < tol (the column then
- * freezes while the others continue) or after max_iter iterations.
+ * freezes while the others continue) or after max_iter iterations.  On an
+ * undirected graph (real spectrum) the iterates between those tests are
+ * Chebyshev steps over an interval each column estimates from the settled
+ * contraction ratio of its first power steps (tuning key "batch_cheb" = 0
+ * turns them off): the test is still the change one power step makes,
+ * ||G(x) - x||_1 < tol, and the column returns that step, G(x), as the
+ * reference does; only the sequence of iterates before it is shorter.
  * tile_vec: columns per tile = 32 * tile_vec (1, 2 or 4; 0 = autotuned or 1).
  * out: host float[n * K], out[v * K + k].  column_iters: optional host
  * uint32[K].  Validation follows _vs: empty seed list or vertex >= n ->

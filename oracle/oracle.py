@@ -52,6 +52,9 @@ def lib():
                               _u32p, _u32p, C.c_int]
         L.or_uniform_weights.restype = None
         L.or_uniform_weights.argtypes = [C.c_uint64, C.c_uint64, C.c_double, C.c_double, _f64p]
+        L.or_ppr_residuals.restype = C.c_int
+        L.or_ppr_residuals.argtypes = [C.c_uint32, C.c_uint64, _u32p, _u32p, C.c_int, C.c_uint32, C.c_void_p,
+                                       C.c_void_p, C.c_double, C.c_void_p, C.c_void_p, C.c_int]
         L.or_free.restype = None
         L.or_free.argtypes = [C.c_void_p]
         L.or_pagerank.restype = C.c_int
@@ -280,6 +283,25 @@ def pagerank_tight(n, frm, to, directed, weights=None, reset=None, damping=0.85,
         None if r is None else r.ctypes.data_as(C.c_void_p),
         damping, tol, max_iter, int(start is not None), out, C.byref(ld), nthreads or (os.cpu_count() or 1))
     return out[:n], int(it), ld.value
+
+
+def ppr_residuals(n, frm, to, directed, seed_lists, X, damping=0.85, nthreads=0):
+    """||G_k(x_k) - x_k||_1 per column of a batched result X (float32 [n, K])
+    under the personalized_pagerank operator with the _vs reset of each
+    seed list; ||x_k - x*_k||_1 <= res / (1 - damping)."""
+    f, t = _edges(frm, to)
+    K = len(seed_lists)
+    off = np.zeros(K + 1, np.uint64)
+    off[1:] = np.cumsum([len(x) for x in seed_lists])
+    seeds = np.ascontiguousarray(np.concatenate([np.asarray(x, np.uint32) for x in seed_lists]), dtype=np.uint32)
+    X = np.ascontiguousarray(X, dtype=np.float32)
+    assert X.shape == (n, K)
+    res = np.zeros(K, np.float64)
+    L = lib()
+    L.or_ppr_residuals(n, len(f), f, t, int(directed), K, off.ctypes.data_as(C.c_void_p),
+                       seeds.ctypes.data_as(C.c_void_p), damping, X.ctypes.data_as(C.c_void_p),
+                       res.ctypes.data_as(C.c_void_p), nthreads or (os.cpu_count() or 1))
+    return res
 
 
 class RefAdjacency:

@@ -594,6 +594,91 @@ int or_personalized_pagerank(uint32_t n, uint64_t m, const uint32_t *from, const
     return 0;
 }
 
+/* Residuals of K personalized vectors against the operator of
+ * personalized_pagerank.rs:149-182: for column k with reset r_k uniform over
+ * seeds[off[k] .. off[k+1]) (duplicates add weight, as _vs builds it at
+ * :241-268) and the vector x_k = X[v*K + k] (float, row-major, as the
+ * batched solver returns it), res[k] = ||G_k(x_k) - x_k||_1 with
+ *   G_k(x)[v] = (1-d) r_k[v] + d (sum_{u->v} x[u]/outdeg[u] + dsum_k(x) r_k[v]),
+ * in FP64.  G_k is an L1 contraction with factor d, so ||x_k - x*_k||_1 <=
+ * res[k] / (1 - d): a certificate for every column from one pass.
+ * Multithreaded over row chunks. */
+typedef struct {
+    uint32_t n, K; const uint64_t *rp; const uint32_t *src; const double *inv;
+    const float *X; const uint64_t *sp; const uint32_t *scol; const double *sw;
+    const double *dsum; double damping; double *part; int nchunk;
+} pres_ctx;
+static void pres_part(void *c_, int t, int nt) {
+    pres_ctx *c = (pres_ctx *)c_;
+    const uint32_t K = c->K;
+    double *acc = (double *)malloc((size_t)K * sizeof(double));
+    double *r = (double *)malloc((size_t)K * sizeof(double));
+    double *pr = c->part + (size_t)t * K;
+    for (uint32_t k = 0; k < K; k++) pr[k] = 0.0;
+    for (int ch = t; ch < c->nchunk; ch += nt) {
+        uint64_t lo = (uint64_t)c->n * ch / c->nchunk, hi = (uint64_t)c->n * (ch + 1) / c->nchunk;
+        for (uint64_t v = lo; v < hi; v++) {
+            for (uint32_t k = 0; k < K; k++) { acc[k] = 0.0; r[k] = 0.0; }
+            for (uint64_t p = c->rp[v]; p < c->rp[v + 1]; p++) {
+                const uint32_t u = c->src[p];
+                const double iv = c->inv[u];
+                const float *xu = c->X + (size_t)u * K;
+                for (uint32_t k = 0; k < K; k++) acc[k] += (double)xu[k] * iv;
+            }
+            for (uint64_t e = c->sp[v]; e < c->sp[v + 1]; e++) r[c->scol[e]] += c->sw[e];
+            const float *xv = c->X + (size_t)v * K;
+            for (uint32_t k = 0; k < K; k++) {
+                const double g = (1.0 - c->damping) * r[k] + c->damping * (acc[k] + c->dsum[k] * r[k]);
+                pr[k] += fabs(g - (double)xv[k]);
+            }
+        }
+    }
+    free(acc); free(r);
+}
+int or_ppr_residuals(uint32_t n, uint64_t m, const uint32_t *from, const uint32_t *to, int directed, uint32_t K,
+                     const uint64_t *off, const uint32_t *seeds, double damping, const float *X, double *res,
+                     int nthreads) {
+    if (n == 0 || K == 0) return 0;
+    if (nthreads < 1) nthreads = 1;
+    if (nthreads > 256) nthreads = 256;
+    uint64_t *deg = out_degrees(n, m, from, to, directed);
+    double *inv = (double *)malloc((size_t)n * sizeof(double));
+    for (uint32_t v = 0; v < n; v++) inv[v] = deg[v] ? 1.0 / (double)deg[v] : 0.0;
+    uint64_t *rp; uint32_t *src;
+    build_in_adj(n, m, from, to, directed, NULL, &rp, &src, NULL);
+    /* seed entries as a vertex-major list of (column, weight) */
+    const uint64_t S = off[K];
+    uint64_t *sp = (uint64_t *)calloc((size_t)n + 1, sizeof(uint64_t));
+    for (uint64_t i = 0; i < S; i++) sp[seeds[i] + 1]++;
+    for (uint32_t v = 0; v < n; v++) sp[v + 1] += sp[v];
+    uint64_t *cur = (uint64_t *)malloc(((size_t)n + 1) * sizeof(uint64_t));
+    memcpy(cur, sp, ((size_t)n + 1) * sizeof(uint64_t));
+    uint32_t *scol = (uint32_t *)malloc((S ? S : 1) * sizeof(uint32_t));
+    double *sw = (double *)malloc((S ? S : 1) * sizeof(double));
+    for (uint32_t k = 0; k < K; k++) {
+        const double w = 1.0 / (double)(off[k + 1] - off[k]);
+        for (uint64_t i = off[k]; i < off[k + 1]; i++) {
+            const uint64_t p = cur[seeds[i]]++;
+            scol[p] = k;
+            sw[p] = w;
+        }
+    }
+    double *dsum = (double *)calloc(K, sizeof(double));
+    for (uint32_t v = 0; v < n; v++)
+        if (deg[v] == 0)
+            for (uint32_t k = 0; k < K; k++) dsum[k] += (double)X[(size_t)v * K + k];
+    double *part = (double *)calloc((size_t)nthreads * K, sizeof(double));
+    pres_ctx c = {n, K, rp, src, inv, X, sp, scol, sw, dsum, damping, part, 1024};
+    par_run(nthreads, pres_part, &c);
+    for (uint32_t k = 0; k < K; k++) {
+        double tot = 0.0;
+        for (int t = 0; t < nthreads; t++) tot += part[(size_t)t * K + k];
+        res[k] = tot;
+    }
+    free(deg); free(inv); free(rp); free(src); free(sp); free(cur); free(scol); free(sw); free(dsum); free(part);
+    return 0;
+}
+
 /* Timed CPU-baseline kernel: `iters` iterations of the pagerank.rs:107-140
  * loop over a prebuilt in-adjacency, starting from the uniform vector. The
  * adjacency build (pagerank.rs:63-101) is a separate call so the two phases

@@ -1134,6 +1134,8 @@ static int32_t batch_common(prg_graph *h, uint32_t K, const uint64_t *off, const
         st->tile_width = 32 * bs.vec;
         st->kernel_launches = bs.kernel_launches;
         st->ms = bs.ms;
+        st->chebyshev = bs.chebyshev;
+        st->pad = 0;
     }
     if (rc == PRG_ERR_TIMEOUT) return fail(PRG_ERR_TIMEOUT, "batched solve: a grid barrier timed out");
     if (rc != 0) return fail(PRG_ERR_INTERNAL, "batched solve: device status " + std::to_string(rc));
@@ -1342,6 +1344,9 @@ int32_t prg_set_tuning(const char *key, int64_t value) {
         t.batch_vec = (uint32_t)value;
     } else if (k == "refine_switch_e12") {
         t.refine_switch = (double)value * 1e-12;
+    } else if (k == "batch_cheb") {
+        if (value != 0 && value != 1) return fail(PRG_ERR_INVALID_ARGUMENT, "batch_cheb must be 0 or 1");
+        t.batch_cheb = (uint32_t)value;
     } else if (k == "batch_barrier_extra") {
         if (value > 1) return fail(PRG_ERR_INVALID_ARGUMENT, "batch_barrier_extra must be 0 or 1");
         t.batch_barrier_extra = (uint32_t)value;

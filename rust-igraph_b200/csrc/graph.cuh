@@ -79,7 +79,8 @@ struct Tuning {
     double refine_switch = 5e-7;
     uint32_t batch_vec = 1;
     double krylov_rel = 1e-4;
-    uint32_t batch_barrier_extra = 0;  // test hook: batched grid barriers wait for arrivals that never come  // refined Krylov: relative residual reduction per FP32 inner solve
+    uint32_t batch_barrier_extra = 0;  // test hook: batched grid barriers wait for arrivals that never come
+    uint32_t batch_cheb = 1;           // batched solver on undirected graphs: 1 Chebyshev steps, 0 plain steps
 };
 Tuning &tuning();
 

@@ -17,6 +17,23 @@
 // destination row at a time.  Reset vectors are sparse: a per-vertex seed
 // list (vertex-sorted CSR of (column, weight) entries).
 //
+// Undirected graphs (by default) take Chebyshev semi-iteration in place of
+// the plain step.  The iteration x -> G(x) = d P^T(x/s) + d (dangling mass)
+// r + (1-d) r has a real spectrum in [-d, d] there: P = D^-1 A is similar to
+// the symmetric D^-1/2 A D^-1/2, and the dangling term only adds a block
+// that is triangular to it.  Once the column's own contraction ratio
+// (successive changes of its plain steps) has settled, it gives an interval
+// [-beta, beta] (beta <= d), and each later step is
+//     x_{k+1} = w_{k+1} (G(x_k) - x_{k-1}) + x_{k-1},
+//     w_2 = 2 / (2 - beta^2),  w_{k+1} = 1 / (1 - beta^2 w_k / 4)
+// (Golub & Varga's recurrence).  For a symmetric interval the iteration
+// converges for every eigenvalue of modulus < 1, so a low estimate of beta
+// only slows it.  The stop test is the reference's: the change a power step
+// makes, ||G(x_k) - x_k||_1 < tol, and the column's answer is that step,
+// G(x_k), kept in F; it lies within d/(1-d) tol of the fixed point, as the
+// reference's answer does.  Directed graphs (complex spectra) always take
+// the plain step.
+//
 // One cooperative persistent launch runs all iterations of a tile.  Phases
 // are separated by a grid barrier whose spin is bounded: if a barrier does
 // not complete within ~1.5 s the kernel records PRG_ERR_TIMEOUT in its status
@@ -43,8 +60,19 @@ struct ColState {
     uint32_t iters;
     uint32_t active;  // 1 until the column converged or hit max_iter
     uint32_t final_buf;
-    uint32_t pad;
+    uint32_t cheb_steps;  // Chebyshev steps taken (0 = still in the plain phase)
+    double prev_diff;     // the change before `diff`
+    double prev_ratio;    // the contraction ratio before the last one
+    double beta;          // Chebyshev interval half-width
+    double omega;         // weight of the next step (0 = plain step)
 };
+
+// A column leaves its plain steps once its contraction ratio diff/prev_diff
+// has settled (two successive ratios within kChebSettle, at least
+// kChebMinPower steps) or after kChebMaxPower steps; the ratio, which by
+// then follows the slowest modes, times kChebMargin is the half-width beta.
+constexpr uint32_t kChebMinPower = 6, kChebMaxPower = 24;
+constexpr double kChebSettle = 0.01, kChebMargin = 1.05;
 
 struct TileArgs {
     const uint32_t *row_ptr;
@@ -57,8 +85,10 @@ struct TileArgs {
     const uint32_t *seed_ptr;  // n+1, vertex-sorted seed entries
     const uint32_t *seed_col;  // global column of each entry
     const float *seed_w;       // weight of each entry
-    float *X[2];
+    float *X[3];        // iterates; X[2] only with Chebyshev steps (x_{k-1})
     float *XT[2];
+    float *F;           // Chebyshev: each active column's last G(x_k), the answer once it freezes
+    int cheb;           // 1: Chebyshev semi-iteration (undirected graphs)
     ColState *cs;       // tile_w entries
     double *bpart;      // [gridDim][W][2] per-block (diff, dsum) partials
     uint32_t *bar;      // [0] arrivals, [1] generation
@@ -198,12 +228,29 @@ __device__ __forceinline__ void reduce_columns(const TileArgs &a, int parity_new
             if (init) {
                 s.dsum = ty;
             } else if (s.active) {
+                s.prev_diff = s.diff;
                 s.diff = tx;
                 s.dsum = ty;
                 s.iters += 1u;
                 if (tx < a.tol || s.iters >= a.max_iter) {
                     s.active = 0u;
                     s.final_buf = (uint32_t)parity_new;
+                } else if (a.cheb) {
+                    const double ratio = s.prev_diff > 0.0 ? tx / s.prev_diff : a.damping;
+                    if (s.cheb_steps == 0u && s.iters >= kChebMinPower &&
+                        (fabs(ratio - s.prev_ratio) <= kChebSettle || s.iters >= kChebMaxPower)) {
+                        // settled contraction ratio of the plain steps -> interval
+                        double b = kChebMargin * ratio;
+                        if (!(b > 0.05)) b = 0.05;
+                        if (!(b < a.damping)) b = a.damping;
+                        s.beta = b;
+                        s.omega = 2.0 / (2.0 - b * b);
+                        s.cheb_steps = 1u;
+                    } else if (s.cheb_steps > 0u) {
+                        s.omega = 1.0 / (1.0 - 0.25 * s.beta * s.beta * s.omega);
+                        s.cheb_steps += 1u;
+                    }
+                    s.prev_ratio = ratio;
                 }
             }
         }
@@ -239,15 +286,22 @@ __global__ void __launch_bounds__(kBThreads) ppr_tile_kernel(const TileArgs a) {
 
     for (uint32_t it = 0;; it++) {
         const int cur = it & 1, nxt = cur ^ 1;
-        // column flags and dangling shares for this iteration (column state
-        // was written by other blocks before the last barrier)
+        // iterate buffers: two in rotation, three with Chebyshev steps
+        const int xc = a.cheb ? (int)(it % 3u) : cur;
+        const int xn_ = a.cheb ? (int)((it + 1u) % 3u) : nxt;
+        const int xp = (int)((it + 2u) % 3u);
+        // column flags, dangling shares and step weights for this iteration
+        // (column state was written by other blocks before the last barrier)
         bool act[VEC];
-        float dsh[VEC];
+        float dsh[VEC], om[VEC];
+        bool any_om = false;
 #pragma unroll
         for (int j = 0; j < VEC; j++) {
             const uint32_t c = lane * VEC + j;
             act[j] = c < a.tile_w && __ldcg(&a.cs[c].active) != 0u;
             dsh[j] = act[j] ? (float)__ldcg(&a.cs[c].dsum) : 0.0f;
+            om[j] = act[j] && a.cheb ? (float)__ldcg(&a.cs[c].omega) : 0.0f;
+            any_om |= om[j] != 0.0f;
         }
         if (threadIdx.x < 32) {
             int anyc = 0;
@@ -305,25 +359,37 @@ __global__ void __launch_bounds__(kBThreads) ppr_tile_kernel(const TileArgs a) {
                     if (c == a.tile_base + lane * VEC + j) r[j] += w;
             }
             const float iv = __ldg(&a.inv32[v]);
-            const Vec<VEC> old = ldv_cg<VEC>(a.X[cur] + (size_t)v * W + lane * VEC);
-            Vec<VEC> xn, xtn;
+            const Vec<VEC> old = ldv_cg<VEC>(a.X[xc] + (size_t)v * W + lane * VEC);
+            Vec<VEC> prev{};
+            if (any_om) prev = ldv_cg<VEC>(a.X[xp] + (size_t)v * W + lane * VEC);
+            Vec<VEC> xn, xtn, gv;
 #pragma unroll
             for (int j = 0; j < VEC; j++) {
-                // personalized_pagerank.rs:169-170 in FP32
+                // personalized_pagerank.rs:169-170 in FP32: g = G(x_k)
                 const float val = (1.0f - d) * r[j] + d * (acc[j] + dsh[j] * r[j]);
-                xn.v[j] = act[j] ? val : old.v[j];
+                gv.v[j] = val;
+                // Chebyshev step, or the plain step when om == 0
+                const float step = om[j] != 0.0f ? __fmaf_rn(om[j], val - prev.v[j], prev.v[j]) : val;
+                xn.v[j] = act[j] ? step : old.v[j];
                 xtn.v[j] = xn.v[j] * iv;
                 if (act[j]) {
                     pd[j] += fabs((double)val - (double)old.v[j]);
-                    if (iv == 0.0f) pds[j] += (double)val;
+                    if (iv == 0.0f) pds[j] += (double)xn.v[j];
                 }
             }
-            stv<VEC>(a.X[nxt] + (size_t)v * W + lane * VEC, xn);
+            stv<VEC>(a.X[xn_] + (size_t)v * W + lane * VEC, xn);
             stv<VEC>(a.XT[nxt] + (size_t)v * W + lane * VEC, xtn);
+            if (a.cheb) {
+                // the answer of a column that freezes now: its power step
+                float *f = a.F + (size_t)v * W + lane * VEC;
+#pragma unroll
+                for (int j = 0; j < VEC; j++)
+                    if (act[j]) f[j] = gv.v[j];
+            }
         }
         block_columns<VEC>(a, pd, pds, sh);
         if (!grid_sync(a)) return;
-        reduce_columns<VEC>(a, nxt, false, sh);
+        reduce_columns<VEC>(a, xn_, false, sh);
         if (!grid_sync(a)) return;
     }
 }
@@ -431,11 +497,16 @@ int ppr_batch(const DeviceGraph &g, uint32_t K, const uint64_t *seed_offsets, co
     PRG_CUDA(cudaMemcpyAsync(sptr, hptr.data(), ((size_t)n + 1) * 4, cudaMemcpyHostToDevice, s));
     uint32_t *kk = ev;
 
-    // tile buffers
-    float *X[2], *XT[2];
+    // tile buffers (Chebyshev steps need a third iterate and the answers F)
+    const bool cheb = !g.directed && tuning().batch_cheb != 0;
+    float *X[3] = {nullptr, nullptr, nullptr}, *XT[2], *F = nullptr;
     for (int i = 0; i < 2; i++) {
         A((void **)&X[i], (size_t)n * W * 4);
         A((void **)&XT[i], (size_t)n * W * 4);
+    }
+    if (cheb) {
+        A((void **)&X[2], (size_t)n * W * 4);
+        A((void **)&F, (size_t)n * W * 4);
     }
     const int grid = vec == 4 ? tile_grid<4>() : vec == 2 ? tile_grid<2>() : tile_grid<1>();
     ColState *cs = nullptr;
@@ -480,8 +551,11 @@ int ppr_batch(const DeviceGraph &g, uint32_t K, const uint64_t *seed_offsets, co
         a.seed_w = ews;
         a.X[0] = X[0];
         a.X[1] = X[1];
+        a.X[2] = X[2];
         a.XT[0] = XT[0];
         a.XT[1] = XT[1];
+        a.F = F;
+        a.cheb = cheb ? 1 : 0;
         a.cs = cs;
         a.bpart = bpart;
         a.bar = bar;
@@ -492,7 +566,8 @@ int ppr_batch(const DeviceGraph &g, uint32_t K, const uint64_t *seed_offsets, co
         if (vec == 4) run_tile<4>(a, grid, s);
         else if (vec == 2) run_tile<2>(a, grid, s);
         else run_tile<1>(a, grid, s);
-        tile_writeback<<<148 * 8, 256, 0, s>>>(X[0], X[1], cs, n, W, tw, tb, K, g.perm, d_out);
+        if (cheb) tile_writeback<<<148 * 8, 256, 0, s>>>(F, F, cs, n, W, tw, tb, K, g.perm, d_out);
+        else tile_writeback<<<148 * 8, 256, 0, s>>>(X[0], X[1], cs, n, W, tw, tb, K, g.perm, d_out);
         PRG_CUDA(cudaGetLastError());
         int32_t hs = 0;
         PRG_CUDA(cudaMemcpyAsync(&hs, status, 4, cudaMemcpyDeviceToHost, s));
@@ -515,11 +590,12 @@ int ppr_batch(const DeviceGraph &g, uint32_t K, const uint64_t *seed_offsets, co
     st.ms = ms;
     st.vec = vec;
     st.grid = (uint32_t)grid;
+    st.chebyshev = cheb ? 1u : 0u;
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    for (void *p : {(void *)ev, (void *)ews, (void *)ecs, (void *)sptr, (void *)X[0], (void *)X[1], (void *)XT[0],
-                    (void *)XT[1], (void *)cs, (void *)bpart, (void *)bar, (void *)status})
-        cudaFreeAsync(p, s);
+    for (void *p : {(void *)ev, (void *)ews, (void *)ecs, (void *)sptr, (void *)X[0], (void *)X[1], (void *)X[2],
+                    (void *)F, (void *)XT[0], (void *)XT[1], (void *)cs, (void *)bpart, (void *)bar, (void *)status})
+        if (p) cudaFreeAsync(p, s);
     PRG_CUDA(cudaStreamSynchronize(s));
     return rc;
 }

@@ -17,6 +17,7 @@ struct BatchStats {
     uint32_t tiles = 0;
     uint32_t vec = 1;  // tile width = 32 * vec columns
     uint32_t grid = 0;
+    uint32_t chebyshev = 0;  // 1: Chebyshev steps (undirected graph), 0: plain power steps
     uint32_t kernel_launches = 0;
     float ms = 0.f;
 };

@@ -99,7 +99,8 @@ class prg_stats(C.Structure):
 
 class prg_batch_stats(C.Structure):
     _fields_ = [("column_iterations", C.c_uint64), ("max_iters", C.c_uint32), ("tiles", C.c_uint32),
-                ("tile_width", C.c_uint32), ("kernel_launches", C.c_uint32), ("ms", C.c_double)]
+                ("tile_width", C.c_uint32), ("kernel_launches", C.c_uint32), ("ms", C.c_double),
+                ("chebyshev", C.c_uint32), ("pad", C.c_uint32)]
 
 
 class prg_tune_result(C.Structure):
@@ -705,7 +706,8 @@ class DeviceGraph:
             _check(lib().prg_ppr_batch(self._h, K, _ptr(off), _ptr(seeds), damping, tol, max_iter, vec, _ptr(X),
                                        _ptr(iters), C.byref(st)))
         stats = {"column_iterations": st.column_iterations, "max_iters": st.max_iters, "tiles": st.tiles,
-                 "tile_width": st.tile_width, "kernel_launches": st.kernel_launches, "ms": st.ms}
+                 "tile_width": st.tile_width, "kernel_launches": st.kernel_launches, "ms": st.ms,
+                 "chebyshev": bool(st.chebyshev)}
         return X, iters[:K], stats
 
     def gather_probe(self, reps: int = 20) -> float:

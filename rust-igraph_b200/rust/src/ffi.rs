@@ -99,6 +99,8 @@ pub struct prg_batch_stats {
     pub tile_width: u32,
     pub kernel_launches: u32,
     pub ms: f64,
+    pub chebyshev: u32,
+    pub pad: u32,
 }
 
 unsafe extern "C" {

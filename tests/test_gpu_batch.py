@@ -1,5 +1,6 @@
-"""Batched personalized PageRank (FP32 SpMM, per-column freeze) against the
-oracle's FP64 personalized_pagerank on every column.
+"""Batched personalized PageRank (FP32 SpMM, per-column freeze; Chebyshev
+steps on undirected graphs) against the oracle's FP64 personalized_pagerank
+on every column.
 
 Tolerance: each column stops at a successive L1 change < 1e-8, so its
 error is <= 1e-8 * d/(1-d) ~ 5.7e-8 from the stop rule plus FP32 rounding
@@ -51,6 +52,41 @@ def test_batch_matches_oracle_sbm(cuda_ok, vec):
         assert err <= L1_COL, (k, err, iters[k])
         assert abs(X[:, k].sum() - 1) < 1e-5
     assert iters.min() >= 5 and iters.max() < 1000
+
+
+def test_chebyshev_steps_on_undirected_graphs(cuda_ok):
+    # Undirected graphs take Chebyshev steps between the reference's stop
+    # tests (batch_cheb = 1, the default); batch_cheb = 0 gives the plain
+    # power steps.  Both meet the oracle on every column, the Chebyshev
+    # columns in fewer iterations, and directed graphs never take them.
+    blocks, bs = 32, 1500
+    n = blocks * bs
+    pin, pout = 16 / (bs - 1), 4 / ((blocks - 1) * bs)
+    pref = [[pin if i == j else pout for j in range(blocks)] for i in range(blocks)]
+    f, t = O.sbm_game(pref, [bs] * blocks, False, False, False, 12)
+    rng = np.random.default_rng(23)
+    seeds = seed_sets(n, 48, rng, max_seeds=300)
+    out = {}
+    try:
+        for cheb in (1, 0):
+            ig.set_tuning("batch_cheb", cheb)
+            with ig.DeviceGraph.from_host(n, f, t, False) as dg:
+                out[cheb] = dg.ppr_batch(seeds, 0.85, TOL_COL, 1000)
+    finally:
+        ig.reset_tuning()
+    assert out[1][2]["chebyshev"] and not out[0][2]["chebyshev"]
+    for k in range(len(seeds)):
+        ref = O.personalized_pagerank(n, f, t, False, reset_of(n, seeds[k]), 0.85)
+        for cheb in (1, 0):
+            err = np.abs(out[cheb][0][:, k].astype(np.float64) - ref).sum()
+            assert err <= L1_COL, (cheb, k, err)
+    it_cheb, it_plain = out[1][1].astype(np.int64), out[0][1].astype(np.int64)
+    print({"chebyshev_column_iterations": int(it_cheb.sum()), "plain_column_iterations": int(it_plain.sum())})
+    assert it_cheb.sum() < 0.8 * it_plain.sum(), (it_cheb.sum(), it_plain.sum())
+    ff, tt = O.erdos_renyi_gnm(3000, 20_000, True, False, 4)
+    with ig.DeviceGraph.from_host(3000, ff, tt, True) as dg:
+        _, _, st = dg.ppr_batch([np.array([1, 2], np.uint32)], 0.85, TOL_COL, 1000)
+    assert not st["chebyshev"]
 
 
 def test_batch_relabelled_directed_with_dangling(cuda_ok):

@@ -153,3 +153,24 @@ def test_tight_oracle_weighted_and_reset():
     ref = O.personalized_pagerank(500, f, t, False, r, D)
     tight, _, _ = O.pagerank_tight(500, f, t, False, reset=r, tol=1e-15)
     assert np.abs(ref - tight).sum() <= D / (1 - D) * 1e-10 * 1.01
+
+
+def test_ppr_residuals_certify_batched_columns():
+    # the residual pass behind the full-size batched check: the restatement's
+    # own answers (stored in FP32) have residuals near FP32 rounding, and a
+    # perturbation of one entry shows up with the factor (1 + d) it must have
+    n = 3000
+    f, t = O.erdos_renyi_gnm(n, 15_000, False, False, 5)
+    seeds = [np.array([1, 2, 2, 50], np.uint32), np.array([7], np.uint32), np.array([0, 2999], np.uint32)]
+    X = np.zeros((n, 3), np.float32)
+    for k, sl in enumerate(seeds):
+        r = np.zeros(n)
+        for v in sl:
+            r[v] += 1 / len(sl)
+        X[:, k] = O.personalized_pagerank(n, f, t, False, r, 0.85)
+    res = O.ppr_residuals(n, f, t, False, seeds, X)
+    assert res.max() < 1e-7
+    X2 = X.copy()
+    X2[10, 1] += np.float32(1e-4)
+    res2 = O.ppr_residuals(n, f, t, False, seeds, X2)
+    assert abs(res2[1] - 1e-4 * (1 + 0.85)) < 2e-5 and np.allclose(res2[[0, 2]], res[[0, 2]])
