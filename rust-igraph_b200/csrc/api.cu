@@ -135,6 +135,8 @@ static prg_graph *new_handle(uint32_t n, uint64_t m, int32_t directed, cudaStrea
     h->g.blocks_per_sm = t.blocks_per_sm;
     h->g.relabel = relabel >= 0 ? relabel : t.relabel;
     h->g.hot_cache = t.hot_cache;
+    h->g.hot_cache64 = t.hot_cache64;
+    h->g.hot_threads = t.hot_threads;
     h->g.l1_hot32 = t.l1_hot32;
     h->g.l1_hot64 = t.l1_hot64;
     h->ws.unroll = t.unroll;
@@ -1356,9 +1358,14 @@ int32_t prg_set_tuning(const char *key, int64_t value) {
         t.l1_hot64 = (uint32_t)std::min<int64_t>(value, 0xFFFFFFFFll);
     } else if (k == "krylov_rel_e12") {
         t.krylov_rel = (double)value * 1e-12;
-    } else if (k == "hot_cache") {
-        if (value > 65536) return fail(PRG_ERR_INVALID_ARGUMENT, "hot_cache must be at most 65536 entries");
-        t.hot_cache = (uint32_t)value;
+    } else if (k == "hot_cache" || k == "hot_cache32" || k == "hot_cache64") {
+        if (value > 65536) return fail(PRG_ERR_INVALID_ARGUMENT, k + " must be at most 65536 entries");
+        if (k != "hot_cache64") t.hot_cache = (uint32_t)value;
+        if (k != "hot_cache32") t.hot_cache64 = (uint32_t)value;
+    } else if (k == "hot_threads") {
+        if (value != 256 && value != 512 && value != 1024)
+            return fail(PRG_ERR_INVALID_ARGUMENT, "hot_threads must be 256, 512 or 1024");
+        t.hot_threads = (uint32_t)value;
     } else if (k == "unroll") {
         if (value < 1 || value > 64) return fail(PRG_ERR_INVALID_ARGUMENT, "unroll must be in 1..=64");
         t.unroll = (int)value;

@@ -39,7 +39,11 @@ struct DeviceGraph {
     uint32_t split = kSplit;
     uint32_t blocks_per_sm = 0;  // persistent grid = SMs x this (0 = occupancy maximum)
     int relabel = 2;             // 0 keep caller ids, 1 degree-sorted ids, 2 decide from the degree skew
-    uint32_t hot_cache = 0;      // relabelled graphs: entries of the rank vector's hot prefix each block keeps in shared memory (0 = off)
+    // relabelled graphs: entries of the gathered vector's hot prefix each
+    // block of an FP32 / FP64 pass keeps in shared memory (0 = off), and the
+    // block size of those passes (256: several blocks per SM; 512 or 1024:
+    // one block per SM with a larger prefix)
+    uint32_t hot_cache = 0, hot_cache64 = 0, hot_threads = kThreads;
     // relabelled graphs: gathers of ids >= l1_hot32 (FP32 passes) / l1_hot64
     // (FP64 passes) bypass L1, keeping it for the hot prefix (0 = all allocate)
     uint32_t l1_hot32 = 16384, l1_hot64 = 2048;
@@ -74,7 +78,7 @@ struct Tuning {
     uint32_t capw = kCapW, shortmax = kShortMax, split = kSplit, blocks_per_sm = 0;
     int relabel = 2;
     int unroll = 8;
-    uint32_t hot_cache = 0;
+    uint32_t hot_cache = 0, hot_cache64 = 0, hot_threads = kThreads;
     uint32_t l1_hot32 = 16384, l1_hot64 = 2048;
     double refine_switch = 5e-7;
     uint32_t batch_vec = 1;

@@ -77,10 +77,10 @@ void workspace_ensure(Workspace &ws, const DeviceGraph &g, cudaStream_t s) {
     ws.nrb = g.nrb;
     ws.nhub = g.nhub;
     unsigned gmax = kPrepParts;
-    const uint32_t hot = g.perm != nullptr ? g.hot_cache : 0u;
     for (int m = 0; m < kModes; m++) {
-        ws.cfg[m] = iteration_config(m, g.weighted, hot, g.blocks_per_sm, g.n);
         const bool fp32 = m == MODE_CORR32 || m == MODE_KRY32;
+        const uint32_t hot = g.perm != nullptr ? (fp32 ? g.hot_cache : g.hot_cache64) : 0u;
+        ws.cfg[m] = iteration_config(m, g.weighted, hot, g.blocks_per_sm, g.n, g.hot_threads);
         const uint32_t l1 = fp32 ? g.l1_hot32 : g.l1_hot64;
         if (g.perm != nullptr && l1) ws.cfg[m].l1hot = l1;
         gmax = std::max(gmax, ws.cfg[m].grid);

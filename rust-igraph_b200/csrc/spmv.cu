@@ -324,10 +324,13 @@ __device__ __forceinline__ typename ModeT<MODE>::A warp_row_sum(const IterArgs &
 }
 
 // Dynamic shared memory layout: [NT/32 warp buffers of kWarpBuf][hot prefix].
-template <int MODE, bool W, bool HOT>
-__global__ void __launch_bounds__(kThreads, HOT ? (kIs32<MODE> ? 4 : 3) : (kIs32<MODE> ? 5 : 4)) iter_kernel(const IterArgs a) {
+// NT = kThreads: several blocks per SM, each with its own (small) hot prefix.
+// NT = 512 / 1024 (hot variants only): one block per SM whose hot prefix takes
+// the shared memory the warp buffers leave, up to ~48 K FP32 entries.
+template <int MODE, bool W, bool HOT, int NT>
+__global__ void __launch_bounds__(NT, NT != kThreads ? 1 : HOT ? (kIs32<MODE> ? 4 : 3) : (kIs32<MODE> ? 5 : 4))
+    iter_kernel(const IterArgs a) {
     using A = typename ModeT<MODE>::A;
-    constexpr int NT = kThreads;
     constexpr int kW = NT / 32;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     A *s_buf = reinterpret_cast<A *>(smem_raw);
@@ -537,7 +540,7 @@ __global__ void __launch_bounds__(kThreads, HOT ? (kIs32<MODE> ? 4 : 3) : (kIs32
     }
 }
 
-template <int MODE, bool W, bool HOT>
+template <int MODE, bool W, bool HOT, int NT>
 static void kernel_config(uint32_t hot_entries, uint32_t blocks_per_sm, uint32_t n, LaunchCfg &c) {
     using A = typename ModeT<MODE>::A;
     static int sms = 0, smem_optin = 0;
@@ -547,7 +550,7 @@ static void kernel_config(uint32_t hot_entries, uint32_t blocks_per_sm, uint32_t
         PRG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
         PRG_CUDA(cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
     }
-    const size_t bufs = (size_t)(kThreads / 32) * kWarpBuf * sizeof(A);
+    const size_t bufs = (size_t)(NT / 32) * kWarpBuf * sizeof(A);
     size_t hot = 0;
     if (HOT) {
         // leave room for the kernel's static shared memory (reduction scratch)
@@ -556,50 +559,68 @@ static void kernel_config(uint32_t hot_entries, uint32_t blocks_per_sm, uint32_t
     }
     c.smem = bufs + hot * sizeof(A);
     c.hot = (uint32_t)hot;
-    c.threads = kThreads;
-    PRG_CUDA(cudaFuncSetAttribute(iter_kernel<MODE, W, HOT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c.smem));
+    c.threads = NT;
+    PRG_CUDA(cudaFuncSetAttribute(iter_kernel<MODE, W, HOT, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)c.smem));
     int occ = 0;
-    PRG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, iter_kernel<MODE, W, HOT>, kThreads, c.smem));
+    PRG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, iter_kernel<MODE, W, HOT, NT>, NT, c.smem));
     int per = occ > 0 ? occ : 1;
     if (blocks_per_sm > 0 && (int)blocks_per_sm < per) per = (int)blocks_per_sm;
     c.grid = (unsigned)(sms * per);
 }
 
+template <int MODE, bool W>
+static void hot_config(uint32_t hot, uint32_t hot_threads, uint32_t bps, uint32_t n, LaunchCfg &c) {
+    if (hot_threads == 1024) kernel_config<MODE, W, true, 1024>(hot, bps, n, c);
+    else if (hot_threads == 512) kernel_config<MODE, W, true, 512>(hot, bps, n, c);
+    else kernel_config<MODE, W, true, kThreads>(hot, bps, n, c);
+}
+
 template <int MODE>
-static void mode_config(bool weighted, uint32_t hot, uint32_t bps, uint32_t n, LaunchCfg &c) {
+static void mode_config(bool weighted, uint32_t hot, uint32_t hot_threads, uint32_t bps, uint32_t n, LaunchCfg &c) {
     if (hot) {
-        if (weighted) kernel_config<MODE, true, true>(hot, bps, n, c);
-        else kernel_config<MODE, false, true>(hot, bps, n, c);
+        if (weighted) hot_config<MODE, true>(hot, hot_threads, bps, n, c);
+        else hot_config<MODE, false>(hot, hot_threads, bps, n, c);
     } else {
-        if (weighted) kernel_config<MODE, true, false>(0, bps, n, c);
-        else kernel_config<MODE, false, false>(0, bps, n, c);
+        if (weighted) kernel_config<MODE, true, false, kThreads>(0, bps, n, c);
+        else kernel_config<MODE, false, false, kThreads>(0, bps, n, c);
     }
 }
 
-LaunchCfg iteration_config(int mode, bool weighted, uint32_t hot_entries, uint32_t blocks_per_sm, uint32_t n) {
+LaunchCfg iteration_config(int mode, bool weighted, uint32_t hot_entries, uint32_t blocks_per_sm, uint32_t n,
+                           uint32_t hot_threads) {
     LaunchCfg c;
+    const uint32_t ht = hot_threads;
     switch (mode) {
-        case MODE_PLAIN64: mode_config<MODE_PLAIN64>(weighted, hot_entries, blocks_per_sm, n, c); break;
-        case MODE_PPR64: mode_config<MODE_PPR64>(weighted, hot_entries, blocks_per_sm, n, c); break;
-        case MODE_RESID64: mode_config<MODE_RESID64>(weighted, hot_entries, blocks_per_sm, n, c); break;
-        case MODE_CORR32: mode_config<MODE_CORR32>(weighted, hot_entries, blocks_per_sm, n, c); break;
-        case MODE_KRY32: mode_config<MODE_KRY32>(weighted, hot_entries, blocks_per_sm, n, c); break;
-        case MODE_KRY64: mode_config<MODE_KRY64>(weighted, hot_entries, blocks_per_sm, n, c); break;
-        case MODE_EIG64: mode_config<MODE_EIG64>(weighted, hot_entries, blocks_per_sm, n, c); break;
-        default: mode_config<MODE_KRES64>(weighted, hot_entries, blocks_per_sm, n, c); break;
+        case MODE_PLAIN64: mode_config<MODE_PLAIN64>(weighted, hot_entries, ht, blocks_per_sm, n, c); break;
+        case MODE_PPR64: mode_config<MODE_PPR64>(weighted, hot_entries, ht, blocks_per_sm, n, c); break;
+        case MODE_RESID64: mode_config<MODE_RESID64>(weighted, hot_entries, ht, blocks_per_sm, n, c); break;
+        case MODE_CORR32: mode_config<MODE_CORR32>(weighted, hot_entries, ht, blocks_per_sm, n, c); break;
+        case MODE_KRY32: mode_config<MODE_KRY32>(weighted, hot_entries, ht, blocks_per_sm, n, c); break;
+        case MODE_KRY64: mode_config<MODE_KRY64>(weighted, hot_entries, ht, blocks_per_sm, n, c); break;
+        case MODE_EIG64: mode_config<MODE_EIG64>(weighted, hot_entries, ht, blocks_per_sm, n, c); break;
+        default: mode_config<MODE_KRES64>(weighted, hot_entries, ht, blocks_per_sm, n, c); break;
     }
     return c;
+}
+
+template <int MODE, bool W>
+static void hot_launch(const IterArgs &a, const LaunchCfg &c, cudaStream_t s) {
+    const dim3 grid(c.grid), block(c.threads);
+    if (c.threads == 1024) iter_kernel<MODE, W, true, 1024><<<grid, block, c.smem, s>>>(a);
+    else if (c.threads == 512) iter_kernel<MODE, W, true, 512><<<grid, block, c.smem, s>>>(a);
+    else iter_kernel<MODE, W, true, kThreads><<<grid, block, c.smem, s>>>(a);
 }
 
 template <int MODE>
 static void mode_launch(bool weighted, const IterArgs &a, const LaunchCfg &c, cudaStream_t s) {
     const dim3 grid(c.grid), block(c.threads);
     if (c.hot) {
-        if (weighted) iter_kernel<MODE, true, true><<<grid, block, c.smem, s>>>(a);
-        else iter_kernel<MODE, false, true><<<grid, block, c.smem, s>>>(a);
+        if (weighted) hot_launch<MODE, true>(a, c, s);
+        else hot_launch<MODE, false>(a, c, s);
     } else {
-        if (weighted) iter_kernel<MODE, true, false><<<grid, block, c.smem, s>>>(a);
-        else iter_kernel<MODE, false, false><<<grid, block, c.smem, s>>>(a);
+        if (weighted) iter_kernel<MODE, true, false, kThreads><<<grid, block, c.smem, s>>>(a);
+        else iter_kernel<MODE, false, false, kThreads><<<grid, block, c.smem, s>>>(a);
     }
 }
 

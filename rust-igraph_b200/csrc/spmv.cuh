@@ -98,7 +98,10 @@ struct LaunchCfg {
 // Persistent launch shape of the iteration kernel on this device: 256-thread
 // blocks, as many per SM as fit (or blocks_per_sm), each optionally holding
 // the first hot_entries values of the gathered vector in shared memory.
-LaunchCfg iteration_config(int mode, bool weighted, uint32_t hot_entries, uint32_t blocks_per_sm, uint32_t n);
+// With a hot prefix, hot_threads = 512 or 1024 gives one block of that size
+// per SM instead, whose hot prefix can take most of the SM's shared memory.
+LaunchCfg iteration_config(int mode, bool weighted, uint32_t hot_entries, uint32_t blocks_per_sm, uint32_t n,
+                           uint32_t hot_threads = kThreads);
 void launch_iteration(int mode, bool weighted, const IterArgs &a, const LaunchCfg &c, cudaStream_t s);
 
 // Average time (ms) of a pass that only streams g's column indices and gathers

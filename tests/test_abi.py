@@ -171,3 +171,18 @@ def test_infomap_flow_validation_and_trivial_graphs():
     assert len(ig.infomap_flow(ig.Graph.with_vertices(0))) == 0
     assert list(ig.infomap_flow(ig.Graph.with_vertices(1))) == [1.0]
     assert list(ig.infomap_flow(ig.Graph.with_vertices(1), vertex_weights=[3.0])) == [1.0]
+
+
+def test_tuning_keys_are_validated_on_the_host():
+    # prg_set_tuning checks its values before any graph uses them
+    for key, bad, msg in (("hot_threads", 300, "hot_threads must be 256, 512 or 1024"),
+                          ("hot_cache64", 70000, "hot_cache64 must be at most 65536 entries"),
+                          ("hot_cache32", 70000, "hot_cache32 must be at most 65536 entries"),
+                          ("batch_cheb", 2, "batch_cheb must be 0 or 1")):
+        with pytest.raises(ig.InvalidArgument, match=msg):
+            ig.set_tuning(key, bad)
+    try:
+        for key, good in (("hot_threads", 512), ("hot_cache64", 16384), ("batch_cheb", 0)):
+            ig.set_tuning(key, good)
+    finally:
+        ig.reset_tuning()
