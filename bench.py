@@ -367,13 +367,23 @@ def main():
         net.predict(dg, start.data_ptr())
         inf_ms = [net.predict(dg, start.data_ptr()) for _ in range(2)]
         msw, stw = timed(opt_ref, 2, start=start.data_ptr())
+        l1_warm = float((out - x_ref).abs().sum().item())
+        # the plain FP64 power iteration from the same start: the pass count
+        # the network saves the method it was trained on
+        msw64, stw64 = timed(opt_64, 1, start=start.data_ptr())
         uni = torch.full((n,), 1.0 / n, dtype=torch.float64, device=dev)
+        total = min(inf_ms) + msw / len(stw)
         warm = {"inference_ms": min(inf_ms), "solve_ms": msw / len(stw),
-                "total_ms": min(inf_ms) + msw / len(stw), "passes": stw[-1].iterations,
+                "total_ms": total, "passes": stw[-1].iterations,
                 "fp32_passes": stw[-1].fp32_passes, "uniform_passes": stats[-1].iterations,
+                "net_gain_vs_uniform_refined_ms": t_ref - total,
+                "fp64_power": {"passes": stw64[-1].iterations, "uniform_passes": p_plain,
+                               "total_ms": min(inf_ms) + stw64[-1].solve_ms, "uniform_ms": t64,
+                               "net_gain_ms": t64 - (min(inf_ms) + stw64[-1].solve_ms)},
                 "start_l1_error": float((start - x_ref).abs().sum().item()),
                 "uniform_start_l1_error": float((uni - x_ref).abs().sum().item()),
-                "l1_vs_refined": float((out - x_ref).abs().sum().item())}
+                "l1_vs_refined": l1_warm,
+                "note": "a negative net gain means the warm start loses wall time to the uniform start"}
         net.close()
         del start, uni
 
