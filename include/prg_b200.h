@@ -300,6 +300,7 @@ int32_t prg_autotune(prg_graph *g, int32_t tune_batch, const char *cache_path, p
  * i.e. 1e-4), "l1_hot32" / "l1_hot64" (relabelled graphs: FP32 / FP64
  * passes gather sources with ids >= value without allocating in L1, so L1
  * keeps the most-gathered prefix; defaults 16384 / 2048, 0 = all allocate),
+ * "defaults" (any value: every key back to its default),
  * "batch_cheb" (batched solver on undirected graphs: 1 Chebyshev steps, the
  * default, 0 plain power steps),
  * "batch_barrier_extra" (failure-detection test hook, 0 or 1: with 1 every

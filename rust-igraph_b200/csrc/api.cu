@@ -1334,7 +1334,8 @@ int32_t prg_set_tuning(const char *key, int64_t value) {
     prg::Tuning &t = prg::tuning();
     const std::string k(key);
     if (value < 0) return fail(PRG_ERR_INVALID_ARGUMENT, "tuning value must be >= 0");
-    if (k == "capw") t.capw = (uint32_t)value;
+    if (k == "defaults") t = prg::Tuning{};  // every key back to its default
+    else if (k == "capw") t.capw = (uint32_t)value;
     else if (k == "shortmax") t.shortmax = (uint32_t)value;
     else if (k == "split") t.split = (uint32_t)value;
     else if (k == "blocks_per_sm") t.blocks_per_sm = (uint32_t)value;

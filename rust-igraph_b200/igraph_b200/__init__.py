@@ -750,14 +750,9 @@ def set_tuning(key: str, value: int) -> None:
     _check(lib().prg_set_tuning(key.encode(), int(value)))
 
 
-TUNING_DEFAULTS = {"capw": 256, "shortmax": 256, "split": 8192, "blocks_per_sm": 0, "relabel": 2, "unroll": 8,
-                   "hot_cache": 0, "refine_switch_e12": 500000, "batch_vec": 1, "krylov_rel_e12": 100_000_000, "l1_hot32": 16384,
-                   "l1_hot64": 2048, "batch_barrier_extra": 0}
-
-
 def reset_tuning() -> None:
-    for k, v in TUNING_DEFAULTS.items():
-        set_tuning(k, v)
+    """Every tuning key back to its default (prg_set_tuning("defaults", 0))."""
+    set_tuning("defaults", 0)
 
 
 def rmat_device(scale: int, m: int, d_from: int, d_to: int, a=0.57, b=0.19, c=0.19, seed=1, stream: int = 0):
