@@ -60,11 +60,14 @@ struct ColState {
     uint32_t iters;
     uint32_t active;  // 1 until the column converged or hit max_iter
     uint32_t final_buf;
-    uint32_t cheb_steps;  // Chebyshev steps taken (0 = still in the plain phase)
+    uint32_t cheb_steps;  // Chebyshev steps taken (0 = still in the plain phase, kChebOff = left for good)
     double prev_diff;     // the change before `diff`
     double prev_ratio;    // the contraction ratio before the last one
     double beta;          // Chebyshev interval half-width
     double omega;         // weight of the next step (0 = plain step)
+    double best_diff;     // smallest change seen during the Chebyshev steps
+    uint32_t stall;       // Chebyshev steps since best_diff last fell
+    uint32_t pad2;
 };
 
 // A column leaves its plain steps once its contraction ratio diff/prev_diff
@@ -73,6 +76,12 @@ struct ColState {
 // then follows the slowest modes, times kChebMargin is the half-width beta.
 constexpr uint32_t kChebMinPower = 6, kChebMaxPower = 24;
 constexpr double kChebSettle = 0.01, kChebMargin = 1.05;
+// FP32 rounding sets a floor under ||G(x) - x||_1 for Chebyshev iterates (a
+// weighted combination never becomes an exact FP32 fixed point, while the
+// plain step does, after which its change is 0): a column whose change has
+// not reached a new minimum for kChebStall Chebyshev steps finishes with
+// plain steps.
+constexpr uint32_t kChebStall = 3, kChebOff = 0xFFFFFFFFu;
 
 struct TileArgs {
     const uint32_t *row_ptr;
@@ -246,9 +255,22 @@ __device__ __forceinline__ void reduce_columns(const TileArgs &a, int parity_new
                         s.beta = b;
                         s.omega = 2.0 / (2.0 - b * b);
                         s.cheb_steps = 1u;
-                    } else if (s.cheb_steps > 0u) {
-                        s.omega = 1.0 / (1.0 - 0.25 * s.beta * s.beta * s.omega);
-                        s.cheb_steps += 1u;
+                        s.best_diff = tx;
+                        s.stall = 0u;
+                    } else if (s.cheb_steps > 0u && s.cheb_steps != kChebOff) {
+                        if (tx < s.best_diff) {
+                            s.best_diff = tx;
+                            s.stall = 0u;
+                        } else {
+                            s.stall += 1u;
+                        }
+                        if (s.stall >= kChebStall) {
+                            s.omega = 0.0;  // plain steps from here on
+                            s.cheb_steps = kChebOff;
+                        } else {
+                            s.omega = 1.0 / (1.0 - 0.25 * s.beta * s.beta * s.omega);
+                            s.cheb_steps += 1u;
+                        }
                     }
                     s.prev_ratio = ratio;
                 }
