@@ -78,10 +78,10 @@ constexpr uint32_t kChebMinPower = 6, kChebMaxPower = 24;
 constexpr double kChebSettle = 0.01, kChebMargin = 1.05;
 // FP32 rounding sets a floor under ||G(x) - x||_1 for Chebyshev iterates (a
 // weighted combination never becomes an exact FP32 fixed point, while the
-// plain step does, after which its change is 0): a column whose change has
-// not reached a new minimum for kChebStall Chebyshev steps finishes with
-// plain steps.
-constexpr uint32_t kChebStall = 3, kChebOff = 0xFFFFFFFFu;
+// plain step does, after which its change is 0).  At that floor the change
+// only wanders, so a column whose change has not halved for kChebStall
+// Chebyshev steps finishes with plain steps.
+constexpr uint32_t kChebStall = 4, kChebOff = 0xFFFFFFFFu;
 
 struct TileArgs {
     const uint32_t *row_ptr;
@@ -258,7 +258,7 @@ __device__ __forceinline__ void reduce_columns(const TileArgs &a, int parity_new
                         s.best_diff = tx;
                         s.stall = 0u;
                     } else if (s.cheb_steps > 0u && s.cheb_steps != kChebOff) {
-                        if (tx < s.best_diff) {
+                        if (tx < 0.5 * s.best_diff) {
                             s.best_diff = tx;
                             s.stall = 0u;
                         } else {

@@ -255,34 +255,43 @@ __device__ __forceinline__ void quad(const IterArgs &a, uint32_t base, uint32_t 
     }
 }
 
+// Quads each lane has in flight per step of `stage`: 32-bit passes take four
+// (16 gathers per lane outstanding), FP64 passes two (register budget).
+template <int MODE>
+constexpr int kStageQuads = kIs32<MODE> ? 4 : 2;
+
 // Warp: stage products of arcs [lo, hi) (hi - lo <= kWarpBuf) into buf[p - lo].
+// Each step issues the index loads and gathers of kStageQuads quads per lane
+// before storing any product, so a stream row-block of <= kWarpBuf arcs takes
+// one or two round trips to memory, not four.
 template <int MODE, bool W, bool HOT>
 __device__ __forceinline__ void stage(const IterArgs &a, uint32_t lo, uint32_t hi, typename ModeT<MODE>::A *buf,
                                       uint32_t lane, uint64_t pol_s, uint64_t pol_g,
                                       const typename ModeT<MODE>::A *s_hot, uint32_t hot) {
     using A = typename ModeT<MODE>::A;
+    constexpr int QN = kStageQuads<MODE>;
     const uint32_t a0 = lo & ~3u;
     const uint32_t nvec = (hi - a0 + 3u) >> 2;
-    uint32_t vi = lane;
-    for (; vi + 32 < nvec; vi += 64) {
-        A g0[4], g1[4];
-        quad<MODE, W, HOT>(a, a0 + 4u * vi, lo, hi, pol_s, pol_g, s_hot, hot, g0);
-        quad<MODE, W, HOT>(a, a0 + 4u * (vi + 32), lo, hi, pol_s, pol_g, s_hot, hot, g1);
+    for (uint32_t vi = lane; vi < nvec; vi += 32u * QN) {
+        A g[QN][4];
 #pragma unroll
-        for (int k = 0; k < 4; k++) {
-            uint32_t p = a0 + 4u * vi + k;
-            if (p >= lo && p < hi) buf[p - lo] = g0[k];
-            p = a0 + 4u * (vi + 32) + k;
-            if (p >= lo && p < hi) buf[p - lo] = g1[k];
+        for (int j = 0; j < QN; j++) {
+            const uint32_t q = vi + 32u * j;
+            if (q < nvec) {
+                quad<MODE, W, HOT>(a, a0 + 4u * q, lo, hi, pol_s, pol_g, s_hot, hot, g[j]);
+            } else {
+#pragma unroll
+                for (int k = 0; k < 4; k++) g[j][k] = A(0);
+            }
         }
-    }
-    if (vi < nvec) {
-        A g0[4];
-        quad<MODE, W, HOT>(a, a0 + 4u * vi, lo, hi, pol_s, pol_g, s_hot, hot, g0);
 #pragma unroll
-        for (int k = 0; k < 4; k++) {
-            const uint32_t p = a0 + 4u * vi + k;
-            if (p >= lo && p < hi) buf[p - lo] = g0[k];
+        for (int j = 0; j < QN; j++) {
+            const uint32_t q = vi + 32u * j;
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                const uint32_t p = a0 + 4u * q + k;
+                if (q < nvec && p >= lo && p < hi) buf[p - lo] = g[j][k];
+            }
         }
     }
 }
@@ -328,7 +337,7 @@ __device__ __forceinline__ typename ModeT<MODE>::A warp_row_sum(const IterArgs &
 // NT = 512 / 1024 (hot variants only): one block per SM whose hot prefix takes
 // the shared memory the warp buffers leave, up to ~48 K FP32 entries.
 template <int MODE, bool W, bool HOT, int NT>
-__global__ void __launch_bounds__(NT, NT != kThreads ? 1 : HOT ? (kIs32<MODE> ? 4 : 3) : (kIs32<MODE> ? 5 : 4))
+__global__ void __launch_bounds__(NT, NT != kThreads ? 1 : HOT ? (kIs32<MODE> ? 4 : 3) : 4)
     iter_kernel(const IterArgs a) {
     using A = typename ModeT<MODE>::A;
     constexpr int kW = NT / 32;
