@@ -76,12 +76,17 @@ struct ColState {
 // then follows the slowest modes, times kChebMargin is the half-width beta.
 constexpr uint32_t kChebMinPower = 6, kChebMaxPower = 24;
 constexpr double kChebSettle = 0.01, kChebMargin = 1.05;
-// FP32 rounding sets a floor under ||G(x) - x||_1 for Chebyshev iterates (a
-// weighted combination never becomes an exact FP32 fixed point, while the
-// plain step does, after which its change is 0).  At that floor the change
-// only wanders, so a column whose change has not halved for kChebStall
-// Chebyshev steps finishes with plain steps.
+// FP32 rounding sets a floor under ||G(x) - x||_1 (about n ulp of the
+// column's mass): a weighted combination of iterates never becomes an exact
+// FP32 fixed point, and plain FP32 steps started from a Chebyshev iterate can
+// settle into a cycle of a few ulp flips instead of a fixed point.  At that
+// floor the change only wanders.  A Chebyshev column whose change has not
+// halved for kChebStall steps therefore freezes there if the change is within
+// kChebFloor x tol (its answer G(x) is then within d/(1-d) of that change of
+// the fixed point), and otherwise finishes with plain steps, which freeze the
+// same way after kChebStall * 2 steps without halving.
 constexpr uint32_t kChebStall = 4, kChebOff = 0xFFFFFFFFu;
+constexpr double kChebFloor = 100.0;
 
 struct TileArgs {
     const uint32_t *row_ptr;
@@ -257,17 +262,25 @@ __device__ __forceinline__ void reduce_columns(const TileArgs &a, int parity_new
                         s.cheb_steps = 1u;
                         s.best_diff = tx;
                         s.stall = 0u;
-                    } else if (s.cheb_steps > 0u && s.cheb_steps != kChebOff) {
+                    } else if (s.cheb_steps > 0u) {
                         if (tx < 0.5 * s.best_diff) {
                             s.best_diff = tx;
                             s.stall = 0u;
                         } else {
                             s.stall += 1u;
                         }
-                        if (s.stall >= kChebStall) {
-                            s.omega = 0.0;  // plain steps from here on
-                            s.cheb_steps = kChebOff;
-                        } else {
+                        const bool plain = s.cheb_steps == kChebOff;
+                        if (s.stall >= (plain ? 2u * kChebStall : kChebStall)) {
+                            if (tx < kChebFloor * a.tol) {
+                                // at the FP32 floor: freeze with this step's G(x)
+                                s.active = 0u;
+                                s.final_buf = (uint32_t)parity_new;
+                            } else if (!plain) {
+                                s.omega = 0.0;  // plain steps from here on
+                                s.cheb_steps = kChebOff;
+                                s.stall = 0u;
+                            }
+                        } else if (!plain) {
                             s.omega = 1.0 / (1.0 - 0.25 * s.beta * s.beta * s.omega);
                             s.cheb_steps += 1u;
                         }
