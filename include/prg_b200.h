@@ -335,8 +335,8 @@ typedef struct prg_batch_stats {
  * ||G(x) - x||_1 < tol, and the column returns that step, G(x), as the
  * reference does; only the sequence of iterates before it is shorter.  FP32
  * rounding puts a floor of about n ulp under that change; a Chebyshev column
- * whose change stops halving within 100 x tol of it freezes there (its
- * answer is then within d/(1-d) of that change of the fixed point).
+ * whose change stops falling within 4 x tol freezes there (its answer is then
+ * within d/(1-d) of that change of the fixed point).
  * tile_vec: columns per tile = 32 * tile_vec (1, 2 or 4; 0 = autotuned or 1).
  * out: host float[n * K], out[v * K + k].  column_iters: optional host
  * uint32[K].  Validation follows _vs: empty seed list or vertex >= n ->

@@ -137,6 +137,8 @@ static prg_graph *new_handle(uint32_t n, uint64_t m, int32_t directed, cudaStrea
     h->g.hot_cache = t.hot_cache;
     h->g.hot_cache64 = t.hot_cache64;
     h->g.hot_threads = t.hot_threads;
+    h->g.seg_kry32 = t.seg_kry32;
+    h->g.seg_hot = t.seg_hot;
     h->g.l1_hot32 = t.l1_hot32;
     h->g.l1_hot64 = t.l1_hot64;
     h->ws.unroll = t.unroll;
@@ -1363,6 +1365,12 @@ int32_t prg_set_tuning(const char *key, int64_t value) {
         if (value > 65536) return fail(PRG_ERR_INVALID_ARGUMENT, k + " must be at most 65536 entries");
         if (k != "hot_cache64") t.hot_cache = (uint32_t)value;
         if (k != "hot_cache32") t.hot_cache64 = (uint32_t)value;
+    } else if (k == "seg_kry32") {
+        if (value > 1) return fail(PRG_ERR_INVALID_ARGUMENT, "seg_kry32 must be 0 or 1");
+        t.seg_kry32 = (uint32_t)value;
+    } else if (k == "seg_hot") {
+        if (value > 49152) return fail(PRG_ERR_INVALID_ARGUMENT, "seg_hot must be at most 49152 entries");
+        t.seg_hot = (uint32_t)value;
     } else if (k == "hot_threads") {
         if (value != 256 && value != 512 && value != 1024)
             return fail(PRG_ERR_INVALID_ARGUMENT, "hot_threads must be 256, 512 or 1024");

@@ -584,15 +584,15 @@ static InnerResult bicgstab(const DeviceGraph &g, Workspace &ws, KrylovWs &k, KB
         PRG_CUDA(cudaEventRecord(ev[1], s));
         launch_iteration(mode, g.weighted, m1, cfg, s);
         PRG_CUDA(cudaEventRecord(ev[2], s));
-        kv2<T><<<kVB, kVT, 0, s>>>(n, q, k.st, k.part2, cfg.grid, ws.hub_rec, g.nhub, r, b.v, b.s, b.st, g.inv32,
+        kv2<T><<<kVB, kVT, 0, s>>>(n, q, k.st, k.part2, cfg.grid, ws.hub_rec, cfg.hub_recs, r, b.v, b.s, b.st, g.inv32,
                                     g.dval, k.part3);
         PRG_CUDA(cudaEventRecord(ev[3], s));
         launch_iteration(mode, g.weighted, m2, cfg, s);
         PRG_CUDA(cudaEventRecord(ev[4], s));
-        kv3<T><<<kVB, kVT, 0, s>>>(n, q, k.st, k.part4, cfg.grid, ws.hub_rec, g.nhub, k.part3, b.rh, b.p, b.s, b.t,
+        kv3<T><<<kVB, kVT, 0, s>>>(n, q, k.st, k.part4, cfg.grid, ws.hub_rec, cfg.hub_recs, k.part3, b.rh, b.p, b.s, b.t,
                                     b.e, r, k.part5);
         PRG_CUDA(cudaEventRecord(ev[5], s));
-        res.launches += 5u;
+        res.launches += cfg.seg ? 7u : 5u;  // the segmented matvec is two kernels
     };
     // batches of `per` steps; the state copy of batch j is read while batch
     // j+1 runs (kernels of a finished solve return at once)

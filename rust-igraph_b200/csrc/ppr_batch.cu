@@ -81,12 +81,13 @@ constexpr double kChebSettle = 0.01, kChebMargin = 1.05;
 // FP32 fixed point, and plain FP32 steps started from a Chebyshev iterate can
 // settle into a cycle of a few ulp flips instead of a fixed point.  At that
 // floor the change only wanders.  A Chebyshev column whose change has not
-// halved for kChebStall steps therefore freezes there if the change is within
-// kChebFloor x tol (its answer G(x) is then within d/(1-d) of that change of
-// the fixed point), and otherwise finishes with plain steps, which freeze the
-// same way after kChebStall * 2 steps without halving.
-constexpr uint32_t kChebStall = 4, kChebOff = 0xFFFFFFFFu;
-constexpr double kChebFloor = 100.0;
+// reached a new minimum for kChebStall steps therefore freezes there if the
+// change is within kChebFloor x tol (its answer G(x) is then within d/(1-d)
+// of that change of the fixed point), and otherwise finishes with plain
+// steps, which freeze the same way after kChebStall more steps without a new
+// minimum.
+constexpr uint32_t kChebStall = 6, kChebOff = 0xFFFFFFFFu;
+constexpr double kChebFloor = 4.0;
 
 struct TileArgs {
     const uint32_t *row_ptr;
@@ -263,14 +264,14 @@ __device__ __forceinline__ void reduce_columns(const TileArgs &a, int parity_new
                         s.best_diff = tx;
                         s.stall = 0u;
                     } else if (s.cheb_steps > 0u) {
-                        if (tx < 0.5 * s.best_diff) {
+                        if (tx < s.best_diff) {
                             s.best_diff = tx;
                             s.stall = 0u;
                         } else {
                             s.stall += 1u;
                         }
                         const bool plain = s.cheb_steps == kChebOff;
-                        if (s.stall >= (plain ? 2u * kChebStall : kChebStall)) {
+                        if (s.stall >= kChebStall) {
                             if (tx < kChebFloor * a.tol) {
                                 // at the FP32 floor: freeze with this step's G(x)
                                 s.active = 0u;

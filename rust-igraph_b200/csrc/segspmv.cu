@@ -1,0 +1,363 @@
+// segspmv.cu — the FP32 Krylov matvec y = A p (MODE_KRY32) as a
+// tile-segmented pass over the in-CSR, for unweighted graphs.
+//
+// The row-block kernel (spmv.cu) walks rows: each warp stages a row-block's
+// products and sums them per row, so every step waits on an index load and
+// then on its gathers, and row pointers, descriptors and partial quads add
+// load requests.  Here the arcs are cut into tiles of kSegTile = 256 and the
+// pass streams them like a gather-only loop: a warp takes tiles in a
+// grid-stride order (neighbouring warps read neighbouring tiles), each lane
+// loads two 16-byte index quads and gathers their eight sources, and the row
+// sums come from a segmented scan in registers, driven by a bit per arc that
+// marks the last arc of a row (built once per graph):
+//   * in each lane, a running sum over its 4 arcs that restarts after a row end;
+//   * across the 32 lanes, an inclusive scan of the lanes' open tails (5
+//     shuffles) whose segment breaks come from one ballot of "lane holds a
+//     row end", with no flag shuffles;
+//   * the k-th row end of tile t belongs to nz_row[tile_j0[t] + k] (the rows
+//     that have arcs, in order), and its lane applies the epilogue there.
+// A row that began in an earlier tile is finished by a second, small kernel:
+// tile t leaves the sum before its first row end (head) and the open sum
+// after its last (tail); the row's total is the tails of the tiles it spans
+// plus the head, added in tile order in FP64.  The same kernel applies the
+// epilogue to the rows without arcs.  With degree-sorted ids the first 48 K
+// entries of the gathered vector (about 45 % of the arcs' sources on R-MAT)
+// sit in shared memory of the one 1024-thread block per SM.
+//
+// The epilogue and the records are those of iter_kernel<MODE_KRY32>:
+//   y = p - d sum - d (dangling mass of p) t,  records (rh.y, y.p, y.y),
+// with the dangling mass summed from the producer's block records in a fixed
+// order and the half-step skip (ktol) decided the same way in both kernels.
+// The schedule is static and all reductions use fixed trees, so the result
+// is bit-reproducible run to run.
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <algorithm>
+
+#include "prims.cuh"
+#include "spmv.cuh"
+
+namespace prg {
+
+constexpr int kSegNT = 1024;       // threads of the tile kernel (one block per SM)
+constexpr int kSegFixNT = 256;     // threads of the finishing kernel
+constexpr uint32_t kSegHotMax = 49152;  // hot-prefix entries (192 KB of shared memory)
+
+// ------------------------------------------------------------------ index build
+
+__global__ void seg_rowend_kernel(const uint32_t *rp, uint32_t n, uint32_t *mask, uint32_t *nonempty) {
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+        const uint32_t a = rp[v], b = rp[v + 1];
+        nonempty[v] = b > a ? 1u : 0u;
+        if (b > a) atomicOr(&mask[(b - 1) >> 5], 1u << ((b - 1) & 31));
+    }
+}
+
+__global__ void seg_tilecount_kernel(const uint32_t *mask, uint64_t ntiles, uint32_t *cnt) {
+    for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < ntiles;
+         t += (uint64_t)gridDim.x * blockDim.x) {
+        uint32_t c = 0;
+#pragma unroll
+        for (int w = 0; w < (int)(kSegTile / 32); w++) c += __popc(mask[t * (kSegTile / 32) + w]);
+        cnt[t] = c;
+    }
+}
+
+__global__ void seg_split_rows_kernel(const uint32_t *nonempty, const uint32_t *pos, uint32_t n, uint32_t *nz,
+                                      uint32_t *empty) {
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+        if (nonempty[v]) nz[pos[v]] = v;
+        else empty[v - pos[v]] = v;
+    }
+}
+
+template <class T>
+static T *salloc(uint64_t count, cudaStream_t s) {
+    T *p = nullptr;
+    PRG_CUDA(cudaMallocAsync((void **)&p, std::max<uint64_t>(count, 1) * sizeof(T), s));
+    return p;
+}
+
+void seg_free(SegIndex &x, cudaStream_t s) {
+    for (void *p : {(void *)x.mask, (void *)x.tile_j0, (void *)x.nz_row, (void *)x.empty_row, (void *)x.head,
+                    (void *)x.tail})
+        if (p) cudaFreeAsync(p, s);
+    x = SegIndex{};
+}
+
+void seg_build(const DeviceGraph &g, SegIndex &x, cudaStream_t s) {
+    seg_free(x, s);
+    const uint32_t n = g.n;
+    const uint64_t ntiles = (g.arcs + kSegTile - 1) / kSegTile;
+    const uint64_t words = ntiles * (kSegTile / 32) + 8;
+    x.ntiles = ntiles;
+    x.mask = salloc<uint32_t>(words, s);
+    x.tile_j0 = salloc<uint32_t>(ntiles + 1, s);
+    PRG_CUDA(cudaMemsetAsync(x.mask, 0, words * 4, s));
+    uint32_t *nonempty = salloc<uint32_t>(n, s);
+    uint32_t *pos = salloc<uint32_t>((uint64_t)n + 1, s);
+    uint32_t *cnt = salloc<uint32_t>(ntiles, s);
+    const unsigned gb = 148u * 8u;
+    seg_rowend_kernel<<<gb, 256, 0, s>>>(g.row_ptr, n, x.mask, nonempty);
+    seg_tilecount_kernel<<<gb, 256, 0, s>>>(x.mask, ntiles, cnt);
+    PRG_CUDA(cudaGetLastError());
+    exclusive_scan_u32(cnt, x.tile_j0, ntiles, s);
+    exclusive_scan_u32(nonempty, pos, n, s);
+    uint32_t nnz = 0;
+    PRG_CUDA(cudaMemcpyAsync(&nnz, pos + n, 4, cudaMemcpyDeviceToHost, s));
+    PRG_CUDA(cudaStreamSynchronize(s));
+    x.n_nz = nnz;
+    x.n_empty = n - nnz;
+    x.nz_row = salloc<uint32_t>(x.n_nz, s);
+    x.empty_row = salloc<uint32_t>(x.n_empty, s);
+    seg_split_rows_kernel<<<gb, 256, 0, s>>>(nonempty, pos, n, x.nz_row, x.empty_row);
+    PRG_CUDA(cudaGetLastError());
+    x.head = salloc<float>(ntiles, s);
+    x.tail = salloc<float>(ntiles, s);
+    cudaFreeAsync(nonempty, s);
+    cudaFreeAsync(pos, s);
+    cudaFreeAsync(cnt, s);
+}
+
+// ------------------------------------------------------------------ kernels
+
+__device__ __forceinline__ void seg_block_sum3(double &a, double &b, double &c, double *sh) {
+    a = warp_sum(a);
+    b = warp_sum(b);
+    c = warp_sum(c);
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31, nw = blockDim.x >> 5;
+    __syncthreads();
+    if (l == 0) {
+        sh[w] = a;
+        sh[32 + w] = b;
+        sh[64 + w] = c;
+    }
+    __syncthreads();
+    if (w == 0) {
+        a = l < nw ? sh[l] : 0.0;
+        b = l < nw ? sh[32 + l] : 0.0;
+        c = l < nw ? sh[64 + l] : 0.0;
+        a = warp_sum(a);
+        b = warp_sum(b);
+        c = warp_sum(c);
+    }
+}
+
+// Dangling mass of the input (the producer's block records summed by warp 0
+// in a fixed order, so both kernels of a launch and all their blocks get the
+// same bits) and the half-step skip.  Returns false when the launch has
+// nothing to do.
+__device__ __forceinline__ bool seg_prologue(const IterArgs &a, double &dz) {
+    __shared__ double s_dz;
+    __shared__ int s_skip;
+    if (threadIdx.x < 32) {
+        double z0 = 0.0, z1 = 0.0, z2 = 0.0;
+        for (uint32_t i = threadIdx.x; i < a.kpart_n; i += 32) {
+            const double4 q = a.kpart_in[i];
+            z0 += q.x;
+            z1 += q.y;
+            z2 += q.z;
+        }
+        z0 = warp_sum(z0);
+        z1 = warp_sum(z1);
+        z2 = warp_sum(z2);
+        if (threadIdx.x == 0) {
+            s_dz = z0;
+            s_skip = a.ktol != nullptr && !((a.knorm2 ? sqrt(z2) : z1) > *a.ktol);
+        }
+    }
+    __syncthreads();
+    dz = s_dz;
+    return !s_skip;
+}
+
+struct SegEpi {
+    float d, dshare;
+    double pd, pds, ps;
+    // y = p - (d sum + d dsum t) and its records, as iter_kernel<MODE_KRY32>
+    __device__ __forceinline__ void row(const IterArgs &a, uint32_t v, float sum) {
+        const float pin = __ldcs(a.x32_in + v);
+        const float rh = a.rh32 ? __ldcs(a.rh32 + v) : 0.0f;
+        const float t = a.t32 ? a.t32[v] : (float)a.inv_n;
+        const float out = pin - (d * sum + dshare * t);
+        __stcs(a.x32_out + v, out);
+        pd += (double)rh * (double)out;
+        pds += (double)out * (double)pin;
+        ps += (double)out * (double)out;
+    }
+};
+
+// Segmented sums of one 128-arc block (lane owns 4 consecutive arcs).  v: the
+// lane's products; f: their row-end bits.  carry: the open sum entering the
+// block, updated to the one leaving it.  emit(rank, sum, first) for every
+// row end in arc order, rank counted within the block, `first` for the
+// block's first row end.
+template <class Emit>
+__device__ __forceinline__ void seg_block(const float (&v)[4], uint32_t f, float &carry, uint32_t lane, Emit emit) {
+    const float s0 = v[0];
+    const float s1 = (f & 1u) ? v[1] : s0 + v[1];
+    const float s2 = (f & 2u) ? v[2] : s1 + v[2];
+    const float s3 = (f & 4u) ? v[3] : s2 + v[3];
+    const float sk[4] = {s0, s1, s2, s3};
+    float tv = (f & 8u) ? 0.0f : s3;  // the lane's open tail
+    const uint32_t E = __ballot_sync(0xffffffffu, f != 0u);
+    // inclusive scan of the open tails; lane L stops adding once a lane of
+    // the range it already covers, (L - o, L], holds a row end
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const float ov = __shfl_up_sync(0xffffffffu, tv, o);
+        if (lane >= (uint32_t)o) {
+            const uint32_t hi = lane == 31u ? 0xffffffffu : ((1u << (lane + 1)) - 1u);
+            const uint32_t rng = hi & ~((1u << (lane - o + 1)) - 1u);
+            if ((E & rng) == 0u) tv += ov;
+        }
+    }
+    float cin = __shfl_up_sync(0xffffffffu, tv, 1);
+    const uint32_t below = E & lanemask_lt();
+    if (lane == 0) cin = 0.0f;
+    if (below == 0u) cin += carry;
+    uint32_t rank = 0;
+#pragma unroll
+    for (int k = 0; k < 4; k++) rank += __popc(__ballot_sync(0xffffffffu, (f >> k) & 1u) & lanemask_lt());
+    bool first = true;
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        if ((f >> k) & 1u) {
+            emit(rank, sk[k] + (first ? cin : 0.0f), first && below == 0u);
+            first = false;
+            rank++;
+        }
+    }
+    const float last = __shfl_sync(0xffffffffu, tv, 31);
+    carry = E ? last : carry + last;
+}
+
+template <bool HOT>
+__global__ void __launch_bounds__(kSegNT, 1) kry32_seg_kernel(const IterArgs a) {
+    extern __shared__ __align__(16) float s_hot[];
+    __shared__ double s_red[96];
+    if (*(volatile const int32_t *)a.kdone) return;
+    const uint32_t H = HOT ? a.hot : 0u;
+    if (HOT) {
+        // hot prefix of the gathered vector (H is a multiple of 4; the
+        // vector is 256-byte aligned)
+        for (uint32_t i = threadIdx.x * 4; i < H; i += kSegNT * 4)
+            *reinterpret_cast<uint4 *>(s_hot + i) = __ldcg(reinterpret_cast<const uint4 *>(a.xt32_in + i));
+    }
+    double dz = 0.0;
+    if (!seg_prologue(a, dz)) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) a.kpart_out[0] = make_double4(0.0, 0.0, 0.0, 1.0);
+        return;
+    }
+    SegEpi ep{(float)a.damping, (float)(a.damping * dz), 0.0, 0.0, 0.0};
+    const uint32_t lane = threadIdx.x & 31;
+    const uint64_t warp = (blockIdx.x * (uint64_t)kSegNT + threadIdx.x) >> 5;
+    const uint64_t nwarps = (gridDim.x * (uint64_t)kSegNT) >> 5;
+    const float *xt = a.xt32_in;
+    for (uint64_t t = warp; t < a.seg_ntiles; t += nwarps) {
+        const uint64_t P0 = t * kSegTile;
+        uint4 c[2];
+#pragma unroll
+        for (int u = 0; u < 2; u++) {
+            const uint64_t pos = P0 + 4u * (lane + 32u * u);
+            // a quad that starts before the last arc stays inside col's padding
+            c[u] = pos < a.arcs ? ld_stream_u4(reinterpret_cast<const uint4 *>(a.col + pos), policy_evict_first())
+                                : make_uint4(0u, 0u, 0u, 0u);
+        }
+        const uint32_t mw0 = __ldg(&a.seg_mask[t * (kSegTile / 32) + (lane >> 3)]);
+        const uint32_t mw1 = __ldg(&a.seg_mask[t * (kSegTile / 32) + 4 + (lane >> 3)]);
+        const uint32_t j0 = __ldg(&a.seg_tile_j0[t]);
+        float v[2][4];
+        const uint64_t pol_g = policy_evict_last();
+#pragma unroll
+        for (int u = 0; u < 2; u++) {
+            const uint32_t cc[4] = {c[u].x, c[u].y, c[u].z, c[u].w};
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                const uint64_t p = P0 + 4u * (lane + 32u * u) + k;
+                float g = 0.0f;
+                if (p < a.arcs) {
+                    if (HOT && cc[k] < H) g = s_hot[cc[k]];
+                    else g = cc[k] < a.l1hot ? ld_gather(xt + cc[k], pol_g) : ld_gather_na(xt + cc[k], pol_g);
+                }
+                v[u][k] = g;
+            }
+        }
+        const uint32_t sh = (4u * lane) & 31u;
+        const uint32_t f0 = (mw0 >> sh) & 0xFu, f1 = (mw1 >> sh) & 0xFu;
+        const uint32_t cnt0 = __reduce_add_sync(0xffffffffu, __popc(f0));
+        float carry = 0.0f;
+        // a row end closes a row; the tile's first one may close a row that
+        // began in an earlier tile: then only its partial sum is kept (head)
+        auto close = [&](uint32_t rank, float sum, bool tile_first) {
+            const uint32_t row = __ldg(&a.seg_nz[j0 + rank]);
+            if (tile_first && __ldg(&a.row_ptr[row]) < P0) {
+                a.seg_head[t] = sum;
+                return;
+            }
+            ep.row(a, row, sum);
+        };
+        seg_block(v[0], f0, carry, lane, [&](uint32_t r, float sum, bool first) { close(r, sum, first); });
+        seg_block(v[1], f1, carry, lane,
+                  [&](uint32_t r, float sum, bool first) { close(cnt0 + r, sum, first && cnt0 == 0u); });
+        if (lane == 0) a.seg_tail[t] = carry;
+    }
+    seg_block_sum3(ep.pd, ep.pds, ep.ps, s_red);
+    if (threadIdx.x == 0) a.kpart_out[blockIdx.x] = make_double4(ep.pd, ep.pds, ep.ps, 0.0);
+}
+
+// Rows that span tiles (one thread per tile whose first row end closes a row
+// begun earlier) and rows without arcs; records after the tile kernel's.
+__global__ void __launch_bounds__(kSegFixNT) kry32_seg_finish(const IterArgs a, unsigned rec0) {
+    __shared__ double s_red[96];
+    if (*(volatile const int32_t *)a.kdone) return;
+    double dz = 0.0;
+    if (!seg_prologue(a, dz)) return;
+    SegEpi ep{(float)a.damping, (float)(a.damping * dz), 0.0, 0.0, 0.0};
+    const uint64_t tid = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    const uint64_t nth = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t b = tid; b < a.seg_ntiles; b += nth) {
+        const uint32_t j = a.seg_tile_j0[b];
+        if (a.seg_tile_j0[b + 1] == j) continue;  // no row ends in this tile
+        const uint32_t row = a.seg_nz[j];
+        const uint64_t t0 = a.row_ptr[row] / kSegTile;
+        if (t0 == b) continue;  // begun in this tile: finished by the tile kernel
+        double sum = 0.0;
+#pragma unroll 8
+        for (uint64_t t = t0; t < b; t++) sum += (double)__ldcg(&a.seg_tail[t]);
+        sum += (double)__ldcg(&a.seg_head[b]);
+        ep.row(a, row, (float)sum);
+    }
+    for (uint64_t i = tid; i < a.seg_nempty; i += nth) ep.row(a, a.seg_empty[i], 0.0f);
+    seg_block_sum3(ep.pd, ep.pds, ep.ps, s_red);
+    if (threadIdx.x == 0) a.kpart_out[rec0 + blockIdx.x] = make_double4(ep.pd, ep.pds, ep.ps, 0.0);
+}
+
+LaunchCfg seg_config(const DeviceGraph &g, uint32_t hot_entries) {
+    int dev = 0, sms = 0;
+    PRG_CUDA(cudaGetDevice(&dev));
+    PRG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    LaunchCfg c;
+    c.seg = 1;
+    c.threads = kSegNT;
+    c.hot = std::min<uint32_t>(std::min<uint32_t>(hot_entries, kSegHotMax), g.n) & ~3u;
+    c.smem = (size_t)c.hot * sizeof(float);
+    if (c.hot)
+        PRG_CUDA(cudaFuncSetAttribute(kry32_seg_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)c.smem));
+    c.seg_g1 = (unsigned)sms;
+    c.seg_g2 = (unsigned)sms * 4u;
+    c.grid = c.seg_g1 + c.seg_g2;  // block records the consumers add
+    c.hub_recs = 0;
+    return c;
+}
+
+void launch_kry32_seg(const IterArgs &a, const LaunchCfg &c, cudaStream_t s) {
+    if (c.hot) kry32_seg_kernel<true><<<c.seg_g1, kSegNT, c.smem, s>>>(a);
+    else kry32_seg_kernel<false><<<c.seg_g1, kSegNT, 0, s>>>(a);
+    kry32_seg_finish<<<c.seg_g2, kSegFixNT, 0, s>>>(a, c.seg_g1);
+    PRG_CUDA(cudaGetLastError());
+}
+
+}  // namespace prg

@@ -40,6 +40,7 @@ void workspace_free(Workspace &ws, cudaStream_t s) {
     for (auto &kv : ws.graphs) cudaGraphExecDestroy(kv.second);
     ws.graphs.clear();
     krylov_free(ws.kry, s);
+    seg_free(ws.seg, s);
     for (int i = 0; i < 2; i++) {
         wfree(ws.x64[i], s);
         wfree(ws.xt64[i], s);
@@ -77,14 +78,18 @@ void workspace_ensure(Workspace &ws, const DeviceGraph &g, cudaStream_t s) {
     ws.nrb = g.nrb;
     ws.nhub = g.nhub;
     unsigned gmax = kPrepParts;
+    const bool seg = !g.weighted && g.seg_kry32 != 0 && g.arcs > 0;
     for (int m = 0; m < kModes; m++) {
         const bool fp32 = m == MODE_CORR32 || m == MODE_KRY32;
         const uint32_t hot = g.perm != nullptr ? (fp32 ? g.hot_cache : g.hot_cache64) : 0u;
-        ws.cfg[m] = iteration_config(m, g.weighted, hot, g.blocks_per_sm, g.n, g.hot_threads);
+        if (m == MODE_KRY32 && seg) ws.cfg[m] = seg_config(g, g.perm != nullptr ? g.seg_hot : 0u);
+        else ws.cfg[m] = iteration_config(m, g.weighted, hot, g.blocks_per_sm, g.n, g.hot_threads);
+        if (!ws.cfg[m].seg) ws.cfg[m].hub_recs = g.nhub;
         const uint32_t l1 = fp32 ? g.l1_hot32 : g.l1_hot64;
         if (g.perm != nullptr && l1) ws.cfg[m].l1hot = l1;
         gmax = std::max(gmax, ws.cfg[m].grid);
     }
+    if (seg) seg_build(g, ws.seg, s);
     const uint64_t n = g.n;
     for (int i = 0; i < 2; i++) {
         walloc(ws.x64[i], n, s);
@@ -128,6 +133,15 @@ IterArgs base_args(const DeviceGraph &g, Workspace &ws, double damping) {
     a.n = g.n;
     a.damping = damping;
     a.inv_n = 1.0 / (double)g.n;
+    a.arcs = g.arcs;
+    a.seg_mask = ws.seg.mask;
+    a.seg_tile_j0 = ws.seg.tile_j0;
+    a.seg_nz = ws.seg.nz_row;
+    a.seg_empty = ws.seg.empty_row;
+    a.seg_head = ws.seg.head;
+    a.seg_tail = ws.seg.tail;
+    a.seg_ntiles = ws.seg.ntiles;
+    a.seg_nempty = ws.seg.n_empty;
     a.ctl = ws.ctl;
     a.blk_part = ws.blk_part;
     a.chunk_part = ws.chunk_part;

@@ -57,6 +57,7 @@ struct Workspace {
     const void *graphs_rb = nullptr;  // row-block list the cached graphs were captured with
     int unroll = 8;  // iteration pairs per graph launch
     KrylovWs *kry = nullptr;  // Krylov vectors, allocated on first use
+    SegIndex seg;             // row-end index of the tile-segmented FP32 Krylov matvec (when used)
 };
 
 void workspace_ensure(Workspace &ws, const DeviceGraph &g, cudaStream_t s);

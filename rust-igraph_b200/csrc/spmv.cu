@@ -637,6 +637,10 @@ void launch_iteration(int mode, bool weighted, const IterArgs &a_in, const Launc
     IterArgs a = a_in;
     a.hot = c.hot;
     a.l1hot = c.l1hot;
+    if (mode == MODE_KRY32 && c.seg) {
+        launch_kry32_seg(a, c, s);
+        return;
+    }
     switch (mode) {
         case MODE_PLAIN64: mode_launch<MODE_PLAIN64>(weighted, a, c, s); break;
         case MODE_PPR64: mode_launch<MODE_PPR64>(weighted, a, c, s); break;

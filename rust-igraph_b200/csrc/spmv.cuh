@@ -36,6 +36,22 @@ enum IterMode : int {
 };
 constexpr int kModes = 8;
 
+// Row-end index of the in-CSR for the tile-segmented matvec (segspmv.cu):
+// the arcs are cut into tiles of kSegTile; bit p of `mask` is set when arc p
+// is the last arc of its row; tile_j0[t] counts the row ends before tile t;
+// nz_row lists the rows that have arcs and empty_row those that have none.
+constexpr uint32_t kSegTile = 256;
+struct SegIndex {
+    uint64_t ntiles = 0;
+    uint32_t *mask = nullptr;       // ntiles * 8 words (+ 8 pad)
+    uint32_t *tile_j0 = nullptr;    // ntiles + 1
+    uint32_t *nz_row = nullptr;     // n_nz
+    uint32_t *empty_row = nullptr;  // n_empty
+    uint32_t n_nz = 0, n_empty = 0;
+    float *head = nullptr;          // per tile: the sum up to its first row end
+    float *tail = nullptr;          // per tile: the open sum after its last row end
+};
+
 struct IterArgs {
     // graph
     const uint32_t *row_ptr;
@@ -78,6 +94,12 @@ struct IterArgs {
     // scalars
     double damping;
     double inv_n;
+    // tile-segmented FP32 Krylov matvec (MODE_KRY32 with LaunchCfg::seg)
+    uint64_t arcs;
+    const uint32_t *seg_mask, *seg_tile_j0, *seg_nz, *seg_empty;
+    float *seg_head, *seg_tail;
+    uint64_t seg_ntiles;
+    uint32_t seg_nempty;
     // reduction scratch
     Ctl *ctl;
     double4 *blk_part;   // one record per block of the persistent grid
@@ -88,11 +110,14 @@ struct IterArgs {
 };
 
 struct LaunchCfg {
-    unsigned grid = 0;
+    unsigned grid = 0;  // persistent grid; for the segmented matvec, the record count seg_g1 + seg_g2
     int threads = kThreads;
     size_t smem = 0;   // dynamic shared memory (warp buffers + hot prefix)
     uint32_t hot = 0;  // hot-prefix length (vertices)
     uint32_t l1hot = 0xFFFFFFFFu;  // gathers of ids >= l1hot bypass L1
+    uint32_t hub_recs = 0;  // hub-row records a Krylov consumer adds after the block records
+    int seg = 0;            // MODE_KRY32: tile-segmented kernel pair (segspmv.cu)
+    unsigned seg_g1 = 0, seg_g2 = 0;  // its main and finishing grids
 };
 
 // Persistent launch shape of the iteration kernel on this device: 256-thread
@@ -103,6 +128,15 @@ struct LaunchCfg {
 LaunchCfg iteration_config(int mode, bool weighted, uint32_t hot_entries, uint32_t blocks_per_sm, uint32_t n,
                            uint32_t hot_threads = kThreads);
 void launch_iteration(int mode, bool weighted, const IterArgs &a, const LaunchCfg &c, cudaStream_t s);
+
+// Tile-segmented FP32 Krylov matvec (segspmv.cu): builds the row-end index of
+// g (unweighted graphs), frees it, gives its launch shape (hot prefix of up
+// to hot_entries vertices in shared memory) and launches it (two kernels:
+// the tiles, then the rows that span tiles and the rows without arcs).
+void seg_build(const DeviceGraph &g, SegIndex &x, cudaStream_t s);
+void seg_free(SegIndex &x, cudaStream_t s);
+LaunchCfg seg_config(const DeviceGraph &g, uint32_t hot_entries);
+void launch_kry32_seg(const IterArgs &a, const LaunchCfg &c, cudaStream_t s);
 
 // Average time (ms) of a pass that only streams g's column indices and gathers
 // one FP32 value per arc with the FP32 matvec's load policies (reps timed

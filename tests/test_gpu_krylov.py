@@ -185,3 +185,49 @@ def test_linsys_stop_rule_erdos_renyi(cuda_ok, directed):
     assert np.max(np.abs(x - tight)) <= 1e-13
     # the power-iteration drop-in agrees within the reference's 1e-9 contract
     assert np.max(np.abs(x - ig.pagerank(g))) <= 1e-9
+
+
+@pytest.mark.parametrize("case", ["rmat_relabelled", "star_hub", "tiny", "sparse_many_empty", "undirected_ba"])
+def test_segmented_fp32_matvec_matches_row_block_kernel(cuda_ok, case):
+    # The FP32 Krylov matvec of unweighted graphs runs as the tile-segmented
+    # pass (segspmv.cu, tuning seg_kry32 = 1, the default) or as the
+    # row-block kernel (0).  Both refined solves meet the tight oracle, and
+    # the segmented one is bit-reproducible.  The cases cover rows that span
+    # many tiles (a hub with every arc), graphs smaller than one tile, rows
+    # without arcs, and undirected graphs.
+    directed = True
+    if case == "rmat_relabelled":
+        n = 1 << 15
+        f, t = O.rmat(15, 16 * n, seed=44)
+    elif case == "star_hub":
+        n = 5000
+        f = np.arange(1, n, dtype=np.uint32).repeat(3)
+        t = np.zeros(len(f), np.uint32)
+        f = np.concatenate([f, np.array([0, 0, 7], np.uint32)])
+        t = np.concatenate([t, np.array([1, 2, 3], np.uint32)])
+    elif case == "tiny":
+        n = 40
+        f, t = O.erdos_renyi_gnm(n, 120, True, False, 3)
+    elif case == "sparse_many_empty":
+        n = 200_000
+        f, t = O.erdos_renyi_gnm(n, 150_000, True, False, 9)
+    else:
+        n = 30_000
+        f, t = O.barabasi_game_bag(n, 5, False, False, 12)
+        directed = False
+    tight, _, _ = O.pagerank_tight(n, f, t, directed, tol=1e-15)
+    xs = {}
+    try:
+        for seg in (1, 0):
+            ig.set_tuning("seg_kry32", seg)
+            with ig.DeviceGraph.from_host(n, f, t, directed) as dg:
+                x, st = dg.solve(ig.Options(precision=ig.PRECISION_FP32_REFINED))
+                assert np.abs(x - tight).sum() <= 1e-10, (seg, np.abs(x - tight).sum())
+                assert st.error_bound <= 1e-10
+                if seg:
+                    x2, _ = dg.solve(ig.Options(precision=ig.PRECISION_FP32_REFINED))
+                    assert np.array_equal(x.view(np.uint64), x2.view(np.uint64))
+                xs[seg] = x
+    finally:
+        ig.reset_tuning()
+    assert np.abs(xs[1] - xs[0]).sum() <= 2e-10
