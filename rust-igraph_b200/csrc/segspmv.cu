@@ -15,7 +15,9 @@
 //     shuffles) whose segment breaks come from one ballot of "lane holds a
 //     row end", with no flag shuffles;
 //   * the k-th row end of tile t belongs to nz_row[tile_j0[t] + k] (the rows
-//     that have arcs, in order), and its lane applies the epilogue there.
+//     that have arcs, in order); its sum goes to the warp's shared buffer at
+//     rank k, and the epilogues then run with lane i on rank i, so the loads
+//     of the rows' operands coalesce.
 // A row that began in an earlier tile is finished by a second, small kernel:
 // tile t leaves the sum before its first row end (head) and the open sum
 // after its last (tail); the row's total is the tails of the tiles it spans
@@ -233,9 +235,12 @@ __device__ __forceinline__ void seg_block(const float (&v)[4], uint32_t f, float
     carry = E ? last : carry + last;
 }
 
+// Dynamic shared memory: [32 warp buffers of kSegTile row sums][hot prefix].
 template <bool HOT>
 __global__ void __launch_bounds__(kSegNT, 1) kry32_seg_kernel(const IterArgs a) {
-    extern __shared__ __align__(16) float s_hot[];
+    extern __shared__ __align__(16) float s_dyn[];
+    float *s_sums = s_dyn;                            // per warp: the tile's row sums by rank
+    float *s_hot = s_dyn + (kSegNT / 32) * kSegTile;  // hot prefix
     __shared__ double s_red[96];
     if (*(volatile const int32_t *)a.kdone) return;
     const uint32_t H = HOT ? a.hot : 0u;
@@ -252,6 +257,7 @@ __global__ void __launch_bounds__(kSegNT, 1) kry32_seg_kernel(const IterArgs a) 
     }
     SegEpi ep{(float)a.damping, (float)(a.damping * dz), 0.0, 0.0, 0.0};
     const uint32_t lane = threadIdx.x & 31;
+    float *sums = s_sums + (threadIdx.x >> 5) * kSegTile;
     const uint64_t warp = (blockIdx.x * (uint64_t)kSegNT + threadIdx.x) >> 5;
     const uint64_t nwarps = (gridDim.x * (uint64_t)kSegNT) >> 5;
     const float *xt = a.xt32_in;
@@ -287,21 +293,29 @@ __global__ void __launch_bounds__(kSegNT, 1) kry32_seg_kernel(const IterArgs a) 
         const uint32_t sh = (4u * lane) & 31u;
         const uint32_t f0 = (mw0 >> sh) & 0xFu, f1 = (mw1 >> sh) & 0xFu;
         const uint32_t cnt0 = __reduce_add_sync(0xffffffffu, __popc(f0));
+        const uint32_t cnt = cnt0 + __reduce_add_sync(0xffffffffu, __popc(f1));
         float carry = 0.0f;
-        // a row end closes a row; the tile's first one may close a row that
-        // began in an earlier tile: then only its partial sum is kept (head)
-        auto close = [&](uint32_t rank, float sum, bool tile_first) {
-            const uint32_t row = __ldg(&a.seg_nz[j0 + rank]);
-            if (tile_first && __ldg(&a.row_ptr[row]) < P0) {
-                a.seg_head[t] = sum;
-                return;
-            }
-            ep.row(a, row, sum);
-        };
-        seg_block(v[0], f0, carry, lane, [&](uint32_t r, float sum, bool first) { close(r, sum, first); });
-        seg_block(v[1], f1, carry, lane,
-                  [&](uint32_t r, float sum, bool first) { close(cnt0 + r, sum, first && cnt0 == 0u); });
+        // each row end leaves its sum at its rank; the tile's first one also
+        // as the head (the finishing kernel uses it when that row began in
+        // an earlier tile)
+        seg_block(v[0], f0, carry, lane, [&](uint32_t r, float sum, bool first) {
+            sums[r] = sum;
+            if (first) a.seg_head[t] = sum;
+        });
+        seg_block(v[1], f1, carry, lane, [&](uint32_t r, float sum, bool first) {
+            sums[cnt0 + r] = sum;
+            if (first && cnt0 == 0u) a.seg_head[t] = sum;
+        });
         if (lane == 0) a.seg_tail[t] = carry;
+        __syncwarp();
+        // epilogues of the tile's rows, lane i taking rank i: their rows are
+        // consecutive in nz_row order, so the operand loads coalesce
+        for (uint32_t i = lane; i < cnt; i += 32) {
+            const uint32_t row = __ldg(&a.seg_nz[j0 + i]);
+            if (i == 0 && __ldg(&a.row_ptr[row]) < P0) continue;  // begun earlier: finished later
+            ep.row(a, row, sums[i]);
+        }
+        __syncwarp();
     }
     seg_block_sum3(ep.pd, ep.pds, ep.ps, s_red);
     if (threadIdx.x == 0) a.kpart_out[blockIdx.x] = make_double4(ep.pd, ep.pds, ep.ps, 0.0);
@@ -342,10 +356,9 @@ LaunchCfg seg_config(const DeviceGraph &g, uint32_t hot_entries) {
     c.seg = 1;
     c.threads = kSegNT;
     c.hot = std::min<uint32_t>(std::min<uint32_t>(hot_entries, kSegHotMax), g.n) & ~3u;
-    c.smem = (size_t)c.hot * sizeof(float);
-    if (c.hot)
-        PRG_CUDA(cudaFuncSetAttribute(kry32_seg_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)c.smem));
+    c.smem = ((size_t)(kSegNT / 32) * kSegTile + c.hot) * sizeof(float);
+    PRG_CUDA(cudaFuncSetAttribute(c.hot ? (const void *)kry32_seg_kernel<true> : (const void *)kry32_seg_kernel<false>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c.smem));
     c.seg_g1 = (unsigned)sms;
     c.seg_g2 = (unsigned)sms * 4u;
     c.grid = c.seg_g1 + c.seg_g2;  // block records the consumers add
@@ -355,7 +368,7 @@ LaunchCfg seg_config(const DeviceGraph &g, uint32_t hot_entries) {
 
 void launch_kry32_seg(const IterArgs &a, const LaunchCfg &c, cudaStream_t s) {
     if (c.hot) kry32_seg_kernel<true><<<c.seg_g1, kSegNT, c.smem, s>>>(a);
-    else kry32_seg_kernel<false><<<c.seg_g1, kSegNT, 0, s>>>(a);
+    else kry32_seg_kernel<false><<<c.seg_g1, kSegNT, c.smem, s>>>(a);
     kry32_seg_finish<<<c.seg_g2, kSegFixNT, 0, s>>>(a, c.seg_g1);
     PRG_CUDA(cudaGetLastError());
 }
