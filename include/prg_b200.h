@@ -334,9 +334,11 @@ typedef struct prg_batch_stats {
  * turns them off): the test is still the change one power step makes,
  * ||G(x) - x||_1 < tol, and the column returns that step, G(x), as the
  * reference does; only the sequence of iterates before it is shorter.  FP32
- * rounding puts a floor of about n ulp under that change; a Chebyshev column
- * whose change stops falling within 4 x tol freezes there (its answer is then
- * within d/(1-d) of that change of the fixed point).
+ * rounding puts a floor of about n ulp under that change, so a Chebyshev
+ * column finishes with plain steps once its change is below 100 x tol; if
+ * those stop falling within 10 x tol (a rounding cycle at the floor) it
+ * freezes there, its answer within d/(1-d) of that change of the fixed
+ * point.
  * tile_vec: columns per tile = 32 * tile_vec (1, 2 or 4; 0 = autotuned or 1).
  * out: host float[n * K], out[v * K + k].  column_iters: optional host
  * uint32[K].  Validation follows _vs: empty seed list or vertex >= n ->

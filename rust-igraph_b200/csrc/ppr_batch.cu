@@ -77,17 +77,18 @@ struct ColState {
 constexpr uint32_t kChebMinPower = 6, kChebMaxPower = 24;
 constexpr double kChebSettle = 0.01, kChebMargin = 1.05;
 // FP32 rounding sets a floor under ||G(x) - x||_1 (about n ulp of the
-// column's mass): a weighted combination of iterates never becomes an exact
-// FP32 fixed point, and plain FP32 steps started from a Chebyshev iterate can
-// settle into a cycle of a few ulp flips instead of a fixed point.  At that
-// floor the change only wanders.  A Chebyshev column whose change has not
-// reached a new minimum for kChebStall steps therefore freezes there if the
-// change is within kChebFloor x tol (its answer G(x) is then within d/(1-d)
-// of that change of the fixed point), and otherwise finishes with plain
-// steps, which freeze the same way after kChebStall more steps without a new
-// minimum.
+// column's mass, which at n = 2 M sits near the 1e-8 tolerance): a weighted
+// combination of iterates never becomes an exact FP32 fixed point, and plain
+// FP32 steps started from a Chebyshev iterate at that floor can settle into a
+// cycle of a few ulp flips.  So a Chebyshev column hands over to plain steps
+// once its change is below kChebHandoff x tol (or has not reached a new
+// minimum for kChebStall steps); the plain steps then converge as the
+// reference's do, to the FP32 fixed point where the change is 0.  As a last
+// guard, a plain column that makes no new minimum for kChebStall steps with
+// its change within kChebFloor x tol freezes there (its answer G(x) is then
+// within d/(1-d) of that change of the fixed point).
 constexpr uint32_t kChebStall = 6, kChebOff = 0xFFFFFFFFu;
-constexpr double kChebFloor = 4.0;
+constexpr double kChebHandoff = 100.0, kChebFloor = 10.0;
 
 struct TileArgs {
     const uint32_t *row_ptr;
@@ -270,20 +271,20 @@ __device__ __forceinline__ void reduce_columns(const TileArgs &a, int parity_new
                         } else {
                             s.stall += 1u;
                         }
-                        const bool plain = s.cheb_steps == kChebOff;
-                        if (s.stall >= kChebStall) {
-                            if (tx < kChebFloor * a.tol) {
-                                // at the FP32 floor: freeze with this step's G(x)
-                                s.active = 0u;
-                                s.final_buf = (uint32_t)parity_new;
-                            } else if (!plain) {
+                        if (s.cheb_steps != kChebOff) {
+                            if (tx < kChebHandoff * a.tol || s.stall >= kChebStall) {
                                 s.omega = 0.0;  // plain steps from here on
                                 s.cheb_steps = kChebOff;
                                 s.stall = 0u;
+                            } else {
+                                s.omega = 1.0 / (1.0 - 0.25 * s.beta * s.beta * s.omega);
+                                s.cheb_steps += 1u;
                             }
-                        } else if (!plain) {
-                            s.omega = 1.0 / (1.0 - 0.25 * s.beta * s.beta * s.omega);
-                            s.cheb_steps += 1u;
+                        } else if (s.stall >= kChebStall && tx < kChebFloor * a.tol) {
+                            // plain steps caught in a rounding cycle at the
+                            // FP32 floor: freeze with this step's G(x)
+                            s.active = 0u;
+                            s.final_buf = (uint32_t)parity_new;
                         }
                     }
                     s.prev_ratio = ratio;
