@@ -46,7 +46,7 @@ struct DeviceGraph {
     uint32_t hot_cache = 0, hot_cache64 = 0, hot_threads = kThreads;
     // unweighted graphs: the FP32 Krylov matvec as the tile-segmented pass
     // (segspmv.cu), with a hot prefix of seg_hot entries on relabelled graphs
-    uint32_t seg_kry32 = 1, seg_hot = 49152;
+    uint32_t seg_kry32 = 1, seg_hot = 32768;
     // relabelled graphs: gathers of ids >= l1_hot32 (FP32 passes) / l1_hot64
     // (FP64 passes) bypass L1, keeping it for the hot prefix (0 = all allocate)
     uint32_t l1_hot32 = 16384, l1_hot64 = 2048;
@@ -83,7 +83,7 @@ struct Tuning {
     int unroll = 8;
     uint32_t hot_cache = 0, hot_cache64 = 0, hot_threads = kThreads;
     uint32_t seg_kry32 = 1;      // unweighted graphs: tile-segmented FP32 Krylov matvec (0 = row-block kernel)
-    uint32_t seg_hot = 49152;    // its shared-memory hot prefix on relabelled graphs (entries)
+    uint32_t seg_hot = 32768;    // its shared-memory hot prefix on relabelled graphs (entries)
     uint32_t l1_hot32 = 16384, l1_hot64 = 2048;
     double refine_switch = 5e-7;
     uint32_t batch_vec = 1;

@@ -74,6 +74,36 @@ __global__ void seg_split_rows_kernel(const uint32_t *nonempty, const uint32_t *
     }
 }
 
+// Tiles whose first row end closes a row begun in an earlier tile: kind 1
+// (short span) or 2 (more than kSegLongSpan tiles), else 0.
+__global__ void seg_span_kind_kernel(const uint32_t *rp, const uint32_t *tile_j0, const uint32_t *nz, uint64_t ntiles,
+                                     uint32_t *is_short, uint32_t *is_long) {
+    for (uint64_t b = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; b < ntiles;
+         b += (uint64_t)gridDim.x * blockDim.x) {
+        uint32_t k = 0;
+        const uint32_t j = tile_j0[b];
+        if (tile_j0[b + 1] != j) {
+            const uint64_t t0 = rp[nz[j]] / kSegTile;
+            if (t0 < b) k = b - t0 > kSegLongSpan ? 2u : 1u;
+        }
+        is_short[b] = k == 1u;
+        is_long[b] = k == 2u;
+    }
+}
+
+__global__ void seg_span_fill_kernel(const uint32_t *rp, const uint32_t *tile_j0, const uint32_t *nz, uint64_t ntiles,
+                                     const uint32_t *is_short, const uint32_t *pos_short, const uint32_t *is_long,
+                                     const uint32_t *pos_long, uint4 *span, uint4 *span_long) {
+    for (uint64_t b = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; b < ntiles;
+         b += (uint64_t)gridDim.x * blockDim.x) {
+        if (!is_short[b] && !is_long[b]) continue;
+        const uint32_t row = nz[tile_j0[b]];
+        const uint4 e = make_uint4(row, (uint32_t)(rp[row] / kSegTile), (uint32_t)b, 0u);
+        if (is_short[b]) span[pos_short[b]] = e;
+        else span_long[pos_long[b]] = e;
+    }
+}
+
 template <class T>
 static T *salloc(uint64_t count, cudaStream_t s) {
     T *p = nullptr;
@@ -83,7 +113,7 @@ static T *salloc(uint64_t count, cudaStream_t s) {
 
 void seg_free(SegIndex &x, cudaStream_t s) {
     for (void *p : {(void *)x.mask, (void *)x.tile_j0, (void *)x.nz_row, (void *)x.empty_row, (void *)x.head,
-                    (void *)x.tail})
+                    (void *)x.tail, (void *)x.span, (void *)x.span_long})
         if (p) cudaFreeAsync(p, s);
     x = SegIndex{};
 }
@@ -117,9 +147,27 @@ void seg_build(const DeviceGraph &g, SegIndex &x, cudaStream_t s) {
     PRG_CUDA(cudaGetLastError());
     x.head = salloc<float>(ntiles, s);
     x.tail = salloc<float>(ntiles, s);
-    cudaFreeAsync(nonempty, s);
-    cudaFreeAsync(pos, s);
-    cudaFreeAsync(cnt, s);
+    // the rows that span tiles, as two compacted lists in tile order
+    uint32_t *is_short = salloc<uint32_t>(ntiles, s), *is_long = salloc<uint32_t>(ntiles, s);
+    uint32_t *pos_short = salloc<uint32_t>(ntiles + 1, s), *pos_long = salloc<uint32_t>(ntiles + 1, s);
+    seg_span_kind_kernel<<<gb, 256, 0, s>>>(g.row_ptr, x.tile_j0, x.nz_row, ntiles, is_short, is_long);
+    PRG_CUDA(cudaGetLastError());
+    exclusive_scan_u32(is_short, pos_short, ntiles, s);
+    exclusive_scan_u32(is_long, pos_long, ntiles, s);
+    uint32_t ns = 0, nl = 0;
+    PRG_CUDA(cudaMemcpyAsync(&ns, pos_short + ntiles, 4, cudaMemcpyDeviceToHost, s));
+    PRG_CUDA(cudaMemcpyAsync(&nl, pos_long + ntiles, 4, cudaMemcpyDeviceToHost, s));
+    PRG_CUDA(cudaStreamSynchronize(s));
+    x.n_span = ns;
+    x.n_long = nl;
+    x.span = salloc<uint4>(ns, s);
+    x.span_long = salloc<uint4>(nl, s);
+    seg_span_fill_kernel<<<gb, 256, 0, s>>>(g.row_ptr, x.tile_j0, x.nz_row, ntiles, is_short, pos_short, is_long,
+                                            pos_long, x.span, x.span_long);
+    PRG_CUDA(cudaGetLastError());
+    for (void *p : {(void *)nonempty, (void *)pos, (void *)cnt, (void *)is_short, (void *)is_long,
+                    (void *)pos_short, (void *)pos_long})
+        cudaFreeAsync(p, s);
 }
 
 // ------------------------------------------------------------------ kernels
@@ -321,8 +369,11 @@ __global__ void __launch_bounds__(kSegNT, 1) kry32_seg_kernel(const IterArgs a) 
     if (threadIdx.x == 0) a.kpart_out[blockIdx.x] = make_double4(ep.pd, ep.pds, ep.ps, 0.0);
 }
 
-// Rows that span tiles (one thread per tile whose first row end closes a row
-// begun earlier) and rows without arcs; records after the tile kernel's.
+// Rows that span tiles and rows without arcs; records after the tile
+// kernel's.  A spanning row's total is the open tails of the tiles from its
+// first to the one before its closing tile, plus that tile's head, in tile
+// order in FP64: one thread per row for spans of up to kSegLongSpan tiles,
+// one warp (lanes strided over the tiles, then a fixed tree) for longer ones.
 __global__ void __launch_bounds__(kSegFixNT) kry32_seg_finish(const IterArgs a, unsigned rec0) {
     __shared__ double s_red[96];
     if (*(volatile const int32_t *)a.kdone) return;
@@ -331,17 +382,21 @@ __global__ void __launch_bounds__(kSegFixNT) kry32_seg_finish(const IterArgs a, 
     SegEpi ep{(float)a.damping, (float)(a.damping * dz), 0.0, 0.0, 0.0};
     const uint64_t tid = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
     const uint64_t nth = (uint64_t)gridDim.x * blockDim.x;
-    for (uint64_t b = tid; b < a.seg_ntiles; b += nth) {
-        const uint32_t j = a.seg_tile_j0[b];
-        if (a.seg_tile_j0[b + 1] == j) continue;  // no row ends in this tile
-        const uint32_t row = a.seg_nz[j];
-        const uint64_t t0 = a.row_ptr[row] / kSegTile;
-        if (t0 == b) continue;  // begun in this tile: finished by the tile kernel
+    for (uint64_t i = tid; i < a.seg_nspan; i += nth) {
+        const uint4 e = a.seg_span[i];
         double sum = 0.0;
-#pragma unroll 8
-        for (uint64_t t = t0; t < b; t++) sum += (double)__ldcg(&a.seg_tail[t]);
-        sum += (double)__ldcg(&a.seg_head[b]);
-        ep.row(a, row, (float)sum);
+#pragma unroll 4
+        for (uint32_t t = e.y; t < e.z; t++) sum += (double)__ldcg(&a.seg_tail[t]);
+        sum += (double)__ldcg(&a.seg_head[e.z]);
+        ep.row(a, e.x, (float)sum);
+    }
+    const uint32_t lane = threadIdx.x & 31;
+    for (uint64_t i = tid >> 5; i < a.seg_nlong; i += nth >> 5) {
+        const uint4 e = a.seg_span_long[i];
+        double sum = 0.0;
+        for (uint32_t t = e.y + lane; t < e.z; t += 32) sum += (double)__ldcg(&a.seg_tail[t]);
+        sum = warp_sum(sum);
+        if (lane == 0) ep.row(a, e.x, (float)(sum + (double)__ldcg(&a.seg_head[e.z])));
     }
     for (uint64_t i = tid; i < a.seg_nempty; i += nth) ep.row(a, a.seg_empty[i], 0.0f);
     seg_block_sum3(ep.pd, ep.pds, ep.ps, s_red);

@@ -142,6 +142,10 @@ IterArgs base_args(const DeviceGraph &g, Workspace &ws, double damping) {
     a.seg_tail = ws.seg.tail;
     a.seg_ntiles = ws.seg.ntiles;
     a.seg_nempty = ws.seg.n_empty;
+    a.seg_span = ws.seg.span;
+    a.seg_span_long = ws.seg.span_long;
+    a.seg_nspan = ws.seg.n_span;
+    a.seg_nlong = ws.seg.n_long;
     a.ctl = ws.ctl;
     a.blk_part = ws.blk_part;
     a.chunk_part = ws.chunk_part;

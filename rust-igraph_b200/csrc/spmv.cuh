@@ -41,6 +41,7 @@ constexpr int kModes = 8;
 // is the last arc of its row; tile_j0[t] counts the row ends before tile t;
 // nz_row lists the rows that have arcs and empty_row those that have none.
 constexpr uint32_t kSegTile = 256;
+constexpr uint32_t kSegLongSpan = 32;
 struct SegIndex {
     uint64_t ntiles = 0;
     uint32_t *mask = nullptr;       // ntiles * 8 words (+ 8 pad)
@@ -48,6 +49,10 @@ struct SegIndex {
     uint32_t *nz_row = nullptr;     // n_nz
     uint32_t *empty_row = nullptr;  // n_empty
     uint32_t n_nz = 0, n_empty = 0;
+    // rows closed in a later tile than they begin: {row, first tile, closing
+    // tile, 0}, in tile order; spans of more than kSegLongSpan tiles apart
+    uint4 *span = nullptr, *span_long = nullptr;
+    uint32_t n_span = 0, n_long = 0;
     float *head = nullptr;          // per tile: the sum up to its first row end
     float *tail = nullptr;          // per tile: the open sum after its last row end
 };
@@ -98,8 +103,9 @@ struct IterArgs {
     uint64_t arcs;
     const uint32_t *seg_mask, *seg_tile_j0, *seg_nz, *seg_empty;
     float *seg_head, *seg_tail;
+    const uint4 *seg_span, *seg_span_long;
     uint64_t seg_ntiles;
-    uint32_t seg_nempty;
+    uint32_t seg_nempty, seg_nspan, seg_nlong;
     // reduction scratch
     Ctl *ctl;
     double4 *blk_part;   // one record per block of the persistent grid
