@@ -8,7 +8,8 @@
 // pass streams them like a gather-only loop: a warp takes tiles in a
 // grid-stride order (neighbouring warps read neighbouring tiles), each lane
 // loads two 16-byte index quads and gathers their eight sources, and the row
-// sums come from a segmented scan in registers, driven by a bit per arc that
+// sums come from a segmented scan in registers (FP64 partial sums, so a row
+// sum is rounded to FP32 once), driven by a bit per arc that
 // marks the last arc of a row (built once per graph):
 //   * in each lane, a running sum over its 4 arcs that restarts after a row end;
 //   * across the 32 lanes, an inclusive scan of the lanes' open tails (5
@@ -145,8 +146,8 @@ void seg_build(const DeviceGraph &g, SegIndex &x, cudaStream_t s) {
     x.empty_row = salloc<uint32_t>(x.n_empty, s);
     seg_split_rows_kernel<<<gb, 256, 0, s>>>(nonempty, pos, n, x.nz_row, x.empty_row);
     PRG_CUDA(cudaGetLastError());
-    x.head = salloc<float>(ntiles, s);
-    x.tail = salloc<float>(ntiles, s);
+    x.head = salloc<double>(ntiles, s);
+    x.tail = salloc<double>(ntiles, s);
     // the rows that span tiles, as two compacted lists in tile order
     uint32_t *is_short = salloc<uint32_t>(ntiles, s), *is_long = salloc<uint32_t>(ntiles, s);
     uint32_t *pos_short = salloc<uint32_t>(ntiles + 1, s), *pos_long = salloc<uint32_t>(ntiles + 1, s);
@@ -244,28 +245,30 @@ struct SegEpi {
 // row end in arc order, rank counted within the block, `first` for the
 // block's first row end.
 template <class Emit>
-__device__ __forceinline__ void seg_block(const float (&v)[4], uint32_t f, float &carry, uint32_t lane, Emit emit) {
-    const float s0 = v[0];
-    const float s1 = (f & 1u) ? v[1] : s0 + v[1];
-    const float s2 = (f & 2u) ? v[2] : s1 + v[2];
-    const float s3 = (f & 4u) ? v[3] : s2 + v[3];
-    const float sk[4] = {s0, s1, s2, s3};
-    float tv = (f & 8u) ? 0.0f : s3;  // the lane's open tail
+__device__ __forceinline__ void seg_block(const float (&v)[4], uint32_t f, double &carry, uint32_t lane, Emit emit) {
+    // FP64 partial sums: a row's FP32 products are added exactly enough that
+    // the row sum is rounded to FP32 once, at its end
+    const double s0 = v[0];
+    const double s1 = (f & 1u) ? (double)v[1] : s0 + v[1];
+    const double s2 = (f & 2u) ? (double)v[2] : s1 + v[2];
+    const double s3 = (f & 4u) ? (double)v[3] : s2 + v[3];
+    const double sk[4] = {s0, s1, s2, s3};
+    double tv = (f & 8u) ? 0.0 : s3;  // the lane's open tail
     const uint32_t E = __ballot_sync(0xffffffffu, f != 0u);
     // inclusive scan of the open tails; lane L stops adding once a lane of
     // the range it already covers, (L - o, L], holds a row end
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
-        const float ov = __shfl_up_sync(0xffffffffu, tv, o);
+        const double ov = __shfl_up_sync(0xffffffffu, tv, o);
         if (lane >= (uint32_t)o) {
             const uint32_t hi = lane == 31u ? 0xffffffffu : ((1u << (lane + 1)) - 1u);
             const uint32_t rng = hi & ~((1u << (lane - o + 1)) - 1u);
             if ((E & rng) == 0u) tv += ov;
         }
     }
-    float cin = __shfl_up_sync(0xffffffffu, tv, 1);
+    double cin = __shfl_up_sync(0xffffffffu, tv, 1);
     const uint32_t below = E & lanemask_lt();
-    if (lane == 0) cin = 0.0f;
+    if (lane == 0) cin = 0.0;
     if (below == 0u) cin += carry;
     uint32_t rank = 0;
 #pragma unroll
@@ -274,12 +277,12 @@ __device__ __forceinline__ void seg_block(const float (&v)[4], uint32_t f, float
 #pragma unroll
     for (int k = 0; k < 4; k++) {
         if ((f >> k) & 1u) {
-            emit(rank, sk[k] + (first ? cin : 0.0f), first && below == 0u);
+            emit(rank, sk[k] + (first ? cin : 0.0), first && below == 0u);
             first = false;
             rank++;
         }
     }
-    const float last = __shfl_sync(0xffffffffu, tv, 31);
+    const double last = __shfl_sync(0xffffffffu, tv, 31);
     carry = E ? last : carry + last;
 }
 
@@ -342,16 +345,16 @@ __global__ void __launch_bounds__(kSegNT, 1) kry32_seg_kernel(const IterArgs a) 
         const uint32_t f0 = (mw0 >> sh) & 0xFu, f1 = (mw1 >> sh) & 0xFu;
         const uint32_t cnt0 = __reduce_add_sync(0xffffffffu, __popc(f0));
         const uint32_t cnt = cnt0 + __reduce_add_sync(0xffffffffu, __popc(f1));
-        float carry = 0.0f;
+        double carry = 0.0;
         // each row end leaves its sum at its rank; the tile's first one also
         // as the head (the finishing kernel uses it when that row began in
         // an earlier tile)
-        seg_block(v[0], f0, carry, lane, [&](uint32_t r, float sum, bool first) {
-            sums[r] = sum;
+        seg_block(v[0], f0, carry, lane, [&](uint32_t r, double sum, bool first) {
+            sums[r] = (float)sum;
             if (first) a.seg_head[t] = sum;
         });
-        seg_block(v[1], f1, carry, lane, [&](uint32_t r, float sum, bool first) {
-            sums[cnt0 + r] = sum;
+        seg_block(v[1], f1, carry, lane, [&](uint32_t r, double sum, bool first) {
+            sums[cnt0 + r] = (float)sum;
             if (first && cnt0 == 0u) a.seg_head[t] = sum;
         });
         if (lane == 0) a.seg_tail[t] = carry;
@@ -386,17 +389,17 @@ __global__ void __launch_bounds__(kSegFixNT) kry32_seg_finish(const IterArgs a, 
         const uint4 e = a.seg_span[i];
         double sum = 0.0;
 #pragma unroll 4
-        for (uint32_t t = e.y; t < e.z; t++) sum += (double)__ldcg(&a.seg_tail[t]);
-        sum += (double)__ldcg(&a.seg_head[e.z]);
+        for (uint32_t t = e.y; t < e.z; t++) sum += __ldcg(&a.seg_tail[t]);
+        sum += __ldcg(&a.seg_head[e.z]);
         ep.row(a, e.x, (float)sum);
     }
     const uint32_t lane = threadIdx.x & 31;
     for (uint64_t i = tid >> 5; i < a.seg_nlong; i += nth >> 5) {
         const uint4 e = a.seg_span_long[i];
         double sum = 0.0;
-        for (uint32_t t = e.y + lane; t < e.z; t += 32) sum += (double)__ldcg(&a.seg_tail[t]);
+        for (uint32_t t = e.y + lane; t < e.z; t += 32) sum += __ldcg(&a.seg_tail[t]);
         sum = warp_sum(sum);
-        if (lane == 0) ep.row(a, e.x, (float)(sum + (double)__ldcg(&a.seg_head[e.z])));
+        if (lane == 0) ep.row(a, e.x, (float)(sum + __ldcg(&a.seg_head[e.z])));
     }
     for (uint64_t i = tid; i < a.seg_nempty; i += nth) ep.row(a, a.seg_empty[i], 0.0f);
     seg_block_sum3(ep.pd, ep.pds, ep.ps, s_red);

@@ -53,8 +53,8 @@ struct SegIndex {
     // tile, 0}, in tile order; spans of more than kSegLongSpan tiles apart
     uint4 *span = nullptr, *span_long = nullptr;
     uint32_t n_span = 0, n_long = 0;
-    float *head = nullptr;          // per tile: the sum up to its first row end
-    float *tail = nullptr;          // per tile: the open sum after its last row end
+    double *head = nullptr;         // per tile: the sum up to its first row end
+    double *tail = nullptr;         // per tile: the open sum after its last row end
 };
 
 struct IterArgs {
@@ -102,7 +102,7 @@ struct IterArgs {
     // tile-segmented FP32 Krylov matvec (MODE_KRY32 with LaunchCfg::seg)
     uint64_t arcs;
     const uint32_t *seg_mask, *seg_tile_j0, *seg_nz, *seg_empty;
-    float *seg_head, *seg_tail;
+    double *seg_head, *seg_tail;
     const uint4 *seg_span, *seg_span_long;
     uint64_t seg_ntiles;
     uint32_t seg_nempty, seg_nspan, seg_nlong;
