@@ -301,6 +301,13 @@ int32_t prg_autotune(prg_graph *g, int32_t tune_batch, const char *cache_path, p
  * passes gather sources with ids >= value without allocating in L1, so L1
  * keeps the most-gathered prefix; defaults 16384 / 2048, 0 = all allocate),
  * "defaults" (any value: every key back to its default),
+ * "krylov_floor_pct" (Krylov inner solves aim at this percentage of the
+ * certified final threshold, 1-90; default 20), "seg_kry32" (unweighted
+ * graphs: 1 the tile-segmented FP32 Krylov matvec, 0 the row-block kernel),
+ * "seg_hot" (its shared-memory hot prefix on relabelled graphs, entries),
+ * "hot_cache32" / "hot_cache64" (hot prefix of the row-block kernel's FP32 /
+ * FP64 passes), "hot_threads" (256, 512 or 1024: the row-block kernel's block
+ * size when it keeps a hot prefix),
  * "batch_cheb" (batched solver on undirected graphs: 1 Chebyshev steps, the
  * default, 0 plain power steps),
  * "batch_barrier_extra" (failure-detection test hook, 0 or 1: with 1 every

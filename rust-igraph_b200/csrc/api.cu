@@ -1359,6 +1359,9 @@ int32_t prg_set_tuning(const char *key, int64_t value) {
         t.l1_hot32 = (uint32_t)std::min<int64_t>(value, 0xFFFFFFFFll);
     } else if (k == "l1_hot64") {
         t.l1_hot64 = (uint32_t)std::min<int64_t>(value, 0xFFFFFFFFll);
+    } else if (k == "krylov_floor_pct") {
+        if (value < 1 || value > 90) return fail(PRG_ERR_INVALID_ARGUMENT, "krylov_floor_pct must be in [1, 90]");
+        t.krylov_floor = (double)value / 100.0;
     } else if (k == "krylov_rel_e12") {
         t.krylov_rel = (double)value * 1e-12;
     } else if (k == "hot_cache" || k == "hot_cache32" || k == "hot_cache64") {
