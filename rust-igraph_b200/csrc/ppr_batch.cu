@@ -29,10 +29,11 @@
 // (Golub & Varga's recurrence).  For a symmetric interval the iteration
 // converges for every eigenvalue of modulus < 1, so a low estimate of beta
 // only slows it.  The stop test is the reference's: the change a power step
-// makes, ||G(x_k) - x_k||_1 < tol, and the column's answer is that step,
-// G(x_k), kept in F; it lies within d/(1-d) tol of the fixed point, as the
-// reference's answer does.  Directed graphs (complex spectra) always take
-// the plain step.
+// makes, ||G(x_k) - x_k||_1 < tol.  A column freezes only on a plain step,
+// whose iterate is that G(x_k) (one that meets the test on a Chebyshev step
+// takes one plain step more), so its answer lies within d/(1-d) tol of the
+// fixed point, as the reference's answer does.  Directed graphs (complex
+// spectra) always take the plain step.
 //
 // One cooperative persistent launch runs all iterations of a tile.  Phases
 // are separated by a grid barrier whose spin is bounded: if a barrier does
@@ -103,7 +104,6 @@ struct TileArgs {
     const float *seed_w;       // weight of each entry
     float *X[3];        // iterates; X[2] only with Chebyshev steps (x_{k-1})
     float *XT[2];
-    float *F;           // Chebyshev: each active column's last G(x_k), the answer once it freezes
     int cheb;           // 1: Chebyshev semi-iteration (undirected graphs)
     ColState *cs;       // tile_w entries
     double *bpart;      // [gridDim][W][2] per-block (diff, dsum) partials
@@ -248,7 +248,14 @@ __device__ __forceinline__ void reduce_columns(const TileArgs &a, int parity_new
                 s.diff = tx;
                 s.dsum = ty;
                 s.iters += 1u;
-                if (tx < a.tol || s.iters >= a.max_iter) {
+                const bool cheb_step = a.cheb && s.cheb_steps != 0u && s.cheb_steps != kChebOff;
+                if (tx < a.tol && cheb_step && s.iters < a.max_iter) {
+                    // met the test on a Chebyshev step, whose iterate is not
+                    // G(x): one plain step more, and the column freezes on it
+                    s.omega = 0.0;
+                    s.cheb_steps = kChebOff;
+                    s.stall = 0u;
+                } else if (tx < a.tol || s.iters >= a.max_iter) {
                     s.active = 0u;
                     s.final_buf = (uint32_t)parity_new;
                 } else if (a.cheb) {
@@ -399,12 +406,11 @@ __global__ void __launch_bounds__(kBThreads) ppr_tile_kernel(const TileArgs a) {
             const Vec<VEC> old = ldv_cg<VEC>(a.X[xc] + (size_t)v * W + lane * VEC);
             Vec<VEC> prev{};
             if (any_om) prev = ldv_cg<VEC>(a.X[xp] + (size_t)v * W + lane * VEC);
-            Vec<VEC> xn, xtn, gv;
+            Vec<VEC> xn, xtn;
 #pragma unroll
             for (int j = 0; j < VEC; j++) {
                 // personalized_pagerank.rs:169-170 in FP32: g = G(x_k)
                 const float val = (1.0f - d) * r[j] + d * (acc[j] + dsh[j] * r[j]);
-                gv.v[j] = val;
                 // Chebyshev step, or the plain step when om == 0
                 const float step = om[j] != 0.0f ? __fmaf_rn(om[j], val - prev.v[j], prev.v[j]) : val;
                 xn.v[j] = act[j] ? step : old.v[j];
@@ -416,13 +422,6 @@ __global__ void __launch_bounds__(kBThreads) ppr_tile_kernel(const TileArgs a) {
             }
             stv<VEC>(a.X[xn_] + (size_t)v * W + lane * VEC, xn);
             stv<VEC>(a.XT[nxt] + (size_t)v * W + lane * VEC, xtn);
-            if (a.cheb) {
-                // the answer of a column that freezes now: its power step
-                float *f = a.F + (size_t)v * W + lane * VEC;
-#pragma unroll
-                for (int j = 0; j < VEC; j++)
-                    if (act[j]) f[j] = gv.v[j];
-            }
         }
         block_columns<VEC>(a, pd, pds, sh);
         if (!grid_sync(a)) return;
@@ -458,12 +457,14 @@ __global__ void scale_rows(const float *X, float *XT, const float *inv32, uint32
 }
 
 // out[caller_row * K + tile_base + c] = X_final(c)[internal_row][c]
-__global__ void tile_writeback(const float *X0, const float *X1, const ColState *cs, uint32_t n, uint32_t W,
-                               uint32_t tile_w, uint32_t tile_base, uint32_t K, const uint32_t *perm, float *out) {
+__global__ void tile_writeback(const float *X0, const float *X1, const float *X2, const ColState *cs, uint32_t n,
+                               uint32_t W, uint32_t tile_w, uint32_t tile_base, uint32_t K, const uint32_t *perm,
+                               float *out) {
     const size_t total = (size_t)n * tile_w;
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
         const uint32_t v = (uint32_t)(i / tile_w), c = (uint32_t)(i % tile_w);
-        const float *X = cs[c].final_buf ? X1 : X0;
+        const uint32_t fb = cs[c].final_buf;
+        const float *X = fb == 2u ? X2 : fb == 1u ? X1 : X0;
         const uint32_t ov = perm ? perm[v] : v;
         out[(size_t)ov * K + tile_base + c] = X[(size_t)v * W + c];
     }
@@ -534,16 +535,15 @@ int ppr_batch(const DeviceGraph &g, uint32_t K, const uint64_t *seed_offsets, co
     PRG_CUDA(cudaMemcpyAsync(sptr, hptr.data(), ((size_t)n + 1) * 4, cudaMemcpyHostToDevice, s));
     uint32_t *kk = ev;
 
-    // tile buffers (Chebyshev steps need a third iterate and the answers F)
+    // tile buffers (Chebyshev steps need a third iterate)
     const bool cheb = !g.directed && tuning().batch_cheb != 0;
-    float *X[3] = {nullptr, nullptr, nullptr}, *XT[2], *F = nullptr;
+    float *X[3] = {nullptr, nullptr, nullptr}, *XT[2];
     for (int i = 0; i < 2; i++) {
         A((void **)&X[i], (size_t)n * W * 4);
         A((void **)&XT[i], (size_t)n * W * 4);
     }
     if (cheb) {
         A((void **)&X[2], (size_t)n * W * 4);
-        A((void **)&F, (size_t)n * W * 4);
     }
     const int grid = vec == 4 ? tile_grid<4>() : vec == 2 ? tile_grid<2>() : tile_grid<1>();
     ColState *cs = nullptr;
@@ -591,7 +591,6 @@ int ppr_batch(const DeviceGraph &g, uint32_t K, const uint64_t *seed_offsets, co
         a.X[2] = X[2];
         a.XT[0] = XT[0];
         a.XT[1] = XT[1];
-        a.F = F;
         a.cheb = cheb ? 1 : 0;
         a.cs = cs;
         a.bpart = bpart;
@@ -603,8 +602,7 @@ int ppr_batch(const DeviceGraph &g, uint32_t K, const uint64_t *seed_offsets, co
         if (vec == 4) run_tile<4>(a, grid, s);
         else if (vec == 2) run_tile<2>(a, grid, s);
         else run_tile<1>(a, grid, s);
-        if (cheb) tile_writeback<<<148 * 8, 256, 0, s>>>(F, F, cs, n, W, tw, tb, K, g.perm, d_out);
-        else tile_writeback<<<148 * 8, 256, 0, s>>>(X[0], X[1], cs, n, W, tw, tb, K, g.perm, d_out);
+        tile_writeback<<<148 * 8, 256, 0, s>>>(X[0], X[1], X[2], cs, n, W, tw, tb, K, g.perm, d_out);
         PRG_CUDA(cudaGetLastError());
         int32_t hs = 0;
         PRG_CUDA(cudaMemcpyAsync(&hs, status, 4, cudaMemcpyDeviceToHost, s));
@@ -631,7 +629,7 @@ int ppr_batch(const DeviceGraph &g, uint32_t K, const uint64_t *seed_offsets, co
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     for (void *p : {(void *)ev, (void *)ews, (void *)ecs, (void *)sptr, (void *)X[0], (void *)X[1], (void *)X[2],
-                    (void *)F, (void *)XT[0], (void *)XT[1], (void *)cs, (void *)bpart, (void *)bar, (void *)status})
+                    (void *)XT[0], (void *)XT[1], (void *)cs, (void *)bpart, (void *)bar, (void *)status})
         if (p) cudaFreeAsync(p, s);
     PRG_CUDA(cudaStreamSynchronize(s));
     return rc;
