@@ -405,7 +405,8 @@ def main():
     traffic = tr["kry32_traffic_per_alg_byte"] * bytes_launch if "kry32_traffic_per_alg_byte" in tr else None
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak if achieved else None, "traffic": traffic, "peak_source": peak_src,
-                "kernel": "iter_kernel<MODE_KRY32> (FP32 Krylov matvec y = A p with fused dot products)",
+                "kernel": "FP32 Krylov matvec y = A p with fused dot products: kry32_seg_kernel + kry32_seg_finish "
+                          "(tile-segmented pass, segspmv.cu) on unweighted graphs",
                 "bytes_per_launch": bytes_launch, "avg_launch_us": avg_launch_s * 1e6, "launches_timed": mv_n}
     # the same index stream gathered once per arc and nothing else: the floor
     # this access pattern sets (L1 wavefronts of random gathers), measured live

@@ -308,8 +308,8 @@ int32_t prg_autotune(prg_graph *g, int32_t tune_batch, const char *cache_path, p
  * "hot_cache32" / "hot_cache64" (hot prefix of the row-block kernel's FP32 /
  * FP64 passes), "hot_threads" (256, 512 or 1024: the row-block kernel's block
  * size when it keeps a hot prefix),
- * "batch_cheb" (batched solver on undirected graphs: 1 Chebyshev steps, the
- * default, 0 plain power steps),
+ * "batch_cheb" (batched solver on undirected graphs: 1 Chebyshev steps, 0
+ * plain power steps, the default),
  * "batch_barrier_extra" (failure-detection test hook, 0 or 1: with 1 every
  * grid barrier of the batched solver waits for an arrival that never comes,
  * so its bounded wait (about 1.5 s) expires and the call returns
@@ -335,10 +335,11 @@ typedef struct prg_batch_stats {
  * with seeds_k = seeds[seed_offsets[k] .. seed_offsets[k+1]) in caller ids,
  * stopped per column when its successive L1 change is < tol (the column then
  * freezes while the others continue) or after max_iter iterations.  On an
- * undirected graph (real spectrum) the iterates between those tests are
- * Chebyshev steps over an interval each column estimates from the settled
- * contraction ratio of its first power steps (tuning key "batch_cheb" = 0
- * turns them off): the test is still the change one power step makes,
+ * undirected graph (real spectrum) and with tuning key "batch_cheb" = 1, the
+ * iterates between those tests are Chebyshev steps over an interval each
+ * column estimates from the settled contraction ratio of its first power
+ * steps (default 0: plain steps throughout): the test is still the change
+ * one power step makes,
  * ||G(x) - x||_1 < tol, and the column returns that step, G(x), as the
  * reference does; only the sequence of iterates before it is shorter.  FP32
  * rounding puts a floor of about n ulp under that change, so a Chebyshev
@@ -346,7 +347,7 @@ typedef struct prg_batch_stats {
  * those stop falling within 10 x tol (a rounding cycle at the floor) it
  * freezes there, its answer within d/(1-d) of that change of the fixed
  * point.
- * tile_vec: columns per tile = 32 * tile_vec (1, 2 or 4; 0 = autotuned or 1).
+ * tile_vec: columns per tile = 32 * tile_vec (1, 2 or 4; 0 = autotuned or 2).
  * out: host float[n * K], out[v * K + k].  column_iters: optional host
  * uint32[K].  Validation follows _vs: empty seed list or vertex >= n ->
  * PRG_ERR_INVALID_ARGUMENT; a device barrier that times out -> PRG_ERR_TIMEOUT. */

@@ -88,11 +88,11 @@ struct Tuning {
     uint32_t seg_hot = 40960;    // its shared-memory hot prefix on relabelled graphs (entries)
     uint32_t l1_hot32 = 16384, l1_hot64 = 2048;
     double refine_switch = 5e-7;
-    uint32_t batch_vec = 1;
+    uint32_t batch_vec = 2;
     double krylov_rel = 1e-4;
     double krylov_floor = 0.2;         // refined / Krylov inner solves aim at this fraction of the final threshold
     uint32_t batch_barrier_extra = 0;  // test hook: batched grid barriers wait for arrivals that never come
-    uint32_t batch_cheb = 1;           // batched solver on undirected graphs: 1 Chebyshev steps, 0 plain steps
+    uint32_t batch_cheb = 0;           // batched solver on undirected graphs: 1 Chebyshev steps, 0 plain steps
 };
 Tuning &tuning();
 

@@ -17,9 +17,12 @@
 // destination row at a time.  Reset vectors are sparse: a per-vertex seed
 // list (vertex-sorted CSR of (column, weight) entries).
 //
-// Undirected graphs (by default) take Chebyshev semi-iteration in place of
-// the plain step.  The iteration x -> G(x) = d P^T(x/s) + d (dangling mass)
-// r + (1-d) r has a real spectrum in [-d, d] there: P = D^-1 A is similar to
+// Undirected graphs can take Chebyshev semi-iteration in place of the plain
+// step (tuning batch_cheb = 1; plain steps by default, because a tile runs
+// until its slowest column freezes and a Chebyshev step reads one more
+// iterate, so the fewer column-iterations did not shorten the batch).  The
+// iteration x -> G(x) = d P^T(x/s) + d (dangling mass) r + (1-d) r has a real
+// spectrum in [-d, d] there: P = D^-1 A is similar to
 // the symmetric D^-1/2 A D^-1/2, and the dangling term only adds a block
 // that is triangular to it.  Once the column's own contraction ratio
 // (successive changes of its plain steps) has settled, it gives an interval

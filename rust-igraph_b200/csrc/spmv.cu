@@ -657,43 +657,70 @@ void launch_iteration(int mode, bool weighted, const IterArgs &a_in, const Launc
 
 // ------------------------------------------------------------------ gather probe
 
-// Diagnostic: the FP32 matvec's loads and nothing else.  Consecutive threads
-// stream consecutive 16-byte quads of col (evict-first, as the iteration
-// kernel does) and gather x at each source with the same L1 policy (ids >=
-// l1hot bypass L1); the sums go to out so nothing is optimised away.  No row
-// structure, staging, reduction or epilogue: the time is a floor for any pass
-// that reads this index stream and gathers once per arc.
-__global__ void __launch_bounds__(kThreads) gather_probe_kernel(const uint32_t *col, uint64_t arcs, const float *x,
-                                                                uint32_t l1hot, float *out) {
+// Diagnostic: the FP32 matvec's gathers and nothing else, in the fastest
+// arrangement measured for this access pattern: one 1024-thread block per SM,
+// each thread streaming two 16-byte quads of col per step (grid-stride, so
+// neighbouring warps read neighbouring quads, evict-first) and gathering
+// their sources, with the first `hot` entries of x (degree-sorted graphs) in
+// shared memory and the other ids >= l1hot gathered without L1 allocation.
+// The sums go to out so nothing is optimised away.  No row structure, scan,
+// reduction or epilogue: the time is a floor for any pass that reads this
+// index stream and gathers once per arc.
+constexpr int kProbeNT = 1024;
+constexpr uint32_t kProbeHot = 49152;
+
+__global__ void __launch_bounds__(kProbeNT, 1) gather_probe_kernel(const uint32_t *col, uint64_t arcs, const float *x,
+                                                                   uint32_t hot, uint32_t l1hot, float *out) {
+    extern __shared__ __align__(16) float s_hot[];
+    for (uint32_t i = threadIdx.x * 4; i < hot; i += kProbeNT * 4)
+        *reinterpret_cast<uint4 *>(s_hot + i) = __ldcg(reinterpret_cast<const uint4 *>(x + i));
+    __syncthreads();
     const uint64_t nq = (arcs + 3) >> 2;  // col carries kColPad slots past the last arc
     const uint64_t pol_g = policy_evict_last();
+    const uint64_t stride = (uint64_t)gridDim.x * kProbeNT;
     float acc = 0.f;
-    for (uint64_t q = (uint64_t)blockIdx.x * kThreads + threadIdx.x; q < nq; q += (uint64_t)gridDim.x * kThreads) {
-        const uint4 c = ld_stream_u4(reinterpret_cast<const uint4 *>(col) + q, policy_evict_first());
-        auto g = [&](uint32_t v, uint64_t p) {
-            return p < arcs ? (v < l1hot ? ld_gather(x + v, pol_g) : ld_gather_na(x + v, pol_g)) : 0.f;
-        };
-        acc += (g(c.x, 4 * q) + g(c.y, 4 * q + 1)) + (g(c.z, 4 * q + 2) + g(c.w, 4 * q + 3));
+    auto g = [&](uint32_t v, uint64_t p) -> float {
+        if (p >= arcs) return 0.f;
+        if (v < hot) return s_hot[v];
+        return v < l1hot ? ld_gather(x + v, pol_g) : ld_gather_na(x + v, pol_g);
+    };
+    for (uint64_t q0 = (uint64_t)blockIdx.x * kProbeNT + threadIdx.x; q0 < nq; q0 += 2 * stride) {
+        uint4 c[2];
+#pragma unroll
+        for (int u = 0; u < 2; u++) {
+            const uint64_t q = q0 + u * stride;
+            c[u] = q < nq ? ld_stream_u4(reinterpret_cast<const uint4 *>(col) + q, policy_evict_first())
+                          : make_uint4(0u, 0u, 0u, 0u);
+        }
+#pragma unroll
+        for (int u = 0; u < 2; u++) {
+            const uint64_t q = q0 + u * stride;
+            const uint64_t p = q < nq ? 4 * q : arcs;
+            acc += (g(c[u].x, p) + g(c[u].y, p + 1)) + (g(c[u].z, p + 2) + g(c[u].w, p + 3));
+        }
     }
-    out[(uint64_t)blockIdx.x * kThreads + threadIdx.x] = acc;
+    out[(uint64_t)blockIdx.x * kProbeNT + threadIdx.x] = acc;
 }
 
 float gather_probe(const DeviceGraph &g, int reps, cudaStream_t s) {
     int dev = 0, sms = 0;
     PRG_CUDA(cudaGetDevice(&dev));
     PRG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    const unsigned grid = (unsigned)sms * 8u;  // 2048 resident threads per SM
+    const unsigned grid = (unsigned)sms;
     float *x = nullptr, *out = nullptr;
-    PRG_CUDA(cudaMallocAsync((void **)&x, std::max<uint64_t>(g.n, 1) * 4, s));
-    PRG_CUDA(cudaMallocAsync((void **)&out, (uint64_t)grid * kThreads * 4, s));
-    PRG_CUDA(cudaMemsetAsync(x, 0, std::max<uint64_t>(g.n, 1) * 4, s));
+    PRG_CUDA(cudaMallocAsync((void **)&x, std::max<uint64_t>(g.n, 4) * 4, s));
+    PRG_CUDA(cudaMallocAsync((void **)&out, (uint64_t)grid * kProbeNT * 4, s));
+    PRG_CUDA(cudaMemsetAsync(x, 0, std::max<uint64_t>(g.n, 4) * 4, s));
     const uint32_t l1hot = g.perm != nullptr && g.l1_hot32 ? g.l1_hot32 : 0xFFFFFFFFu;
+    const uint32_t hot = g.perm != nullptr ? std::min<uint32_t>(kProbeHot, g.n) & ~3u : 0u;
+    const size_t smem = (size_t)hot * 4;
+    PRG_CUDA(cudaFuncSetAttribute(gather_probe_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     cudaEvent_t e0, e1;
     PRG_CUDA(cudaEventCreate(&e0));
     PRG_CUDA(cudaEventCreate(&e1));
-    gather_probe_kernel<<<grid, kThreads, 0, s>>>(g.col, g.arcs, x, l1hot, out);  // warm-up
+    gather_probe_kernel<<<grid, kProbeNT, smem, s>>>(g.col, g.arcs, x, hot, l1hot, out);  // warm-up
     PRG_CUDA(cudaEventRecord(e0, s));
-    for (int r = 0; r < reps; r++) gather_probe_kernel<<<grid, kThreads, 0, s>>>(g.col, g.arcs, x, l1hot, out);
+    for (int r = 0; r < reps; r++) gather_probe_kernel<<<grid, kProbeNT, smem, s>>>(g.col, g.arcs, x, hot, l1hot, out);
     PRG_CUDA(cudaEventRecord(e1, s));
     PRG_CUDA(cudaGetLastError());
     PRG_CUDA(cudaEventSynchronize(e1));

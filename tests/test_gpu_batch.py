@@ -55,8 +55,8 @@ def test_batch_matches_oracle_sbm(cuda_ok, vec):
 
 
 def test_chebyshev_steps_on_undirected_graphs(cuda_ok):
-    # Undirected graphs take Chebyshev steps between the reference's stop
-    # tests (batch_cheb = 1, the default); batch_cheb = 0 gives the plain
+    # With batch_cheb = 1, undirected graphs take Chebyshev steps between the
+    # reference's stop tests; batch_cheb = 0 (the default) gives the plain
     # power steps.  Both meet the oracle on every column, the Chebyshev
     # columns in fewer iterations, and directed graphs never take them.
     blocks, bs = 32, 1500
@@ -84,8 +84,12 @@ def test_chebyshev_steps_on_undirected_graphs(cuda_ok):
     print({"chebyshev_column_iterations": int(it_cheb.sum()), "plain_column_iterations": int(it_plain.sum())})
     assert it_cheb.sum() < 0.8 * it_plain.sum(), (it_cheb.sum(), it_plain.sum())
     ff, tt = O.erdos_renyi_gnm(3000, 20_000, True, False, 4)
-    with ig.DeviceGraph.from_host(3000, ff, tt, True) as dg:
-        _, _, st = dg.ppr_batch([np.array([1, 2], np.uint32)], 0.85, TOL_COL, 1000)
+    ig.set_tuning("batch_cheb", 1)
+    try:
+        with ig.DeviceGraph.from_host(3000, ff, tt, True) as dg:
+            _, _, st = dg.ppr_batch([np.array([1, 2], np.uint32)], 0.85, TOL_COL, 1000)
+    finally:
+        ig.reset_tuning()
     assert not st["chebyshev"]
 
 
