@@ -302,7 +302,13 @@ void preload_gather_f64() {
 // that are gathered most often are those with the largest out-degree; giving
 // them the smallest internal ids packs the hot part of the rank vector into a
 // few cache lines (L1/L2 hits instead of one sector per arc).  The order is
-// out-degree descending, ties by caller id (stable sort).
+// out-degree descending; on directed graphs, among vertices of one
+// out-degree, those with in-arcs before those without; then caller id
+// (stable sort).  The second key keeps the rows without arcs (most of them
+// on power-law graphs are also vertices without out-arcs) in one run at the
+// end instead of interleaved with rows that have arcs, so that a pass that
+// treats the two kinds separately reads each 32-byte sector of a vertex
+// array once.
 
 __global__ void max_u32_kernel(const uint32_t *a, uint32_t n, uint32_t *out) {
     uint32_t mx = 0;
@@ -312,11 +318,26 @@ __global__ void max_u32_kernel(const uint32_t *a, uint32_t n, uint32_t *out) {
     if ((threadIdx.x & 31) == 0) atomicMax(out, mx);
 }
 
-__global__ void relabel_keys(const uint32_t *deg, uint32_t n, uint32_t maxdeg, uint32_t *key, uint32_t *val) {
+// noin: 1 for a vertex without in-arcs (null: no second key)
+__global__ void relabel_keys(const uint32_t *deg, const uint8_t *noin, uint32_t n, uint32_t maxdeg, uint32_t *key,
+                             uint32_t *val) {
     for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
-        key[v] = maxdeg - deg[v];
+        key[v] = noin ? ((maxdeg - deg[v]) << 1) | noin[v] : maxdeg - deg[v];
         val[v] = v;
     }
+}
+
+// noin[v] = 0 for every arc head v (noin starts as all ones)
+__global__ void mark_heads(const uint32_t *to, uint64_t m, uint32_t n, uint8_t *noin) {
+    for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e < m; e += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t v = to[e];
+        if (v < n) noin[v] = 0;
+    }
+}
+
+__global__ void mark_empty_rows(const uint32_t *cnt, uint32_t n, uint8_t *noin) {
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x)
+        noin[v] = cnt[v] == 0u ? 1 : 0;
 }
 
 __global__ void relabel_finish(const uint32_t *perm, const uint32_t *deg_old, uint32_t n, uint32_t *iperm,
@@ -578,8 +599,11 @@ static void finish_graph(DeviceGraph &g, double *&strength, cudaStream_t s) {
 // Degree-sorted relabelling of the vertices when g.relabel asks for it (1) or
 // the degree distribution is skewed (2: max degree >= 32 x mean, n >= 4096):
 // g.perm (new -> old), g.iperm (old -> new) and g.deg in new ids.  Needs
-// g.deg (out-degree) and g.arcs.  Returns whether it relabelled.
-static bool relabel_vertices(DeviceGraph &g, cudaStream_t s) {
+// g.deg (out-degree) and g.arcs; on directed graphs either the arc heads
+// (to, m) or the in-degrees in caller ids (in_cnt).  Returns whether it
+// relabelled.
+static bool relabel_vertices(DeviceGraph &g, cudaStream_t s, const uint32_t *to, uint64_t m,
+                             const uint32_t *in_cnt = nullptr) {
     const uint32_t n = g.n;
     if (n < 2 || g.relabel == 0) return false;
     const unsigned gn = grid_for(n, kThreads);
@@ -594,8 +618,20 @@ static bool relabel_vertices(DeviceGraph &g, cudaStream_t s) {
     if (g.relabel != 1 && !skewed) return false;
     uint32_t *pk = dalloc<uint32_t>(n, s), *pv = dalloc<uint32_t>(n, s);
     uint32_t *pk1 = dalloc<uint32_t>(n, s), *pv1 = dalloc<uint32_t>(n, s);
-    relabel_keys<<<gn, kThreads, 0, s>>>(g.deg, n, maxdeg, pk, pv);
-    radix_sort_pairs(&pk, &pv, &pk1, &pv1, n, bits_for(maxdeg), s);
+    // second key: directed graphs whose doubled key fits 32 bits
+    uint8_t *noin = nullptr;
+    if (g.directed && bits_for(maxdeg) < 32 && (in_cnt || to)) {
+        noin = dalloc<uint8_t>(n, s);
+        if (in_cnt) {
+            mark_empty_rows<<<gn, kThreads, 0, s>>>(in_cnt, n, noin);
+        } else {
+            PRG_CUDA(cudaMemsetAsync(noin, 1, n, s));
+            if (m) mark_heads<<<grid_for(m, kThreads), kThreads, 0, s>>>(to, m, n, noin);
+        }
+    }
+    relabel_keys<<<gn, kThreads, 0, s>>>(g.deg, noin, n, maxdeg, pk, pv);
+    radix_sort_pairs(&pk, &pv, &pk1, &pv1, n, bits_for(maxdeg) + (noin ? 1 : 0), s);
+    dfree(noin, s);
     PRG_CUDA(cudaMallocAsync((void **)&g.perm, (uint64_t)n * 4, s));
     PRG_CUDA(cudaMallocAsync((void **)&g.iperm, (uint64_t)n * 4, s));
     PRG_CUDA(cudaMemcpyAsync(g.perm, pv, (uint64_t)n * 4, cudaMemcpyDeviceToDevice, s));
@@ -632,7 +668,7 @@ void build_graph(DeviceGraph &g, const uint32_t *d_from, const uint32_t *d_to, c
     // is built from becomes (ef, et)
     const uint32_t *ef = d_from, *et = d_to;
     uint32_t *rf = nullptr, *rt = nullptr;
-    if (relabel_vertices(g, s)) {
+    if (relabel_vertices(g, s, d_to, m)) {
         rf = dalloc<uint32_t>(m, s);
         rt = dalloc<uint32_t>(m, s);
         if (m) relabel_edges<<<ge, kThreads, 0, s>>>(d_from, d_to, m, g.iperm, rf, rt);
@@ -884,7 +920,7 @@ bool build_graph_host(DeviceGraph &g, const uint32_t *h_from, const uint32_t *h_
     }
 
     const unsigned gn = grid_for(n, kThreads), ga = grid_for(arcs, kThreads);
-    const bool relabelled = relabel_vertices(g, s);
+    const bool relabelled = relabel_vertices(g, s, nullptr, 0, cnt);
     if (trace) PRG_CUDA(cudaEventRecord(t_tail[0], s));
     uint32_t *rows = cnt;
     if (relabelled) {

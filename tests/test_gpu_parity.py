@@ -267,6 +267,47 @@ def test_rmat_auto_relabel(cuda_ok):
     assert maxabs(x, O.pagerank(n, f, t, True)) <= PARITY
 
 
+@pytest.mark.parametrize("directed", [True, False])
+def test_relabel_order(cuda_ok, directed):
+    # internal ids: out-degree descending; on directed graphs vertices with
+    # in-arcs before those without at equal out-degree; then caller id
+    import ctypes as C
+    import torch
+
+    scale = 14
+    n = 1 << scale
+    f, t = O.rmat(scale, 16 * n, seed=5)
+    fa, ta = np.asarray(f, np.int64), np.asarray(t, np.int64)
+    if directed:
+        od, noin = np.bincount(fa, minlength=n), np.bincount(ta, minlength=n) == 0
+    else:
+        od = np.bincount(fa, minlength=n) + np.bincount(ta, minlength=n)
+        noin = np.zeros(n, bool)
+    want = np.lexsort((np.arange(n), noin, -od))
+    ig.set_tuning("relabel", 1)
+    try:
+        with ig.DeviceGraph.from_host(n, f, t, directed) as dg:
+            assert dg.relabelled
+            rp, col, perm, inv = C.c_void_p(), C.c_void_p(), C.c_void_p(), C.c_void_p()
+            L = ig.lib()
+            L.prg_graph_device_csr.restype = C.c_int32
+            L.prg_graph_device_csr.argtypes = [C.c_void_p] + [C.POINTER(C.c_void_p)] * 4
+            assert L.prg_graph_device_csr(dg._h, C.byref(rp), C.byref(col), C.byref(perm), C.byref(inv)) == 0
+
+            class _View:
+                __cuda_array_interface__ = {"shape": (n,), "typestr": "<i4", "data": (perm.value, False), "version": 3}
+
+            got = torch.as_tensor(_View(), device="cuda").cpu().numpy()
+            x, _ = dg.solve(ig.Options())
+    finally:
+        ig.reset_tuning()
+    assert np.array_equal(got, want)
+    if directed:  # the rows without arcs form one run at the end of each out-degree class
+        e = noin[got]
+        assert e[np.flatnonzero(od[got] == 0)].tolist() == sorted(e[np.flatnonzero(od[got] == 0)].tolist())
+    assert maxabs(x, O.pagerank(n, f, t, directed)) <= PARITY
+
+
 def test_shared_memory_hot_prefix_keeps_parity(cuda_ok):
     # the optional per-block shared-memory copy of the hot prefix changes where
     # gathers read from, never what they read
