@@ -58,7 +58,40 @@ def parse():
     p.add_argument("--cpu-iters", type=int, default=2)
     p.add_argument("--no-autotune", action="store_true")
     p.add_argument("--no-warm", action="store_true")
+    p.add_argument("--profile-case", action="store_true",
+                   help="build the R-MAT graph of --scale, run one FP32-refined solve and exit: the command the "
+                        "kernel captures under profiles/ run")
+    p.add_argument("--tuning", action="append", default=[], metavar="KEY=VALUE",
+                   help="with --profile-case: a tuning key to set before the graph is built (repeatable)")
     return p.parse_args()
+
+
+def run_profile_case(args):
+    """One refined solve on the bench's R-MAT at --scale (edge arrays freed
+    before it), for ncu captures of single kernels on a small case."""
+    import torch
+
+    import igraph_b200 as ig
+
+    for kv in args.tuning:
+        k, v = kv.split("=", 1)
+        ig.set_tuning(k, int(v))
+    n, m = 1 << args.scale, args.edge_factor << args.scale
+    df = torch.empty(m, dtype=torch.int32, device="cuda")
+    dt = torch.empty(m, dtype=torch.int32, device="cuda")
+    ig.rmat_device(args.scale, m, df.data_ptr(), dt.data_ptr(), *RMAT, seed=SEED)
+    torch.cuda.synchronize()
+    dg = ig.DeviceGraph.from_device(n, m, df.data_ptr(), dt.data_ptr(), True)
+    del df, dt
+    torch.cuda.empty_cache()
+    out = torch.empty(n, dtype=torch.float64, device="cuda")
+    st = dg.solve_device(out.data_ptr(), ig.Options(precision=ig.PRECISION_FP32_REFINED, eps=EPS, damping=D))
+    print(json.dumps({"profile_case": {"scale": args.scale, "tuning": args.tuning, "passes": st.iterations,
+                                       "fp32_matvecs": st.fp32_passes, "solve_ms": st.solve_ms,
+                                       "matvec_us": st.spmv_ms / max(st.spmv_launches, 1) * 1e3,
+                                       "error_bound": st.error_bound,
+                                       "device_gb": torch.cuda.max_memory_allocated() / 1e9}}), flush=True)
+    dg.close()
 
 
 def dist_env():
@@ -247,6 +280,9 @@ def load_traffic():
 
 def main():
     args = parse()
+    if args.profile_case:
+        run_profile_case(args)
+        return
     if args.impl == "reference":
         run_reference(args)
         return

@@ -241,6 +241,20 @@ int32_t prg_graph_device_csr(const prg_graph *g, const uint32_t **row_ptr, const
  * once per arc; bench.py reports the matvec against it. */
 int32_t prg_graph_gather_probe(prg_graph *g, int32_t reps, double *ms_per_pass);
 
+/* Diagnostic with no counterpart in the reference: one FP32 Krylov matvec
+ * y = p - d (A pt + dz / n), the operator the refined and FP32 Krylov solves
+ * apply, on the graph's INTERNAL ids (prg_graph_device_csr gives the CSR
+ * and numbering).  A sums pt over each row's in-arcs; pt is p scaled by
+ * 1/out-degree (inv32) and dz the dangling mass of p, both the caller's.
+ * kernel: 0 the row-block pass, 1 the tile-segmented pass with 4-arc lane
+ * quads, 2 the tile-segmented pass with 8 consecutive arcs per lane (1 and 2
+ * need an unweighted graph).  dots (3 doubles, optional) = (p.y, y.p, y.y)
+ * as the kernel's block records sum them; ms (optional) = its device time.
+ * Device pointers, n entries each.  Tests compare the three kernels with an
+ * FP64 restatement through it. */
+int32_t prg_graph_matvec32(prg_graph *g, int32_t kernel, const float *d_p, const float *d_pt, double dz,
+                           double damping, float *d_y, double *dots, double *ms);
+
 /* ---- learned warm start --------------------------------------------------- */
 /* A two-layer message-passing network (hidden 32, 8-channel messages scaled
  * by 1/out-degree, BF16 weights, FP32 accumulation on the tensor cores) that

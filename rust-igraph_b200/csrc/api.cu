@@ -1049,6 +1049,26 @@ int32_t prg_graph_gather_probe(prg_graph *h, int32_t reps, double *ms_per_pass) 
     PRG_GUARD_END
 }
 
+int32_t prg_graph_matvec32(prg_graph *h, int32_t kernel, const float *d_p, const float *d_pt, double dz,
+                           double damping, float *d_y, double *dots, double *ms) {
+    g_err.clear();
+    PRG_GUARD_BEGIN
+    if (!h) return fail(PRG_ERR_INVALID_ARGUMENT, "null graph handle");
+    if (kernel < 0 || kernel > 2) return fail(PRG_ERR_INVALID_ARGUMENT, "kernel must be 0, 1 or 2");
+    if (kernel != 0 && h->g.weighted)
+        return fail(PRG_ERR_UNSUPPORTED, "the tile-segmented matvec serves unweighted graphs");
+    if (!(damping >= 0.0 && damping <= 1.0)) return fail(PRG_ERR_INVALID_ARGUMENT, "damping must be in [0, 1]");
+    if (h->g.n == 0 || h->g.arcs == 0) return fail(PRG_ERR_INVALID_ARGUMENT, "the graph has no arcs");
+    if (!d_p || !d_pt || !d_y) return fail(PRG_ERR_INVALID_ARGUMENT, "null vector");
+    double d[3];
+    float t = 0.f;
+    prg::matvec32_probe(h->g, h->ws, kernel, d_p, d_pt, dz, damping, d_y, d, &t, h->stream);
+    if (dots) std::memcpy(dots, d, sizeof(d));
+    if (ms) *ms = (double)t;
+    return PRG_OK;
+    PRG_GUARD_END
+}
+
 int32_t prg_solve(prg_graph *h, const prg_options *opt, const double *reset, double *out, prg_stats *st) {
     g_err.clear();
     PRG_GUARD_BEGIN
@@ -1369,7 +1389,7 @@ int32_t prg_set_tuning(const char *key, int64_t value) {
         if (k != "hot_cache64") t.hot_cache = (uint32_t)value;
         if (k != "hot_cache32") t.hot_cache64 = (uint32_t)value;
     } else if (k == "seg_kry32") {
-        if (value > 1) return fail(PRG_ERR_INVALID_ARGUMENT, "seg_kry32 must be 0 or 1");
+        if (value > 2) return fail(PRG_ERR_INVALID_ARGUMENT, "seg_kry32 must be 0, 1 or 2");
         t.seg_kry32 = (uint32_t)value;
     } else if (k == "seg_hot") {
         if (value > 49152) return fail(PRG_ERR_INVALID_ARGUMENT, "seg_hot must be at most 49152 entries");

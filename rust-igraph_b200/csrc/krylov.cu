@@ -794,4 +794,62 @@ void solve_krylov(const DeviceGraph &g, Workspace &ws, const SolveOpts &o, const
     st.error_bound = st.residual_l1 * o.damping / (1.0 - o.damping);
 }
 
+// One FP32 Krylov matvec y = p - d (A pt + dz t), t = 1/n, through the
+// row-block kernel (kernel 0) or a tile-segmented one (1, 2), with rh = p:
+// dots = the launch's summed records (p.y, y.p, y.y) in record order, ms =
+// its device time.  A diagnostic: its inputs live in internal ids.
+void matvec32_probe(const DeviceGraph &g, Workspace &ws, int kernel, const float *p, const float *pt, double dz,
+                    double damping, float *y, double dots[3], float *ms, cudaStream_t s) {
+    workspace_ensure(ws, g, s);
+    LaunchCfg c;
+    if (kernel == 0) {
+        c = iteration_config(MODE_KRY32, g.weighted, g.perm != nullptr ? g.hot_cache : 0u, g.blocks_per_sm, g.n,
+                             g.hot_threads);
+        c.hub_recs = g.nhub;
+    } else {
+        if (ws.seg.mask == nullptr) seg_build(g, ws.seg, s);
+        c = seg_config(g, g.perm != nullptr ? g.seg_hot : 0u, kernel);
+    }
+    if (g.perm != nullptr && g.l1_hot32) c.l1hot = g.l1_hot32;
+    IterArgs a = base_args(g, ws, damping);
+    a.x32_in = p;
+    a.xt32_in = pt;
+    a.x32_out = y;
+    a.rh32 = p;
+    // [kdone][record in][records out]
+    const uint32_t nrec = c.grid;
+    double4 *buf = nullptr;
+    PRG_CUDA(cudaMallocAsync((void **)&buf, (2 + (uint64_t)nrec) * sizeof(double4), s));
+    PRG_CUDA(cudaMemsetAsync(buf, 0, (2 + (uint64_t)nrec) * sizeof(double4), s));
+    const double4 rin = make_double4(dz, 0.0, 0.0, 0.0);
+    PRG_CUDA(cudaMemcpyAsync(buf + 1, &rin, sizeof(double4), cudaMemcpyHostToDevice, s));
+    a.kdone = reinterpret_cast<const int32_t *>(buf);
+    a.kpart_in = buf + 1;
+    a.kpart_n = 1;
+    a.kpart_out = buf + 2;
+    a.ktol = nullptr;
+    PRG_CUDA(cudaEventRecord(ws.eva, s));
+    launch_iteration(MODE_KRY32, g.weighted, a, c, s);
+    PRG_CUDA(cudaEventRecord(ws.evb, s));
+    std::vector<double4> rec(nrec), hub(c.hub_recs);
+    PRG_CUDA(cudaMemcpyAsync(rec.data(), buf + 2, (uint64_t)nrec * sizeof(double4), cudaMemcpyDeviceToHost, s));
+    if (c.hub_recs)
+        PRG_CUDA(cudaMemcpyAsync(hub.data(), ws.hub_rec, (uint64_t)c.hub_recs * sizeof(double4),
+                                 cudaMemcpyDeviceToHost, s));
+    PRG_CUDA(cudaStreamSynchronize(s));
+    PRG_CUDA(cudaEventElapsedTime(ms, ws.eva, ws.evb));
+    cudaFreeAsync(buf, s);
+    dots[0] = dots[1] = dots[2] = 0.0;
+    for (const double4 &q : rec) {
+        dots[0] += q.x;
+        dots[1] += q.y;
+        dots[2] += q.z;
+    }
+    for (const double4 &q : hub) {
+        dots[0] += q.x;
+        dots[1] += q.y;
+        dots[2] += q.z;
+    }
+}
+
 }  // namespace prg

@@ -105,6 +105,27 @@ __global__ void seg_span_fill_kernel(const uint32_t *rp, const uint32_t *tile_j0
     }
 }
 
+// Per-tile record of the 8-arcs-per-lane kernel: {tile_j0, the running
+// row-end counts before mask words 0-3 and 4-7 as bytes, row ends in the
+// tile | 1 << 31 when its first row end closes a row begun in an earlier
+// tile}.
+__global__ void seg_meta_kernel(const uint32_t *mask, const uint32_t *tile_j0, const uint32_t *rp,
+                                const uint32_t *nz, uint64_t ntiles, uint4 *meta) {
+    for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < ntiles;
+         t += (uint64_t)gridDim.x * blockDim.x) {
+        uint32_t lo = 0, hi = 0, c = 0;
+#pragma unroll
+        for (int w = 0; w < (int)(kSegTile / 32); w++) {
+            if (w < 4) lo |= c << (8 * w);
+            else hi |= c << (8 * (w - 4));
+            c += __popc(mask[t * (kSegTile / 32) + w]);
+        }
+        const uint32_t j = tile_j0[t];
+        const uint32_t began = c != 0u && (uint64_t)rp[nz[j]] < t * kSegTile ? 1u : 0u;
+        meta[t] = make_uint4(j, lo, hi, c | began << 31);
+    }
+}
+
 template <class T>
 static T *salloc(uint64_t count, cudaStream_t s) {
     T *p = nullptr;
@@ -113,7 +134,7 @@ static T *salloc(uint64_t count, cudaStream_t s) {
 }
 
 void seg_free(SegIndex &x, cudaStream_t s) {
-    for (void *p : {(void *)x.mask, (void *)x.tile_j0, (void *)x.nz_row, (void *)x.empty_row, (void *)x.head,
+    for (void *p : {(void *)x.mask, (void *)x.tile_j0, (void *)x.meta, (void *)x.nz_row, (void *)x.empty_row, (void *)x.head,
                     (void *)x.tail, (void *)x.span, (void *)x.span_long})
         if (p) cudaFreeAsync(p, s);
     x = SegIndex{};
@@ -145,6 +166,8 @@ void seg_build(const DeviceGraph &g, SegIndex &x, cudaStream_t s) {
     x.nz_row = salloc<uint32_t>(x.n_nz, s);
     x.empty_row = salloc<uint32_t>(x.n_empty, s);
     seg_split_rows_kernel<<<gb, 256, 0, s>>>(nonempty, pos, n, x.nz_row, x.empty_row);
+    x.meta = salloc<uint4>(ntiles, s);
+    seg_meta_kernel<<<gb, 256, 0, s>>>(x.mask, x.tile_j0, g.row_ptr, x.nz_row, ntiles, x.meta);
     PRG_CUDA(cudaGetLastError());
     x.head = salloc<double>(ntiles, s);
     x.tail = salloc<double>(ntiles, s);
@@ -195,16 +218,20 @@ __device__ __forceinline__ void seg_block_sum3(double &a, double &b, double &c, 
     }
 }
 
-// Dangling mass of the input (the producer's block records summed by warp 0
-// in a fixed order, so both kernels of a launch and all their blocks get the
-// same bits) and the half-step skip.  Returns false when the launch has
-// nothing to do.
+// Dangling mass of the input (the producer's block records summed in a
+// fixed layout by the first kSegSumWarps warps, then in warp order by one
+// thread, so both kernels of a launch and all their blocks get the same
+// bits) and the half-step skip.  Returns false when the launch has nothing
+// to do.
+constexpr int kSegSumWarps = 8;  // both kernels have at least this many warps
 __device__ __forceinline__ bool seg_prologue(const IterArgs &a, double &dz) {
+    __shared__ double s_z[3][kSegSumWarps];
     __shared__ double s_dz;
     __shared__ int s_skip;
-    if (threadIdx.x < 32) {
+    const uint32_t w = threadIdx.x >> 5;
+    if (w < (uint32_t)kSegSumWarps) {
         double z0 = 0.0, z1 = 0.0, z2 = 0.0;
-        for (uint32_t i = threadIdx.x; i < a.kpart_n; i += 32) {
+        for (uint32_t i = threadIdx.x; i < a.kpart_n; i += 32 * kSegSumWarps) {
             const double4 q = a.kpart_in[i];
             z0 += q.x;
             z1 += q.y;
@@ -213,30 +240,53 @@ __device__ __forceinline__ bool seg_prologue(const IterArgs &a, double &dz) {
         z0 = warp_sum(z0);
         z1 = warp_sum(z1);
         z2 = warp_sum(z2);
-        if (threadIdx.x == 0) {
-            s_dz = z0;
-            s_skip = a.ktol != nullptr && !((a.knorm2 ? sqrt(z2) : z1) > *a.ktol);
+        if ((threadIdx.x & 31) == 0) {
+            s_z[0][w] = z0;
+            s_z[1][w] = z1;
+            s_z[2][w] = z2;
         }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double z0 = 0.0, z1 = 0.0, z2 = 0.0;
+        for (int k = 0; k < kSegSumWarps; k++) {
+            z0 += s_z[0][k];
+            z1 += s_z[1][k];
+            z2 += s_z[2][k];
+        }
+        s_dz = z0;
+        s_skip = a.ktol != nullptr && !((a.knorm2 ? sqrt(z2) : z1) > *a.ktol);
     }
     __syncthreads();
     dz = s_dz;
     return !s_skip;
 }
 
+// Epilogue operands of one row, loaded apart from the epilogue so that their
+// latency can overlap other work.
+struct SegPre {
+    float in, rh, t;
+};
+
 struct SegEpi {
     float d, dshare;
     double pd, pds, ps;
+    __device__ __forceinline__ SegPre load(const IterArgs &a, uint32_t v) const {
+        SegPre q;
+        q.in = __ldcs(a.x32_in + v);
+        q.rh = a.rh32 ? __ldcs(a.rh32 + v) : 0.0f;
+        q.t = a.t32 ? a.t32[v] : (float)a.inv_n;
+        return q;
+    }
     // y = p - (d sum + d dsum t) and its records, as iter_kernel<MODE_KRY32>
-    __device__ __forceinline__ void row(const IterArgs &a, uint32_t v, float sum) {
-        const float pin = __ldcs(a.x32_in + v);
-        const float rh = a.rh32 ? __ldcs(a.rh32 + v) : 0.0f;
-        const float t = a.t32 ? a.t32[v] : (float)a.inv_n;
-        const float out = pin - (d * sum + dshare * t);
+    __device__ __forceinline__ void fin(const IterArgs &a, uint32_t v, const SegPre &q, float sum) {
+        const float out = q.in - (d * sum + dshare * q.t);
         __stcs(a.x32_out + v, out);
-        pd += (double)rh * (double)out;
-        pds += (double)out * (double)pin;
+        pd += (double)q.rh * (double)out;
+        pds += (double)out * (double)q.in;
         ps += (double)out * (double)out;
     }
+    __device__ __forceinline__ void row(const IterArgs &a, uint32_t v, float sum) { fin(a, v, load(a, v), sum); }
 };
 
 // Segmented sums of one 128-arc block (lane owns 4 consecutive arcs).  v: the
@@ -372,6 +422,135 @@ __global__ void __launch_bounds__(kSegNT, 1) kry32_seg_kernel(const IterArgs a) 
     if (threadIdx.x == 0) a.kpart_out[blockIdx.x] = make_double4(ep.pd, ep.pds, ep.ps, 0.0);
 }
 
+// One 32-byte index load (eight consecutive u32, 32-byte aligned address),
+// evict-first in L2 and not allocated in L1.
+__device__ __forceinline__ void ld_stream_u8(const uint32_t *p, uint64_t pol, uint32_t (&c)[8]) {
+    asm("ld.global.nc.L1::no_allocate.L2::cache_hint.v8.u32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8], %9;"
+        : "=r"(c[0]), "=r"(c[1]), "=r"(c[2]), "=r"(c[3]), "=r"(c[4]), "=r"(c[5]), "=r"(c[6]), "=r"(c[7])
+        : "l"(p), "l"(pol));
+}
+
+// The same pass with lane L owning the 8 consecutive arcs 8L..8L+7 of the
+// tile (one 32-byte index load, one scan per tile):
+//   * in the lane, a running FP64 sum over its arcs that restarts after each
+//     row end; the rows that begin and end inside the lane go straight to
+//     the warp's buffer, the part before the lane's first row end is kept;
+//   * across lanes, one unsegmented inclusive scan S of the lanes' open
+//     tails with exclusive form X; the row that closes first in lane L began
+//     after the last row end in a lane jb < L (jb = 0 if none), so its sum is
+//     the kept part + X[L] - X[jb];
+//   * ranks come from the tile record (row ends before the lane's mask word)
+//     and the population count of the word's lower bits.
+// The operands of the tile's first 32 rows are loaded while the gathers are
+// in flight.  With HOT, sources at or above the hot prefix are gathered
+// without L1 allocation.
+template <bool HOT>
+__global__ void __launch_bounds__(kSegNT, 1) kry32_seg8_kernel(const IterArgs a) {
+    extern __shared__ __align__(16) float s_dyn[];
+    float *s_sums = s_dyn;                            // per warp: the tile's row sums by rank
+    float *s_hot = s_dyn + (kSegNT / 32) * kSegTile;  // hot prefix
+    __shared__ double s_red[96];
+    if (*(volatile const int32_t *)a.kdone) return;
+    const uint32_t H = HOT ? a.hot : 0u;
+    if (HOT) {
+        for (uint32_t i = threadIdx.x * 4; i < H; i += kSegNT * 4)
+            *reinterpret_cast<uint4 *>(s_hot + i) = __ldcg(reinterpret_cast<const uint4 *>(a.xt32_in + i));
+    }
+    double dz = 0.0;
+    if (!seg_prologue(a, dz)) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) a.kpart_out[0] = make_double4(0.0, 0.0, 0.0, 1.0);
+        return;
+    }
+    SegEpi ep{(float)a.damping, (float)(a.damping * dz), 0.0, 0.0, 0.0};
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t lt = lanemask_lt();
+    const uint32_t fshift = (lane & 3u) * 8u;  // the lane's byte in its mask word
+    const uint32_t lower = (1u << fshift) - 1u;
+    const uint32_t wsel = lane >> 2;            // the lane's mask word in the tile
+    float *sums = s_sums + (threadIdx.x >> 5) * kSegTile;
+    const uint64_t warp = (blockIdx.x * (uint64_t)kSegNT + threadIdx.x) >> 5;
+    const uint64_t nwarps = (gridDim.x * (uint64_t)kSegNT) >> 5;
+    const float *xt = a.xt32_in;
+    const uint32_t L1 = a.l1hot;
+    for (uint64_t t = warp; t < a.seg_ntiles; t += nwarps) {
+        const uint64_t P0 = t * kSegTile;
+        const uint64_t q0 = P0 + 8u * lane;
+        uint32_t cc[8];
+        // a lane that starts before the last arc stays inside col's padding
+        if (q0 < a.arcs) {
+            ld_stream_u8(a.col + q0, policy_evict_first(), cc);
+        } else {
+#pragma unroll
+            for (int k = 0; k < 8; k++) cc[k] = 0u;
+        }
+        const uint32_t mw = __ldg(&a.seg_mask[t * (kSegTile / 32) + wsel]);
+        const uint4 meta = __ldg(&a.seg_meta[t]);
+        const bool full = P0 + kSegTile <= a.arcs;
+        float v[8];
+        const uint64_t pol_g = policy_evict_last();
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+            float g;
+            if (HOT) g = cc[k] < H ? s_hot[cc[k]] : ld_gather_na(xt + cc[k], pol_g);
+            else g = cc[k] < L1 ? ld_gather(xt + cc[k], pol_g) : ld_gather_na(xt + cc[k], pol_g);
+            v[k] = (full || q0 + k < a.arcs) ? g : 0.0f;
+        }
+        const uint32_t j0 = meta.x, cnt = meta.w & 0x7FFFFFFFu;
+        const bool began = (meta.w >> 31) != 0u;
+        // rank i's row (i < 32), skipping the one begun in an earlier tile
+        const bool mine = lane < cnt && !(lane == 0u && began);
+        uint32_t row = 0;
+        SegPre pre{0.0f, 0.0f, 0.0f};
+        if (mine) {
+            row = __ldg(&a.seg_nz[j0 + lane]);
+            pre = ep.load(a, row);
+        }
+        // in-lane segmented sums
+        const uint32_t f = (mw >> fshift) & 0xFFu;
+        const uint32_t wpre = ((wsel < 4u ? meta.y : meta.z) >> (8u * (wsel & 3u))) & 0xFFu;
+        const uint32_t r0 = wpre + __popc(mw & lower);
+        uint32_t r = r0;
+        double acc = 0.0, h = 0.0;
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+            acc += (double)v[k];
+            if ((f >> k) & 1u) {
+                if (r == r0) h = acc;
+                else sums[r] = (float)acc;
+                r++;
+                acc = 0.0;
+            }
+        }
+        // across lanes
+        double S = acc;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const double ov = __shfl_up_sync(0xffffffffu, S, o);
+            if (lane >= (uint32_t)o) S += ov;
+        }
+        double X = __shfl_up_sync(0xffffffffu, S, 1);
+        if (lane == 0u) X = 0.0;
+        const uint32_t E = __ballot_sync(0xffffffffu, f != 0u);
+        const uint32_t below = E & lt;
+        const int jb = below ? 31 - __clz(below) : 0;
+        const int jl = E ? 31 - __clz(E) : 0;
+        const double Xb = __shfl_sync(0xffffffffu, X, jb);
+        const double Xl = __shfl_sync(0xffffffffu, X, jl);
+        if (f) {
+            const double first = h + (X - Xb);
+            sums[r0] = (float)first;
+            if (r0 == 0u && began) a.seg_head[t] = first;  // closes a spanning row
+        }
+        if (lane == 31u) a.seg_tail[t] = S - Xl;
+        __syncwarp();
+        if (mine) ep.fin(a, row, pre, sums[lane]);
+        for (uint32_t i = lane + 32u; i < cnt; i += 32u) ep.row(a, __ldg(&a.seg_nz[j0 + i]), sums[i]);
+        __syncwarp();
+    }
+    seg_block_sum3(ep.pd, ep.pds, ep.ps, s_red);
+    if (threadIdx.x == 0) a.kpart_out[blockIdx.x] = make_double4(ep.pd, ep.pds, ep.ps, 0.0);
+}
+
 // Rows that span tiles and rows without arcs; records after the tile
 // kernel's.  A spanning row's total is the open tails of the tiles from its
 // first to the one before its closing tile, plus that tile's head, in tile
@@ -401,22 +580,35 @@ __global__ void __launch_bounds__(kSegFixNT) kry32_seg_finish(const IterArgs a, 
         sum = warp_sum(sum);
         if (lane == 0) ep.row(a, e.x, (float)(sum + __ldcg(&a.seg_head[e.z])));
     }
-    for (uint64_t i = tid; i < a.seg_nempty; i += nth) ep.row(a, a.seg_empty[i], 0.0f);
+    // rows without arcs, four per thread and step (the list is 256-byte
+    // aligned), their operand loads issued together
+    const uint64_t ne4 = a.seg_nempty >> 2;
+    const uint4 *e4 = reinterpret_cast<const uint4 *>(a.seg_empty);
+    for (uint64_t i = tid; i < ne4; i += nth) {
+        const uint4 q = __ldg(e4 + i);
+        const SegPre p0 = ep.load(a, q.x), p1 = ep.load(a, q.y), p2 = ep.load(a, q.z), p3 = ep.load(a, q.w);
+        ep.fin(a, q.x, p0, 0.0f);
+        ep.fin(a, q.y, p1, 0.0f);
+        ep.fin(a, q.z, p2, 0.0f);
+        ep.fin(a, q.w, p3, 0.0f);
+    }
+    for (uint64_t i = (ne4 << 2) + tid; i < a.seg_nempty; i += nth) ep.row(a, a.seg_empty[i], 0.0f);
     seg_block_sum3(ep.pd, ep.pds, ep.ps, s_red);
     if (threadIdx.x == 0) a.kpart_out[rec0 + blockIdx.x] = make_double4(ep.pd, ep.pds, ep.ps, 0.0);
 }
 
-LaunchCfg seg_config(const DeviceGraph &g, uint32_t hot_entries) {
+LaunchCfg seg_config(const DeviceGraph &g, uint32_t hot_entries, int variant) {
     int dev = 0, sms = 0;
     PRG_CUDA(cudaGetDevice(&dev));
     PRG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     LaunchCfg c;
-    c.seg = 1;
+    c.seg = variant == 2 ? 2 : 1;
     c.threads = kSegNT;
     c.hot = std::min<uint32_t>(std::min<uint32_t>(hot_entries, kSegHotMax), g.n) & ~3u;
     c.smem = ((size_t)(kSegNT / 32) * kSegTile + c.hot) * sizeof(float);
-    PRG_CUDA(cudaFuncSetAttribute(c.hot ? (const void *)kry32_seg_kernel<true> : (const void *)kry32_seg_kernel<false>,
-                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c.smem));
+    const void *k = c.seg == 2 ? (c.hot ? (const void *)kry32_seg8_kernel<true> : (const void *)kry32_seg8_kernel<false>)
+                               : (c.hot ? (const void *)kry32_seg_kernel<true> : (const void *)kry32_seg_kernel<false>);
+    PRG_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c.smem));
     c.seg_g1 = (unsigned)sms;
     c.seg_g2 = (unsigned)sms * 4u;
     c.grid = c.seg_g1 + c.seg_g2;  // block records the consumers add
@@ -425,8 +617,14 @@ LaunchCfg seg_config(const DeviceGraph &g, uint32_t hot_entries) {
 }
 
 void launch_kry32_seg(const IterArgs &a, const LaunchCfg &c, cudaStream_t s) {
-    if (c.hot) kry32_seg_kernel<true><<<c.seg_g1, kSegNT, c.smem, s>>>(a);
-    else kry32_seg_kernel<false><<<c.seg_g1, kSegNT, c.smem, s>>>(a);
+    if (c.seg == 2) {
+        if (c.hot) kry32_seg8_kernel<true><<<c.seg_g1, kSegNT, c.smem, s>>>(a);
+        else kry32_seg8_kernel<false><<<c.seg_g1, kSegNT, c.smem, s>>>(a);
+    } else if (c.hot) {
+        kry32_seg_kernel<true><<<c.seg_g1, kSegNT, c.smem, s>>>(a);
+    } else {
+        kry32_seg_kernel<false><<<c.seg_g1, kSegNT, c.smem, s>>>(a);
+    }
     kry32_seg_finish<<<c.seg_g2, kSegFixNT, 0, s>>>(a, c.seg_g1);
     PRG_CUDA(cudaGetLastError());
 }

@@ -82,7 +82,7 @@ void workspace_ensure(Workspace &ws, const DeviceGraph &g, cudaStream_t s) {
     for (int m = 0; m < kModes; m++) {
         const bool fp32 = m == MODE_CORR32 || m == MODE_KRY32;
         const uint32_t hot = g.perm != nullptr ? (fp32 ? g.hot_cache : g.hot_cache64) : 0u;
-        if (m == MODE_KRY32 && seg) ws.cfg[m] = seg_config(g, g.perm != nullptr ? g.seg_hot : 0u);
+        if (m == MODE_KRY32 && seg) ws.cfg[m] = seg_config(g, g.perm != nullptr ? g.seg_hot : 0u, (int)g.seg_kry32);
         else ws.cfg[m] = iteration_config(m, g.weighted, hot, g.blocks_per_sm, g.n, g.hot_threads);
         if (!ws.cfg[m].seg) ws.cfg[m].hub_recs = g.nhub;
         const uint32_t l1 = fp32 ? g.l1_hot32 : g.l1_hot64;
@@ -136,6 +136,7 @@ IterArgs base_args(const DeviceGraph &g, Workspace &ws, double damping) {
     a.arcs = g.arcs;
     a.seg_mask = ws.seg.mask;
     a.seg_tile_j0 = ws.seg.tile_j0;
+    a.seg_meta = ws.seg.meta;
     a.seg_nz = ws.seg.nz_row;
     a.seg_empty = ws.seg.empty_row;
     a.seg_head = ws.seg.head;

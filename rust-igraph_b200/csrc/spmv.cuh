@@ -46,6 +46,10 @@ struct SegIndex {
     uint64_t ntiles = 0;
     uint32_t *mask = nullptr;       // ntiles * 8 words (+ 8 pad)
     uint32_t *tile_j0 = nullptr;    // ntiles + 1
+    // per tile: {tile_j0, running row-end counts before mask words 0-3 and
+    // 4-7 (one byte each), row ends in the tile | 1 << 31 when its first
+    // row end closes a row begun in an earlier tile}
+    uint4 *meta = nullptr;
     uint32_t *nz_row = nullptr;     // n_nz
     uint32_t *empty_row = nullptr;  // n_empty
     uint32_t n_nz = 0, n_empty = 0;
@@ -102,6 +106,7 @@ struct IterArgs {
     // tile-segmented FP32 Krylov matvec (MODE_KRY32 with LaunchCfg::seg)
     uint64_t arcs;
     const uint32_t *seg_mask, *seg_tile_j0, *seg_nz, *seg_empty;
+    const uint4 *seg_meta;
     double *seg_head, *seg_tail;
     const uint4 *seg_span, *seg_span_long;
     uint64_t seg_ntiles;
@@ -122,7 +127,8 @@ struct LaunchCfg {
     uint32_t hot = 0;  // hot-prefix length (vertices)
     uint32_t l1hot = 0xFFFFFFFFu;  // gathers of ids >= l1hot bypass L1
     uint32_t hub_recs = 0;  // hub-row records a Krylov consumer adds after the block records
-    int seg = 0;            // MODE_KRY32: tile-segmented kernel pair (segspmv.cu)
+    int seg = 0;            // MODE_KRY32: tile-segmented kernel pair (segspmv.cu): 1 = 4-arc lane quads,
+                            // 2 = 8 consecutive arcs per lane
     unsigned seg_g1 = 0, seg_g2 = 0;  // its main and finishing grids
 };
 
@@ -141,7 +147,7 @@ void launch_iteration(int mode, bool weighted, const IterArgs &a, const LaunchCf
 // the tiles, then the rows that span tiles and the rows without arcs).
 void seg_build(const DeviceGraph &g, SegIndex &x, cudaStream_t s);
 void seg_free(SegIndex &x, cudaStream_t s);
-LaunchCfg seg_config(const DeviceGraph &g, uint32_t hot_entries);
+LaunchCfg seg_config(const DeviceGraph &g, uint32_t hot_entries, int variant);
 void launch_kry32_seg(const IterArgs &a, const LaunchCfg &c, cudaStream_t s);
 
 // Average time (ms) of a pass that only streams g's column indices and gathers

@@ -207,6 +207,11 @@ def lib():
                                                   C.c_uint64, f64p, f64p]
     L.prg_graph_gather_probe.restype = C.c_int32
     L.prg_graph_gather_probe.argtypes = [vp, C.c_int32, C.POINTER(C.c_double)]
+    L.prg_graph_matvec32.restype = C.c_int32
+    L.prg_graph_matvec32.argtypes = [vp, C.c_int32, vp, vp, C.c_double, C.c_double, vp, f64p,
+                                     C.POINTER(C.c_double)]
+    L.prg_graph_device_csr.restype = C.c_int32
+    L.prg_graph_device_csr.argtypes = [vp] + [C.POINTER(vp)] * 4
     L.prg_infomap_flow.restype = C.c_int32
     L.prg_infomap_flow.argtypes = [C.c_uint32, C.c_uint64, u32p, u32p, C.c_int32, f64p, C.c_uint64, f64p,
                                    C.c_uint64, f64p, C.POINTER(C.c_uint32)]
@@ -716,6 +721,23 @@ class DeviceGraph:
         ms = C.c_double()
         _check(lib().prg_graph_gather_probe(self._h, int(reps), C.byref(ms)))
         return ms.value
+
+    def matvec32(self, kernel: int, d_p: int, d_pt: int, dz: float, damping: float, d_y: int):
+        """One FP32 Krylov matvec y = p - d (A pt + dz / n) on internal ids
+        through kernel 0 (row-block), 1 or 2 (tile-segmented); device
+        pointers of n float32 each.  Returns ((p.y, y.p, y.y), ms)."""
+        dots = np.zeros(3)
+        ms = C.c_double()
+        _check(lib().prg_graph_matvec32(self._h, int(kernel), C.c_void_p(d_p), C.c_void_p(d_pt), float(dz),
+                                        float(damping), C.c_void_p(d_y), _ptr(dots), C.byref(ms)))
+        return tuple(dots), ms.value
+
+    def device_csr(self):
+        """Device pointers (row_ptr, col, perm or 0, inv32) of the resident
+        in-CSR, in internal ids."""
+        out = [C.c_void_p() for _ in range(4)]
+        _check(lib().prg_graph_device_csr(self._h, *[C.byref(o) for o in out]))
+        return tuple(o.value or 0 for o in out)
 
     def close(self):
         if self._h:

@@ -177,6 +177,17 @@ unsafe extern "C" {
         inv32: *mut *const f32,
     ) -> i32;
     pub fn prg_graph_gather_probe(g: *mut prg_graph, reps: i32, ms_per_pass: *mut f64) -> i32;
+    pub fn prg_graph_matvec32(
+        g: *mut prg_graph,
+        kernel: i32,
+        d_p: *const f32,
+        d_pt: *const f32,
+        dz: f64,
+        damping: f64,
+        d_y: *mut f32,
+        dots: *mut f64,
+        ms: *mut f64,
+    ) -> i32;
 
     // batched personalized PageRank
     pub fn prg_ppr_batch(
