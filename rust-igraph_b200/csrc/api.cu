@@ -139,6 +139,8 @@ static prg_graph *new_handle(uint32_t n, uint64_t m, int32_t directed, cudaStrea
     h->g.hot_threads = t.hot_threads;
     h->g.seg_kry32 = t.seg_kry32;
     h->g.seg_hot = t.seg_hot;
+    h->g.seg_res64 = t.seg_res64;
+    h->g.seg_hot64 = t.seg_hot64;
     h->g.l1_hot32 = t.l1_hot32;
     h->g.l1_hot64 = t.l1_hot64;
     h->ws.unroll = t.unroll;
@@ -1391,6 +1393,12 @@ int32_t prg_set_tuning(const char *key, int64_t value) {
     } else if (k == "seg_kry32") {
         if (value > 2) return fail(PRG_ERR_INVALID_ARGUMENT, "seg_kry32 must be 0, 1 or 2");
         t.seg_kry32 = (uint32_t)value;
+    } else if (k == "seg_res64") {
+        if (value > 1) return fail(PRG_ERR_INVALID_ARGUMENT, "seg_res64 must be 0 or 1");
+        t.seg_res64 = (uint32_t)value;
+    } else if (k == "seg_hot64") {
+        if (value > 20480) return fail(PRG_ERR_INVALID_ARGUMENT, "seg_hot64 must be at most 20480 entries");
+        t.seg_hot64 = (uint32_t)value;
     } else if (k == "seg_hot") {
         if (value > 49152) return fail(PRG_ERR_INVALID_ARGUMENT, "seg_hot must be at most 49152 entries");
         t.seg_hot = (uint32_t)value;

@@ -808,7 +808,7 @@ void matvec32_probe(const DeviceGraph &g, Workspace &ws, int kernel, const float
         c.hub_recs = g.nhub;
     } else {
         if (ws.seg.mask == nullptr) seg_build(g, ws.seg, s);
-        c = seg_config(g, g.perm != nullptr ? g.seg_hot : 0u, kernel);
+        c = seg_config(g, g.perm != nullptr ? g.seg_hot : 0u, kernel, MODE_KRY32);
     }
     if (g.perm != nullptr && g.l1_hot32) c.l1hot = g.l1_hot32;
     IterArgs a = base_args(g, ws, damping);

@@ -45,7 +45,8 @@ namespace prg {
 
 constexpr int kSegNT = 1024;       // threads of the tile kernel (one block per SM)
 constexpr int kSegFixNT = 256;     // threads of the finishing kernel
-constexpr uint32_t kSegHotMax = 49152;  // hot-prefix entries (192 KB of shared memory)
+constexpr uint32_t kSegHotMax = 49152;    // FP32 hot-prefix entries (192 KB of shared memory)
+constexpr uint32_t kSegHotMax64 = 20480;  // FP64 hot-prefix entries (160 KB, beside 64 KB of row sums)
 
 // ------------------------------------------------------------------ index build
 
@@ -166,6 +167,13 @@ void seg_build(const DeviceGraph &g, SegIndex &x, cudaStream_t s) {
     x.nz_row = salloc<uint32_t>(x.n_nz, s);
     x.empty_row = salloc<uint32_t>(x.n_empty, s);
     seg_split_rows_kernel<<<gb, 256, 0, s>>>(nonempty, pos, n, x.nz_row, x.empty_row);
+    if (nnz) {
+        // nz_row is increasing and distinct, so it is the identity iff its last entry is nnz - 1
+        uint32_t last = 0;
+        PRG_CUDA(cudaMemcpyAsync(&last, x.nz_row + nnz - 1, 4, cudaMemcpyDeviceToHost, s));
+        PRG_CUDA(cudaStreamSynchronize(s));
+        x.dense = last == nnz - 1 ? 1u : 0u;
+    }
     x.meta = salloc<uint4>(ntiles, s);
     seg_meta_kernel<<<gb, 256, 0, s>>>(x.mask, x.tile_j0, g.row_ptr, x.nz_row, ntiles, x.meta);
     PRG_CUDA(cudaGetLastError());
@@ -430,7 +438,123 @@ __device__ __forceinline__ void ld_stream_u8(const uint32_t *p, uint64_t pol, ui
         : "l"(p), "l"(pol));
 }
 
-// The same pass with lane L owning the 8 consecutive arcs 8L..8L+7 of the
+// ------------------------------------------------------------------ pass kinds
+// The 8-arcs-per-lane tile kernel and the finishing kernel are shared by two
+// passes, which differ in value type, gathered vector, prologue, epilogue and
+// records:
+//   Kry32Pass — the FP32 Krylov matvec above (MODE_KRY32);
+//   Res64Pass — the FP64 residual pass r = G(x) - x of the refined and
+//               Krylov solves (MODE_KRES64), with iter_kernel<MODE_KRES64>'s
+//               epilogue and its Ctl bookkeeping done by the last finishing
+//               block.
+
+struct Kry32Pass {
+    using V = float;
+    using Pre = SegPre;
+    SegEpi ep;
+    __device__ static bool stopped(const IterArgs &a) { return *(volatile const int32_t *)a.kdone != 0; }
+    __device__ static const float *source(const IterArgs &a) { return a.xt32_in; }
+    // false: the half-step skip holds (the tile kernel's block 0 marks it)
+    __device__ bool begin(const IterArgs &a, bool mark) {
+        double dz = 0.0;
+        if (!seg_prologue(a, dz)) {
+            if (mark && blockIdx.x == 0 && threadIdx.x == 0) a.kpart_out[0] = make_double4(0.0, 0.0, 0.0, 1.0);
+            return false;
+        }
+        ep = SegEpi{(float)a.damping, (float)(a.damping * dz), 0.0, 0.0, 0.0};
+        return true;
+    }
+    __device__ Pre load(const IterArgs &a, uint32_t v) const { return ep.load(a, v); }
+    __device__ void fin(const IterArgs &a, uint32_t v, const Pre &q, float sum) { ep.fin(a, v, q, sum); }
+    __device__ void end(const IterArgs &a, unsigned rec0, double *s_red, bool) {
+        seg_block_sum3(ep.pd, ep.pds, ep.ps, s_red);
+        if (threadIdx.x == 0) a.kpart_out[rec0 + blockIdx.x] = make_double4(ep.pd, ep.pds, ep.ps, 0.0);
+    }
+};
+
+struct Res64Pre {
+    double old, t;
+};
+
+struct Res64Pass {
+    using V = double;
+    using Pre = Res64Pre;
+    double d, dsum, tele, dshare, pd, ps;
+    __device__ static bool stopped(const IterArgs &) { return false; }
+    __device__ static const double *source(const IterArgs &a) { return a.xt64_in; }
+    __device__ bool begin(const IterArgs &a, bool) {
+        d = a.damping;
+        dsum = *(volatile const double *)&a.ctl->dsum[a.parity];
+        const double nf = (double)a.n;
+        tele = __ddiv_rn(1.0 - d, nf);
+        dshare = __ddiv_rn(__dmul_rn(d, dsum), nf);
+        pd = ps = 0.0;
+        __syncthreads();  // the hot prefix is in place
+        return true;
+    }
+    __device__ Pre load(const IterArgs &a, uint32_t v) const {
+        Pre q;
+        q.old = __ldcs(a.x64_in + v);
+        q.t = a.t64 ? a.t64[v] : 0.0;
+        return q;
+    }
+    // iter_kernel<MODE_KRES64>'s epilogue: x' = G(x), r = x' - x
+    __device__ void fin(const IterArgs &a, uint32_t v, const Pre &q, double y) {
+        double out;
+        if (a.t64) out = __dadd_rn(__dmul_rn(1.0 - d, q.t), __dmul_rn(d, __dadd_rn(y, __dmul_rn(dsum, q.t))));
+        else out = __dadd_rn(__dadd_rn(tele, dshare), __dmul_rn(d, y));
+        a.x64_out[v] = out;
+        const double r = out - q.old;
+        pd += fabs(r);
+        ps += out;
+        if (a.b64_out) __stcs(a.b64_out + v, r);
+        else __stcs(a.b32_out + v, (float)r);
+    }
+    // block record (|r|, 0, x'); the last block of the last kernel adds all
+    // records in index order and updates Ctl as iter_kernel<MODE_KRES64> does
+    __device__ void end(const IterArgs &a, unsigned rec0, double *s_red, bool last_stage) {
+        __shared__ int s_last;
+        double z = 0.0;
+        seg_block_sum3(pd, z, ps, s_red);
+        if (threadIdx.x == 0) {
+            a.blk_part[rec0 + blockIdx.x] = make_double4(pd, z, ps, 0.0);
+            if (last_stage) {
+                __threadfence();
+                s_last = atomicAdd(&a.ctl->groups_done, 1u) == gridDim.x - 1;
+            }
+        }
+        if (!last_stage) return;
+        __syncthreads();
+        if (!s_last) return;
+        __threadfence();
+        const uint32_t nrec = rec0 + gridDim.x;
+        double x = 0.0, y = 0.0, w = 0.0;
+        for (uint32_t i = threadIdx.x; i < nrec; i += blockDim.x) {
+            const double2 q0 = __ldcg(reinterpret_cast<const double2 *>(&a.blk_part[i]));
+            const double2 q1 = __ldcg(reinterpret_cast<const double2 *>(&a.blk_part[i]) + 1);
+            x += q0.x;
+            y += q0.y;
+            w += q1.x;
+        }
+        seg_block_sum3(x, y, w, s_red);
+        if (threadIdx.x == 0) {
+            Ctl *ctl = a.ctl;
+            ctl->groups_done = 0u;
+            ctl->dsum[a.parity ^ 1] = y;
+            ctl->rnorm = x;
+            ctl->gsum = w;
+            ctl->resid_passes += 1u;
+            const double t = ctl->rho * x;
+            ctl->thr = t > ctl->floor_abs ? t : ctl->floor_abs;
+            ctl->iters = 0u;
+            ctl->done = 0;
+            ctl->parity_last = a.parity;
+            __threadfence();
+        }
+    }
+};
+
+// The tile kernel with lane L owning the 8 consecutive arcs 8L..8L+7 of the
 // tile (one 32-byte index load, one scan per tile):
 //   * in the lane, a running FP64 sum over its arcs that restarts after each
 //     row end; the rows that begin and end inside the lane go straight to
@@ -443,34 +567,34 @@ __device__ __forceinline__ void ld_stream_u8(const uint32_t *p, uint64_t pol, ui
 //     and the population count of the word's lower bits.
 // The operands of the tile's first 32 rows are loaded while the gathers are
 // in flight.  With HOT, sources at or above the hot prefix are gathered
-// without L1 allocation.
-template <bool HOT>
-__global__ void __launch_bounds__(kSegNT, 1) kry32_seg8_kernel(const IterArgs a) {
-    extern __shared__ __align__(16) float s_dyn[];
-    float *s_sums = s_dyn;                            // per warp: the tile's row sums by rank
-    float *s_hot = s_dyn + (kSegNT / 32) * kSegTile;  // hot prefix
+// without L1 allocation.  Dynamic shared memory: [32 warp buffers of
+// kSegTile row sums][hot prefix], both of the pass's value type.
+template <class P, bool HOT>
+__global__ void __launch_bounds__(kSegNT, 1) seg8_kernel(const IterArgs a) {
+    using V = typename P::V;
+    extern __shared__ __align__(16) unsigned char s_raw[];
+    V *s_sums = reinterpret_cast<V *>(s_raw);         // per warp: the tile's row sums by rank
+    V *s_hot = s_sums + (kSegNT / 32) * kSegTile;     // hot prefix
     __shared__ double s_red[96];
-    if (*(volatile const int32_t *)a.kdone) return;
+    if (P::stopped(a)) return;
     const uint32_t H = HOT ? a.hot : 0u;
+    const V *xt = P::source(a);
     if (HOT) {
-        for (uint32_t i = threadIdx.x * 4; i < H; i += kSegNT * 4)
-            *reinterpret_cast<uint4 *>(s_hot + i) = __ldcg(reinterpret_cast<const uint4 *>(a.xt32_in + i));
+        // H is a multiple of 4; the vector is 256-byte aligned
+        constexpr uint32_t kPer = 16 / sizeof(V);
+        for (uint32_t i = threadIdx.x * kPer; i < H; i += kSegNT * kPer)
+            *reinterpret_cast<uint4 *>(s_hot + i) = __ldcg(reinterpret_cast<const uint4 *>(xt + i));
     }
-    double dz = 0.0;
-    if (!seg_prologue(a, dz)) {
-        if (blockIdx.x == 0 && threadIdx.x == 0) a.kpart_out[0] = make_double4(0.0, 0.0, 0.0, 1.0);
-        return;
-    }
-    SegEpi ep{(float)a.damping, (float)(a.damping * dz), 0.0, 0.0, 0.0};
+    P pass;
+    if (!pass.begin(a, true)) return;
     const uint32_t lane = threadIdx.x & 31;
     const uint32_t lt = lanemask_lt();
     const uint32_t fshift = (lane & 3u) * 8u;  // the lane's byte in its mask word
     const uint32_t lower = (1u << fshift) - 1u;
     const uint32_t wsel = lane >> 2;            // the lane's mask word in the tile
-    float *sums = s_sums + (threadIdx.x >> 5) * kSegTile;
+    V *sums = s_sums + (threadIdx.x >> 5) * kSegTile;
     const uint64_t warp = (blockIdx.x * (uint64_t)kSegNT + threadIdx.x) >> 5;
     const uint64_t nwarps = (gridDim.x * (uint64_t)kSegNT) >> 5;
-    const float *xt = a.xt32_in;
     const uint32_t L1 = a.l1hot;
     for (uint64_t t = warp; t < a.seg_ntiles; t += nwarps) {
         const uint64_t P0 = t * kSegTile;
@@ -486,24 +610,24 @@ __global__ void __launch_bounds__(kSegNT, 1) kry32_seg8_kernel(const IterArgs a)
         const uint32_t mw = __ldg(&a.seg_mask[t * (kSegTile / 32) + wsel]);
         const uint4 meta = __ldg(&a.seg_meta[t]);
         const bool full = P0 + kSegTile <= a.arcs;
-        float v[8];
+        V v[8];
         const uint64_t pol_g = policy_evict_last();
 #pragma unroll
         for (int k = 0; k < 8; k++) {
-            float g;
+            V g;
             if (HOT) g = cc[k] < H ? s_hot[cc[k]] : ld_gather_na(xt + cc[k], pol_g);
             else g = cc[k] < L1 ? ld_gather(xt + cc[k], pol_g) : ld_gather_na(xt + cc[k], pol_g);
-            v[k] = (full || q0 + k < a.arcs) ? g : 0.0f;
+            v[k] = (full || q0 + k < a.arcs) ? g : V(0);
         }
         const uint32_t j0 = meta.x, cnt = meta.w & 0x7FFFFFFFu;
         const bool began = (meta.w >> 31) != 0u;
         // rank i's row (i < 32), skipping the one begun in an earlier tile
         const bool mine = lane < cnt && !(lane == 0u && began);
         uint32_t row = 0;
-        SegPre pre{0.0f, 0.0f, 0.0f};
+        typename P::Pre pre{};
         if (mine) {
-            row = __ldg(&a.seg_nz[j0 + lane]);
-            pre = ep.load(a, row);
+            row = a.seg_dense ? j0 + lane : __ldg(&a.seg_nz[j0 + lane]);
+            pre = pass.load(a, row);
         }
         // in-lane segmented sums
         const uint32_t f = (mw >> fshift) & 0xFFu;
@@ -516,7 +640,7 @@ __global__ void __launch_bounds__(kSegNT, 1) kry32_seg8_kernel(const IterArgs a)
             acc += (double)v[k];
             if ((f >> k) & 1u) {
                 if (r == r0) h = acc;
-                else sums[r] = (float)acc;
+                else sums[r] = (V)acc;
                 r++;
                 acc = 0.0;
             }
@@ -538,17 +662,19 @@ __global__ void __launch_bounds__(kSegNT, 1) kry32_seg8_kernel(const IterArgs a)
         const double Xl = __shfl_sync(0xffffffffu, X, jl);
         if (f) {
             const double first = h + (X - Xb);
-            sums[r0] = (float)first;
+            sums[r0] = (V)first;
             if (r0 == 0u && began) a.seg_head[t] = first;  // closes a spanning row
         }
         if (lane == 31u) a.seg_tail[t] = S - Xl;
         __syncwarp();
-        if (mine) ep.fin(a, row, pre, sums[lane]);
-        for (uint32_t i = lane + 32u; i < cnt; i += 32u) ep.row(a, __ldg(&a.seg_nz[j0 + i]), sums[i]);
+        if (mine) pass.fin(a, row, pre, sums[lane]);
+        for (uint32_t i = lane + 32u; i < cnt; i += 32u) {
+            const uint32_t rw = a.seg_dense ? j0 + i : __ldg(&a.seg_nz[j0 + i]);
+            pass.fin(a, rw, pass.load(a, rw), sums[i]);
+        }
         __syncwarp();
     }
-    seg_block_sum3(ep.pd, ep.pds, ep.ps, s_red);
-    if (threadIdx.x == 0) a.kpart_out[blockIdx.x] = make_double4(ep.pd, ep.pds, ep.ps, 0.0);
+    pass.end(a, 0u, s_red, false);
 }
 
 // Rows that span tiles and rows without arcs; records after the tile
@@ -556,12 +682,13 @@ __global__ void __launch_bounds__(kSegNT, 1) kry32_seg8_kernel(const IterArgs a)
 // first to the one before its closing tile, plus that tile's head, in tile
 // order in FP64: one thread per row for spans of up to kSegLongSpan tiles,
 // one warp (lanes strided over the tiles, then a fixed tree) for longer ones.
-__global__ void __launch_bounds__(kSegFixNT) kry32_seg_finish(const IterArgs a, unsigned rec0) {
+template <class P>
+__global__ void __launch_bounds__(kSegFixNT) seg_finish(const IterArgs a, unsigned rec0) {
+    using V = typename P::V;
     __shared__ double s_red[96];
-    if (*(volatile const int32_t *)a.kdone) return;
-    double dz = 0.0;
-    if (!seg_prologue(a, dz)) return;
-    SegEpi ep{(float)a.damping, (float)(a.damping * dz), 0.0, 0.0, 0.0};
+    if (P::stopped(a)) return;
+    P pass;
+    if (!pass.begin(a, false)) return;
     const uint64_t tid = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
     const uint64_t nth = (uint64_t)gridDim.x * blockDim.x;
     for (uint64_t i = tid; i < a.seg_nspan; i += nth) {
@@ -570,7 +697,7 @@ __global__ void __launch_bounds__(kSegFixNT) kry32_seg_finish(const IterArgs a, 
 #pragma unroll 4
         for (uint32_t t = e.y; t < e.z; t++) sum += __ldcg(&a.seg_tail[t]);
         sum += __ldcg(&a.seg_head[e.z]);
-        ep.row(a, e.x, (float)sum);
+        pass.fin(a, e.x, pass.load(a, e.x), (V)sum);
     }
     const uint32_t lane = threadIdx.x & 31;
     for (uint64_t i = tid >> 5; i < a.seg_nlong; i += nth >> 5) {
@@ -578,36 +705,63 @@ __global__ void __launch_bounds__(kSegFixNT) kry32_seg_finish(const IterArgs a, 
         double sum = 0.0;
         for (uint32_t t = e.y + lane; t < e.z; t += 32) sum += __ldcg(&a.seg_tail[t]);
         sum = warp_sum(sum);
-        if (lane == 0) ep.row(a, e.x, (float)(sum + __ldcg(&a.seg_head[e.z])));
+        if (lane == 0) pass.fin(a, e.x, pass.load(a, e.x), (V)(sum + __ldcg(&a.seg_head[e.z])));
     }
     // rows without arcs, four per thread and step (the list is 256-byte
-    // aligned), their operand loads issued together
+    // aligned), their operand loads issued together; with dense ids they are
+    // the range n - nempty .. n-1
+    if (a.seg_dense) {
+        const uint32_t e0 = a.n - a.seg_nempty;
+        for (uint64_t i = tid; i < (a.seg_nempty + 3u) >> 2; i += nth) {
+            const uint32_t v = e0 + 4u * (uint32_t)i;
+            typename P::Pre q[4];
+#pragma unroll
+            for (int k = 0; k < 4; k++)
+                if (v + k < a.n) q[k] = pass.load(a, v + k);
+#pragma unroll
+            for (int k = 0; k < 4; k++)
+                if (v + k < a.n) pass.fin(a, v + k, q[k], V(0));
+        }
+        pass.end(a, rec0, s_red, true);
+        return;
+    }
     const uint64_t ne4 = a.seg_nempty >> 2;
     const uint4 *e4 = reinterpret_cast<const uint4 *>(a.seg_empty);
     for (uint64_t i = tid; i < ne4; i += nth) {
         const uint4 q = __ldg(e4 + i);
-        const SegPre p0 = ep.load(a, q.x), p1 = ep.load(a, q.y), p2 = ep.load(a, q.z), p3 = ep.load(a, q.w);
-        ep.fin(a, q.x, p0, 0.0f);
-        ep.fin(a, q.y, p1, 0.0f);
-        ep.fin(a, q.z, p2, 0.0f);
-        ep.fin(a, q.w, p3, 0.0f);
+        const typename P::Pre p0 = pass.load(a, q.x), p1 = pass.load(a, q.y), p2 = pass.load(a, q.z),
+                              p3 = pass.load(a, q.w);
+        pass.fin(a, q.x, p0, V(0));
+        pass.fin(a, q.y, p1, V(0));
+        pass.fin(a, q.z, p2, V(0));
+        pass.fin(a, q.w, p3, V(0));
     }
-    for (uint64_t i = (ne4 << 2) + tid; i < a.seg_nempty; i += nth) ep.row(a, a.seg_empty[i], 0.0f);
-    seg_block_sum3(ep.pd, ep.pds, ep.ps, s_red);
-    if (threadIdx.x == 0) a.kpart_out[rec0 + blockIdx.x] = make_double4(ep.pd, ep.pds, ep.ps, 0.0);
+    for (uint64_t i = (ne4 << 2) + tid; i < a.seg_nempty; i += nth) {
+        const uint32_t v = a.seg_empty[i];
+        pass.fin(a, v, pass.load(a, v), V(0));
+    }
+    pass.end(a, rec0, s_red, true);
 }
 
-LaunchCfg seg_config(const DeviceGraph &g, uint32_t hot_entries, int variant) {
+template <class P>
+static const void *seg8_entry(bool hot) {
+    return hot ? (const void *)seg8_kernel<P, true> : (const void *)seg8_kernel<P, false>;
+}
+
+LaunchCfg seg_config(const DeviceGraph &g, uint32_t hot_entries, int variant, int mode) {
     int dev = 0, sms = 0;
     PRG_CUDA(cudaGetDevice(&dev));
     PRG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    const bool res = mode == MODE_KRES64;
+    const size_t vb = res ? sizeof(double) : sizeof(float);
     LaunchCfg c;
-    c.seg = variant == 2 ? 2 : 1;
+    c.seg = res || variant == 2 ? 2 : 1;
     c.threads = kSegNT;
-    c.hot = std::min<uint32_t>(std::min<uint32_t>(hot_entries, kSegHotMax), g.n) & ~3u;
-    c.smem = ((size_t)(kSegNT / 32) * kSegTile + c.hot) * sizeof(float);
-    const void *k = c.seg == 2 ? (c.hot ? (const void *)kry32_seg8_kernel<true> : (const void *)kry32_seg8_kernel<false>)
-                               : (c.hot ? (const void *)kry32_seg_kernel<true> : (const void *)kry32_seg_kernel<false>);
+    c.hot = std::min<uint32_t>(std::min<uint32_t>(hot_entries, res ? kSegHotMax64 : kSegHotMax), g.n) & ~3u;
+    c.smem = ((size_t)(kSegNT / 32) * kSegTile + c.hot) * vb;
+    const void *k = res ? seg8_entry<Res64Pass>(c.hot != 0)
+                        : c.seg == 2 ? seg8_entry<Kry32Pass>(c.hot != 0)
+                                     : (c.hot ? (const void *)kry32_seg_kernel<true> : (const void *)kry32_seg_kernel<false>);
     PRG_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c.smem));
     c.seg_g1 = (unsigned)sms;
     c.seg_g2 = (unsigned)sms * 4u;
@@ -616,16 +770,22 @@ LaunchCfg seg_config(const DeviceGraph &g, uint32_t hot_entries, int variant) {
     return c;
 }
 
-void launch_kry32_seg(const IterArgs &a, const LaunchCfg &c, cudaStream_t s) {
-    if (c.seg == 2) {
-        if (c.hot) kry32_seg8_kernel<true><<<c.seg_g1, kSegNT, c.smem, s>>>(a);
-        else kry32_seg8_kernel<false><<<c.seg_g1, kSegNT, c.smem, s>>>(a);
-    } else if (c.hot) {
-        kry32_seg_kernel<true><<<c.seg_g1, kSegNT, c.smem, s>>>(a);
+void launch_seg(int mode, const IterArgs &a, const LaunchCfg &c, cudaStream_t s) {
+    if (mode == MODE_KRES64) {
+        if (c.hot) seg8_kernel<Res64Pass, true><<<c.seg_g1, kSegNT, c.smem, s>>>(a);
+        else seg8_kernel<Res64Pass, false><<<c.seg_g1, kSegNT, c.smem, s>>>(a);
+        seg_finish<Res64Pass><<<c.seg_g2, kSegFixNT, 0, s>>>(a, c.seg_g1);
     } else {
-        kry32_seg_kernel<false><<<c.seg_g1, kSegNT, c.smem, s>>>(a);
+        if (c.seg == 2) {
+            if (c.hot) seg8_kernel<Kry32Pass, true><<<c.seg_g1, kSegNT, c.smem, s>>>(a);
+            else seg8_kernel<Kry32Pass, false><<<c.seg_g1, kSegNT, c.smem, s>>>(a);
+        } else if (c.hot) {
+            kry32_seg_kernel<true><<<c.seg_g1, kSegNT, c.smem, s>>>(a);
+        } else {
+            kry32_seg_kernel<false><<<c.seg_g1, kSegNT, c.smem, s>>>(a);
+        }
+        seg_finish<Kry32Pass><<<c.seg_g2, kSegFixNT, 0, s>>>(a, c.seg_g1);
     }
-    kry32_seg_finish<<<c.seg_g2, kSegFixNT, 0, s>>>(a, c.seg_g1);
     PRG_CUDA(cudaGetLastError());
 }
 

@@ -637,8 +637,8 @@ void launch_iteration(int mode, bool weighted, const IterArgs &a_in, const Launc
     IterArgs a = a_in;
     a.hot = c.hot;
     a.l1hot = c.l1hot;
-    if (mode == MODE_KRY32 && c.seg) {
-        launch_kry32_seg(a, c, s);
+    if (c.seg && (mode == MODE_KRY32 || mode == MODE_KRES64)) {
+        launch_seg(mode, a, c, s);
         return;
     }
     switch (mode) {

@@ -53,6 +53,9 @@ struct SegIndex {
     uint32_t *nz_row = nullptr;     // n_nz
     uint32_t *empty_row = nullptr;  // n_empty
     uint32_t n_nz = 0, n_empty = 0;
+    // the rows with arcs are ids 0 .. n_nz-1 (nz_row[i] = i; degree-sorted
+    // ids of a directed graph put them first), the others n_nz .. n-1
+    uint32_t dense = 0;
     // rows closed in a later tile than they begin: {row, first tile, closing
     // tile, 0}, in tile order; spans of more than kSegLongSpan tiles apart
     uint4 *span = nullptr, *span_long = nullptr;
@@ -111,6 +114,7 @@ struct IterArgs {
     const uint4 *seg_span, *seg_span_long;
     uint64_t seg_ntiles;
     uint32_t seg_nempty, seg_nspan, seg_nlong;
+    uint32_t seg_dense;  // SegIndex::dense: row of rank j is j, rows without arcs are n - seg_nempty .. n-1
     // reduction scratch
     Ctl *ctl;
     double4 *blk_part;   // one record per block of the persistent grid
@@ -147,8 +151,8 @@ void launch_iteration(int mode, bool weighted, const IterArgs &a, const LaunchCf
 // the tiles, then the rows that span tiles and the rows without arcs).
 void seg_build(const DeviceGraph &g, SegIndex &x, cudaStream_t s);
 void seg_free(SegIndex &x, cudaStream_t s);
-LaunchCfg seg_config(const DeviceGraph &g, uint32_t hot_entries, int variant);
-void launch_kry32_seg(const IterArgs &a, const LaunchCfg &c, cudaStream_t s);
+LaunchCfg seg_config(const DeviceGraph &g, uint32_t hot_entries, int variant, int mode = MODE_KRY32);
+void launch_seg(int mode, const IterArgs &a, const LaunchCfg &c, cudaStream_t s);
 
 // Average time (ms) of a pass that only streams g's column indices and gathers
 // one FP32 value per arc with the FP32 matvec's load policies (reps timed

@@ -178,11 +178,15 @@ def test_tuning_keys_are_validated_on_the_host():
     for key, bad, msg in (("hot_threads", 300, "hot_threads must be 256, 512 or 1024"),
                           ("hot_cache64", 70000, "hot_cache64 must be at most 65536 entries"),
                           ("hot_cache32", 70000, "hot_cache32 must be at most 65536 entries"),
-                          ("batch_cheb", 2, "batch_cheb must be 0 or 1")):
+                          ("batch_cheb", 2, "batch_cheb must be 0 or 1"),
+                          ("seg_kry32", 3, "seg_kry32 must be 0, 1 or 2"),
+                          ("seg_res64", 2, "seg_res64 must be 0 or 1"),
+                          ("seg_hot64", 20481, "seg_hot64 must be at most 20480 entries")):
         with pytest.raises(ig.InvalidArgument, match=msg):
             ig.set_tuning(key, bad)
     try:
-        for key, good in (("hot_threads", 512), ("hot_cache64", 16384), ("batch_cheb", 0)):
+        for key, good in (("hot_threads", 512), ("hot_cache64", 16384), ("batch_cheb", 0), ("seg_res64", 0),
+                          ("seg_hot64", 20480)):
             ig.set_tuning(key, good)
     finally:
         ig.reset_tuning()

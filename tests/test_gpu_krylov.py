@@ -218,16 +218,73 @@ def test_segmented_fp32_matvec_matches_row_block_kernel(cuda_ok, case):
     tight, _, _ = O.pagerank_tight(n, f, t, directed, tol=1e-15)
     xs = {}
     try:
-        for seg in (1, 0):
-            ig.set_tuning("seg_kry32", seg)
+        # (seg_kry32, seg_res64): both segmented passes, the 4-arc-quad
+        # matvec, the row-block kernels only
+        for seg in ((2, 1), (1, 1), (0, 0)):
+            ig.set_tuning("seg_kry32", seg[0])
+            ig.set_tuning("seg_res64", seg[1])
             with ig.DeviceGraph.from_host(n, f, t, directed) as dg:
                 x, st = dg.solve(ig.Options(precision=ig.PRECISION_FP32_REFINED))
                 assert np.abs(x - tight).sum() <= 1e-10, (seg, np.abs(x - tight).sum())
                 assert st.error_bound <= 1e-10
-                if seg:
+                if seg[0]:
                     x2, _ = dg.solve(ig.Options(precision=ig.PRECISION_FP32_REFINED))
                     assert np.array_equal(x.view(np.uint64), x2.view(np.uint64))
                 xs[seg] = x
     finally:
         ig.reset_tuning()
-    assert np.abs(xs[1] - xs[0]).sum() <= 2e-10
+    for seg in ((2, 1), (1, 1)):
+        assert np.abs(xs[seg] - xs[(0, 0)]).sum() <= 2e-10
+
+
+def _power_step(n, f, t, directed, x, d=0.85):
+    """G(x) of pagerank.rs:107-140 in float64 (numpy)."""
+    f = np.asarray(f, np.int64)
+    t = np.asarray(t, np.int64)
+    if directed:
+        deg = np.bincount(f, minlength=n)
+        src, dst = f, t
+    else:
+        deg = np.bincount(f, minlength=n) + np.bincount(t, minlength=n)
+        src, dst = np.concatenate([f, t]), np.concatenate([t, f])
+    xt = np.where(deg > 0, x / np.maximum(deg, 1), 0.0)
+    y = np.bincount(dst, weights=xt[src], minlength=n)
+    return (1.0 - d) / n + d * (y + x[deg == 0].sum() / n)
+
+
+@pytest.mark.parametrize("case", ["rmat_relabelled", "star_hub", "sparse_many_empty", "undirected_ba"])
+@pytest.mark.parametrize("seg_res64", [1, 0])
+def test_residual_pass_matches_fp64_restatement(cuda_ok, case, seg_res64):
+    # The FP64 residual pass (the tile-segmented one by default on unweighted
+    # graphs, or the row-block kernel) gives the certificate
+    # ||x - x*||_1 <= ||G(x) - x||_1 d / (1 - d).  From a start within the
+    # final threshold the refined solve stops after that one pass, so its
+    # residual_l1 is ||G(x0) - x0||_1, checked here against numpy.
+    directed = True
+    if case == "rmat_relabelled":  # n above the FP64 hot prefix: both gather paths
+        n = 1 << 17
+        f, t = O.rmat(17, 16 * n, seed=45)
+    elif case == "star_hub":
+        n = 5000
+        f = np.arange(1, n, dtype=np.uint32).repeat(3)
+        t = np.zeros(len(f), np.uint32)
+    elif case == "sparse_many_empty":
+        n = 200_000
+        f, t = O.erdos_renyi_gnm(n, 150_000, True, False, 10)
+    else:
+        n = 30_000
+        f, t = O.barabasi_game_bag(n, 5, False, False, 13)
+        directed = False
+    tight, _, _ = O.pagerank_tight(n, f, t, directed, tol=1e-15)
+    rng = np.random.default_rng(3)
+    x0 = tight * (1.0 + 2e-12 * rng.standard_normal(n))
+    want = np.abs(_power_step(n, f, t, directed, x0) - x0).sum()
+    ig.set_tuning("seg_res64", seg_res64)
+    try:
+        with ig.DeviceGraph.from_host(n, f, t, directed) as dg:
+            x, st = dg.solve(ig.Options(precision=ig.PRECISION_FP32_REFINED), start=x0)
+    finally:
+        ig.reset_tuning()
+    assert st.residual_passes == 1 and st.fp32_passes == 0, st
+    assert abs(st.residual_l1 - want) <= 1e-3 * want + 1e-15, (st.residual_l1, want)
+    assert np.abs(x - tight).sum() <= 1e-10
