@@ -263,8 +263,8 @@ def whole_job_value(units, ms, world_size, device):
 def load_traffic():
     """DRAM traffic of the FP32 Krylov matvec from the committed ncu summary
     (profiles/ncu_traffic.txt, `key value` lines): bytes read + written per
-    launch divided by the launch's algorithmic bytes, measured on a smaller
-    graph of the same family (traffic scales with the bytes processed)."""
+    launch (tile kernel + finishing kernel) divided by the launch's
+    algorithmic bytes, measured at the bench's own size."""
     path = os.path.join(ROOT, "profiles", "ncu_traffic.txt")
     out = {}
     try:
@@ -441,8 +441,9 @@ def main():
     traffic = tr["kry32_traffic_per_alg_byte"] * bytes_launch if "kry32_traffic_per_alg_byte" in tr else None
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak if achieved else None, "traffic": traffic, "peak_source": peak_src,
-                "kernel": "FP32 Krylov matvec y = A p with fused dot products: kry32_seg_kernel + kry32_seg_finish "
-                          "(tile-segmented pass, segspmv.cu) on unweighted graphs",
+                "kernel": "FP32 Krylov matvec y = A p with fused dot products: seg8_kernel<Kry32Pass> + "
+                          "seg_finish<Kry32Pass> (tile-segmented pass, 8 arcs per lane, segspmv.cu) on unweighted "
+                          "graphs",
                 "bytes_per_launch": bytes_launch, "avg_launch_us": avg_launch_s * 1e6, "launches_timed": mv_n}
     # the same index stream gathered once per arc and nothing else: the floor
     # this access pattern sets (L1 wavefronts of random gathers), measured live

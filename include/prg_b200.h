@@ -316,13 +316,14 @@ int32_t prg_autotune(prg_graph *g, int32_t tune_batch, const char *cache_path, p
  * keeps the most-gathered prefix; defaults 16384 / 2048, 0 = all allocate),
  * "defaults" (any value: every key back to its default),
  * "krylov_floor_pct" (Krylov inner solves aim at this percentage of the
- * certified final threshold, 1-90; default 30), "seg_kry32" (unweighted
+ * certified final threshold, 1-90; default 70), "seg_kry32" (unweighted
  * graphs: the tile-segmented FP32 Krylov matvec, 1 with 4-arc lane quads, 2
  * with 8 consecutive arcs per lane; 0 the row-block kernel),
  * "seg_hot" (its shared-memory hot prefix on relabelled graphs, entries),
  * "seg_res64" (unweighted graphs: 1 the tile-segmented FP64 residual pass
  * of the refined and Krylov solves, 0 the row-block kernel), "seg_hot64"
- * (its hot prefix, at most 20480 entries),
+ * (its hot prefix, at most 20480 entries), "seg_prefetch" (segmented passes:
+ * 1 each warp prefetches its next tile of column indices into L2, 0 off),
  * "hot_cache32" / "hot_cache64" (hot prefix of the row-block kernel's FP32 /
  * FP64 passes), "hot_threads" (256, 512 or 1024: the row-block kernel's block
  * size when it keeps a hot prefix),

@@ -141,6 +141,7 @@ static prg_graph *new_handle(uint32_t n, uint64_t m, int32_t directed, cudaStrea
     h->g.seg_hot = t.seg_hot;
     h->g.seg_res64 = t.seg_res64;
     h->g.seg_hot64 = t.seg_hot64;
+    h->g.seg_prefetch = t.seg_prefetch;
     h->g.l1_hot32 = t.l1_hot32;
     h->g.l1_hot64 = t.l1_hot64;
     h->ws.unroll = t.unroll;
@@ -1396,6 +1397,9 @@ int32_t prg_set_tuning(const char *key, int64_t value) {
     } else if (k == "seg_res64") {
         if (value > 1) return fail(PRG_ERR_INVALID_ARGUMENT, "seg_res64 must be 0 or 1");
         t.seg_res64 = (uint32_t)value;
+    } else if (k == "seg_prefetch") {
+        if (value > 1) return fail(PRG_ERR_INVALID_ARGUMENT, "seg_prefetch must be 0 or 1");
+        t.seg_prefetch = (uint32_t)value;
     } else if (k == "seg_hot64") {
         if (value > 20480) return fail(PRG_ERR_INVALID_ARGUMENT, "seg_hot64 must be at most 20480 entries");
         t.seg_hot64 = (uint32_t)value;

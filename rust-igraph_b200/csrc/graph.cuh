@@ -49,7 +49,8 @@ struct DeviceGraph {
     uint32_t seg_kry32 = 2, seg_hot = 32768;
     // ... and the FP64 residual pass of the refined / Krylov solves, with a
     // hot prefix of seg_hot64 entries
-    uint32_t seg_res64 = 1, seg_hot64 = 16384;
+    uint32_t seg_res64 = 1, seg_hot64 = 8192;
+    uint32_t seg_prefetch = 1;  // segmented passes: prefetch each warp's next index tile into L2
     // relabelled graphs: gathers of ids >= l1_hot32 (FP32 passes) / l1_hot64
     // (FP64 passes) bypass L1, keeping it for the hot prefix (0 = all allocate)
     uint32_t l1_hot32 = 16384, l1_hot64 = 2048;
@@ -91,12 +92,13 @@ struct Tuning {
                                  // (1 with 4-arc lane quads, 0 = row-block kernel)
     uint32_t seg_hot = 32768;    // its shared-memory hot prefix on relabelled graphs (entries)
     uint32_t seg_res64 = 1;      // unweighted graphs: tile-segmented FP64 residual pass (0 = row-block kernel)
-    uint32_t seg_hot64 = 16384;  // its hot prefix (entries)
+    uint32_t seg_hot64 = 8192;   // its hot prefix (entries)
+    uint32_t seg_prefetch = 1;   // segmented passes: L2 prefetch of each warp's next index tile
     uint32_t l1_hot32 = 16384, l1_hot64 = 2048;
     double refine_switch = 5e-7;
     uint32_t batch_vec = 2;
     double krylov_rel = 1e-4;
-    double krylov_floor = 0.3;         // refined / Krylov inner solves aim at this fraction of the final threshold
+    double krylov_floor = 0.7;         // refined / Krylov inner solves aim at this fraction of the final threshold
     uint32_t batch_barrier_extra = 0;  // test hook: batched grid barriers wait for arrivals that never come
     uint32_t batch_cheb = 0;           // batched solver on undirected graphs: 1 Chebyshev steps, 0 plain steps
 };

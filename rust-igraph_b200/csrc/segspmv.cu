@@ -554,6 +554,11 @@ struct Res64Pass {
     }
 };
 
+// Bulk prefetch of `bytes` (a multiple of 16, 16-byte aligned address) into L2.
+__device__ __forceinline__ void prefetch_l2(const void *p, uint32_t bytes) {
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+}
+
 // The tile kernel with lane L owning the 8 consecutive arcs 8L..8L+7 of the
 // tile (one 32-byte index load, one scan per tile):
 //   * in the lane, a running FP64 sum over its arcs that restarts after each
@@ -599,6 +604,10 @@ __global__ void __launch_bounds__(kSegNT, 1) seg8_kernel(const IterArgs a) {
     for (uint64_t t = warp; t < a.seg_ntiles; t += nwarps) {
         const uint64_t P0 = t * kSegTile;
         const uint64_t q0 = P0 + 8u * lane;
+        // the warp's next tile of indices into L2 (full tiles only, so the
+        // range stays inside col)
+        if (a.seg_prefetch && lane == 0u && P0 + (nwarps + 1u) * kSegTile <= a.arcs)
+            prefetch_l2(a.col + P0 + nwarps * kSegTile, kSegTile * 4u);
         uint32_t cc[8];
         // a lane that starts before the last arc stays inside col's padding
         if (q0 < a.arcs) {

@@ -147,6 +147,7 @@ IterArgs base_args(const DeviceGraph &g, Workspace &ws, double damping) {
     a.seg_ntiles = ws.seg.ntiles;
     a.seg_nempty = ws.seg.n_empty;
     a.seg_dense = ws.seg.dense;
+    a.seg_prefetch = g.seg_prefetch;
     a.seg_span = ws.seg.span;
     a.seg_span_long = ws.seg.span_long;
     a.seg_nspan = ws.seg.n_span;

@@ -115,6 +115,7 @@ struct IterArgs {
     uint64_t seg_ntiles;
     uint32_t seg_nempty, seg_nspan, seg_nlong;
     uint32_t seg_dense;  // SegIndex::dense: row of rank j is j, rows without arcs are n - seg_nempty .. n-1
+    uint32_t seg_prefetch;  // the tile kernel prefetches each warp's next index tile into L2
     // reduction scratch
     Ctl *ctl;
     double4 *blk_part;   // one record per block of the persistent grid
