@@ -328,11 +328,14 @@ __global__ void relabel_keys(const uint32_t *deg, const uint8_t *noin, uint32_t 
     }
 }
 
-// noin[v] = 0 for every arc head v (noin starts as all ones)
+// noin[v] = 0 for every arc head v (noin starts as all ones).  Flags only
+// fall from 1 to 0, so a read that still sees 1 just leads to a repeated
+// store; reading first keeps the stores to one per vertex instead of one per
+// arc (the hot heads of a skewed graph are read from cache).
 __global__ void mark_heads(const uint32_t *to, uint64_t m, uint32_t n, uint8_t *noin) {
     for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e < m; e += (uint64_t)gridDim.x * blockDim.x) {
         const uint32_t v = to[e];
-        if (v < n) noin[v] = 0;
+        if (v < n && noin[v]) noin[v] = 0;
     }
 }
 
@@ -403,14 +406,26 @@ __global__ void __launch_bounds__(kDegThreads) out_degree_kernel(const uint32_t 
         if (bins[i]) atomicAdd(&deg[i], bins[i]);
 }
 
-// row_ptr of a CSR from its sorted row keys: rows (key[i-1], key[i]] start at
-// arc i (every entry of row_ptr[0..n] is written exactly once).
-__global__ void row_ptr_from_sorted(const uint32_t *key, uint64_t N, uint32_t n, uint32_t *row_ptr) {
-    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i <= N; i += (uint64_t)gridDim.x * blockDim.x) {
-        const uint64_t lo = i == 0 ? 0 : (uint64_t)key[i - 1] + 1;
-        const uint64_t hi = i == N ? n : key[i];
-        for (uint64_t r = lo; r <= hi; r++) row_ptr[r] = (uint32_t)i;
+// row_ptr of a CSR from its sorted row keys, through the rows' arc counts:
+// the first arc i of a row leaves i, the row's last arc turns it into
+// last + 1 - i, and rows without arcs keep 0; an exclusive scan of the counts
+// gives row_ptr[0..n].  Work is one thread per arc however long the runs of
+// rows without arcs are.
+__global__ void row_first_arc(const uint32_t *key, uint64_t N, uint32_t *cnt) {
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < N; i += (uint64_t)gridDim.x * blockDim.x)
+        if (i == 0 || key[i - 1] != key[i]) cnt[key[i]] = (uint32_t)i;
+}
+__global__ void row_last_arc(const uint32_t *key, uint64_t N, uint32_t *cnt) {
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < N; i += (uint64_t)gridDim.x * blockDim.x)
+        if (i + 1 == N || key[i + 1] != key[i]) cnt[key[i]] = (uint32_t)(i + 1) - cnt[key[i]];
+}
+static void row_ptr_from_sorted(const uint32_t *key, uint64_t N, uint32_t n, uint32_t *row_ptr, cudaStream_t s) {
+    PRG_CUDA(cudaMemsetAsync(row_ptr, 0, ((uint64_t)n + 1) * 4, s));
+    if (N) {
+        row_first_arc<<<grid_for(N, kThreads), kThreads, 0, s>>>(key, N, row_ptr);
+        row_last_arc<<<grid_for(N, kThreads), kThreads, 0, s>>>(key, N, row_ptr);
     }
+    exclusive_scan_u32(row_ptr, row_ptr, n, s);  // in place; writes row_ptr[n] = N
 }
 
 // After sorting arc ids: fetch source and weight of every arc.
@@ -686,7 +701,7 @@ void build_graph(DeviceGraph &g, const uint32_t *d_from, const uint32_t *d_to, c
 
     // row_ptr from the boundaries of the sorted destinations
     PRG_CUDA(cudaMallocAsync((void **)&g.row_ptr, (uint64_t)(n + 1) * 4, s));
-    row_ptr_from_sorted<<<grid_for(arcs + 1, kThreads), kThreads, 0, s>>>(k0, arcs, n, g.row_ptr);
+    row_ptr_from_sorted(k0, arcs, n, g.row_ptr, s);
     PRG_CUDA(cudaGetLastError());
 
     const uint64_t padded = arcs + kColPad;
@@ -716,7 +731,7 @@ void build_graph(DeviceGraph &g, const uint32_t *d_from, const uint32_t *d_to, c
                 make_arcs<<<ge, kThreads, 0, s>>>(ef, et, m, true, true, sk1, sv);  // sv = edge ids
             }
             radix_sort_pairs(&sk, &sv, &sk1, &sv1, m, bits_for(n ? n - 1 : 0), s);
-            row_ptr_from_sorted<<<grid_for(m + 1, kThreads), kThreads, 0, s>>>(sk, m, n, optr);
+            row_ptr_from_sorted(sk, m, n, optr, s);
             row_weight_sums<<<grid_for((uint64_t)n * 32, kThreads), kThreads, 0, s>>>(optr, d_w, sv, n, strength);
             dfree(sk, s);
             dfree(sv, s);
