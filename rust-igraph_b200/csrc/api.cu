@@ -142,6 +142,8 @@ static prg_graph *new_handle(uint32_t n, uint64_t m, int32_t directed, cudaStrea
     h->g.seg_res64 = t.seg_res64;
     h->g.seg_hot64 = t.seg_hot64;
     h->g.seg_prefetch = t.seg_prefetch;
+    h->g.seg_threads = t.seg_threads;
+    h->g.seg_pipe = t.seg_pipe;
     h->g.l1_hot32 = t.l1_hot32;
     h->g.l1_hot64 = t.l1_hot64;
     h->ws.unroll = t.unroll;
@@ -1397,6 +1399,13 @@ int32_t prg_set_tuning(const char *key, int64_t value) {
     } else if (k == "seg_res64") {
         if (value > 1) return fail(PRG_ERR_INVALID_ARGUMENT, "seg_res64 must be 0 or 1");
         t.seg_res64 = (uint32_t)value;
+    } else if (k == "seg_threads") {
+        if (value != 1024 && value != 768 && value != 512)
+            return fail(PRG_ERR_INVALID_ARGUMENT, "seg_threads must be 1024, 768 or 512");
+        t.seg_threads = (uint32_t)value;
+    } else if (k == "seg_pipe") {
+        if (value > 1) return fail(PRG_ERR_INVALID_ARGUMENT, "seg_pipe must be 0 or 1");
+        t.seg_pipe = (uint32_t)value;
     } else if (k == "seg_prefetch") {
         if (value > 1) return fail(PRG_ERR_INVALID_ARGUMENT, "seg_prefetch must be 0 or 1");
         t.seg_prefetch = (uint32_t)value;

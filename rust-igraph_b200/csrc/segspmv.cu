@@ -572,14 +572,16 @@ __device__ __forceinline__ void prefetch_l2(const void *p, uint32_t bytes) {
 //     and the population count of the word's lower bits.
 // The operands of the tile's first 32 rows are loaded while the gathers are
 // in flight.  With HOT, sources at or above the hot prefix are gathered
-// without L1 allocation.  Dynamic shared memory: [32 warp buffers of
-// kSegTile row sums][hot prefix], both of the pass's value type.
-template <class P, bool HOT>
-__global__ void __launch_bounds__(kSegNT, 1) seg8_kernel(const IterArgs a) {
+// without L1 allocation.  Dynamic shared memory: [NT/32 warp buffers of
+// kSegTile row sums][hot prefix], both of the pass's value type.  NT threads
+// in one block per SM; with PIPE each warp loads its next tile's indices,
+// mask word and record while it works on the current one.
+template <class P, bool HOT, int NT, bool PIPE>
+__global__ void __launch_bounds__(NT, 1) seg8_kernel(const IterArgs a) {
     using V = typename P::V;
     extern __shared__ __align__(16) unsigned char s_raw[];
     V *s_sums = reinterpret_cast<V *>(s_raw);         // per warp: the tile's row sums by rank
-    V *s_hot = s_sums + (kSegNT / 32) * kSegTile;     // hot prefix
+    V *s_hot = s_sums + (NT / 32) * kSegTile;         // hot prefix
     __shared__ double s_red[96];
     if (P::stopped(a)) return;
     const uint32_t H = HOT ? a.hot : 0u;
@@ -587,7 +589,7 @@ __global__ void __launch_bounds__(kSegNT, 1) seg8_kernel(const IterArgs a) {
     if (HOT) {
         // H is a multiple of 4; the vector is 256-byte aligned
         constexpr uint32_t kPer = 16 / sizeof(V);
-        for (uint32_t i = threadIdx.x * kPer; i < H; i += kSegNT * kPer)
+        for (uint32_t i = threadIdx.x * kPer; i < H; i += NT * kPer)
             *reinterpret_cast<uint4 *>(s_hot + i) = __ldcg(reinterpret_cast<const uint4 *>(xt + i));
     }
     P pass;
@@ -598,26 +600,43 @@ __global__ void __launch_bounds__(kSegNT, 1) seg8_kernel(const IterArgs a) {
     const uint32_t lower = (1u << fshift) - 1u;
     const uint32_t wsel = lane >> 2;            // the lane's mask word in the tile
     V *sums = s_sums + (threadIdx.x >> 5) * kSegTile;
-    const uint64_t warp = (blockIdx.x * (uint64_t)kSegNT + threadIdx.x) >> 5;
-    const uint64_t nwarps = (gridDim.x * (uint64_t)kSegNT) >> 5;
+    const uint64_t warp = (blockIdx.x * (uint64_t)NT + threadIdx.x) >> 5;
+    const uint64_t nwarps = (gridDim.x * (uint64_t)NT) >> 5;
     const uint32_t L1 = a.l1hot;
+    // tile t's indices (a lane that starts before the last arc stays inside
+    // col's padding), the lane's mask word and the tile record
+    auto load_tile = [&](uint64_t t, uint32_t (&c)[8], uint32_t &w, uint4 &m) {
+        const uint64_t q = t * kSegTile + 8u * lane;
+        if (t < a.seg_ntiles && q < a.arcs) {
+            ld_stream_u8(a.col + q, policy_evict_first(), c);
+        } else {
+#pragma unroll
+            for (int k = 0; k < 8; k++) c[k] = 0u;
+        }
+        if (t < a.seg_ntiles) {
+            w = __ldg(&a.seg_mask[t * (kSegTile / 32) + wsel]);
+            m = __ldg(&a.seg_meta[t]);
+        } else {
+            w = 0u;
+            m = make_uint4(0u, 0u, 0u, 0u);
+        }
+    };
+    uint32_t cc[8], mw = 0u;
+    uint4 meta = make_uint4(0u, 0u, 0u, 0u);
+    if (PIPE) load_tile(warp, cc, mw, meta);
     for (uint64_t t = warp; t < a.seg_ntiles; t += nwarps) {
         const uint64_t P0 = t * kSegTile;
         const uint64_t q0 = P0 + 8u * lane;
-        // the warp's next tile of indices into L2 (full tiles only, so the
-        // range stays inside col)
-        if (a.seg_prefetch && lane == 0u && P0 + (nwarps + 1u) * kSegTile <= a.arcs)
-            prefetch_l2(a.col + P0 + nwarps * kSegTile, kSegTile * 4u);
-        uint32_t cc[8];
-        // a lane that starts before the last arc stays inside col's padding
-        if (q0 < a.arcs) {
-            ld_stream_u8(a.col + q0, policy_evict_first(), cc);
-        } else {
-#pragma unroll
-            for (int k = 0; k < 8; k++) cc[k] = 0u;
-        }
-        const uint32_t mw = __ldg(&a.seg_mask[t * (kSegTile / 32) + wsel]);
-        const uint4 meta = __ldg(&a.seg_meta[t]);
+        // a later tile of the warp's indices into L2 (full tiles only, so the
+        // range stays inside col): the next one, or the one after it when the
+        // next is already being loaded
+        constexpr uint32_t ahead = PIPE ? 2u : 1u;
+        if (a.seg_prefetch && lane == 0u && P0 + (ahead * nwarps + 1u) * kSegTile <= a.arcs)
+            prefetch_l2(a.col + P0 + ahead * nwarps * kSegTile, kSegTile * 4u);
+        uint32_t ccn[8], mwn = 0u;
+        uint4 metan;
+        if (PIPE) load_tile(t + nwarps, ccn, mwn, metan);
+        else load_tile(t, cc, mw, meta);
         const bool full = P0 + kSegTile <= a.arcs;
         V v[8];
         const uint64_t pol_g = policy_evict_last();
@@ -682,6 +701,12 @@ __global__ void __launch_bounds__(kSegNT, 1) seg8_kernel(const IterArgs a) {
             pass.fin(a, rw, pass.load(a, rw), sums[i]);
         }
         __syncwarp();
+        if (PIPE) {
+#pragma unroll
+            for (int k = 0; k < 8; k++) cc[k] = ccn[k];
+            mw = mwn;
+            meta = metan;
+        }
     }
     pass.end(a, 0u, s_red, false);
 }
@@ -752,9 +777,34 @@ __global__ void __launch_bounds__(kSegFixNT) seg_finish(const IterArgs a, unsign
     pass.end(a, rec0, s_red, true);
 }
 
+// The tile kernel of pass P for a launch shape: hot prefix or not, threads
+// per block (1024, 768 or 512), pipelined tile loads or not.
+template <class P, bool HOT, int NT, bool PIPE>
+static void seg8_go(const IterArgs &a, const LaunchCfg &c, cudaStream_t s) {
+    seg8_kernel<P, HOT, NT, PIPE><<<c.seg_g1, NT, c.smem, s>>>(a);
+}
+using Seg8Go = void (*)(const IterArgs &, const LaunchCfg &, cudaStream_t);
 template <class P>
-static const void *seg8_entry(bool hot) {
-    return hot ? (const void *)seg8_kernel<P, true> : (const void *)seg8_kernel<P, false>;
+static Seg8Go seg8_pick(bool hot, int nt, bool pipe, const void **entry) {
+#define PRG_SEG8_PICK(H, N, Q)                                          \
+    if (hot == H && nt == N && pipe == Q) {                             \
+        if (entry) *entry = (const void *)seg8_kernel<P, H, N, Q>;      \
+        return seg8_go<P, H, N, Q>;                                     \
+    }
+    PRG_SEG8_PICK(true, 1024, false)
+    PRG_SEG8_PICK(true, 1024, true)
+    PRG_SEG8_PICK(true, 768, false)
+    PRG_SEG8_PICK(true, 768, true)
+    PRG_SEG8_PICK(true, 512, false)
+    PRG_SEG8_PICK(true, 512, true)
+    PRG_SEG8_PICK(false, 1024, false)
+    PRG_SEG8_PICK(false, 1024, true)
+    PRG_SEG8_PICK(false, 768, false)
+    PRG_SEG8_PICK(false, 768, true)
+    PRG_SEG8_PICK(false, 512, false)
+    PRG_SEG8_PICK(false, 512, true)
+#undef PRG_SEG8_PICK
+    throw CudaError(cudaErrorInvalidValue, "segmented pass: unsupported launch shape");
 }
 
 LaunchCfg seg_config(const DeviceGraph &g, uint32_t hot_entries, int variant, int mode) {
@@ -765,12 +815,14 @@ LaunchCfg seg_config(const DeviceGraph &g, uint32_t hot_entries, int variant, in
     const size_t vb = res ? sizeof(double) : sizeof(float);
     LaunchCfg c;
     c.seg = res || variant == 2 ? 2 : 1;
-    c.threads = kSegNT;
+    c.threads = c.seg == 2 ? (int)g.seg_threads : kSegNT;
+    c.seg_pipe = c.seg == 2 && g.seg_pipe != 0;
     c.hot = std::min<uint32_t>(std::min<uint32_t>(hot_entries, res ? kSegHotMax64 : kSegHotMax), g.n) & ~3u;
-    c.smem = ((size_t)(kSegNT / 32) * kSegTile + c.hot) * vb;
-    const void *k = res ? seg8_entry<Res64Pass>(c.hot != 0)
-                        : c.seg == 2 ? seg8_entry<Kry32Pass>(c.hot != 0)
-                                     : (c.hot ? (const void *)kry32_seg_kernel<true> : (const void *)kry32_seg_kernel<false>);
+    c.smem = ((size_t)(c.threads / 32) * kSegTile + c.hot) * vb;
+    const void *k = nullptr;
+    if (res) seg8_pick<Res64Pass>(c.hot != 0, c.threads, c.seg_pipe, &k);
+    else if (c.seg == 2) seg8_pick<Kry32Pass>(c.hot != 0, c.threads, c.seg_pipe, &k);
+    else k = c.hot ? (const void *)kry32_seg_kernel<true> : (const void *)kry32_seg_kernel<false>;
     PRG_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c.smem));
     c.seg_g1 = (unsigned)sms;
     c.seg_g2 = (unsigned)sms * 4u;
@@ -781,18 +833,12 @@ LaunchCfg seg_config(const DeviceGraph &g, uint32_t hot_entries, int variant, in
 
 void launch_seg(int mode, const IterArgs &a, const LaunchCfg &c, cudaStream_t s) {
     if (mode == MODE_KRES64) {
-        if (c.hot) seg8_kernel<Res64Pass, true><<<c.seg_g1, kSegNT, c.smem, s>>>(a);
-        else seg8_kernel<Res64Pass, false><<<c.seg_g1, kSegNT, c.smem, s>>>(a);
+        seg8_pick<Res64Pass>(c.hot != 0, c.threads, c.seg_pipe, nullptr)(a, c, s);
         seg_finish<Res64Pass><<<c.seg_g2, kSegFixNT, 0, s>>>(a, c.seg_g1);
     } else {
-        if (c.seg == 2) {
-            if (c.hot) seg8_kernel<Kry32Pass, true><<<c.seg_g1, kSegNT, c.smem, s>>>(a);
-            else seg8_kernel<Kry32Pass, false><<<c.seg_g1, kSegNT, c.smem, s>>>(a);
-        } else if (c.hot) {
-            kry32_seg_kernel<true><<<c.seg_g1, kSegNT, c.smem, s>>>(a);
-        } else {
-            kry32_seg_kernel<false><<<c.seg_g1, kSegNT, c.smem, s>>>(a);
-        }
+        if (c.seg == 2) seg8_pick<Kry32Pass>(c.hot != 0, c.threads, c.seg_pipe, nullptr)(a, c, s);
+        else if (c.hot) kry32_seg_kernel<true><<<c.seg_g1, kSegNT, c.smem, s>>>(a);
+        else kry32_seg_kernel<false><<<c.seg_g1, kSegNT, c.smem, s>>>(a);
         seg_finish<Kry32Pass><<<c.seg_g2, kSegFixNT, 0, s>>>(a, c.seg_g1);
     }
     PRG_CUDA(cudaGetLastError());

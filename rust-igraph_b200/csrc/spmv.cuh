@@ -135,6 +135,7 @@ struct LaunchCfg {
     int seg = 0;            // MODE_KRY32: tile-segmented kernel pair (segspmv.cu): 1 = 4-arc lane quads,
                             // 2 = 8 consecutive arcs per lane
     unsigned seg_g1 = 0, seg_g2 = 0;  // its main and finishing grids
+    bool seg_pipe = false;            // its tile kernel loads each warp's next tile ahead
 };
 
 // Persistent launch shape of the iteration kernel on this device: 256-thread

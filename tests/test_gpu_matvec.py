@@ -124,3 +124,33 @@ def test_matvec_rejects_bad_arguments(cuda_ok):
     with ig.DeviceGraph.from_host(n, f, t, True, weights=w) as dg:
         with pytest.raises(ig.IgraphError):
             dg.matvec32(2, dp.data_ptr(), dp.data_ptr(), 0.0, D, dp.data_ptr())
+
+
+@pytest.mark.parametrize("case", ["rmat_relabelled", "star_hub", "cycle", "sparse_many_empty"])
+def test_segmented_launch_shapes_agree(cuda_ok, case):
+    # The tile kernel's block size and its pipelined tile loads change which
+    # warp takes a tile, never how a tile is summed: y is bit-identical, the
+    # block records agree to rounding.
+    n, f, t, directed = _graph(case)
+    rng = np.random.default_rng(8)
+    p = rng.standard_normal(n).astype(np.float32) / np.float32(n)
+    dp = torch.from_numpy(p).cuda()
+    out = {}
+    try:
+        for shape in ((1024, 0), (1024, 1), (768, 0), (768, 1), (512, 1)):
+            ig.set_tuning("seg_threads", shape[0])
+            ig.set_tuning("seg_pipe", shape[1])
+            with ig.DeviceGraph.from_host(n, f, t, directed) as dg:
+                inv = _host(dg.device_csr()[3], n, "<f4")
+                dpt = torch.from_numpy((p * inv).astype(np.float32)).cuda()
+                dz = float(p[inv == 0].astype(np.float64).sum())
+                dy = torch.empty(n, dtype=torch.float32, device="cuda")
+                dots, _ = dg.matvec32(2, dp.data_ptr(), dpt.data_ptr(), dz, D, dy.data_ptr())
+                out[shape] = (dy.cpu().numpy(), dots)
+    finally:
+        ig.reset_tuning()
+    y0, d0 = out[(1024, 0)]
+    for shape, (y, dots) in out.items():
+        assert np.array_equal(y.view(np.int32), y0.view(np.int32)), shape
+        for a, b in zip(dots, d0):
+            assert abs(a - b) <= 1e-12 * (abs(b) + float(np.abs(y0.astype(np.float64)) @ np.abs(p))), shape
