@@ -61,6 +61,8 @@ def parse():
     p.add_argument("--profile-case", action="store_true",
                    help="build the R-MAT graph of --scale, run one FP32-refined solve and exit: the command the "
                         "kernel captures under profiles/ run")
+    p.add_argument("--profile-warm", action="store_true",
+                   help="with --profile-case: run the warm-start network's inference twice before the solve")
     p.add_argument("--tuning", action="append", default=[], metavar="KEY=VALUE",
                    help="with --profile-case: a tuning key to set before the graph is built (repeatable)")
     return p.parse_args()
@@ -85,8 +87,14 @@ def run_profile_case(args):
     del df, dt
     torch.cuda.empty_cache()
     out = torch.empty(n, dtype=torch.float64, device="cuda")
+    inf_ms = None
+    if args.profile_warm:
+        from igraph_b200 import warmstart as wsm
+
+        net = wsm.WarmStartNet.load(os.path.join(ROOT, "rust-igraph_b200", "igraph_b200", "warmstart_weights.f32"))
+        inf_ms = [net.predict(dg, out.data_ptr()) for _ in range(2)]
     st = dg.solve_device(out.data_ptr(), ig.Options(precision=ig.PRECISION_FP32_REFINED, eps=EPS, damping=D))
-    print(json.dumps({"profile_case": {"scale": args.scale, "tuning": args.tuning, "passes": st.iterations,
+    print(json.dumps({"profile_case": {"inference_ms": inf_ms,"scale": args.scale, "tuning": args.tuning, "passes": st.iterations,
                                        "fp32_matvecs": st.fp32_passes, "solve_ms": st.solve_ms,
                                        "matvec_us": st.spmv_ms / max(st.spmv_launches, 1) * 1e3,
                                        "error_bound": st.error_bound,
