@@ -247,8 +247,8 @@ int32_t prg_graph_gather_probe(prg_graph *g, int32_t reps, double *ms_per_pass);
  * and numbering).  A sums pt over each row's in-arcs; pt is p scaled by
  * 1/out-degree (inv32) and dz the dangling mass of p, both the caller's.
  * kernel: 0 the row-block pass, 1 the tile-segmented pass with 4-arc lane
- * quads, 2 the tile-segmented pass with 8 consecutive arcs per lane, 3 the
- * same with 16 per lane over pairs of tiles (1-3 need an unweighted graph).  dots (3 doubles, optional) = (p.y, y.p, y.y)
+ * quads, 2 the tile-segmented pass with 8 consecutive arcs per lane (1 and 2
+ * need an unweighted graph).  dots (3 doubles, optional) = (p.y, y.p, y.y)
  * as the kernel's block records sum them; ms (optional) = its device time.
  * Device pointers, n entries each.  Tests compare the three kernels with an
  * FP64 restatement through it. */
@@ -318,8 +318,7 @@ int32_t prg_autotune(prg_graph *g, int32_t tune_batch, const char *cache_path, p
  * "krylov_floor_pct" (Krylov inner solves aim at this percentage of the
  * certified final threshold, 1-90; default 70), "seg_kry32" (unweighted
  * graphs: the tile-segmented FP32 Krylov matvec, 1 with 4-arc lane quads, 2
- * with 8 consecutive arcs per lane, 3 with 16 per lane over pairs of tiles;
- * 0 the row-block kernel),
+ * with 8 consecutive arcs per lane; 0 the row-block kernel),
  * "seg_hot" (its shared-memory hot prefix on relabelled graphs, entries),
  * "seg_res64" (unweighted graphs: 1 the tile-segmented FP64 residual pass
  * of the refined and Krylov solves, 0 the row-block kernel), "seg_hot64"

@@ -1059,7 +1059,7 @@ int32_t prg_graph_matvec32(prg_graph *h, int32_t kernel, const float *d_p, const
     g_err.clear();
     PRG_GUARD_BEGIN
     if (!h) return fail(PRG_ERR_INVALID_ARGUMENT, "null graph handle");
-    if (kernel < 0 || kernel > 3) return fail(PRG_ERR_INVALID_ARGUMENT, "kernel must be 0, 1, 2 or 3");
+    if (kernel < 0 || kernel > 2) return fail(PRG_ERR_INVALID_ARGUMENT, "kernel must be 0, 1 or 2");
     if (kernel != 0 && h->g.weighted)
         return fail(PRG_ERR_UNSUPPORTED, "the tile-segmented matvec serves unweighted graphs");
     if (!(damping >= 0.0 && damping <= 1.0)) return fail(PRG_ERR_INVALID_ARGUMENT, "damping must be in [0, 1]");
@@ -1394,7 +1394,7 @@ int32_t prg_set_tuning(const char *key, int64_t value) {
         if (k != "hot_cache64") t.hot_cache = (uint32_t)value;
         if (k != "hot_cache32") t.hot_cache64 = (uint32_t)value;
     } else if (k == "seg_kry32") {
-        if (value > 3) return fail(PRG_ERR_INVALID_ARGUMENT, "seg_kry32 must be 0, 1, 2 or 3");
+        if (value > 2) return fail(PRG_ERR_INVALID_ARGUMENT, "seg_kry32 must be 0, 1 or 2");
         t.seg_kry32 = (uint32_t)value;
     } else if (k == "seg_res64") {
         if (value > 1) return fail(PRG_ERR_INVALID_ARGUMENT, "seg_res64 must be 0 or 1");

@@ -795,7 +795,7 @@ void solve_krylov(const DeviceGraph &g, Workspace &ws, const SolveOpts &o, const
 }
 
 // One FP32 Krylov matvec y = p - d (A pt + dz t), t = 1/n, through the
-// row-block kernel (kernel 0) or a tile-segmented one (1-3), with rh = p:
+// row-block kernel (kernel 0) or a tile-segmented one (1, 2), with rh = p:
 // dots = the launch's summed records (p.y, y.p, y.y) in record order, ms =
 // its device time.  A diagnostic: its inputs live in internal ids.
 void matvec32_probe(const DeviceGraph &g, Workspace &ws, int kernel, const float *p, const float *pt, double dz,

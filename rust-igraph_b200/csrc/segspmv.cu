@@ -47,7 +47,6 @@ constexpr int kSegNT = 1024;       // threads of the tile kernel (one block per 
 constexpr int kSegFixNT = 256;     // threads of the finishing kernel
 constexpr uint32_t kSegHotMax = 49152;    // FP32 hot-prefix entries (192 KB of shared memory)
 constexpr uint32_t kSegHotMax64 = 20480;  // FP64 hot-prefix entries (160 KB, beside 64 KB of row sums)
-constexpr uint32_t kSegHotMax16 = 40960;  // FP32 hot-prefix entries beside the pair kernel's 64 KB of row sums
 
 // ------------------------------------------------------------------ index build
 
@@ -622,15 +621,31 @@ __global__ void __launch_bounds__(NT, 1) seg8_kernel(const IterArgs a) {
             m = make_uint4(0u, 0u, 0u, 0u);
         }
     };
+    // the 8 gathered values of tile t (zero past the last arc)
+    auto gather_tile = [&](uint64_t t, const uint32_t (&c)[8], V (&v)[8]) {
+        const uint64_t q = t * kSegTile + 8u * lane;
+        const bool full = (t + 1) * kSegTile <= a.arcs;
+        const uint64_t pol_g = policy_evict_last();
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+            V g;
+            if (HOT) g = c[k] < H ? s_hot[c[k]] : ld_gather_na(xt + c[k], pol_g);
+            else g = c[k] < L1 ? ld_gather(xt + c[k], pol_g) : ld_gather_na(xt + c[k], pol_g);
+            v[k] = (full || q + k < a.arcs) ? g : V(0);
+        }
+    };
+    // with PIPE the next tile's indices, mask word and record are loaded while
+    // the warp works on the current tile (issuing its gathers early as well
+    // measured slower: the pass is bound by L1TEX and MIO throughput, not by
+    // the latency that more loads in flight would hide)
     uint32_t cc[8], mw = 0u;
     uint4 meta = make_uint4(0u, 0u, 0u, 0u);
+    V v[8];
     if (PIPE) load_tile(warp, cc, mw, meta);
     for (uint64_t t = warp; t < a.seg_ntiles; t += nwarps) {
         const uint64_t P0 = t * kSegTile;
-        const uint64_t q0 = P0 + 8u * lane;
         // a later tile of the warp's indices into L2 (full tiles only, so the
-        // range stays inside col): the next one, or the one after it when the
-        // next is already being loaded
+        // range stays inside col): the first one not yet being loaded
         constexpr uint32_t ahead = PIPE ? 2u : 1u;
         if (a.seg_prefetch && lane == 0u && P0 + (ahead * nwarps + 1u) * kSegTile <= a.arcs)
             prefetch_l2(a.col + P0 + ahead * nwarps * kSegTile, kSegTile * 4u);
@@ -638,16 +653,7 @@ __global__ void __launch_bounds__(NT, 1) seg8_kernel(const IterArgs a) {
         uint4 metan;
         if (PIPE) load_tile(t + nwarps, ccn, mwn, metan);
         else load_tile(t, cc, mw, meta);
-        const bool full = P0 + kSegTile <= a.arcs;
-        V v[8];
-        const uint64_t pol_g = policy_evict_last();
-#pragma unroll
-        for (int k = 0; k < 8; k++) {
-            V g;
-            if (HOT) g = cc[k] < H ? s_hot[cc[k]] : ld_gather_na(xt + cc[k], pol_g);
-            else g = cc[k] < L1 ? ld_gather(xt + cc[k], pol_g) : ld_gather_na(xt + cc[k], pol_g);
-            v[k] = (full || q0 + k < a.arcs) ? g : V(0);
-        }
+        gather_tile(t, cc, v);
         const uint32_t j0 = meta.x, cnt = meta.w & 0x7FFFFFFFu;
         const bool began = (meta.w >> 31) != 0u;
         // rank i's row (i < 32), skipping the one begun in an earlier tile
@@ -705,164 +711,6 @@ __global__ void __launch_bounds__(NT, 1) seg8_kernel(const IterArgs a) {
         if (PIPE) {
 #pragma unroll
             for (int k = 0; k < 8; k++) cc[k] = ccn[k];
-            mw = mwn;
-            meta = metan;
-        }
-    }
-    pass.end(a, 0u, s_red, false);
-}
-
-// The FP32 matvec with two consecutive tiles per warp step (a pair): lane L
-// owns the 16 consecutive arcs 16L..16L+15 of the pair, lanes 0-15 in its
-// first tile, lanes 16-31 in its second.  One scan covers 512 arcs; the scan
-// restarts at lane 16 for the second tile's head, and each tile keeps its own
-// head, tail and record, so the finishing kernel is the same.  Ranks run over
-// the pair (the second tile's after the first's: tile_j0 is a running count).
-// With PIPE each warp loads its next pair's indices, mask word and record
-// while it works on the current one.
-template <class P, bool HOT, bool PIPE>
-__global__ void __launch_bounds__(kSegNT, 1) seg16_kernel(const IterArgs a) {
-    using V = typename P::V;
-    constexpr int NT = kSegNT;
-    extern __shared__ __align__(16) unsigned char s_raw[];
-    V *s_sums = reinterpret_cast<V *>(s_raw);          // per warp: the pair's row sums by rank
-    V *s_hot = s_sums + (NT / 32) * 2 * kSegTile;      // hot prefix
-    __shared__ double s_red[96];
-    if (P::stopped(a)) return;
-    const uint32_t H = HOT ? a.hot : 0u;
-    const V *xt = P::source(a);
-    if (HOT) {
-        constexpr uint32_t kPer = 16 / sizeof(V);
-        for (uint32_t i = threadIdx.x * kPer; i < H; i += NT * kPer)
-            *reinterpret_cast<uint4 *>(s_hot + i) = __ldcg(reinterpret_cast<const uint4 *>(xt + i));
-    }
-    P pass;
-    if (!pass.begin(a, true)) return;
-    const uint32_t lane = threadIdx.x & 31;
-    const uint32_t lt = lanemask_lt();
-    const uint32_t half = lane >> 4;               // 0: the pair's first tile, 1: its second
-    const uint32_t fshift = (lane & 1u) * 16u;     // the lane's half of its mask word
-    const uint32_t lower = (1u << fshift) - 1u;
-    const uint32_t wsel = (lane & 15u) >> 1;       // the lane's mask word in its tile
-    const int base = (int)(half * 16u);            // first lane of the lane's tile
-    V *sums = s_sums + (threadIdx.x >> 5) * 2 * kSegTile;
-    const uint64_t warp = (blockIdx.x * (uint64_t)NT + threadIdx.x) >> 5;
-    const uint64_t nwarps = (gridDim.x * (uint64_t)NT) >> 5;
-    const uint64_t npairs = (a.seg_ntiles + 1) / 2;
-    const uint32_t L1 = a.l1hot;
-    // pair s: the lane's 16 indices (a lane that starts before the last arc
-    // stays inside col's padding of 16), mask word and its tile's record
-    auto load_pair = [&](uint64_t s, uint32_t (&c0)[8], uint32_t (&c1)[8], uint32_t &w, uint4 &m) {
-        const uint64_t q = s * 2 * kSegTile + 16u * lane;
-        const uint64_t t = 2 * s + half;
-        if (s < npairs && q < a.arcs) {
-            ld_stream_u8(a.col + q, policy_evict_first(), c0);
-            ld_stream_u8(a.col + q + 8, policy_evict_first(), c1);
-        } else {
-#pragma unroll
-            for (int k = 0; k < 8; k++) c0[k] = c1[k] = 0u;
-        }
-        if (s < npairs && t < a.seg_ntiles) {
-            w = __ldg(&a.seg_mask[t * (kSegTile / 32) + wsel]);
-            m = __ldg(&a.seg_meta[t]);
-        } else {
-            w = 0u;
-            m = make_uint4(0u, 0u, 0u, 0u);
-        }
-    };
-    uint32_t c0[8], c1[8], mw = 0u;
-    uint4 meta = make_uint4(0u, 0u, 0u, 0u);
-    if (PIPE) load_pair(warp, c0, c1, mw, meta);
-    for (uint64_t s = warp; s < npairs; s += nwarps) {
-        const uint64_t P0 = s * 2 * kSegTile;
-        const uint64_t q0 = P0 + 16u * lane;
-        const uint64_t t = 2 * s + half;  // the lane's tile
-        constexpr uint32_t ahead = PIPE ? 2u : 1u;
-        if (a.seg_prefetch && lane == 0u && P0 + (ahead * nwarps + 1u) * 2 * kSegTile <= a.arcs)
-            prefetch_l2(a.col + P0 + ahead * nwarps * 2 * kSegTile, 2 * kSegTile * 4u);
-        uint32_t n0[8], n1[8], mwn = 0u;
-        uint4 metan;
-        if (PIPE) load_pair(s + nwarps, n0, n1, mwn, metan);
-        else load_pair(s, c0, c1, mw, meta);
-        const bool full = P0 + 2 * kSegTile <= a.arcs;
-        V v[16];
-        const uint64_t pol_g = policy_evict_last();
-#pragma unroll
-        for (int k = 0; k < 16; k++) {
-            const uint32_t c = k < 8 ? c0[k] : c1[k - 8];
-            V g;
-            if (HOT) g = c < H ? s_hot[c] : ld_gather_na(xt + c, pol_g);
-            else g = c < L1 ? ld_gather(xt + c, pol_g) : ld_gather_na(xt + c, pol_g);
-            v[k] = (full || q0 + k < a.arcs) ? g : V(0);
-        }
-        // the pair's records: first rank and counts of both tiles
-        const uint32_t j0 = __shfl_sync(0xffffffffu, meta.x, 0);
-        const uint32_t w0 = __shfl_sync(0xffffffffu, meta.w, 0);
-        const uint32_t w1 = __shfl_sync(0xffffffffu, meta.w, 16);
-        const uint32_t cnt0 = w0 & 0x7FFFFFFFu, cnt = cnt0 + (w1 & 0x7FFFFFFFu);
-        const bool began0 = (w0 >> 31) != 0u, began1 = (w1 >> 31) != 0u;
-        // rank i's row (i < 32), skipping rows begun before their closing tile
-        const bool mine = lane < cnt && !(lane == 0u && began0) && !(lane == cnt0 && began1);
-        uint32_t row = 0;
-        typename P::Pre pre{};
-        if (mine) {
-            row = a.seg_dense ? j0 + lane : __ldg(&a.seg_nz[j0 + lane]);
-            pre = pass.load(a, row);
-        }
-        // in-lane segmented sums
-        const uint32_t f = (mw >> fshift) & 0xFFFFu;
-        const uint32_t wpre = ((wsel < 4u ? meta.y : meta.z) >> (8u * (wsel & 3u))) & 0xFFu;
-        const uint32_t tr0 = half ? cnt0 : 0u;  // the lane's tile's first rank in the pair
-        const uint32_t r0 = tr0 + wpre + __popc(mw & lower);
-        uint32_t r = r0;
-        double acc = 0.0, h = 0.0;
-#pragma unroll
-        for (int k = 0; k < 16; k++) {
-            acc += (double)v[k];
-            if ((f >> k) & 1u) {
-                if (r == r0) h = acc;
-                else sums[r] = (V)acc;
-                r++;
-                acc = 0.0;
-            }
-        }
-        // across lanes; a tile's first row end counts from its own first lane
-        double S = acc;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const double ov = __shfl_up_sync(0xffffffffu, S, o);
-            if (lane >= (uint32_t)o) S += ov;
-        }
-        double X = __shfl_up_sync(0xffffffffu, S, 1);
-        if (lane == 0u) X = 0.0;
-        const uint32_t E = __ballot_sync(0xffffffffu, f != 0u);
-        const uint32_t below = E & lt;
-        const int jb = max(below ? 31 - __clz(below) : 0, base);
-        const uint32_t E0 = E & 0xFFFFu;
-        const int jl = half ? ((E >> 16) ? 31 - __clz(E) : 16) : (E0 ? 31 - __clz(E0) : 0);
-        const double Xb = __shfl_sync(0xffffffffu, X, jb);
-        const double Xl = __shfl_sync(0xffffffffu, X, jl);
-        if (f) {
-            const double first = h + (X - Xb);
-            sums[r0] = (V)first;
-            if (r0 == tr0 && (half ? began1 : began0)) a.seg_head[t] = first;  // closes a spanning row
-        }
-        // each tile's open sum after its last row end, from its last lane
-        if ((lane & 15u) == 15u && t < a.seg_ntiles) a.seg_tail[t] = S - Xl;
-        __syncwarp();
-        if (mine) pass.fin(a, row, pre, sums[lane]);
-        for (uint32_t i = lane + 32u; i < cnt; i += 32u) {
-            if (i == cnt0 && began1) continue;
-            const uint32_t rw = a.seg_dense ? j0 + i : __ldg(&a.seg_nz[j0 + i]);
-            pass.fin(a, rw, pass.load(a, rw), sums[i]);
-        }
-        __syncwarp();
-        if (PIPE) {
-#pragma unroll
-            for (int k = 0; k < 8; k++) {
-                c0[k] = n0[k];
-                c1[k] = n1[k];
-            }
             mw = mwn;
             meta = metan;
         }
@@ -943,19 +791,6 @@ static void seg8_go(const IterArgs &a, const LaunchCfg &c, cudaStream_t s) {
     seg8_kernel<P, HOT, NT, PIPE><<<c.seg_g1, NT, c.smem, s>>>(a);
 }
 using Seg8Go = void (*)(const IterArgs &, const LaunchCfg &, cudaStream_t);
-template <bool HOT, bool PIPE>
-static void seg16_go(const IterArgs &a, const LaunchCfg &c, cudaStream_t s) {
-    seg16_kernel<Kry32Pass, HOT, PIPE><<<c.seg_g1, kSegNT, c.smem, s>>>(a);
-}
-static Seg8Go seg16_pick(bool hot, bool pipe, const void **entry) {
-    const void *k = hot ? (pipe ? (const void *)seg16_kernel<Kry32Pass, true, true>
-                                : (const void *)seg16_kernel<Kry32Pass, true, false>)
-                        : (pipe ? (const void *)seg16_kernel<Kry32Pass, false, true>
-                                : (const void *)seg16_kernel<Kry32Pass, false, false>);
-    if (entry) *entry = k;
-    return hot ? (pipe ? seg16_go<true, true> : seg16_go<true, false>)
-               : (pipe ? seg16_go<false, true> : seg16_go<false, false>);
-}
 template <class P>
 static Seg8Go seg8_pick(bool hot, int nt, bool pipe, const void **entry) {
 #define PRG_SEG8_PICK(H, N, Q)                                          \
@@ -986,15 +821,13 @@ LaunchCfg seg_config(const DeviceGraph &g, uint32_t hot_entries, int variant, in
     const bool res = mode == MODE_KRES64;
     const size_t vb = res ? sizeof(double) : sizeof(float);
     LaunchCfg c;
-    c.seg = res ? 2 : (variant == 2 || variant == 3) ? variant : 1;
+    c.seg = res || variant == 2 ? 2 : 1;
     c.threads = c.seg == 2 ? (int)g.seg_threads : kSegNT;
-    c.seg_pipe = c.seg >= 2 && g.seg_pipe != 0;
-    const uint32_t cap = res ? kSegHotMax64 : c.seg == 3 ? kSegHotMax16 : kSegHotMax;
-    c.hot = std::min<uint32_t>(std::min<uint32_t>(hot_entries, cap), g.n) & ~3u;
-    c.smem = ((size_t)(c.threads / 32) * kSegTile * (c.seg == 3 ? 2 : 1) + c.hot) * vb;
+    c.seg_pipe = c.seg == 2 && g.seg_pipe != 0;
+    c.hot = std::min<uint32_t>(std::min<uint32_t>(hot_entries, res ? kSegHotMax64 : kSegHotMax), g.n) & ~3u;
+    c.smem = ((size_t)(c.threads / 32) * kSegTile + c.hot) * vb;
     const void *k = nullptr;
     if (res) seg8_pick<Res64Pass>(c.hot != 0, c.threads, c.seg_pipe, &k);
-    else if (c.seg == 3) seg16_pick(c.hot != 0, c.seg_pipe, &k);
     else if (c.seg == 2) seg8_pick<Kry32Pass>(c.hot != 0, c.threads, c.seg_pipe, &k);
     else k = c.hot ? (const void *)kry32_seg_kernel<true> : (const void *)kry32_seg_kernel<false>;
     PRG_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c.smem));
@@ -1010,8 +843,7 @@ void launch_seg(int mode, const IterArgs &a, const LaunchCfg &c, cudaStream_t s)
         seg8_pick<Res64Pass>(c.hot != 0, c.threads, c.seg_pipe, nullptr)(a, c, s);
         seg_finish<Res64Pass><<<c.seg_g2, kSegFixNT, 0, s>>>(a, c.seg_g1);
     } else {
-        if (c.seg == 3) seg16_pick(c.hot != 0, c.seg_pipe, nullptr)(a, c, s);
-        else if (c.seg == 2) seg8_pick<Kry32Pass>(c.hot != 0, c.threads, c.seg_pipe, nullptr)(a, c, s);
+        if (c.seg == 2) seg8_pick<Kry32Pass>(c.hot != 0, c.threads, c.seg_pipe, nullptr)(a, c, s);
         else if (c.hot) kry32_seg_kernel<true><<<c.seg_g1, kSegNT, c.smem, s>>>(a);
         else kry32_seg_kernel<false><<<c.seg_g1, kSegNT, c.smem, s>>>(a);
         seg_finish<Kry32Pass><<<c.seg_g2, kSegFixNT, 0, s>>>(a, c.seg_g1);

@@ -78,7 +78,7 @@ void solve(const DeviceGraph &g, Workspace &ws, const SolveOpts &o, const double
 void solve_krylov(const DeviceGraph &g, Workspace &ws, const SolveOpts &o, const double *d_t, double *d_out,
                   SolveStats &st, cudaStream_t s, bool fp64_inner, bool linsys);
 void krylov_free(KrylovWs *&k, cudaStream_t s);
-// One FP32 Krylov matvec through kernel 0 (row-block), 1-3 (tile-segmented),
+// One FP32 Krylov matvec through kernel 0 (row-block), 1 or 2 (tile-segmented),
 // for tests and measurement (krylov.cu).
 void matvec32_probe(const DeviceGraph &g, Workspace &ws, int kernel, const float *p, const float *pt, double dz,
                     double damping, float *y, double dots[3], float *ms, cudaStream_t s);

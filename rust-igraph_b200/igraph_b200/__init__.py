@@ -724,7 +724,7 @@ class DeviceGraph:
 
     def matvec32(self, kernel: int, d_p: int, d_pt: int, dz: float, damping: float, d_y: int):
         """One FP32 Krylov matvec y = p - d (A pt + dz / n) on internal ids
-        through kernel 0 (row-block), 1, 2 or 3 (tile-segmented); device
+        through kernel 0 (row-block), 1 or 2 (tile-segmented); device
         pointers of n float32 each.  Returns ((p.y, y.p, y.y), ms)."""
         dots = np.zeros(3)
         ms = C.c_double()

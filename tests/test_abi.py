@@ -179,7 +179,7 @@ def test_tuning_keys_are_validated_on_the_host():
                           ("hot_cache64", 70000, "hot_cache64 must be at most 65536 entries"),
                           ("hot_cache32", 70000, "hot_cache32 must be at most 65536 entries"),
                           ("batch_cheb", 2, "batch_cheb must be 0 or 1"),
-                          ("seg_kry32", 4, "seg_kry32 must be 0, 1, 2 or 3"),
+                          ("seg_kry32", 3, "seg_kry32 must be 0, 1 or 2"),
                           ("seg_res64", 2, "seg_res64 must be 0 or 1"),
                           ("seg_hot64", 20481, "seg_hot64 must be at most 20480 entries"),
                           ("seg_threads", 640, "seg_threads must be 1024, 768 or 512"),
