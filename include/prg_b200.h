@@ -322,7 +322,11 @@ int32_t prg_autotune(prg_graph *g, int32_t tune_batch, const char *cache_path, p
  * "seg_hot" (its shared-memory hot prefix on relabelled graphs, entries),
  * "seg_res64" (unweighted graphs: 1 the tile-segmented FP64 residual pass
  * of the refined and Krylov solves, 0 the row-block kernel), "seg_hot64"
- * (its hot prefix, at most 20480 entries), "seg_prefetch" (segmented passes:
+ * (its hot prefix, at most 20480 entries; the FP64 power step shares it),
+ * "seg_plain64" (unweighted graphs: 1 the tile-segmented FP64 power step of
+ * the drop-ins and the certified FP64 loop, and the FP64 Krylov matvec of
+ * the FP64 Krylov and pagerank_linsys solves; 0 the row-block kernel),
+ * "seg_prefetch" (segmented passes:
  * 1 each warp prefetches its next tile of column indices into L2, 0 off),
  * "seg_threads" (their tile kernel's block size, one block per SM: 1024, 768
  * or 512), "seg_pipe" (1: each warp of the tile kernel loads its next tile

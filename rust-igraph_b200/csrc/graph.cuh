@@ -50,6 +50,9 @@ struct DeviceGraph {
     // ... and the FP64 residual pass of the refined / Krylov solves, with a
     // hot prefix of seg_hot64 entries
     uint32_t seg_res64 = 1, seg_hot64 = 8192;
+    // ... and the FP64 power step of the drop-ins and the certified loop, and
+    // the FP64 Krylov matvec
+    uint32_t seg_plain64 = 1;
     uint32_t seg_prefetch = 1;  // segmented passes: prefetch each warp's next index tile into L2
     // their tile kernel: threads of its one block per SM (1024, 768 or 512)
     // and whether each warp loads its next tile while working on the current
@@ -96,6 +99,8 @@ struct Tuning {
     uint32_t seg_hot = 32768;    // its shared-memory hot prefix on relabelled graphs (entries)
     uint32_t seg_res64 = 1;      // unweighted graphs: tile-segmented FP64 residual pass (0 = row-block kernel)
     uint32_t seg_hot64 = 8192;   // its hot prefix (entries)
+    uint32_t seg_plain64 = 1;    // unweighted graphs: tile-segmented FP64 power step and Krylov matvec
+                                 // (0 = row-block kernels)
     uint32_t seg_prefetch = 1;   // segmented passes: L2 prefetch of each warp's next index tile
     uint32_t seg_threads = 1024;  // segmented passes: tile-kernel block size (1024, 768 or 512)
     uint32_t seg_pipe = 1;        // segmented passes: load each warp's next tile ahead

@@ -472,6 +472,49 @@ struct Kry32Pass {
     }
 };
 
+// FP64 Krylov matvec (MODE_KRY64): iter_kernel<MODE_KRY64>'s epilogue,
+// y = p - (d sum + d dsum t) with records (rh.y, y.p, y.y).
+struct Kry64Pre {
+    double in, rh, t;
+};
+
+struct Kry64Pass {
+    using V = double;
+    using Pre = Kry64Pre;
+    double d, dshare, pd, pds, ps;
+    __device__ static bool stopped(const IterArgs &a) { return *(volatile const int32_t *)a.kdone != 0; }
+    __device__ static const double *source(const IterArgs &a) { return a.xt64_in; }
+    __device__ bool begin(const IterArgs &a, bool mark) {
+        double dz = 0.0;
+        if (!seg_prologue(a, dz)) {
+            if (mark && blockIdx.x == 0 && threadIdx.x == 0) a.kpart_out[0] = make_double4(0.0, 0.0, 0.0, 1.0);
+            return false;
+        }
+        d = a.damping;
+        dshare = a.damping * dz;
+        pd = pds = ps = 0.0;
+        return true;
+    }
+    __device__ Pre load(const IterArgs &a, uint32_t v) const {
+        Pre q;
+        q.in = __ldcs(a.x64_in + v);
+        q.rh = a.rh64 ? __ldcs(a.rh64 + v) : 0.0;
+        q.t = a.t64 ? a.t64[v] : a.inv_n;
+        return q;
+    }
+    __device__ void fin(const IterArgs &a, uint32_t v, const Pre &q, double y) {
+        const double out = q.in - (d * y + dshare * q.t);
+        __stcs(a.x64_out + v, out);
+        pd += q.rh * out;
+        pds += out * q.in;
+        ps += out * out;
+    }
+    __device__ void end(const IterArgs &a, unsigned rec0, double *s_red, bool) {
+        seg_block_sum3(pd, pds, ps, s_red);
+        if (threadIdx.x == 0) a.kpart_out[rec0 + blockIdx.x] = make_double4(pd, pds, ps, 0.0);
+    }
+};
+
 struct Res64Pre {
     double old, t;
 };
@@ -558,6 +601,98 @@ struct Res64Pass {
 __device__ __forceinline__ void prefetch_l2(const void *p, uint32_t bytes) {
     asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
 }
+
+struct Plain64Pre {
+    double old, dv, t;
+};
+
+// The FP64 power step of the drop-ins and the certified FP64 loop
+// (MODE_PLAIN64 / MODE_PPR64): iter_kernel's epilogue (the reference's update
+// in its rounding order, the L1 change, the next dangling mass, the next
+// scaled vector x'/outdeg) and its Ctl bookkeeping, done by the last
+// finishing block; both kernels return at once after convergence.
+struct Plain64Pass {
+    using V = double;
+    using Pre = Plain64Pre;
+    double d, dsum, tele, dshare, pd, pds;
+    __device__ static bool stopped(const IterArgs &a) { return *(volatile const int32_t *)&a.ctl->done != 0; }
+    __device__ static const double *source(const IterArgs &a) { return a.xt64_in; }
+    __device__ bool begin(const IterArgs &a, bool) {
+        d = a.damping;
+        dsum = *(volatile const double *)&a.ctl->dsum[a.parity];
+        const double nf = (double)a.n;
+        tele = __ddiv_rn(1.0 - d, nf);
+        dshare = __ddiv_rn(__dmul_rn(d, dsum), nf);
+        pd = pds = 0.0;
+        __syncthreads();  // the hot prefix is in place
+        return true;
+    }
+    __device__ Pre load(const IterArgs &a, uint32_t v) const {
+        Pre q;
+        q.old = a.x64_in[v];
+        q.dv = a.dval[v];
+        q.t = a.t64 ? a.t64[v] : 0.0;
+        return q;
+    }
+    __device__ void fin(const IterArgs &a, uint32_t v, const Pre &q, double y) {
+        double out;
+        if (a.t64) {
+            // personalized_pagerank.rs:169-170
+            out = __dadd_rn(__dmul_rn(1.0 - d, q.t), __dmul_rn(d, __dadd_rn(y, __dmul_rn(dsum, q.t))));
+        } else {
+            // pagerank.rs:129: teleport + dangling_share + d * incoming
+            out = __dadd_rn(__dadd_rn(tele, dshare), __dmul_rn(d, y));
+        }
+        a.x64_out[v] = out;
+        pd += fabs(out - q.old);
+        if (q.dv == 0.0) {
+            pds += out;
+            a.xt64_out[v] = 0.0;
+        } else {
+            a.xt64_out[v] = out / q.dv;  // the reference's pr[u] / out_deg(u)
+        }
+    }
+    // block record (|x' - x|, dangling x', 0); the last block of the last
+    // kernel adds all records in index order and updates Ctl as
+    // iter_kernel<MODE_PLAIN64> does
+    __device__ void end(const IterArgs &a, unsigned rec0, double *s_red, bool last_stage) {
+        __shared__ int s_last;
+        double z = 0.0;
+        seg_block_sum3(pd, pds, z, s_red);
+        if (threadIdx.x == 0) {
+            a.blk_part[rec0 + blockIdx.x] = make_double4(pd, pds, z, 0.0);
+            if (last_stage) {
+                __threadfence();
+                s_last = atomicAdd(&a.ctl->groups_done, 1u) == gridDim.x - 1;
+            }
+        }
+        if (!last_stage) return;
+        __syncthreads();
+        if (!s_last) return;
+        __threadfence();
+        const uint32_t nrec = rec0 + gridDim.x;
+        double x = 0.0, y = 0.0, w = 0.0;
+        for (uint32_t i = threadIdx.x; i < nrec; i += blockDim.x) {
+            const double2 q0 = __ldcg(reinterpret_cast<const double2 *>(&a.blk_part[i]));
+            const double2 q1 = __ldcg(reinterpret_cast<const double2 *>(&a.blk_part[i]) + 1);
+            x += q0.x;
+            y += q0.y;
+            w += q1.x;
+        }
+        seg_block_sum3(x, y, w, s_red);
+        if (threadIdx.x == 0) {
+            Ctl *ctl = a.ctl;
+            ctl->groups_done = 0u;
+            ctl->dsum[a.parity ^ 1] = y;
+            ctl->diff = x;
+            ctl->iters += 1u;
+            ctl->total_iters += 1u;
+            ctl->parity_last = a.parity;
+            if (x < ctl->thr || ctl->iters >= ctl->max_iter) ctl->done = 1;
+            __threadfence();
+        }
+    }
+};
 
 // The tile kernel with lane L owning the 8 consecutive arcs 8L..8L+7 of the
 // tile (one 32-byte index load, one scan per tile):
@@ -818,7 +953,7 @@ LaunchCfg seg_config(const DeviceGraph &g, uint32_t hot_entries, int variant, in
     int dev = 0, sms = 0;
     PRG_CUDA(cudaGetDevice(&dev));
     PRG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    const bool res = mode == MODE_KRES64;
+    const bool res = mode != MODE_KRY32;  // FP64 passes
     const size_t vb = res ? sizeof(double) : sizeof(float);
     LaunchCfg c;
     c.seg = res || variant == 2 ? 2 : 1;
@@ -827,7 +962,9 @@ LaunchCfg seg_config(const DeviceGraph &g, uint32_t hot_entries, int variant, in
     c.hot = std::min<uint32_t>(std::min<uint32_t>(hot_entries, res ? kSegHotMax64 : kSegHotMax), g.n) & ~3u;
     c.smem = ((size_t)(c.threads / 32) * kSegTile + c.hot) * vb;
     const void *k = nullptr;
-    if (res) seg8_pick<Res64Pass>(c.hot != 0, c.threads, c.seg_pipe, &k);
+    if (mode == MODE_KRES64) seg8_pick<Res64Pass>(c.hot != 0, c.threads, c.seg_pipe, &k);
+    else if (mode == MODE_KRY64) seg8_pick<Kry64Pass>(c.hot != 0, c.threads, c.seg_pipe, &k);
+    else if (res) seg8_pick<Plain64Pass>(c.hot != 0, c.threads, c.seg_pipe, &k);
     else if (c.seg == 2) seg8_pick<Kry32Pass>(c.hot != 0, c.threads, c.seg_pipe, &k);
     else k = c.hot ? (const void *)kry32_seg_kernel<true> : (const void *)kry32_seg_kernel<false>;
     PRG_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c.smem));
@@ -842,6 +979,12 @@ void launch_seg(int mode, const IterArgs &a, const LaunchCfg &c, cudaStream_t s)
     if (mode == MODE_KRES64) {
         seg8_pick<Res64Pass>(c.hot != 0, c.threads, c.seg_pipe, nullptr)(a, c, s);
         seg_finish<Res64Pass><<<c.seg_g2, kSegFixNT, 0, s>>>(a, c.seg_g1);
+    } else if (mode == MODE_KRY64) {
+        seg8_pick<Kry64Pass>(c.hot != 0, c.threads, c.seg_pipe, nullptr)(a, c, s);
+        seg_finish<Kry64Pass><<<c.seg_g2, kSegFixNT, 0, s>>>(a, c.seg_g1);
+    } else if (mode == MODE_PLAIN64 || mode == MODE_PPR64) {
+        seg8_pick<Plain64Pass>(c.hot != 0, c.threads, c.seg_pipe, nullptr)(a, c, s);
+        seg_finish<Plain64Pass><<<c.seg_g2, kSegFixNT, 0, s>>>(a, c.seg_g1);
     } else {
         if (c.seg == 2) seg8_pick<Kry32Pass>(c.hot != 0, c.threads, c.seg_pipe, nullptr)(a, c, s);
         else if (c.hot) kry32_seg_kernel<true><<<c.seg_g1, kSegNT, c.smem, s>>>(a);

@@ -637,7 +637,8 @@ void launch_iteration(int mode, bool weighted, const IterArgs &a_in, const Launc
     IterArgs a = a_in;
     a.hot = c.hot;
     a.l1hot = c.l1hot;
-    if (c.seg && (mode == MODE_KRY32 || mode == MODE_KRES64)) {
+    if (c.seg && (mode == MODE_KRY32 || mode == MODE_KRY64 || mode == MODE_KRES64 || mode == MODE_PLAIN64 ||
+                  mode == MODE_PPR64)) {
         launch_seg(mode, a, c, s);
         return;
     }

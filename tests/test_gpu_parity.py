@@ -345,3 +345,42 @@ def test_graph_methods_delegate(cuda_ok):
     assert np.abs(g.personalized_pagerank(r) - O.personalized_pagerank(n, f, t, False, r, 0.85)).max() \
         <= 1e-10
     assert np.array_equal(g.pagerank_linsys(), ig.pagerank_linsys(g))
+
+
+@pytest.mark.parametrize("case", ["rmat", "er_sparse", "ba_undirected"])
+def test_segmented_power_step_matches_row_block(cuda_ok, case):
+    # The FP64 power step of unweighted graphs runs as the tile-segmented
+    # pass (seg_plain64 = 1, the default) or the row-block kernel (0); both
+    # meet the restatement of pagerank() / personalized_pagerank(), with the
+    # same iteration count to within one
+    if case == "rmat":
+        n = 1 << 16
+        f, t = O.rmat(16, 16 * n, seed=61)
+        directed = True
+    elif case == "er_sparse":
+        n = 100_000
+        f, t = O.erdos_renyi_gnm(n, 150_000, True, False, 62)
+        directed = True
+    else:
+        n = 40_000
+        f, t = O.barabasi_game_bag(n, 4, False, False, 63)
+        directed = False
+    ref, iters = O.pagerank(n, f, t, directed, return_iters=True)
+    r = np.zeros(n)
+    r[[1, 7, n - 1]] = [1.0, 2.0, 0.5]
+    pref = O.personalized_pagerank(n, f, t, directed, r, 0.85)
+    out = {}
+    try:
+        for seg in (1, 0):
+            ig.set_tuning("seg_plain64", seg)
+            with ig.DeviceGraph.from_host(n, f, t, directed) as dg:
+                x, st = dg.solve(ig.Options())
+            g = G(n, f, t, directed)
+            out[seg] = (x, st.iterations, ig.personalized_pagerank(g, r, 0.85))
+    finally:
+        ig.reset_tuning()
+    for seg, (x, it, xp) in out.items():
+        assert maxabs(x, ref) <= PARITY, seg
+        assert abs(it - iters) <= 1, (seg, it, iters)
+        assert maxabs(xp, pref) <= PARITY, seg
+    assert maxabs(out[1][0], out[0][0]) <= 1e-13
