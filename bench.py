@@ -61,6 +61,9 @@ def parse():
     p.add_argument("--profile-case", action="store_true",
                    help="build the R-MAT graph of --scale, run one FP32-refined solve and exit: the command the "
                         "kernel captures under profiles/ run")
+    p.add_argument("--profile-form", default="refined", choices=["refined", "fp64", "fp64_krylov"],
+                   help="with --profile-case: the solve to run (FP32-refined, the certified FP64 power "
+                        "iteration, or the FP64 Krylov form)")
     p.add_argument("--profile-warm", action="store_true",
                    help="with --profile-case: run the warm-start network's inference twice before the solve")
     p.add_argument("--tuning", action="append", default=[], metavar="KEY=VALUE",
@@ -93,8 +96,11 @@ def run_profile_case(args):
 
         net = wsm.WarmStartNet.load(os.path.join(ROOT, "rust-igraph_b200", "igraph_b200", "warmstart_weights.f32"))
         inf_ms = [net.predict(dg, out.data_ptr()) for _ in range(2)]
-    st = dg.solve_device(out.data_ptr(), ig.Options(precision=ig.PRECISION_FP32_REFINED, eps=EPS, damping=D))
-    print(json.dumps({"profile_case": {"inference_ms": inf_ms,"scale": args.scale, "tuning": args.tuning, "passes": st.iterations,
+    opts = {"refined": ig.Options(precision=ig.PRECISION_FP32_REFINED, eps=EPS, damping=D),
+            "fp64": ig.Options(precision=ig.PRECISION_FP64, stop=ig.STOP_ERROR_BOUND, eps=EPS, damping=D),
+            "fp64_krylov": ig.Options(precision=ig.PRECISION_FP64_KRYLOV, eps=EPS, damping=D)}
+    st = dg.solve_device(out.data_ptr(), opts[args.profile_form])
+    print(json.dumps({"profile_case": {"form": args.profile_form, "inference_ms": inf_ms,"scale": args.scale, "tuning": args.tuning, "passes": st.iterations,
                                        "fp32_matvecs": st.fp32_passes, "solve_ms": st.solve_ms,
                                        "matvec_us": st.spmv_ms / max(st.spmv_launches, 1) * 1e3,
                                        "error_bound": st.error_bound,
