@@ -142,6 +142,7 @@ static prg_graph *new_handle(uint32_t n, uint64_t m, int32_t directed, cudaStrea
     h->g.seg_res64 = t.seg_res64;
     h->g.seg_hot64 = t.seg_hot64;
     h->g.seg_plain64 = t.seg_plain64;
+    h->g.seg_eig64 = t.seg_eig64;
     h->g.seg_prefetch = t.seg_prefetch;
     h->g.seg_threads = t.seg_threads;
     h->g.seg_pipe = t.seg_pipe;
@@ -1403,6 +1404,9 @@ int32_t prg_set_tuning(const char *key, int64_t value) {
     } else if (k == "seg_plain64") {
         if (value > 1) return fail(PRG_ERR_INVALID_ARGUMENT, "seg_plain64 must be 0 or 1");
         t.seg_plain64 = (uint32_t)value;
+    } else if (k == "seg_eig64") {
+        if (value > 1) return fail(PRG_ERR_INVALID_ARGUMENT, "seg_eig64 must be 0 or 1");
+        t.seg_eig64 = (uint32_t)value;
     } else if (k == "seg_threads") {
         if (value != 1024 && value != 768 && value != 512)
             return fail(PRG_ERR_INVALID_ARGUMENT, "seg_threads must be 1024, 768 or 512");

@@ -485,17 +485,17 @@ static void run_until_done(State *d_st, State *h_st, uint32_t max_iter, cudaStre
 static double rayleigh(const Product &pr, const double *x, double *tmp, double4 *recs, cudaStream_t s) {
     product(pr, x, tmp, 0.0, recs, nullptr, s);
     const unsigned nb = pr.ws->cfg[MODE_EIG64].grid;
-    std::vector<double4> h(nb), hh(std::max<uint32_t>(pr.g->nhub, 1));
+    const uint32_t nh = pr.ws->cfg[MODE_EIG64].hub_recs;  // 0 for the segmented product
+    std::vector<double4> h(nb), hh(std::max<uint32_t>(nh, 1));
     PRG_CUDA(cudaMemcpyAsync(h.data(), recs, nb * sizeof(double4), cudaMemcpyDeviceToHost, s));
-    if (pr.g->nhub)
-        PRG_CUDA(cudaMemcpyAsync(hh.data(), pr.ws->hub_rec, pr.g->nhub * sizeof(double4), cudaMemcpyDeviceToHost, s));
+    if (nh) PRG_CUDA(cudaMemcpyAsync(hh.data(), pr.ws->hub_rec, nh * sizeof(double4), cudaMemcpyDeviceToHost, s));
     PRG_CUDA(cudaStreamSynchronize(s));
     double num = 0.0, den = 0.0;
     for (const double4 &q : h) {
         num += q.y;
         den += q.z;
     }
-    for (uint32_t i = 0; i < pr.g->nhub; i++) {
+    for (uint32_t i = 0; i < nh; i++) {
         num += hh[i].y;
         den += hh[i].z;
     }
@@ -566,7 +566,8 @@ Result eigenvector_centrality(const DeviceGraph &g, Workspace &ws, double *d_out
                 pivot_kernel<<<kNB, kNT, 0, s>>>(x[q ^ 1], n, g.perm, pvrec, d_st);
                 normalise_signed_kernel<<<kNB, kNT, 0, s>>>(n, pvrec, kNB, x[q ^ 1], x[q], part, d_st);
             } else {
-                normalise_kernel<<<kNB, kNT, 0, s>>>(n, recs, grid, ws.hub_rec, g.nhub, x[q ^ 1], x[q], part, d_st);
+                normalise_kernel<<<kNB, kNT, 0, s>>>(n, recs, grid, ws.hub_rec, ws.cfg[MODE_EIG64].hub_recs, x[q ^ 1],
+                                                     x[q], part, d_st);
             }
             check_kernel<<<1, 256, 0, s>>>(part, kNB, d_st, q ^ 1);
             PRG_CUDA(cudaGetLastError());
@@ -747,7 +748,7 @@ Result hits_directed(const DeviceGraph &g, Workspace &ws, const DeviceGraph &rev
                 pivot_kernel<<<kNB, kNT, 0, s>>>(h[q ^ 1], n, g.perm, pvrec, d_st);
                 normalise_signed_kernel<<<kNB, kNT, 0, s>>>(n, pvrec, kNB, h[q ^ 1], h[q], part, d_st);
             } else {
-                normalise_kernel<<<kNB, kNT, 0, s>>>(n, rout, gout, wsr.hub_rec, rev.nhub, h[q ^ 1], h[q], part,
+                normalise_kernel<<<kNB, kNT, 0, s>>>(n, rout, gout, wsr.hub_rec, wsr.cfg[MODE_EIG64].hub_recs, h[q ^ 1], h[q], part,
                                                      d_st);
             }
             check_kernel<<<1, 256, 0, s>>>(part, kNB, d_st, q ^ 1);
@@ -759,7 +760,8 @@ Result hits_directed(const DeviceGraph &g, Workspace &ws, const DeviceGraph &rev
         if (!negative) clamp_kernel<<<kNB, kNT, 0, s>>>(hf, n);
         // authority = A^T h, rescaled by its max |.|, clamped (non-negative weights)
         product(pin, hf, tmp, 0.0, rin, nullptr, s);
-        normalise_kernel<<<kNB, kNT, 0, s>>>(n, rin, gin, ws.hub_rec, g.nhub, tmp, nullptr, part, nullptr);
+        normalise_kernel<<<kNB, kNT, 0, s>>>(n, rin, gin, ws.hub_rec, ws.cfg[MODE_EIG64].hub_recs, tmp, nullptr, part,
+                                             nullptr);
         if (!negative) clamp_kernel<<<kNB, kNT, 0, s>>>(tmp, n);
         PRG_CUDA(cudaGetLastError());
         PRG_CUDA(cudaMemcpyAsync(d_hub, hf, (uint64_t)n * 8, cudaMemcpyDeviceToDevice, s));

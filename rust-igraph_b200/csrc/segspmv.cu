@@ -515,6 +515,50 @@ struct Kry64Pass {
     }
 };
 
+// The adjacency product of the eigenvector and HITS iterations (MODE_EIG64,
+// unweighted): y = shift x + A x with records (max |y|, x.y, x.x), the first
+// a max over the block.
+struct Eig64Pre {
+    double in;
+};
+
+struct Eig64Pass {
+    using V = double;
+    using Pre = Eig64Pre;
+    double shift, mx, xy, xx;
+    __device__ static bool stopped(const IterArgs &a) { return a.kdone && *(volatile const int32_t *)a.kdone != 0; }
+    __device__ static const double *source(const IterArgs &a) { return a.xt64_in; }
+    __device__ bool begin(const IterArgs &a, bool) {
+        shift = a.shift;
+        mx = xy = xx = 0.0;
+        __syncthreads();  // the hot prefix is in place
+        return true;
+    }
+    __device__ Pre load(const IterArgs &a, uint32_t v) const { return Pre{a.x64_in[v]}; }
+    __device__ void fin(const IterArgs &a, uint32_t v, const Pre &q, double y) {
+        const double out = shift * q.in + y;
+        a.x64_out[v] = out;
+        mx = fmax(mx, fabs(out));
+        xy += q.in * out;
+        xx += q.in * q.in;
+    }
+    __device__ void end(const IterArgs &a, unsigned rec0, double *s_red, bool) {
+        double m = mx;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+        double z = 0.0;
+        seg_block_sum3(z, xy, xx, s_red);
+        __syncthreads();
+        const uint32_t w = threadIdx.x >> 5;
+        if ((threadIdx.x & 31) == 0) s_red[w] = m;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            for (uint32_t k = 1; k < (blockDim.x >> 5); k++) m = fmax(m, s_red[k]);
+            a.kpart_out[rec0 + blockIdx.x] = make_double4(m, xy, xx, 0.0);
+        }
+    }
+};
+
 struct Res64Pre {
     double old, t;
 };
@@ -964,6 +1008,7 @@ LaunchCfg seg_config(const DeviceGraph &g, uint32_t hot_entries, int variant, in
     const void *k = nullptr;
     if (mode == MODE_KRES64) seg8_pick<Res64Pass>(c.hot != 0, c.threads, c.seg_pipe, &k);
     else if (mode == MODE_KRY64) seg8_pick<Kry64Pass>(c.hot != 0, c.threads, c.seg_pipe, &k);
+    else if (mode == MODE_EIG64) seg8_pick<Eig64Pass>(c.hot != 0, c.threads, c.seg_pipe, &k);
     else if (res) seg8_pick<Plain64Pass>(c.hot != 0, c.threads, c.seg_pipe, &k);
     else if (c.seg == 2) seg8_pick<Kry32Pass>(c.hot != 0, c.threads, c.seg_pipe, &k);
     else k = c.hot ? (const void *)kry32_seg_kernel<true> : (const void *)kry32_seg_kernel<false>;
@@ -979,6 +1024,9 @@ void launch_seg(int mode, const IterArgs &a, const LaunchCfg &c, cudaStream_t s)
     if (mode == MODE_KRES64) {
         seg8_pick<Res64Pass>(c.hot != 0, c.threads, c.seg_pipe, nullptr)(a, c, s);
         seg_finish<Res64Pass><<<c.seg_g2, kSegFixNT, 0, s>>>(a, c.seg_g1);
+    } else if (mode == MODE_EIG64) {
+        seg8_pick<Eig64Pass>(c.hot != 0, c.threads, c.seg_pipe, nullptr)(a, c, s);
+        seg_finish<Eig64Pass><<<c.seg_g2, kSegFixNT, 0, s>>>(a, c.seg_g1);
     } else if (mode == MODE_KRY64) {
         seg8_pick<Kry64Pass>(c.hot != 0, c.threads, c.seg_pipe, nullptr)(a, c, s);
         seg_finish<Kry64Pass><<<c.seg_g2, kSegFixNT, 0, s>>>(a, c.seg_g1);

@@ -81,6 +81,7 @@ void workspace_ensure(Workspace &ws, const DeviceGraph &g, cudaStream_t s) {
     const bool seg = !g.weighted && g.seg_kry32 != 0 && g.arcs > 0;
     const bool seg_res = !g.weighted && g.seg_res64 != 0 && g.arcs > 0;
     const bool seg_plain = !g.weighted && g.seg_plain64 != 0 && g.arcs > 0;
+    const bool seg_eig = !g.weighted && g.seg_eig64 != 0 && g.arcs > 0;
     for (int m = 0; m < kModes; m++) {
         const bool fp32 = m == MODE_CORR32 || m == MODE_KRY32;
         const uint32_t hot = g.perm != nullptr ? (fp32 ? g.hot_cache : g.hot_cache64) : 0u;
@@ -89,13 +90,15 @@ void workspace_ensure(Workspace &ws, const DeviceGraph &g, cudaStream_t s) {
             ws.cfg[m] = seg_config(g, g.perm != nullptr ? g.seg_hot64 : 0u, 2, MODE_KRES64);
         else if ((m == MODE_PLAIN64 || m == MODE_PPR64 || m == MODE_KRY64) && seg_plain)
             ws.cfg[m] = seg_config(g, g.perm != nullptr ? g.seg_hot64 : 0u, 2, m);
+        else if (m == MODE_EIG64 && seg_eig)
+            ws.cfg[m] = seg_config(g, g.perm != nullptr ? g.seg_hot64 : 0u, 2, m);
         else ws.cfg[m] = iteration_config(m, g.weighted, hot, g.blocks_per_sm, g.n, g.hot_threads);
         if (!ws.cfg[m].seg) ws.cfg[m].hub_recs = g.nhub;
         const uint32_t l1 = fp32 ? g.l1_hot32 : g.l1_hot64;
         if (g.perm != nullptr && l1) ws.cfg[m].l1hot = l1;
         gmax = std::max(gmax, ws.cfg[m].grid);
     }
-    if (seg || seg_res || seg_plain) seg_build(g, ws.seg, s);
+    if (seg || seg_res || seg_plain || seg_eig) seg_build(g, ws.seg, s);
     const uint64_t n = g.n;
     for (int i = 0; i < 2; i++) {
         walloc(ws.x64[i], n, s);

@@ -638,7 +638,7 @@ void launch_iteration(int mode, bool weighted, const IterArgs &a_in, const Launc
     a.hot = c.hot;
     a.l1hot = c.l1hot;
     if (c.seg && (mode == MODE_KRY32 || mode == MODE_KRY64 || mode == MODE_KRES64 || mode == MODE_PLAIN64 ||
-                  mode == MODE_PPR64)) {
+                  mode == MODE_PPR64 || mode == MODE_EIG64)) {
         launch_seg(mode, a, c, s);
         return;
     }

@@ -184,7 +184,8 @@ def test_tuning_keys_are_validated_on_the_host():
                           ("seg_hot64", 20481, "seg_hot64 must be at most 20480 entries"),
                           ("seg_threads", 640, "seg_threads must be 1024, 768 or 512"),
                           ("seg_pipe", 2, "seg_pipe must be 0 or 1"),
-                          ("seg_plain64", 2, "seg_plain64 must be 0 or 1")):
+                          ("seg_plain64", 2, "seg_plain64 must be 0 or 1"),
+                          ("seg_eig64", 2, "seg_eig64 must be 0 or 1")):
         with pytest.raises(ig.InvalidArgument, match=msg):
             ig.set_tuning(key, bad)
     try:

@@ -329,3 +329,20 @@ def test_negative_weights_match_restatement(cuda_ok, kind):
             assert it < 5000
             assert np.max(np.abs(r.vector - ref)) <= TOL, (mode, np.max(np.abs(r.vector - ref)))
             assert abs(r.eigenvalue - rlam) <= TOL * abs(rlam)
+
+
+@pytest.mark.parametrize("kind", ["er", "ba", "rmat", "loops"])
+def test_segmented_product_matches_restatement(cuda_ok, kind):
+    # the same checks with the adjacency product as the tile-segmented pass
+    # (tuning seg_eig64 = 1): undirected eigenvector centrality, directed
+    # HITS, and the directed modes, unweighted
+    ig.set_tuning("seg_eig64", 1)
+    try:
+        test_eigenvector_matches_restatement(cuda_ok, kind)
+        if kind in ("rmat", "ba"):
+            test_hits_directed_matches_restatement(cuda_ok, kind)
+        if kind in ("rmat", "er", "loops"):
+            for mode in (0, 1, 2):
+                test_directed_matches_restatement(cuda_ok, kind, mode, False)
+    finally:
+        ig.reset_tuning()
