@@ -324,7 +324,7 @@ int32_t prg_autotune(prg_graph *g, int32_t tune_batch, const char *cache_path, p
  * of the refined and Krylov solves, 0 the row-block kernel), "seg_hot64"
  * (its hot prefix, at most 20480 entries; the FP64 power step shares it),
  * "seg_eig64" (unweighted graphs: 1 the tile-segmented adjacency product of
- * the eigenvector and HITS iterations, 0 the row-block kernel, the default),
+ * the eigenvector and HITS iterations, the default; 0 the row-block kernel),
  * "seg_plain64" (unweighted graphs: 1 the tile-segmented FP64 power step of
  * the drop-ins and the certified FP64 loop, and the FP64 Krylov matvec of
  * the FP64 Krylov and pagerank_linsys solves; 0 the row-block kernel),

@@ -54,7 +54,7 @@ struct DeviceGraph {
     // the FP64 Krylov matvec
     uint32_t seg_plain64 = 1;
     // ... and the adjacency product of the eigenvector and HITS iterations
-    uint32_t seg_eig64 = 0;
+    uint32_t seg_eig64 = 1;
     uint32_t seg_prefetch = 1;  // segmented passes: prefetch each warp's next index tile into L2
     // their tile kernel: threads of its one block per SM (1024, 768 or 512)
     // and whether each warp loads its next tile while working on the current
@@ -103,7 +103,7 @@ struct Tuning {
     uint32_t seg_hot64 = 8192;   // its hot prefix (entries)
     uint32_t seg_plain64 = 1;    // unweighted graphs: tile-segmented FP64 power step and Krylov matvec
                                  // (0 = row-block kernels)
-    uint32_t seg_eig64 = 0;      // unweighted graphs: tile-segmented eigenvector / HITS product
+    uint32_t seg_eig64 = 1;      // unweighted graphs: tile-segmented eigenvector / HITS product
     uint32_t seg_prefetch = 1;   // segmented passes: L2 prefetch of each warp's next index tile
     uint32_t seg_threads = 1024;  // segmented passes: tile-kernel block size (1024, 768 or 512)
     uint32_t seg_pipe = 1;        // segmented passes: load each warp's next tile ahead

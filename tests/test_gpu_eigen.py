@@ -332,11 +332,12 @@ def test_negative_weights_match_restatement(cuda_ok, kind):
 
 
 @pytest.mark.parametrize("kind", ["er", "ba", "rmat", "loops"])
-def test_segmented_product_matches_restatement(cuda_ok, kind):
-    # the same checks with the adjacency product as the tile-segmented pass
-    # (tuning seg_eig64 = 1): undirected eigenvector centrality, directed
-    # HITS, and the directed modes, unweighted
-    ig.set_tuning("seg_eig64", 1)
+def test_row_block_product_matches_restatement(cuda_ok, kind):
+    # the same checks with the adjacency product as the row-block pass
+    # (tuning seg_eig64 = 0; the tile-segmented pass is the default for
+    # unweighted graphs): undirected eigenvector centrality, directed HITS,
+    # and the directed modes, unweighted
+    ig.set_tuning("seg_eig64", 0)
     try:
         test_eigenvector_matches_restatement(cuda_ok, kind)
         if kind in ("rmat", "ba"):
