@@ -331,8 +331,8 @@ int32_t prg_autotune(prg_graph *g, int32_t tune_batch, const char *cache_path, p
  * "seg_prefetch" (segmented passes:
  * 1 each warp prefetches its next tile of column indices into L2, 0 off),
  * "seg_threads" (their tile kernel's block size, one block per SM: 1024, 768
- * or 512), "seg_pipe" (1: each warp of the tile kernel loads its next tile
- * while it works on the current one),
+ * or 512), "seg_pipe" (1: each warp of the FP32 tile kernel loads its next
+ * tile while it works on the current one),
  * "hot_cache32" / "hot_cache64" (hot prefix of the row-block kernel's FP32 /
  * FP64 passes), "hot_threads" (256, 512 or 1024: the row-block kernel's block
  * size when it keeps a hot prefix),

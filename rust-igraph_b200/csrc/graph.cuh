@@ -57,7 +57,8 @@ struct DeviceGraph {
     uint32_t seg_eig64 = 1;
     uint32_t seg_prefetch = 1;  // segmented passes: prefetch each warp's next index tile into L2
     // their tile kernel: threads of its one block per SM (1024, 768 or 512)
-    // and whether each warp loads its next tile while working on the current
+    // and, in the FP32 matvec, whether each warp loads its next tile while
+    // working on the current one
     uint32_t seg_threads = 1024, seg_pipe = 1;
     // relabelled graphs: gathers of ids >= l1_hot32 (FP32 passes) / l1_hot64
     // (FP64 passes) bypass L1, keeping it for the hot prefix (0 = all allocate)
@@ -106,7 +107,7 @@ struct Tuning {
     uint32_t seg_eig64 = 1;      // unweighted graphs: tile-segmented eigenvector / HITS product
     uint32_t seg_prefetch = 1;   // segmented passes: L2 prefetch of each warp's next index tile
     uint32_t seg_threads = 1024;  // segmented passes: tile-kernel block size (1024, 768 or 512)
-    uint32_t seg_pipe = 1;        // segmented passes: load each warp's next tile ahead
+    uint32_t seg_pipe = 1;        // segmented FP32 matvec: load each warp's next tile ahead
     uint32_t l1_hot32 = 16384, l1_hot64 = 2048;
     double refine_switch = 5e-7;
     uint32_t batch_vec = 2;

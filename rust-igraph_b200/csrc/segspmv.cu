@@ -931,16 +931,17 @@ __global__ void __launch_bounds__(kSegFixNT) seg_finish(const IterArgs a, unsign
     // aligned), their operand loads issued together; with dense ids they are
     // the range n - nempty .. n-1
     if (a.seg_dense) {
-        const uint32_t e0 = a.n - a.seg_nempty;
-        for (uint64_t i = tid; i < (a.seg_nempty + 3u) >> 2; i += nth) {
-            const uint32_t v = e0 + 4u * (uint32_t)i;
+        // four rows per thread and step, nth apart, so that every load and
+        // store of a warp covers consecutive rows
+        const uint64_t e0 = a.n - a.seg_nempty;
+        for (uint64_t i = tid; i < a.seg_nempty; i += 4 * nth) {
             typename P::Pre q[4];
 #pragma unroll
             for (int k = 0; k < 4; k++)
-                if (v + k < a.n) q[k] = pass.load(a, v + k);
+                if (i + k * nth < a.seg_nempty) q[k] = pass.load(a, (uint32_t)(e0 + i + k * nth));
 #pragma unroll
             for (int k = 0; k < 4; k++)
-                if (v + k < a.n) pass.fin(a, v + k, q[k], V(0));
+                if (i + k * nth < a.seg_nempty) pass.fin(a, (uint32_t)(e0 + i + k * nth), q[k], V(0));
         }
         pass.end(a, rec0, s_red, true);
         return;
@@ -1002,7 +1003,9 @@ LaunchCfg seg_config(const DeviceGraph &g, uint32_t hot_entries, int variant, in
     LaunchCfg c;
     c.seg = res || variant == 2 ? 2 : 1;
     c.threads = c.seg == 2 ? (int)g.seg_threads : kSegNT;
-    c.seg_pipe = c.seg == 2 && g.seg_pipe != 0;
+    // pipelined loads pay in the FP32 matvec; the FP64 passes spill with them
+    // and run about 2 % slower (R-MAT scale 24)
+    c.seg_pipe = c.seg == 2 && !res && g.seg_pipe != 0;
     c.hot = std::min<uint32_t>(std::min<uint32_t>(hot_entries, res ? kSegHotMax64 : kSegHotMax), g.n) & ~3u;
     c.smem = ((size_t)(c.threads / 32) * kSegTile + c.hot) * vb;
     const void *k = nullptr;
