@@ -291,10 +291,16 @@ typedef struct prg_tune_result {
     int32_t from_cache;              /* 1 if read from cache_path instead of timed */
     uint32_t pad;
     double default_ms, best_ms;      /* FP64 + FP32 iteration time before / after */
+    /* unweighted graphs (0 otherwise): the shared-memory hot prefixes chosen
+     * for the tile-segmented FP32 matvec and FP64 passes, and the FP32
+     * matvec's time with the default and the chosen prefix */
+    uint32_t seg_hot, seg_hot64;
+    double seg_default_ms, seg_best_ms;
 } prg_tune_result;
 
 /* Times candidate row-block shapes (stream window, short-row limit, hub
- * split), persistent-grid occupancies and (tune_batch != 0) batched tile
+ * split), persistent-grid occupancies, on unweighted graphs the hot-prefix
+ * lengths of the tile-segmented passes, and (tune_batch != 0) batched tile
  * widths on this graph with CUDA events and keeps the fastest.  cache_path
  * (optional): a text file of earlier results keyed by (n, arcs, directed,
  * weighted); a hit is applied without timing, a new result is appended. */

@@ -1216,6 +1216,10 @@ int32_t prg_autotune(prg_graph *h, int32_t tune_batch, const char *cache_path, p
         out->from_cache = r.from_cache ? 1 : 0;
         out->default_ms = r.default_ms;
         out->best_ms = r.best_ms;
+        out->seg_hot = r.seg_hot;
+        out->seg_hot64 = r.seg_hot64;
+        out->seg_default_ms = r.seg_default_ms;
+        out->seg_best_ms = r.seg_best_ms;
     }
     return PRG_OK;
     PRG_GUARD_END

@@ -8,6 +8,9 @@
 // FP32 correction iteration are each timed over a few back-to-back launches
 // with CUDA events; the candidate with the smallest sum wins.  The persistent
 // grid is then tried at the occupancy maximum and at reduced blocks per SM.
+// On unweighted degree-sorted graphs the hot-prefix lengths of the
+// tile-segmented passes are timed as well: the FP32 matvec's on one matvec,
+// the FP64 passes' on the FP64 power step.
 // The batched solver's tile width (32, 64 or 128 columns per tile) is timed
 // on a few iterations of 128 random single-seed columns.  A result can be
 // cached in a text file keyed by (n, arcs, directed, weighted).
@@ -48,6 +51,8 @@ static bool cache_lookup(const char *path, const DeviceGraph &g, TuneResult &r) 
         k << n << ' ' << arcs << ' ' << dir << ' ' << w;
         if (k.str() != key) continue;
         if (ls >> r.capw >> r.shortmax >> r.split >> r.blocks_per_sm >> r.batch_vec >> r.best_ms) {
+            // hot prefixes of the segmented passes (absent from older lines)
+            if (!(ls >> r.seg_hot >> r.seg_hot64)) r.seg_hot = r.seg_hot64 = 0;
             r.from_cache = true;
             return true;
         }
@@ -60,7 +65,63 @@ static void cache_store(const char *path, const DeviceGraph &g, const TuneResult
     std::ofstream out(path, std::ios::app);
     if (!out) return;
     out << cache_key(g) << ' ' << r.capw << ' ' << r.shortmax << ' ' << r.split << ' ' << r.blocks_per_sm << ' '
-        << r.batch_vec << ' ' << r.best_ms << '\n';
+        << r.batch_vec << ' ' << r.best_ms << ' ' << r.seg_hot << ' ' << r.seg_hot64 << '\n';
+}
+
+// The tile-segmented passes of unweighted graphs (degree-sorted ids only: the
+// hot prefix needs them): the FP32 matvec's hot prefix by timing one matvec
+// on a random direction, the FP64 passes' by timing the FP64 power step.
+static void tune_segmented(DeviceGraph &g, Workspace &ws, cudaStream_t s, TuneResult &r) {
+    r.seg_hot = g.seg_hot;
+    r.seg_hot64 = g.seg_hot64;
+    if (g.weighted || g.perm == nullptr || g.arcs == 0 || g.seg_kry32 != 2) return;
+    const uint64_t n = g.n;
+    float *buf = nullptr;
+    PRG_CUDA(cudaMallocAsync((void **)&buf, 3 * n * sizeof(float), s));
+    PRG_CUDA(cudaMemsetAsync(buf, 0, 3 * n * sizeof(float), s));
+    float *p = buf, *pt = buf + n, *y = buf + 2 * n;
+    auto time32 = [&]() {
+        double best = 1e300, dots[3];
+        for (int rep = 0; rep < 3; rep++) {
+            float ms = 0.f;
+            matvec32_probe(g, ws, 2, p, pt, 0.0, 0.85, y, dots, &ms, s);
+            best = std::min(best, (double)ms);
+        }
+        return best;
+    };
+    r.seg_default_ms = r.seg_best_ms = time32();
+    const uint32_t h0 = g.seg_hot;
+    for (uint32_t h : {24576u, 32768u, 40960u}) {
+        if (h == h0) continue;
+        g.seg_hot = h;
+        const double t = time32();
+        r.tried++;
+        if (t < r.seg_best_ms) {
+            r.seg_best_ms = t;
+            r.seg_hot = h;
+        }
+    }
+    g.seg_hot = r.seg_hot;
+    cudaFreeAsync(buf, s);
+    if (g.seg_plain64) {
+        const uint32_t h64 = g.seg_hot64;
+        workspace_free(ws, s);
+        double best = time_iterations(g, ws, MODE_PLAIN64, 4, s);
+        for (uint32_t h : {4096u, 8192u, 12288u}) {
+            if (h == h64) continue;
+            g.seg_hot64 = h;
+            workspace_free(ws, s);
+            const double t = time_iterations(g, ws, MODE_PLAIN64, 4, s);
+            r.tried++;
+            if (t < best) {
+                best = t;
+                r.seg_hot64 = h;
+            }
+        }
+        g.seg_hot64 = r.seg_hot64;
+    }
+    workspace_free(ws, s);
+    PRG_CUDA(cudaStreamSynchronize(s));
 }
 
 static double probe(DeviceGraph &g, Workspace &ws, cudaStream_t s, uint32_t iters) {
@@ -76,6 +137,8 @@ int autotune(DeviceGraph &g, Workspace &ws, cudaStream_t s, bool tune_batch, con
         ws.ready = ws.ready && false;  // grid shapes depend on blocks_per_sm
         workspace_free(ws, s);
         g.batch_vec = r.batch_vec;
+        if (r.seg_hot) g.seg_hot = r.seg_hot;
+        if (r.seg_hot64) g.seg_hot64 = r.seg_hot64;
         return 0;
     }
     const uint32_t iters = 4;
@@ -117,6 +180,7 @@ int autotune(DeviceGraph &g, Workspace &ws, cudaStream_t s, bool tune_batch, con
     }
     g.blocks_per_sm = r.blocks_per_sm;
     workspace_free(ws, s);
+    tune_segmented(g, ws, s, r);
 
     r.batch_vec = g.batch_vec ? g.batch_vec : 1;
     if (tune_batch && g.n >= 2) {

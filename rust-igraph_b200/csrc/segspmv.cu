@@ -807,31 +807,31 @@ __global__ void __launch_bounds__(NT, 1) seg8_kernel(const IterArgs a) {
         const uint64_t pol_g = policy_evict_last();
 #pragma unroll
         for (int k = 0; k < 8; k++) {
-            V g;
-            if (HOT) g = c[k] < H ? s_hot[c[k]] : ld_gather_na(xt + c[k], pol_g);
-            else g = c[k] < L1 ? ld_gather(xt + c[k], pol_g) : ld_gather_na(xt + c[k], pol_g);
-            v[k] = (full || q + k < a.arcs) ? g : V(0);
+            if (HOT) v[k] = c[k] < H ? s_hot[c[k]] : ld_gather_na(xt + c[k], pol_g);
+            else v[k] = c[k] < L1 ? ld_gather(xt + c[k], pol_g) : ld_gather_na(xt + c[k], pol_g);
+        }
+        if (!full) {  // the last tile (warp-uniform branch)
+#pragma unroll
+            for (int k = 0; k < 8; k++)
+                if (q + k >= a.arcs) v[k] = V(0);
         }
     };
     // with PIPE the next tile's indices, mask word and record are loaded while
     // the warp works on the current tile (issuing its gathers early as well
     // measured slower: the pass is bound by L1TEX and MIO throughput, not by
     // the latency that more loads in flight would hide)
-    uint32_t cc[8], mw = 0u;
-    uint4 meta = make_uint4(0u, 0u, 0u, 0u);
-    V v[8];
-    if (PIPE) load_tile(warp, cc, mw, meta);
-    for (uint64_t t = warp; t < a.seg_ntiles; t += nwarps) {
+    // one tile: its indices, mask word and record are in (cc, mw, meta);
+    // with PIPE the next tile's go to (ccn, mwn, metan)
+    auto work = [&](uint64_t t, const uint32_t (&cc)[8], uint32_t mw, const uint4 &meta, uint32_t (&ccn)[8],
+                    uint32_t &mwn, uint4 &metan) {
         const uint64_t P0 = t * kSegTile;
         // a later tile of the warp's indices into L2 (full tiles only, so the
         // range stays inside col): the first one not yet being loaded
         constexpr uint32_t ahead = PIPE ? 2u : 1u;
         if (a.seg_prefetch && lane == 0u && P0 + (ahead * nwarps + 1u) * kSegTile <= a.arcs)
             prefetch_l2(a.col + P0 + ahead * nwarps * kSegTile, kSegTile * 4u);
-        uint32_t ccn[8], mwn = 0u;
-        uint4 metan;
         if (PIPE) load_tile(t + nwarps, ccn, mwn, metan);
-        else load_tile(t, cc, mw, meta);
+        V v[8];
         gather_tile(t, cc, v);
         const uint32_t j0 = meta.x, cnt = meta.w & 0x7FFFFFFFu;
         const bool began = (meta.w >> 31) != 0u;
@@ -887,11 +887,24 @@ __global__ void __launch_bounds__(NT, 1) seg8_kernel(const IterArgs a) {
             pass.fin(a, rw, pass.load(a, rw), sums[i]);
         }
         __syncwarp();
-        if (PIPE) {
-#pragma unroll
-            for (int k = 0; k < 8; k++) cc[k] = ccn[k];
-            mw = mwn;
-            meta = metan;
+    };
+    if (PIPE) {
+        // two tiles per trip with the buffers' roles swapped, so nothing is
+        // copied between them
+        uint32_t ca[8], cb[8], ma = 0u, mb = 0u;
+        uint4 ea, eb;
+        load_tile(warp, ca, ma, ea);
+        for (uint64_t t = warp; t < a.seg_ntiles; t += 2 * nwarps) {
+            work(t, ca, ma, ea, cb, mb, eb);
+            if (t + nwarps >= a.seg_ntiles) break;
+            work(t + nwarps, cb, mb, eb, ca, ma, ea);
+        }
+    } else {
+        uint32_t cc[8], mw = 0u, cn[8], mn = 0u;
+        uint4 meta, en;
+        for (uint64_t t = warp; t < a.seg_ntiles; t += nwarps) {
+            load_tile(t, cc, mw, meta);
+            work(t, cc, mw, meta, cn, mn, en);
         }
     }
     pass.end(a, 0u, s_red, false);

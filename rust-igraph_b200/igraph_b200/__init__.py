@@ -106,7 +106,9 @@ class prg_batch_stats(C.Structure):
 class prg_tune_result(C.Structure):
     _fields_ = [("capw", C.c_uint32), ("shortmax", C.c_uint32), ("split", C.c_uint32),
                 ("blocks_per_sm", C.c_uint32), ("batch_tile_width", C.c_uint32), ("candidates", C.c_uint32),
-                ("from_cache", C.c_int32), ("pad", C.c_uint32), ("default_ms", C.c_double), ("best_ms", C.c_double)]
+                ("from_cache", C.c_int32), ("pad", C.c_uint32), ("default_ms", C.c_double), ("best_ms", C.c_double),
+                ("seg_hot", C.c_uint32), ("seg_hot64", C.c_uint32), ("seg_default_ms", C.c_double),
+                ("seg_best_ms", C.c_double)]
 
 
 _lib = None

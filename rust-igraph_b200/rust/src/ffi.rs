@@ -88,6 +88,10 @@ pub struct prg_tune_result {
     pub pad: u32,
     pub default_ms: f64,
     pub best_ms: f64,
+    pub seg_hot: u32,
+    pub seg_hot64: u32,
+    pub seg_default_ms: f64,
+    pub seg_best_ms: f64,
 }
 
 #[repr(C)]

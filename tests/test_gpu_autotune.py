@@ -20,6 +20,11 @@ def test_autotune_keeps_parity_and_caches(cuda_ok, tmp_path):
         assert r["candidates"] > 10 and not r["from_cache"]
         assert r["best_ms"] <= r["default_ms"] * 1.0000001
         assert r["capw"] + r["shortmax"] <= 512 and r["batch_tile_width"] in (32, 64, 128)
+        # the segmented passes' hot prefixes (a degree-sorted unweighted graph)
+        assert r["seg_hot"] in (24576, 32768, 40960) and r["seg_hot64"] in (4096, 8192, 12288)
+        assert 0 < r["seg_best_ms"] <= r["seg_default_ms"]
+        xr, st = dg.solve(ig.Options(precision=ig.PRECISION_FP32_REFINED))
+        assert st.error_bound <= 1e-10
         x, _ = dg.solve(ig.Options())
         assert np.abs(x - ref).max() <= 1e-10
         X, iters, st = dg.ppr_batch([np.array([1, 2], np.uint32), np.array([7], np.uint32)])
@@ -27,5 +32,6 @@ def test_autotune_keeps_parity_and_caches(cuda_ok, tmp_path):
     with ig.DeviceGraph.from_host(n, f, t, True) as dg:
         r2 = dg.autotune(batch=True, cache_path=cache)
         assert r2["from_cache"] and (r2["capw"], r2["shortmax"], r2["split"]) == (r["capw"], r["shortmax"], r["split"])
+        assert (r2["seg_hot"], r2["seg_hot64"]) == (r["seg_hot"], r["seg_hot64"])
         x, _ = dg.solve(ig.Options())
         assert np.abs(x - ref).max() <= 1e-10
